@@ -1,0 +1,187 @@
+/*
+ * moons_gpu.h -- C-ABI of the B200 (sm_100a) implementation of the MOONS
+ * time-step hot path.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an
+ * int status (MOONS_OK == 0) and never exits the process; the caller (the
+ * Fortran host through ISO_C_BINDING, or Python through ctypes) decides what
+ * to do with an error, reading the text with moons_last_error().
+ *
+ * Layout contract: a field is the reference's grid_field array f(sx,sy,sz),
+ * Fortran column-major (x fastest), one ghost layer per side, FP64.  With N
+ * interior cells on an axis the node extent is N+3 and the cell extent N+2
+ * (code/generated_code/grid_field/grid_field.f90:39-43,
+ *  code/handwritten/grid_field/grid_field_extend.f90:89-133).
+ * Uploads and downloads copy such arrays verbatim; between calls the fields
+ * stay resident in HBM.
+ *
+ * Calls on one mesh are not re-entrant; all work of a mesh is enqueued on one
+ * CUDA stream and a call returns after its work completed, unless stated.
+ */
+#ifndef MOONS_GPU_H
+#define MOONS_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  MOONS_OK = 0,
+  MOONS_ERR_ARG = 1,     /* bad argument (null pointer, bad enum)            */
+  MOONS_ERR_SHAPE = 2,   /* field shapes / data locations do not fit the op  */
+  MOONS_ERR_CUDA = 3,    /* a CUDA call failed                               */
+  MOONS_ERR_NAN = 4,     /* NaN in solver norms (PCG_solver_algorithm.f90:223-248) */
+  MOONS_ERR_STATE = 5,   /* object used before it was set up                 */
+  MOONS_ERR_NOMEM = 6,   /* device allocation failed                         */
+  MOONS_ERR_LIMIT = 7    /* size beyond a compiled-in maximum                */
+};
+
+/* ---- data locations (code/handwritten/fields/data_location_extend.f90) -- */
+enum {
+  MOONS_CC = 0,
+  MOONS_FX = 1, MOONS_FY = 2, MOONS_FZ = 3, /* face data, normal x/y/z       */
+  MOONS_EX = 4, MOONS_EY = 5, MOONS_EZ = 6, /* edge data, edge along x/y/z   */
+  MOONS_NODE = 7
+};
+
+/* ---- boundary-condition types (bctype, code/handwritten/BCs/base/bctype_extend.f90) */
+enum {
+  MOONS_BC_NONE = 0,       /* field carries no BCs (reference: BCs not defined) */
+  MOONS_BC_DIRICHLET = 1,
+  MOONS_BC_NEUMANN = 2,
+  MOONS_BC_PERIODIC = 3,
+  MOONS_BC_ROBIN = 4
+};
+
+/* Per-field BC description.  Faces are numbered as in the reference:
+ * 1=xmin 2=xmax 3=ymin 4=ymax 5=zmin 6=zmax (face_edge_corner_indexing.f90).
+ * value[] is the uniform boundary value b of each face; order[] is
+ * apply_BC_order (sim_params_aux.f90:37-55), a permutation of 1..6.
+ * Replaces init_Dirichlet/init_Neumann/init_periodic/init_Robin +
+ * init_BC_props + set_prescribed (boundary_conditions_extend.f90:120-340). */
+typedef struct {
+  int type[6];
+  int prescribed[6];
+  double value[6];
+  double c_w[6];
+  int order[6];
+  int all_neumann;   /* SF%all_Neumann, set by hand in the reference
+                        (init_P_BCs.f90:26, init_phi_BCs.f90:27): the PCG
+                        removes the RHS mean (PCG_aux.f90:45) when set */
+} moons_bc_spec;
+
+/* iter_solver_params (code/handwritten/var_set/iter_solver_params_extend.f90:44-63) */
+typedef struct {
+  int iter_max;
+  double tol_rel;
+  double tol_abs;
+  int n_skip_check_res;
+} moons_isp;
+
+/* What a solve reports (PCG_solver_algorithm.f90:180-220 print/export data). */
+typedef struct {
+  int iterations;      /* ISP%iter_per_call                                  */
+  double res0;         /* L2 of the modified RHS over the whole array        */
+  double res;          /* sqrt|dot(r,r)| at exit                             */
+  double rel;          /* res/res0 (res when res0 == 0)                      */
+  int exit_reason;     /* 1 tol_rel, 2 tol_abs, 3 iter_max                   */
+  double ms;           /* device time of the solve, CUDA events              */
+} moons_solve_info;
+
+/* Operators a PCG object applies (matrix_free_operators.f90). */
+enum {
+  MOONS_OP_LAP_UNIFORM = 1,   /* Lap_uniform_SF/VF      :35-90              */
+  MOONS_OP_LAP_PROPS = 2,     /* Lap_nonuniform_props   :92-118  div(k grad) */
+  MOONS_OP_IND_DIFFUSION = 3, /* ind_diffusion          :120-146             */
+  MOONS_OP_MOM_DIFFUSION = 4  /* mom_diffusion          :176-202             */
+};
+/* Diagonal preconditioners (preconditioners.f90). */
+enum {
+  MOONS_PREC_IDENTITY = 0,    /* prec_Identity_SF/VF :27-51                  */
+  MOONS_PREC_LAP = 1,         /* prec_Lap_SF/VF      :55-82                  */
+  MOONS_PREC_MOM = 2,         /* prec_mom_SF/VF      :85-113                 */
+  MOONS_PREC_IND = 3          /* prec_ind_VF         :115-129                */
+};
+
+typedef struct moons_mesh moons_mesh;
+typedef struct moons_sf moons_sf;
+typedef struct moons_pcg moons_pcg;
+typedef struct moons_mhd moons_mhd;
+
+/* ---- error text -------------------------------------------------------- */
+/* Last error message of the calling thread ("" if none). */
+const char* moons_last_error(void);
+
+/* ---- mesh: single block (coordinates_extend.f90:78-173 init_c,
+ *      :506-523 init_stencils_c).  hn_* are the node coordinates including
+ *      the ghost nodes, sn_* their counts; stencil coefficients are built
+ *      from them exactly as init_stencils_c does.  device < 0 keeps the
+ *      current CUDA device. ------------------------------------------------ */
+int moons_mesh_create(moons_mesh** out, const double* hn_x, int sn_x,
+                      const double* hn_y, int sn_y, const double* hn_z,
+                      int sn_z, int device);
+int moons_mesh_destroy(moons_mesh* m);
+int moons_mesh_sync(moons_mesh* m);
+
+/* ---- fields (SF with one block; GEN/fields/SF.f90:43-51) --------------- */
+int moons_sf_create(moons_mesh* m, int data_loc, moons_sf** out);
+int moons_sf_destroy(moons_sf* f);
+int moons_sf_shape(const moons_sf* f, int s[3]);
+/* n must equal s1*s2*s3; host arrays in Fortran order. */
+int moons_sf_upload(moons_sf* f, const double* host, long long n);
+int moons_sf_download(const moons_sf* f, double* host, long long n);
+int moons_sf_fill(moons_sf* f, double val);   /* assign(f,val) */
+/* Attach BCs to the field (init_BC_mesh + init_* + init_BC_props). */
+int moons_sf_set_bcs(moons_sf* f, const moons_bc_spec* spec);
+
+/* ---- BCs (code/handwritten/BCs/apply/apply_BCs.f90:31-64,
+ *      apply_BCs_implicit.f90:18-60) -------------------------------------- */
+int moons_apply_bcs(moons_sf* f);
+int moons_apply_bcs_implicit(moons_sf* f);
+
+/* ---- discrete operators (code/handwritten/ops) ------------------------- */
+/* del%assign/add/subtract (ops_del.f90:236-261): gen 1=assign 2=add
+ * 3=subtract, n=1,2 derivative order, dir 1..3, pad 0/1. */
+int moons_del(moons_sf* out, const moons_sf* in, int n, int dir, int pad,
+              int gen);
+/* grad_SF (ops_discrete.f90:173-182): CC -> 3 faces (or any staggered set). */
+int moons_grad(moons_sf* gx, moons_sf* gy, moons_sf* gz, const moons_sf* u);
+/* div_SF (ops_discrete.f90:158-171) incl. assign_ghost_XPeriodic. */
+int moons_div(moons_sf* out, const moons_sf* ux, const moons_sf* uy,
+              const moons_sf* uz);
+/* curl_VF (ops_discrete.f90:357-365): faces->edges or edges->faces. */
+int moons_curl(moons_sf* ox, moons_sf* oy, moons_sf* oz, const moons_sf* ux,
+               const moons_sf* uy, const moons_sf* uz);
+/* lap_centered_SF_new (ops_discrete.f90:124-132) for CC data and
+ * lap_centered_SF_given_both (:112-122) for staggered data, fused. */
+int moons_lap_centered(moons_sf* out, const moons_sf* u);
+/* lapVarCoeff_VF (ops_discrete.f90:275-285): div(k grad u), k on faces. */
+int moons_lap_var(moons_sf* out, const moons_sf* u, const moons_sf* kx,
+                  const moons_sf* ky, const moons_sf* kz);
+/* interpO2_SF (ops_interp.f90:190-220): C->N (with extrapolation) or N->C
+ * along dir. */
+int moons_interp(moons_sf* out, const moons_sf* in, int dir);
+
+/* ---- PCG (code/handwritten/PCG/PCG_solver_extend.f90:51-291,
+ *      code/handwritten/solvers/PCG/PCG_solver_algorithm.f90:37-179) ------ */
+/* ncomp = 1 (SF) or 3 (VF).  x[] are the unknown's fields (their BCs are
+ * copied, as init(PCG%p,x) does), x_bc[] the fields whose BCs define x_BC,
+ * k[] the coefficient fields the operator reads (faces for LAP_PROPS,
+ * edges for IND_DIFFUSION; NULL otherwise). */
+int moons_pcg_create(moons_mesh* m, int op, int prec, int ncomp,
+                     moons_sf* const* x, moons_sf* const* x_bc,
+                     moons_sf* const* k, moons_pcg** out);
+int moons_pcg_destroy(moons_pcg* s);
+/* update_MFP (PCG_solver_extend.f90:269-291). */
+int moons_pcg_update_mfp(moons_pcg* s, double coeff_implicit_time_split,
+                         int update_preconditioner);
+/* solve (PCG_solver_extend.f90:182-206): x[] updated in place. */
+int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b,
+                    const moons_isp* isp, moons_solve_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOONS_GPU_H */

@@ -1,0 +1,306 @@
+"""ctypes host mirror of the reference's field / operator / solver API.
+
+The objects map one to one onto the reference's Fortran types and routines:
+
+* ``Mesh``   -- a single-block mesh (HW/mesh, HW/grid coordinates)
+* ``Field``  -- an SF with one block: data location, BCs, device array
+* ``PCG``    -- PCG_solver_SF / PCG_solver_VF (HW/PCG/PCG_solver_extend.f90)
+* ``grad/div/curl/lap_centered/lap_var/delta/interp`` -- HW/ops routines
+
+Every call goes through the C-ABI of ``include/moons_gpu.h`` in
+``moons_b200/lib/libmoons_gpu.so``; nothing here computes on the host.  A
+missing library raises immediately -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+from . import build as _build
+
+CC, FX, FY, FZ, EX, EY, EZ, NODE = range(8)
+DIRICHLET, NEUMANN, PERIODIC, ROBIN = 1, 2, 3, 4
+OP_LAP_UNIFORM, OP_LAP_PROPS, OP_IND_DIFFUSION, OP_MOM_DIFFUSION = 1, 2, 3, 4
+PREC_IDENTITY, PREC_LAP, PREC_MOM, PREC_IND = 0, 1, 2, 3
+
+
+class MoonsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"moons error {code}: {msg}")
+        self.code = code
+
+
+class BCSpec(C.Structure):
+    _fields_ = [
+        ("type", C.c_int * 6),
+        ("prescribed", C.c_int * 6),
+        ("value", C.c_double * 6),
+        ("c_w", C.c_double * 6),
+        ("order", C.c_int * 6),
+        ("all_neumann", C.c_int),
+    ]
+
+
+class ISP(C.Structure):
+    _fields_ = [
+        ("iter_max", C.c_int),
+        ("tol_rel", C.c_double),
+        ("tol_abs", C.c_double),
+        ("n_skip_check_res", C.c_int),
+    ]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("res0", C.c_double),
+        ("res", C.c_double),
+        ("rel", C.c_double),
+        ("exit_reason", C.c_int),
+        ("ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def bc_spec(types: Sequence[int], values: Sequence[float] | None = None,
+            prescribed: Sequence[int] | None = None, c_w: Sequence[float] | None = None,
+            order: Sequence[int] | None = None, all_neumann: bool = False) -> BCSpec:
+    s = BCSpec()
+    for f in range(6):
+        s.type[f] = int(types[f])
+        s.value[f] = float(values[f]) if values is not None else 0.0
+        s.prescribed[f] = int(prescribed[f]) if prescribed is not None else 0
+        s.c_w[f] = float(c_w[f]) if c_w is not None else 0.0
+        s.order[f] = int(order[f]) if order is not None else f + 1
+    s.all_neumann = 1 if all_neumann else 0
+    return s
+
+
+def isp(iter_max: int, tol_rel: float, tol_abs: float, n_skip_check_res: int = 1) -> ISP:
+    return ISP(int(iter_max), float(tol_rel), float(tol_abs), int(n_skip_check_res))
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+
+
+class _Lib:
+    """Loads a shared library exposing the MOONS entry points under ``prefix``."""
+
+    def __init__(self, path: str, prefix: str):
+        self.path = path
+        self.lib = C.CDLL(path)
+        self.prefix = prefix
+
+    def fn(self, name, restype, argtypes):
+        f = getattr(self.lib, self.prefix + name)
+        f.restype = restype
+        f.argtypes = argtypes
+        return f
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            raise RuntimeError(f"MOONS CUDA library missing: {path} (run python -m moons_b200.build)")
+        L = C.CDLL(path)
+        sig = {
+            "moons_last_error": (C.c_char_p, []),
+            "moons_mesh_create": (C.c_int, [C.POINTER(_P), _D, C.c_int, _D, C.c_int, _D, C.c_int, C.c_int]),
+            "moons_mesh_destroy": (C.c_int, [_P]),
+            "moons_mesh_sync": (C.c_int, [_P]),
+            "moons_sf_create": (C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+            "moons_sf_destroy": (C.c_int, [_P]),
+            "moons_sf_shape": (C.c_int, [_P, C.POINTER(C.c_int)]),
+            "moons_sf_upload": (C.c_int, [_P, _D, C.c_longlong]),
+            "moons_sf_download": (C.c_int, [_P, _D, C.c_longlong]),
+            "moons_sf_fill": (C.c_int, [_P, C.c_double]),
+            "moons_sf_set_bcs": (C.c_int, [_P, C.POINTER(BCSpec)]),
+            "moons_apply_bcs": (C.c_int, [_P]),
+            "moons_apply_bcs_implicit": (C.c_int, [_P]),
+            "moons_del": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int]),
+            "moons_grad": (C.c_int, [_P, _P, _P, _P]),
+            "moons_div": (C.c_int, [_P, _P, _P, _P]),
+            "moons_curl": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+            "moons_lap_centered": (C.c_int, [_P, _P]),
+            "moons_lap_var": (C.c_int, [_P, _P, _P, _P, _P]),
+            "moons_interp": (C.c_int, [_P, _P, C.c_int]),
+            "moons_pcg_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(_P), C.POINTER(_P),
+                                           C.POINTER(_P), C.POINTER(_P)]),
+            "moons_pcg_destroy": (C.c_int, [_P]),
+            "moons_pcg_update_mfp": (C.c_int, [_P, C.c_double, C.c_int]),
+            "moons_pcg_solve": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(ISP), C.POINTER(SolveInfo)]),
+        }
+        for name, (rt, at) in sig.items():
+            f = getattr(L, name)
+            f.restype = rt
+            f.argtypes = at
+        _lib = L
+    return _lib
+
+
+def _check(code: int):
+    if code != 0:
+        raise MoonsError(code, lib().moons_last_error().decode())
+
+
+def _arr(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_D)
+
+
+class Mesh:
+    def __init__(self, hx, hy, hz, device: int = -1):
+        L = lib()
+        self._keep = [_arr(h)[0] for h in (hx, hy, hz)]
+        h = _P()
+        _check(L.moons_mesh_create(C.byref(h), self._keep[0].ctypes.data_as(_D), len(self._keep[0]),
+                                   self._keep[1].ctypes.data_as(_D), len(self._keep[1]),
+                                   self._keep[2].ctypes.data_as(_D), len(self._keep[2]), device))
+        self.h = h
+        self.sn = tuple(len(k) for k in self._keep)
+
+    def field(self, dl: int) -> "Field":
+        return Field(self, dl)
+
+    def sync(self):
+        _check(lib().moons_mesh_sync(self.h))
+
+    def close(self):
+        if self.h:
+            lib().moons_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Field:
+    def __init__(self, mesh: Mesh, dl: int):
+        self.mesh = mesh
+        self.dl = dl
+        h = _P()
+        _check(lib().moons_sf_create(mesh.h, dl, C.byref(h)))
+        self.h = h
+        s = (C.c_int * 3)()
+        _check(lib().moons_sf_shape(h, s))
+        self.shape = (s[0], s[1], s[2])
+
+    @property
+    def n(self):
+        return self.shape[0] * self.shape[1] * self.shape[2]
+
+    def upload(self, a: np.ndarray):
+        a = np.asarray(a, dtype=np.float64)
+        if a.shape != self.shape:
+            raise ValueError(f"shape {a.shape} != field {self.shape}")
+        flat = np.ascontiguousarray(a.ravel(order="F"))
+        _check(lib().moons_sf_upload(self.h, flat.ctypes.data_as(_D), flat.size))
+
+    def download(self) -> np.ndarray:
+        flat = np.empty(self.n, dtype=np.float64)
+        _check(lib().moons_sf_download(self.h, flat.ctypes.data_as(_D), flat.size))
+        return flat.reshape(self.shape, order="F")
+
+    def fill(self, v: float):
+        _check(lib().moons_sf_fill(self.h, float(v)))
+
+    def set_bcs(self, spec: BCSpec):
+        _check(lib().moons_sf_set_bcs(self.h, C.byref(spec)))
+
+    def apply_bcs(self):
+        _check(lib().moons_apply_bcs(self.h))
+
+    def apply_bcs_implicit(self):
+        _check(lib().moons_apply_bcs_implicit(self.h))
+
+    def close(self):
+        if self.h:
+            lib().moons_sf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def delta(out: Field, inp: Field, n: int, d: int, pad: int, gen: int):
+    _check(lib().moons_del(out.h, inp.h, n, d, pad, gen))
+
+
+def grad(gx: Field, gy: Field, gz: Field, u: Field):
+    _check(lib().moons_grad(gx.h, gy.h, gz.h, u.h))
+
+
+def div(o: Field, ux: Field, uy: Field, uz: Field):
+    _check(lib().moons_div(o.h, ux.h, uy.h, uz.h))
+
+
+def curl(o: Sequence[Field], u: Sequence[Field]):
+    _check(lib().moons_curl(o[0].h, o[1].h, o[2].h, u[0].h, u[1].h, u[2].h))
+
+
+def lap_centered(o: Field, u: Field):
+    _check(lib().moons_lap_centered(o.h, u.h))
+
+
+def lap_var(o: Field, u: Field, k: Sequence[Field]):
+    _check(lib().moons_lap_var(o.h, u.h, k[0].h, k[1].h, k[2].h))
+
+
+def interp(o: Field, i: Field, d: int):
+    _check(lib().moons_interp(o.h, i.h, d))
+
+
+def _ptrs(fs):
+    arr = (_P * 3)()
+    for i, f in enumerate(fs):
+        arr[i] = f.h if f is not None else None
+    return arr
+
+
+class PCG:
+    """PCG_solver_SF (ncomp=1) / PCG_solver_VF (ncomp=3)."""
+
+    def __init__(self, mesh: Mesh, op: int, prec: int, x: Sequence[Field], x_bc: Sequence[Field],
+                 k: Sequence[Field] | None = None):
+        self.mesh = mesh
+        self.nc = len(x)
+        h = _P()
+        _check(lib().moons_pcg_create(mesh.h, op, prec, self.nc, _ptrs(x), _ptrs(x_bc),
+                                      _ptrs(k) if k is not None else None, C.byref(h)))
+        self.h = h
+
+    def update_mfp(self, coeff: float, update_prec: bool = True):
+        _check(lib().moons_pcg_update_mfp(self.h, float(coeff), 1 if update_prec else 0))
+
+    def solve(self, x: Sequence[Field], b: Sequence[Field], params: ISP) -> dict:
+        info = SolveInfo()
+        _check(lib().moons_pcg_solve(self.h, _ptrs(x), _ptrs(b), C.byref(params), C.byref(info)))
+        return info.as_dict()
+
+    def close(self):
+        if self.h:
+            lib().moons_pcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,4 @@
+// all.cu -- single translation unit of the MOONS B200 library (the kernels
+// live in headers shared by the entry-point files).
+#include "mesh.cu"
+#include "pcg.cu"

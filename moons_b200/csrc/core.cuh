@@ -1,0 +1,99 @@
+// core.cuh -- device data model of the MOONS hot path on B200.
+//
+// A field lives in HBM exactly as the reference's grid_field array
+// f(sx,sy,sz): column-major, x fastest, one ghost layer per side, FP64
+// (GEN/grid_field/grid_field.f90:39-43).  Kernels address it with 1-based
+// (i,j,k) so the stencil formulas read like the Fortran they restate.
+// 1-D coefficient arrays are stored 1-based too (element 0 unused).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/moons_gpu.h"
+
+namespace mg {
+
+// ---- 1-D coordinates and stencil coefficients of one axis --------------
+// (HW/grid/coordinates_extend.f90:78-173,506-523)
+struct DCoord {
+  int sn, sc;
+  const double *hn, *hc, *dhn, *dhc;
+  const double *cc2nD, *cc2nU;  // stagCC2N, size sc-1
+  const double *n2ccD, *n2ccU;  // stagN2CC, size sn-1
+  const double *colCC_L[2], *colCC_D[2], *colCC_U[2];  // size sc-2
+  const double *colN_L[2], *colN_D[2], *colN_U[2];     // size sn-2
+  const double *thD, *thU;      // interpolation theta, size sc-1
+};
+struct DGrid {
+  DCoord c[3];
+};
+
+// ---- a field as kernels see it -----------------------------------------
+struct DF {
+  double* f;
+  int s0, s1, s2;  // extents x,y,z
+  int dl;          // data location (MOONS_CC ...)
+  __host__ __device__ int s(int d) const { return d == 1 ? s0 : (d == 2 ? s1 : s2); }
+  __host__ __device__ size_t n() const { return (size_t)s0 * s1 * s2; }
+  __device__ __forceinline__ size_t at(int i, int j, int k) const {
+    return (size_t)(i - 1) + (size_t)s0 * ((size_t)(j - 1) + (size_t)s1 * (size_t)(k - 1));
+  }
+  __device__ __forceinline__ double& operator()(int i, int j, int k) const { return f[at(i, j, k)]; }
+};
+
+// node-location eye of a data location: bit d-1 set when N along d
+__host__ __device__ inline int dl_bits(int dl) {
+  switch (dl) {
+    case MOONS_CC: return 0;
+    case MOONS_FX: return 1;
+    case MOONS_FY: return 2;
+    case MOONS_FZ: return 4;
+    case MOONS_EX: return 6;
+    case MOONS_EY: return 5;
+    case MOONS_EZ: return 3;
+    default: return 7;
+  }
+}
+__host__ __device__ inline bool n_along(int dl, int d) { return (dl_bits(dl) >> (d - 1)) & 1; }
+__host__ inline int dl_from_bits(int b) {
+  for (int d = 0; d < 8; d++)
+    if (dl_bits(d) == b) return d;
+  return -1;
+}
+
+// ---- BCs of one field as kernels see them ------------------------------
+struct DBC {
+  int defined;
+  int type[7];
+  int prescribed[7];
+  double value[7];
+  double c_w[7];
+  double dh[7];
+  double nhat[7];
+  int order[7];
+};
+
+// ---- error plumbing ----------------------------------------------------
+void set_error(const std::string& m);
+int cuda_fail(cudaError_t e, const char* what);
+#define MG_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return mg::cuda_fail(e_, #call); \
+  } while (0)
+
+constexpr int kBlock = 256;
+inline unsigned nblocks(size_t n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }
+
+// index -> (i,j,k) 1-based
+__device__ __forceinline__ void ijk_of(size_t idx, const DF& a, int& i, int& j, int& k) {
+  i = (int)(idx % a.s0) + 1;
+  size_t r = idx / a.s0;
+  j = (int)(r % a.s1) + 1;
+  k = (int)(r / a.s1) + 1;
+}
+__device__ __forceinline__ int pick(int d, int i, int j, int k) { return d == 1 ? i : (d == 2 ? j : k); }
+
+}  // namespace mg

@@ -1,0 +1,215 @@
+"""ctypes wrapper of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Exposes the same Python surface as ``moons_b200.capi`` (Mesh, Field, grad,
+div, curl, lap_centered, lap_var, delta, interp, PCG) but backed by the C++
+restatement in ``oracle/moons_oracle.cpp``.  Only tests, the smoke check and
+the bench's CPU baseline import it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libmoons_oracle.so")
+
+from moons_b200.capi import BCSpec, ISP, SolveInfo  # noqa: E402  (plain ctypes structs)
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    srcs = [os.path.join(HERE, f) for f in ("moons_oracle.cpp", "moons_oracle.hpp", "oracle_capi.cpp", "Makefile")]
+    stale = not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs)
+    if force or stale:
+        subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        sig = {
+            "or_last_error": (C.c_char_p, []),
+            "or_mesh_create": (_P, [_D, C.c_int, _D, C.c_int, _D, C.c_int]),
+            "or_mesh_destroy": (None, [_P]),
+            "or_sf_create": (_P, [_P, C.c_int]),
+            "or_sf_destroy": (None, [_P]),
+            "or_sf_shape": (C.c_int, [_P, C.POINTER(C.c_int)]),
+            "or_sf_upload": (C.c_int, [_P, _D, C.c_longlong]),
+            "or_sf_download": (C.c_int, [_P, _D, C.c_longlong]),
+            "or_sf_set_bcs": (C.c_int, [_P, C.POINTER(BCSpec)]),
+            "or_apply_bcs": (C.c_int, [_P]),
+            "or_apply_bcs_implicit": (C.c_int, [_P]),
+            "or_del": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int]),
+            "or_grad": (C.c_int, [_P, _P, _P, _P]),
+            "or_div": (C.c_int, [_P, _P, _P, _P]),
+            "or_curl": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+            "or_lap_centered": (C.c_int, [_P, _P]),
+            "or_lap_uniform_coeff": (C.c_int, [_P, _P]),
+            "or_lap_var": (C.c_int, [_P, _P, _P, _P, _P]),
+            "or_interp": (C.c_int, [_P, _P, C.c_int]),
+            "or_pcg_create": (_P, [C.c_int, C.c_int, C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P),
+                                   C.c_double]),
+            "or_pcg_destroy": (None, [_P]),
+            "or_pcg_update_mfp": (C.c_int, [_P, C.c_double, C.c_int]),
+            "or_pcg_solve": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(ISP), C.POINTER(SolveInfo)]),
+        }
+        for n, (rt, at) in sig.items():
+            f = getattr(L, n)
+            f.restype = rt
+            f.argtypes = at
+        _lib = L
+    return _lib
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _check(code):
+    if code != 0:
+        raise OracleError(f"oracle error {code}: {lib().or_last_error().decode()}")
+
+
+class Mesh:
+    def __init__(self, hx, hy, hz, device: int = -1):
+        self._keep = [np.ascontiguousarray(h, dtype=np.float64) for h in (hx, hy, hz)]
+        k = self._keep
+        self.h = lib().or_mesh_create(k[0].ctypes.data_as(_D), len(k[0]), k[1].ctypes.data_as(_D), len(k[1]),
+                                      k[2].ctypes.data_as(_D), len(k[2]))
+        if not self.h:
+            raise OracleError(lib().or_last_error().decode())
+        self.sn = tuple(len(x) for x in k)
+
+    def field(self, dl):
+        return Field(self, dl)
+
+    def sync(self):
+        pass
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().or_mesh_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Field:
+    def __init__(self, mesh: Mesh, dl: int):
+        self.mesh = mesh
+        self.dl = dl
+        self.h = lib().or_sf_create(mesh.h, dl)
+        s = (C.c_int * 3)()
+        lib().or_sf_shape(self.h, s)
+        self.shape = (s[0], s[1], s[2])
+
+    @property
+    def n(self):
+        return self.shape[0] * self.shape[1] * self.shape[2]
+
+    def upload(self, a):
+        a = np.asarray(a, dtype=np.float64)
+        assert a.shape == self.shape, (a.shape, self.shape)
+        flat = np.ascontiguousarray(a.ravel(order="F"))
+        _check(lib().or_sf_upload(self.h, flat.ctypes.data_as(_D), flat.size))
+
+    def download(self):
+        flat = np.empty(self.n)
+        _check(lib().or_sf_download(self.h, flat.ctypes.data_as(_D), flat.size))
+        return flat.reshape(self.shape, order="F")
+
+    def fill(self, v):
+        self.upload(np.full(self.shape, float(v)))
+
+    def set_bcs(self, spec):
+        _check(lib().or_sf_set_bcs(self.h, C.byref(spec)))
+
+    def apply_bcs(self):
+        _check(lib().or_apply_bcs(self.h))
+
+    def apply_bcs_implicit(self):
+        _check(lib().or_apply_bcs_implicit(self.h))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().or_sf_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def delta(out, inp, n, d, pad, gen):
+    _check(lib().or_del(out.h, inp.h, n, d, pad, gen))
+
+
+def grad(gx, gy, gz, u):
+    _check(lib().or_grad(gx.h, gy.h, gz.h, u.h))
+
+
+def div(o, ux, uy, uz):
+    _check(lib().or_div(o.h, ux.h, uy.h, uz.h))
+
+
+def curl(o, u):
+    _check(lib().or_curl(o[0].h, o[1].h, o[2].h, u[0].h, u[1].h, u[2].h))
+
+
+def lap_centered(o, u):
+    _check(lib().or_lap_centered(o.h, u.h))
+
+
+def lap_uniform_coeff(o, u):
+    _check(lib().or_lap_uniform_coeff(o.h, u.h))
+
+
+def lap_var(o, u, k):
+    _check(lib().or_lap_var(o.h, u.h, k[0].h, k[1].h, k[2].h))
+
+
+def interp(o, i, d):
+    _check(lib().or_interp(o.h, i.h, d))
+
+
+def _ptrs(fs):
+    arr = (_P * 3)()
+    for i, f in enumerate(fs):
+        arr[i] = f.h if f is not None else None
+    return arr
+
+
+class PCG:
+    def __init__(self, mesh, op, prec, x: Sequence[Field], x_bc: Sequence[Field], k=None, coeff_implicit=0.0):
+        self.mesh = mesh
+        self.nc = len(x)
+        self.h = lib().or_pcg_create(op, prec, self.nc, _ptrs(x), _ptrs(x_bc), _ptrs(k) if k is not None else None,
+                                     float(coeff_implicit))
+        if not self.h:
+            raise OracleError(lib().or_last_error().decode())
+
+    def update_mfp(self, coeff, update_prec=True):
+        _check(lib().or_pcg_update_mfp(self.h, float(coeff), 1 if update_prec else 0))
+
+    def solve(self, x, b, params):
+        info = SolveInfo()
+        _check(lib().or_pcg_solve(self.h, _ptrs(x), _ptrs(b), C.byref(params), C.byref(info)))
+        return info.as_dict()
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().or_pcg_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
