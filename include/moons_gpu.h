@@ -112,6 +112,10 @@ typedef struct moons_mhd moons_mhd;
 /* ---- error text -------------------------------------------------------- */
 /* Last error message of the calling thread ("" if none). */
 const char* moons_last_error(void);
+/* Diagnostic (no reference counterpart): number of kernels the library has
+ * run in this process, host launches plus the launches a solver's
+ * device-side loop executed. */
+long long moons_kernel_launches(void);
 
 /* ---- mesh: single block (coordinates_extend.f90:78-173 init_c,
  *      :506-523 init_stencils_c).  hn_* are the node coordinates including
@@ -179,6 +183,80 @@ int moons_pcg_update_mfp(moons_pcg* s, double coeff_implicit_time_split,
 /* solve (PCG_solver_extend.f90:182-206): x[] updated in place. */
 int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b,
                     const moons_isp* isp, moons_solve_info* info);
+
+/* ---- the MHD time step (HW/MOONS/MOONS_solver.f90:47-144, one RK stage) --
+ * Momentum: add_all_momentum_sources (add_all_momentum_sources.f90:22-86)
+ * + Euler_time_AB2_sources (time_marching_methods.f90:117-150) with PCG_U
+ * (mom_diffusion, prec_mom_VF) and clean_div (clean_divergence.f90:37-59)
+ * with PCG_P (Lap_uniform_SF, prec_Lap_SF).
+ * Induction, MOONS_IND_B: add_all_induction_sources
+ * (add_all_induction_sources.f90:24-60, constrained-transport curl(u x B))
+ * + Euler_time_AB2_sources with PCG_B (ind_diffusion, prec_ind_VF) and
+ * clean_div with PCG_phi; then compute_J, compute_Btot, compute_JCrossB
+ * (induction_extend.f90:441-536).
+ * Induction, MOONS_IND_POTENTIAL: low-Rem electric-potential form (new; not
+ * in the reference): div(sigma grad phi) = div(sigma u x B0) with
+ * Lap_nonuniform_props, J = sigma(-grad phi + u x B0), F += N J x B0. */
+enum { MOONS_IND_OFF = 0, MOONS_IND_B = 1, MOONS_IND_POTENTIAL = 2 };
+
+typedef struct {
+  double dt;
+  int induction;            /* MOONS_IND_*                                  */
+  int finite_Rem;           /* Btot = B0 + B (else B0)                      */
+  int mpg_dir;              /* compute_add_MPG direction (0 = off)          */
+  double mpg_scale;         /* SP%MT%mean_pressure_grad%scale               */
+  double scale_advection_U; /* SP%MT%advection_convection%scale (-1)        */
+  double scale_diffusion_U; /* SP%MT%diffusion%scale = coeff_explicit       */
+  double scale_JxB;         /* SP%MT%JCrossB%scale (N = Ha^2/Re)            */
+  double scale_advection_B; /* SP%IT%advection%scale (1)                    */
+  double scale_diffusion_B; /* SP%IT%diffusion%scale (-beta)                */
+  double scale_current;     /* SP%IT%current%scale (1/Rem)                  */
+  double coeff_implicit_U;  /* SP%VS%U%MFP%coeff_implicit (-1/Re)... see
+                               assign_coeff_implicit_VS: -coeff_natural*alpha */
+  double coeff_implicit_B;  /* SP%VS%B%MFP%coeff_implicit (1/Rem)           */
+  moons_isp isp_U, isp_p, isp_B, isp_phi;
+  moons_bc_spec bc_U[3], bc_p, bc_B[3], bc_phi;
+  int ind_offset[3];        /* first fluid cell inside the induction mesh, minus 1
+                               (0 when both meshes coincide)                  */
+  int prescribed_Ustar;     /* SP%VS%U%SS%prescribed_BCs: Ustar gets prescribed
+                               BCs (set_prescribed_BCs, block_field_extend.f90:810-821) */
+  int prescribed_Bstar;     /* SP%VS%B%SS%prescribed_BCs                      */
+} moons_mhd_params;
+
+typedef struct {
+  int steps;
+  int iters_U, iters_p, iters_B, iters_phi;  /* summed over the steps       */
+  double res_p, res_phi;                     /* last relative residuals     */
+  double ms;                                 /* device time of the steps    */
+} moons_step_info;
+
+/* Field handles of an MHD object (for upload / download / probes). */
+enum {
+  MOONS_MHD_U = 0,        /* comp 0..2, faces on the fluid mesh              */
+  MOONS_MHD_P = 1,        /* CC on the fluid mesh                            */
+  MOONS_MHD_B = 2,        /* comp 0..2, faces on the induction mesh          */
+  MOONS_MHD_B0 = 3,       /* comp 0..2, faces                                */
+  MOONS_MHD_PHI = 4,      /* CC on the induction mesh                        */
+  MOONS_MHD_J = 5,        /* comp 0..2: edges (B form) / faces (potential)   */
+  MOONS_MHD_SIGMA_INV = 6,/* comp 0..2: edges (B form) / sigma on faces (potential) */
+  MOONS_MHD_JXB = 7,      /* comp 0..2, faces on the induction mesh          */
+  MOONS_MHD_DIVU = 8,     /* CC on the fluid mesh (probe)                    */
+  MOONS_MHD_DIVB = 9      /* CC on the induction mesh (probe)                */
+};
+
+/* mesh_ind may equal mesh_mom.  Fields start at 0; upload initial U, B, B0
+ * and sigma through moons_mhd_field, then call moons_mhd_init. */
+int moons_mhd_create(moons_mesh* mesh_mom, moons_mesh* mesh_ind,
+                     const moons_mhd_params* prm, moons_mhd** out);
+int moons_mhd_destroy(moons_mhd* s);
+int moons_mhd_field(moons_mhd* s, int which, int comp, moons_sf** out);
+/* init_mom/init_induction tail + the start of solve_MOONS: apply BCs,
+ * J, Btot, J x B, U at cell centres and edges. */
+int moons_mhd_init(moons_mhd* s);
+int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info);
+/* probes: div U and div B over the whole array (compute_Ln L2, as the
+ * divU/divB probes export) */
+int moons_mhd_divergence(moons_mhd* s, double* l2_divU, double* l2_divB);
 
 #ifdef __cplusplus
 }

@@ -67,6 +67,55 @@ class SolveInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+IND_OFF, IND_B, IND_POTENTIAL = 0, 1, 2
+MHD_U, MHD_P, MHD_B, MHD_B0, MHD_PHI, MHD_J, MHD_SIGMA_INV, MHD_JXB, MHD_DIVU, MHD_DIVB = range(10)
+
+
+class MHDParams(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double),
+        ("induction", C.c_int),
+        ("finite_Rem", C.c_int),
+        ("mpg_dir", C.c_int),
+        ("mpg_scale", C.c_double),
+        ("scale_advection_U", C.c_double),
+        ("scale_diffusion_U", C.c_double),
+        ("scale_JxB", C.c_double),
+        ("scale_advection_B", C.c_double),
+        ("scale_diffusion_B", C.c_double),
+        ("scale_current", C.c_double),
+        ("coeff_implicit_U", C.c_double),
+        ("coeff_implicit_B", C.c_double),
+        ("isp_U", ISP),
+        ("isp_p", ISP),
+        ("isp_B", ISP),
+        ("isp_phi", ISP),
+        ("bc_U", BCSpec * 3),
+        ("bc_p", BCSpec),
+        ("bc_B", BCSpec * 3),
+        ("bc_phi", BCSpec),
+        ("ind_offset", C.c_int * 3),
+        ("prescribed_Ustar", C.c_int),
+        ("prescribed_Bstar", C.c_int),
+    ]
+
+
+class StepInfo(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int),
+        ("iters_U", C.c_int),
+        ("iters_p", C.c_int),
+        ("iters_B", C.c_int),
+        ("iters_phi", C.c_int),
+        ("res_p", C.c_double),
+        ("res_phi", C.c_double),
+        ("ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def bc_spec(types: Sequence[int], values: Sequence[float] | None = None,
             prescribed: Sequence[int] | None = None, c_w: Sequence[float] | None = None,
             order: Sequence[int] | None = None, all_neumann: bool = False) -> BCSpec:
@@ -140,6 +189,13 @@ def lib() -> C.CDLL:
             "moons_pcg_destroy": (C.c_int, [_P]),
             "moons_pcg_update_mfp": (C.c_int, [_P, C.c_double, C.c_int]),
             "moons_pcg_solve": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(ISP), C.POINTER(SolveInfo)]),
+            "moons_mhd_create": (C.c_int, [_P, _P, C.POINTER(MHDParams), C.POINTER(_P)]),
+            "moons_mhd_destroy": (C.c_int, [_P]),
+            "moons_mhd_field": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P)]),
+            "moons_mhd_init": (C.c_int, [_P]),
+            "moons_mhd_step": (C.c_int, [_P, C.c_int, C.POINTER(StepInfo)]),
+            "moons_mhd_divergence": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+            "moons_kernel_launches": (C.c_longlong, []),
         }
         for name, (rt, at) in sig.items():
             f = getattr(L, name)
@@ -274,6 +330,80 @@ def _ptrs(fs):
     return arr
 
 
+class _FieldView:
+    """A field owned by an MHD object (upload/download/shape only)."""
+
+    def __init__(self, owner, h):
+        self.owner = owner
+        self.h = h
+        s = (C.c_int * 3)()
+        _check(lib().moons_sf_shape(h, s))
+        self.shape = (s[0], s[1], s[2])
+
+    @property
+    def n(self):
+        return self.shape[0] * self.shape[1] * self.shape[2]
+
+    upload = Field.upload
+    download = Field.download
+
+    def upload_ptr(self, ptr: int):
+        """Copy n doubles from host address ``ptr`` (e.g. pinned memory)."""
+        _check(lib().moons_sf_upload(self.h, C.cast(ptr, _D), self.n))
+
+    def download_ptr(self, ptr: int):
+        _check(lib().moons_sf_download(self.h, C.cast(ptr, _D), self.n))
+
+
+class MHD:
+    """The MHD time-step object (solve_MOONS for one block pair)."""
+
+    def __init__(self, mesh_mom: Mesh, mesh_ind: Mesh, params: MHDParams):
+        self.meshes = (mesh_mom, mesh_ind)
+        self.params = params
+        h = _P()
+        _check(lib().moons_mhd_create(mesh_mom.h, mesh_ind.h, C.byref(params), C.byref(h)))
+        self.h = h
+
+    def field(self, which: int, comp: int = 0):
+        f = _P()
+        _check(lib().moons_mhd_field(self.h, which, comp, C.byref(f)))
+        return _FieldView(self, f)
+
+    def upload(self, which, comp, a):
+        self.field(which, comp).upload(a)
+
+    def download(self, which, comp=0):
+        return self.field(which, comp).download()
+
+    def shape(self, which, comp=0):
+        return self.field(which, comp).shape
+
+    def init(self):
+        _check(lib().moons_mhd_init(self.h))
+
+    def step(self, n: int = 1) -> dict:
+        info = StepInfo()
+        _check(lib().moons_mhd_step(self.h, int(n), C.byref(info)))
+        return info.as_dict()
+
+    def divergence(self):
+        a, b = C.c_double(), C.c_double()
+        _check(lib().moons_mhd_divergence(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if self.h:
+            lib().moons_mhd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class PCG:
     """PCG_solver_SF (ncomp=1) / PCG_solver_VF (ncomp=3)."""
 
@@ -304,3 +434,9 @@ class PCG:
             self.close()
         except Exception:
             pass
+
+
+def kernel_launches() -> int:
+    """Kernels this process launched through the library (host launches plus
+    the launches executed inside the solver's device-side loop)."""
+    return int(lib().moons_kernel_launches())

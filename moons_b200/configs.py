@@ -1,0 +1,160 @@
+"""Case presets: the reference's compiled-in sim_params for the benchmark cases.
+
+Each builder returns ``(mesh_mom_coords, mesh_ind_coords, params, init)``:
+coordinates with ghost nodes (x, y, z), the C-ABI parameter struct and a
+callable ``init(mhd, rng)`` that uploads the initial fields (seeded noise,
+applied field, conductivity).  The same builder drives the CUDA library and
+the CPU oracle, so both see identical inputs.
+
+* ``ldc``  -- 3D MHD lid-driven cavity (sim_params_default_MHD_LDC_Sergey_uniform:
+  LDC_at_ymax lid, Neumann pressure, uniform B0, solve_method 6), with the
+  low-Rem electric-potential induction form or the reference's B form.
+* ``duct`` -- fully developed MHD duct (sim_params_default_MHD_Shercliff:
+  periodic streamwise, mean pressure gradient, finite Rem, solve_method 6),
+  Roberts two-sided clustering (robertsBoth, beta=1.05) across, and a
+  conducting wall layer in the induction mesh (MD_sigma/MD_fluid split).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import capi as G
+from . import mesh_gen as mg
+
+ORDER_LDC = (5, 6, 1, 2, 3, 4)   # get_apply_BC_order for periodic_dir = 0 (sim_params_aux.f90:41)
+ORDER_PZ = (1, 2, 3, 4, 5, 6)    # get_apply_BC_order for periodic z       (sim_params_aux.f90:48)
+
+
+def _isp(iter_max, tol_rel, tol_abs=1e-15, nskip=1):
+    return G.isp(iter_max, tol_rel, tol_abs, nskip)
+
+
+def _coeffs(prm, Re, Ha, Rem, finite_Rem):
+    # var_set_extend.f90:55-86 with alpha = 1 (backward Euler) -> beta = 0
+    N = Ha ** 2 / Re
+    prm.coeff_implicit_U = -(1.0 / Re)                       # -coeff_natural*alpha, coeff_natural = 1/Re
+    prm.coeff_implicit_B = -(-1.0 / Rem)                     # coeff_natural = -1/Rem
+    prm.scale_advection_U = -1.0
+    prm.scale_diffusion_U = 0.0                              # coeff_natural*beta
+    prm.scale_JxB = N
+    prm.scale_advection_B = 1.0
+    prm.scale_diffusion_B = -0.0                             # -beta
+    prm.scale_current = 1.0 / Rem
+    prm.finite_Rem = 1 if finite_Rem else 0
+    return N
+
+
+def ldc(n: int = 32, Re: float = 400.0, Ha: float = 10.0, dt: float = 1e-3, induction: int = G.IND_POTENTIAL,
+        Rem: float = 1.0, tol: float = 1e-10, noise: float = 1e-6, iter_max: int = 20000):
+    h = mg.add_ghost_nodes(mg.uniform(0.0, 1.0, n))
+    coords = (h, h.copy(), h.copy())
+    prm = G.MHDParams()
+    prm.dt = dt
+    prm.induction = induction
+    _coeffs(prm, Re, Ha, Rem, False)
+    prm.mpg_dir = 0
+    prm.mpg_scale = 0.0
+    for name in ("isp_U", "isp_p", "isp_B", "isp_phi"):
+        setattr(prm, name, _isp(iter_max, tol))
+    for c in range(3):
+        vals = [0.0] * 6
+        if c == 0:
+            vals[3] = 1.0  # LDC_at_ymax: init(U%x%BF(1)%BCs,1.0,4)
+        prm.bc_U[c] = G.bc_spec([G.DIRICHLET] * 6, values=vals, order=ORDER_LDC)
+        t = [G.DIRICHLET] * 6
+        t[2 * c] = t[2 * c + 1] = G.NEUMANN  # pseudo_vacuum (init_B_BCs.f90:83-97)
+        prm.bc_B[c] = G.bc_spec(t, order=ORDER_LDC)
+    prm.bc_p = G.bc_spec([G.NEUMANN] * 6, order=ORDER_LDC, all_neumann=True)
+    if induction == G.IND_POTENTIAL:
+        # insulating walls: J.n = 0 -> homogeneous Neumann for the potential
+        prm.bc_phi = G.bc_spec([G.NEUMANN] * 6, order=ORDER_LDC, all_neumann=True)
+    else:
+        prm.bc_phi = G.bc_spec([G.DIRICHLET] * 6, order=ORDER_LDC)  # init_phi_BCs default
+    prm.prescribed_Ustar = 1
+    prm.prescribed_Bstar = 1
+
+    def init(sim, rng):
+        for c in range(3):
+            s = sim.shape(G.MHD_U, c)
+            sim.upload(G.MHD_U, c, rng.normal(0.0, noise, s))
+            b0 = np.zeros(sim.shape(G.MHD_B0, c))
+            if c == 1:
+                b0[:] = 1.0  # uniform_B_field dir=2
+            sim.upload(G.MHD_B0, c, b0)
+            sim.upload(G.MHD_SIGMA_INV, c, np.ones(sim.shape(G.MHD_SIGMA_INV, c)))
+
+    return coords, coords, prm, init
+
+
+def duct(nx: int = 64, ny: int = 64, nz: int = 256, Re: float = 1000.0, Ha: float = 100.0, dt: float = 5e-4,
+         beta: float = 1.05, n_wall: int = 4, t_wall: float = 1.0, sigma_wall: float = 0.01, Lz: float = 8.0,
+         Rem: float = 1.0, tol: float = 1e-10, noise: float = 1e-4, iter_max: int = 20000):
+    """Streamwise z (periodic), field along y, walls normal to x and y."""
+    hx = mg.roberts_both(-1.0, 1.0, nx, beta)
+    hy = mg.roberts_both(-1.0, 1.0, ny, beta)
+    hz = mg.uniform(0.0, Lz, nz)
+    mom = (mg.add_ghost_nodes(hx), mg.add_ghost_nodes(hy), mg.add_ghost_nodes(hz))
+    if n_wall > 0:
+        w = t_wall / n_wall
+        ext = lambda h: np.concatenate([h[0] - w * np.arange(n_wall, 0, -1), h, h[-1] + w * np.arange(1, n_wall + 1)])
+        ind = (mg.add_ghost_nodes(ext(hx)), mg.add_ghost_nodes(ext(hy)), mg.add_ghost_nodes(hz))
+        off = (n_wall, n_wall, 0)
+    else:
+        ind = mom
+        off = (0, 0, 0)
+    prm = G.MHDParams()
+    prm.dt = dt
+    prm.induction = G.IND_B
+    _coeffs(prm, Re, Ha, Rem, True)
+    prm.mpg_dir = 3
+    prm.mpg_scale = 1.0  # SP%MT%mean_pressure_grad scale (Shercliff preset), dp/dz = -1
+    for name in ("isp_U", "isp_p", "isp_B", "isp_phi"):
+        setattr(prm, name, _isp(iter_max, tol))
+    P, D, N = G.PERIODIC, G.DIRICHLET, G.NEUMANN
+    for c in range(3):
+        prm.bc_U[c] = G.bc_spec([D, D, D, D, P, P], order=ORDER_PZ)
+        t = [D, D, D, D, P, P]
+        if c < 2:
+            t[2 * c] = t[2 * c + 1] = N  # pseudo_vacuum outside the wall layer
+        prm.bc_B[c] = G.bc_spec(t, order=ORDER_PZ)
+    prm.bc_p = G.bc_spec([N, N, N, N, P, P], order=ORDER_PZ, all_neumann=True)
+    prm.bc_phi = G.bc_spec([D, D, D, D, P, P], order=ORDER_PZ)
+    prm.prescribed_Ustar = 1
+    prm.prescribed_Bstar = 1
+    for d in range(3):
+        prm.ind_offset[d] = off[d]
+
+    def init(sim, rng):
+        for c in range(3):
+            sim.upload(G.MHD_U, c, rng.normal(0.0, noise, sim.shape(G.MHD_U, c)))
+            b0 = np.zeros(sim.shape(G.MHD_B0, c))
+            if c == 1:
+                b0[:] = 1.0
+            sim.upload(G.MHD_B0, c, b0)
+        # sigma^-1 on edges: 1 inside the closed fluid box, 1/sigma_wall in the wall layer
+        hn = ind
+        lo = [mom[d][1] for d in range(3)]
+        hi = [mom[d][-2] for d in range(3)]
+        hc = [0.5 * (h[1:] + h[:-1]) for h in hn]
+        tol_ = 1e-12
+        for c in range(3):  # edge along c: CC along c, N elsewhere
+            axes = [hc[d] if d == c else hn[d] for d in range(3)]
+            inside = [(a >= lo[d] - tol_) & (a <= hi[d] + tol_) if d < 2 else np.ones_like(a, bool)
+                      for d, a in enumerate(axes)]
+            m3 = inside[0][:, None, None] & inside[1][None, :, None] & inside[2][None, None, :]
+            si = np.where(m3, 1.0, 1.0 / sigma_wall)
+            sim.upload(G.MHD_SIGMA_INV, c, si)
+
+    return mom, ind, prm, init
+
+
+def make(backend, builder, *args, seed: int = 0, **kw):
+    """Create meshes + the MHD object on ``backend`` (moons_b200.capi or the
+    oracle module) from a builder, upload the seeded initial state and init."""
+    mom, ind, prm, init = builder(*args, **kw)
+    mm = backend.Mesh(*mom)
+    mi = mm if ind is mom else backend.Mesh(*ind)
+    sim = backend.MHD(mm, mi, prm)
+    init(sim, np.random.default_rng(seed))
+    sim.init()
+    return sim

@@ -2,3 +2,4 @@
 // live in headers shared by the entry-point files).
 #include "mesh.cu"
 #include "pcg.cu"
+#include "mhd.cu"

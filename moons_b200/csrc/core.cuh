@@ -84,6 +84,14 @@ int cuda_fail(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return mg::cuda_fail(e_, #call); \
   } while (0)
 
+// every kernel launch of the library goes through MG_LAUNCH, which counts it
+extern long long g_launch_count;
+#define MG_LAUNCH(K, GRID, BLOCK, STREAM, ...)            \
+  do {                                                    \
+    K<<<(GRID), (BLOCK), 0, (STREAM)>>>(__VA_ARGS__);     \
+    ++mg::g_launch_count;                                 \
+  } while (0)
+
 constexpr int kBlock = 256;
 inline unsigned nblocks(size_t n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }
 

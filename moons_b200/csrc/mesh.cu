@@ -10,6 +10,7 @@
 namespace mg {
 
 static thread_local std::string g_err;
+long long g_launch_count = 0;
 void set_error(const std::string& m) { g_err = m; }
 int cuda_fail(cudaError_t e, const char* what) {
   g_err = std::string("CUDA error ") + cudaGetErrorString(e) + " in " + what;
@@ -155,12 +156,12 @@ int launch_del(moons_mesh* m, DF out, DF in, int n, int dir, int pad, int gen) {
     return arg_fail("del: staggered extents do not match the data locations");
   if (diffType <= 2 && in.s(dir) != out.s(dir)) return arg_fail("del: collocated extents differ");
   if (n < 1 || n > 2) return arg_fail("del: n must be 1 or 2");
-  k_del<<<nblocks(out.n()), kBlock, 0, m->stream>>>(out, in, m->dg.c[dir - 1], dir, diffType, n, pad, gen);
+  MG_LAUNCH(k_del, nblocks(out.n()), kBlock, m->stream, out, in, m->dg.c[dir - 1], dir, diffType, n, pad, gen);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
 int launch_pw(moons_mesh* m, int op, DF a, const DF* b, double c) {
-  k_pw<<<nblocks(a.n()), kBlock, 0, m->stream>>>(op, a.f, b ? b->f : nullptr, c, a.n());
+  MG_LAUNCH(k_pw, nblocks(a.n()), kBlock, m->stream, op, a.f, b ? b->f : nullptr, c, a.n());
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
@@ -170,30 +171,30 @@ int launch_bcs(moons_mesh* m, DF u, const DBC& bc, bool implicit) {
     int f = bc.order[o];
     int d = (f + 1) / 2;
     int np = (d == 1 ? u.s1 * u.s2 : (d == 2 ? u.s0 * u.s2 : u.s0 * u.s1));
-    k_bc_face<<<nblocks(np), kBlock, 0, m->stream>>>(u, bc, f, implicit ? 1 : 0);
+    MG_LAUNCH(k_bc_face, nblocks(np), kBlock, m->stream, u, bc, f, implicit ? 1 : 0);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
 int launch_plane(moons_mesh* m, DF u, int d, int idx, double v, int mode) {
   int np = (d == 1 ? u.s1 * u.s2 : (d == 2 ? u.s0 * u.s2 : u.s0 * u.s1));
-  k_plane<<<nblocks(np), kBlock, 0, m->stream>>>(u, d, idx, v, mode);
+  MG_LAUNCH(k_plane, nblocks(np), kBlock, m->stream, u, d, idx, v, mode);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
 int launch_lap_centered(moons_mesh* m, DF out, DF u, int ghost_zero, int scale_mode, double coeff) {
   if (out.dl != u.dl) return arg_fail("lap_centered: data locations differ");
-  k_lap_centered<<<nblocks(out.n()), kBlock, 0, m->stream>>>(out, u, m->dg, ghost_zero, scale_mode, coeff);
+  MG_LAUNCH(k_lap_centered, nblocks(out.n()), kBlock, m->stream, out, u, m->dg, ghost_zero, scale_mode, coeff);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
 int launch_interp(moons_mesh* m, DF out, DF in, int dir) {
   if (n_along(out.dl, dir) && !n_along(in.dl, dir)) {
-    k_interp_c2n<<<nblocks(out.n()), kBlock, 0, m->stream>>>(out, in, m->dg.c[dir - 1], dir);
+    MG_LAUNCH(k_interp_c2n, nblocks(out.n()), kBlock, m->stream, out, in, m->dg.c[dir - 1], dir);
     int a = dir == 1 ? 2 : 1, b = dir == 3 ? 2 : 3;
-    k_extrap<<<nblocks(out.s(a) * out.s(b)), kBlock, 0, m->stream>>>(out, in, dir);
+    MG_LAUNCH(k_extrap, nblocks(out.s(a) * out.s(b)), kBlock, m->stream, out, in, dir);
   } else if (!n_along(out.dl, dir) && n_along(in.dl, dir)) {
-    k_interp_n2c<<<nblocks(out.n()), kBlock, 0, m->stream>>>(out, in, dir);
+    MG_LAUNCH(k_interp_n2c, nblocks(out.n()), kBlock, m->stream, out, in, dir);
   } else {
     return arg_fail("interp: bad data locations");
   }
@@ -286,6 +287,8 @@ using namespace mg;
 extern "C" {
 
 const char* moons_last_error(void) { return g_err.c_str(); }
+
+long long moons_kernel_launches(void) { return g_launch_count; }
 
 int moons_mesh_create(moons_mesh** out, const double* hx, int sx, const double* hy, int sy, const double* hz,
                       int sz, int device) {

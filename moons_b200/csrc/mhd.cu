@@ -1,0 +1,671 @@
+// mhd.cu -- the MOONS MHD time step on one B200 (HW/MOONS/MOONS_solver.f90:47-144).
+//
+// All fields stay in HBM for the whole run; the host only enqueues kernels
+// and the four PCG solves per step (U, p, B, phi).  The sequence follows the
+// reference routine by routine; pointwise chains the reference runs as
+// separate whole-array passes (AB2 RHS build, projection update, cross
+// products) are fused into single kernels that perform the same operations
+// in the same order per point.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kernels.cuh"
+#include "runtime.cuh"
+
+namespace mg {
+
+// ---- fused pointwise kernels ----------------------------------------------
+// AB2 RHS (Euler_time_AB2_sources, time_marching_methods.f90:137-142):
+//   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t + L ; t = t*dt ;
+//   assign_wall_Dirichlet(t,0,X) ; t = t + X ; Xnm1 = X
+__global__ void k_ab2_rhs(DF t, DF F, DF Fm, DF L, DF X, DF Xnm1, double dt, int wallbits) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= t.n()) return;
+  int i, j, k;
+  ijk_of(idx, t, i, j, k);
+  double v = F.f[idx] * 1.5;
+  v = v + Fm.f[idx] * (-0.5);
+  v = v + L.f[idx];
+  v = v * dt;
+  if (wallbits) {
+    if (((wallbits & 1) && i == 2) || ((wallbits & 2) && i == t.s0 - 1) || ((wallbits & 4) && j == 2) ||
+        ((wallbits & 8) && j == t.s1 - 1) || ((wallbits & 16) && k == 2) || ((wallbits & 32) && k == t.s2 - 1))
+      v = 0.0;
+  }
+  double x = X.f[idx];
+  t.f[idx] = v + x;
+  Xnm1.f[idx] = x;
+}
+// clean_div tail: temp_F = grad(phi) ; temp_F *= 1/scale ; X = Xstar - temp_F
+__global__ void k_project(DF X, DF Xstar, DF g, double inv_scale) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= X.n()) return;
+  double gv = g.f[idx] * inv_scale;
+  X.f[idx] = Xstar.f[idx] - gv;
+}
+// cross_product_x/y/z (HW/grid_field/GF_3D/GF_cross_product.f90:17-70)
+__global__ void k_cross(DF o, DF a1, DF a2, DF b1, DF b2, int neg) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= o.n()) return;
+  double v = a1.f[idx] * b2.f[idx] - a2.f[idx] * b1.f[idx];
+  o.f[idx] = neg ? -v : v;
+}
+// embed (ind <- mom) / extract (mom <- ind) over the physical region of the
+// fluid-mesh field (indices 2..s-1), offset o (ops_embedExtract.f90)
+__global__ void k_embed_extract(DF dst, DF src, int o0, int o1, int o2, int embed) {
+  const DF& mom = embed ? src : dst;
+  int ni = mom.s0 - 2, nj = mom.s1 - 2, nk = mom.s2 - 2;
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)ni * nj * nk) return;
+  int i = (int)(idx % ni) + 2;
+  size_t r = idx / ni;
+  int j = (int)(r % nj) + 2;
+  int k = (int)(r / nj) + 2;
+  if (embed) dst(i + o0, j + o1, k + o2) = src(i, j, k);
+  else dst(i, j, k) = src(i + o0, j + o1, k + o2);
+}
+// u += c everywhere (compute_add_MPG: add(U%x, scale*dt))
+__global__ void k_add_scalar(double* a, double c, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = a[i] + c;
+}
+__global__ void k_sumsq(DF a, double* partial, unsigned* ticket, double* out) {
+  double acc = 0.0;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < a.n(); idx += (size_t)gridDim.x * blockDim.x) {
+    double v = a.f[idx];
+    acc += v * v;
+  }
+  double bs = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
+  if (last_block(ticket)) {
+    double t = sum_partials(partial, gridDim.x);
+    if (threadIdx.x == 0) {
+      *out = t;
+      *ticket = 0;
+    }
+  }
+}
+
+}  // namespace mg
+
+using namespace mg;
+
+namespace {
+inline int orth(int a, int b) { return 6 - a - b; }  // 1-based directions
+}
+
+struct moons_mhd {
+  moons_mesh* mm = nullptr;  // fluid mesh
+  moons_mesh* mi = nullptr;  // induction mesh
+  bool same = true;
+  moons_mhd_params P{};
+  std::vector<moons_sf*> owned;
+  // momentum
+  moons_sf *U[3], *Ustar[3], *Unm1[3], *F[3], *Fnm1[3], *L[3], *tF1[3], *tF2[3], *tF3[3], *tCC, *p, *UCC[3], *divU;
+  moons_sf* UE[3][3];
+  moons_pcg *pcgU = nullptr, *pcgP = nullptr;
+  // induction
+  moons_sf *B[3], *Bstar[3], *Bnm1[3], *B0[3], *Btot[3], *Fi[3], *Fnm1i[3], *Li[3], *J[3], *jxb[3], *sig[3], *phi,
+      *tCCi, *tFi1[3], *tFi2[3], *tE[3], *curlUxB[3], *divB, *Ui[3], *E[3];
+  moons_sf *UEi[3][3], *BE[3][3], *TF1[3][3], *TF2[3][3];
+  moons_pcg *pcgB = nullptr, *pcgPhi = nullptr;
+  double coefU = NAN, coefB = NAN;
+  int iters[4] = {0, 0, 0, 0};
+  double res_p = 0, res_phi = 0;
+  double* d_red = nullptr;
+  cudaStream_t mi_stream_saved = nullptr;  // the induction mesh runs on the fluid mesh's stream
+};
+
+namespace {
+
+int mk(moons_mhd* s, moons_mesh* m, int dl, moons_sf** out) {
+  int r = moons_sf_create(m, dl, out);
+  if (!r) s->owned.push_back(*out);
+  return r;
+}
+
+int set_bcs_from(moons_sf* f, const moons_bc_spec& b) { return moons_sf_set_bcs(f, &b); }
+
+// moons_sf view helpers
+inline DF& D(moons_sf* f) { return f->f; }
+
+int launch_cross3(moons_mesh* m, moons_sf* const* o, moons_sf* A[3][3], moons_sf* Bt[3][3]) {
+  // cross_product_TF (TF_extend.f90:385-401)
+  MG_LAUNCH(k_cross, nblocks(D(o[0]).n()), kBlock, m->stream, D(o[0]), D(A[1][0]), D(A[2][0]), D(Bt[1][0]), D(Bt[2][0]), 0);
+  MG_LAUNCH(k_cross, nblocks(D(o[1]).n()), kBlock, m->stream, D(o[1]), D(A[0][1]), D(A[2][1]), D(Bt[0][1]), D(Bt[2][1]), 1);
+  MG_LAUNCH(k_cross, nblocks(D(o[2]).n()), kBlock, m->stream, D(o[2]), D(A[0][2]), D(A[1][2]), D(Bt[0][2]), D(Bt[1][2]), 0);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+int face2edge_nd(moons_mesh* m, moons_sf* E[3][3], moons_sf* const* Fc) {
+  int r = MOONS_OK;
+  for (int c = 0; c < 3 && !r; c++)
+    for (int l = 0; l < 3 && !r; l++)
+      if (c != l) r = launch_interp(m, D(E[c][l]), D(Fc[c]), orth(c + 1, l + 1));
+  return r;
+}
+int edge2face_nd(moons_mesh* m, moons_sf* Fo[3][3], moons_sf* const* Ec) {
+  return face2edge_nd(m, Fo, Ec);  // same index pattern: interp along the orthogonal direction
+}
+int face2face_nd(moons_mesh* m, moons_sf* Fo[3][3], moons_sf* const* Fc, moons_sf* tCC) {
+  int r = MOONS_OK;
+  for (int c = 0; c < 3 && !r; c++)
+    for (int l = 0; l < 3 && !r; l++)
+      if (c != l) {
+        r = launch_interp(m, D(tCC), D(Fc[c]), c + 1);
+        if (!r) r = launch_interp(m, D(Fo[c][l]), D(tCC), l + 1);
+      }
+  return r;
+}
+int curl3(moons_mesh* m, moons_sf* const* o, moons_sf* const* u) {
+  int r;
+  if ((r = launch_del(m, D(o[0]), D(u[2]), 1, 2, 0, 1))) return r;
+  if ((r = launch_del(m, D(o[0]), D(u[1]), 1, 3, 0, 3))) return r;
+  if ((r = launch_del(m, D(o[1]), D(u[0]), 1, 3, 0, 1))) return r;
+  if ((r = launch_del(m, D(o[1]), D(u[2]), 1, 1, 0, 3))) return r;
+  if ((r = launch_del(m, D(o[2]), D(u[1]), 1, 1, 0, 1))) return r;
+  return launch_del(m, D(o[2]), D(u[0]), 1, 2, 0, 3);
+}
+int div3(moons_mesh* m, moons_sf* o, moons_sf* const* u) {
+  int r;
+  if ((r = launch_del(m, D(o), D(u[0]), 1, 1, 0, 1))) return r;
+  if ((r = launch_del(m, D(o), D(u[1]), 1, 2, 0, 2))) return r;
+  if ((r = launch_del(m, D(o), D(u[2]), 1, 3, 0, 2))) return r;
+  return mask_ghost_XPeriodic(m, D(o), o->bc.defined ? &o->bc : nullptr);
+}
+int grad3(moons_mesh* m, moons_sf* const* g, moons_sf* u) {
+  int r;
+  for (int d = 0; d < 3; d++)
+    if ((r = launch_del(m, D(g[d]), D(u), 1, d + 1, 0, 1))) return r;
+  return MOONS_OK;
+}
+int embed_extract(moons_mesh* m, moons_sf* dst, moons_sf* src, const int o[3], bool embed) {
+  const DF& mom = embed ? D(src) : D(dst);
+  size_t n = (size_t)(mom.s0 - 2) * (mom.s1 - 2) * (mom.s2 - 2);
+  MG_LAUNCH(k_embed_extract, nblocks(n), kBlock, m->stream, D(dst), D(src), o[0], o[1], o[2], embed ? 1 : 0);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+int copy(moons_mesh* m, moons_sf* dst, moons_sf* src) {
+  MG_CUDA(cudaMemcpyAsync(D(dst).f, D(src).f, D(src).n() * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+  return MOONS_OK;
+}
+
+int solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp& isp, int* iters, double* rel) {
+  moons_solve_info info{};
+  int r = moons_pcg_solve(s, x, b, &isp, &info);
+  *iters += info.iterations;
+  if (rel) *rel = info.rel;
+  return r;
+}
+
+// Euler_time_AB2_sources + clean_div_PCG (time_marching_methods.f90:117-150,
+// clean_divergence.f90:37-59), scale = 1/dt
+int euler_ab2(moons_mhd* s, moons_mesh* m, moons_pcg* pv, moons_pcg* ps, const moons_isp& iv, const moons_isp& is,
+              moons_sf** X, moons_sf** Xstar, moons_sf** Xnm1, moons_sf* ph, moons_sf** Fn, moons_sf** Fm,
+              moons_sf** Lx, moons_sf** t1, moons_sf* tcc, double coeff_implicit, double* coef_cache, int slot_v,
+              int slot_s, double* res_s) {
+  double dt = s->P.dt;
+  for (int c = 0; c < 3; c++) {
+    int wb = dirichlet_wall_bits(X[c]->bc.defined ? &X[c]->bc : nullptr, D(X[c]).dl);
+    MG_LAUNCH(k_ab2_rhs, nblocks(D(t1[c]).n()), kBlock, m->stream, D(t1[c]), D(Fn[c]), D(Fm[c]), D(Lx[c]), D(X[c]),
+                                                                 D(Xnm1[c]), dt, wb);
+  }
+  MG_CUDA(cudaGetLastError());
+  double c = dt * 1.0 * coeff_implicit;
+  int r;
+  if (!(c == *coef_cache)) {  // update_MFP(...,.true.): the preconditioner only changes with c
+    if ((r = moons_pcg_update_mfp(pv, c, 1))) return r;
+    *coef_cache = c;
+  }
+  if ((r = solve(pv, Xstar, t1, iv, &s->iters[slot_v], nullptr))) return r;
+  double scale = 1.0 / dt;
+  if ((r = div3(m, tcc, Xstar))) return r;
+  if ((r = launch_pw(m, PW_SCALE, D(tcc), nullptr, scale))) return r;
+  moons_sf* xp[1] = {ph};
+  moons_sf* bp[1] = {tcc};
+  if ((r = solve(ps, xp, bp, is, &s->iters[slot_s], res_s))) return r;
+  if ((r = grad3(m, t1, ph))) return r;
+  for (int k = 0; k < 3; k++) {
+    MG_LAUNCH(k_project, nblocks(D(X[k]).n()), kBlock, m->stream, D(X[k]), D(Xstar[k]), D(t1[k]), 1.0 / scale);
+    if ((r = launch_bcs(m, D(X[k]), X[k]->bc, false))) return r;
+  }
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+int compute_J(moons_mhd* s) {
+  moons_mesh* m = s->mi;
+  int r = curl3(m, s->J, s->B);
+  for (int c = 0; c < 3 && !r; c++) r = launch_pw(m, PW_SCALE, D(s->J[c]), nullptr, s->P.scale_current);
+  return r;
+}
+int compute_Btot(moons_mhd* s) {
+  moons_mesh* m = s->mi;
+  int r = MOONS_OK;
+  for (int c = 0; c < 3 && !r; c++) {
+    r = copy(m, s->Btot[c], s->B0[c]);
+    if (!r && s->P.finite_Rem) r = launch_pw(m, PW_ADD, D(s->Btot[c]), &D(s->B[c]), 0.0);
+  }
+  return r;
+}
+int compute_JxB(moons_mhd* s) {
+  moons_mesh* m = s->mi;
+  int r;
+  if (s->P.induction == MOONS_IND_B) r = edge2face_nd(m, s->TF1, s->J);
+  else r = face2face_nd(m, s->TF1, s->J, s->tCCi);
+  if (!r) r = face2face_nd(m, s->TF2, s->Btot, s->tCCi);
+  if (!r) r = launch_cross3(m, s->jxb, s->TF1, s->TF2);
+  for (int c = 0; c < 3 && !r; c++) r = launch_pw(m, PW_SCALE, D(s->jxb[c]), nullptr, s->P.scale_JxB);
+  return r;
+}
+int potential_solve(moons_mhd* s) {
+  moons_mesh* m = s->mi;
+  int r = MOONS_OK;
+  for (int c = 0; c < 3 && !r; c++) {
+    if (s->same) r = copy(m, s->Ui[c], s->U[c]);
+    else r = embed_extract(m, s->Ui[c], s->U[c], s->P.ind_offset, true);
+  }
+  if (!r) r = face2face_nd(m, s->TF1, s->Ui, s->tCCi);
+  if (!r) r = face2face_nd(m, s->TF2, s->Btot, s->tCCi);
+  if (!r) r = launch_cross3(m, s->E, s->TF1, s->TF2);
+  for (int c = 0; c < 3 && !r; c++) {
+    r = copy(m, s->tFi1[c], s->E[c]);
+    if (!r) r = launch_pw(m, PW_MUL, D(s->tFi1[c]), &D(s->sig[c]), 0.0);
+  }
+  if (!r) r = div3(m, s->tCCi, s->tFi1);
+  if (r) return r;
+  moons_sf* xf[1] = {s->phi};
+  moons_sf* bf[1] = {s->tCCi};
+  if ((r = solve(s->pcgPhi, xf, bf, s->P.isp_phi, &s->iters[3], &s->res_phi))) return r;
+  if ((r = grad3(m, s->tFi2, s->phi))) return r;
+  for (int c = 0; c < 3 && !r; c++) {
+    r = copy(m, s->J[c], s->E[c]);
+    if (!r) r = launch_pw(m, PW_SUB, D(s->J[c]), &D(s->tFi2[c]), 0.0);
+    if (!r) r = launch_pw(m, PW_MUL, D(s->J[c]), &D(s->sig[c]), 0.0);
+  }
+  return r;
+}
+
+// advect_U_convection1 (ops_advect.f90:71-127) into tF3
+int advect_U_convection1(moons_mhd* s) {
+  moons_mesh* m = s->mm;
+  int r = MOONS_OK;
+  for (int c = 0; c < 3 && !r; c++) {
+    r = launch_interp(m, D(s->tCC), D(s->U[c]), c + 1);
+    if (!r) r = launch_del(m, D(s->tF3[c]), D(s->tCC), 1, c + 1, 0, 1);
+    if (!r) r = launch_pw(m, PW_MUL, D(s->tF3[c]), &D(s->U[c]), 0.0);
+  }
+  struct T {
+    int c, e, d, v;
+  };
+  const T terms[6] = {{0, 2, 2, 1}, {0, 1, 3, 2}, {1, 2, 1, 0}, {1, 0, 3, 2}, {2, 1, 1, 0}, {2, 0, 2, 1}};
+  for (const T& t : terms) {
+    if (r) break;
+    r = launch_del(m, D(s->tF1[t.c]), D(s->UE[t.c][t.e]), 1, t.d, 0, 1);
+    if (!r) r = launch_interp(m, D(s->tCC), D(s->U[t.v]), t.v + 1);
+    if (!r) r = launch_interp(m, D(s->tF2[t.c]), D(s->tCC), t.c + 1);
+    if (!r) r = launch_pw(m, PW_MUL, D(s->tF1[t.c]), &D(s->tF2[t.c]), 0.0);
+    if (!r) r = launch_pw(m, PW_ADD, D(s->tF3[t.c]), &D(s->tF1[t.c]), 0.0);
+  }
+  return r;
+}
+
+int step_once(moons_mhd* s) {
+  moons_mesh* m = s->mm;
+  const moons_mhd_params& P = s->P;
+  double dt = P.dt;
+  int r = MOONS_OK;
+  // ---- add_all_momentum_sources
+  if (P.mpg_dir >= 1 && P.mpg_dir <= 3) {
+    DF u = D(s->U[P.mpg_dir - 1]);
+    MG_LAUNCH(k_add_scalar, nblocks(u.n()), kBlock, m->stream, u.f, P.mpg_scale * dt, u.n());
+    for (int c = 0; c < 3 && !r; c++) r = launch_bcs(m, D(s->U[c]), s->U[c]->bc, false);
+  }
+  for (int c = 0; c < 3 && !r; c++) {
+    r = copy(m, s->Fnm1[c], s->F[c]);
+    if (!r) r = launch_pw(m, PW_FILL, D(s->L[c]), nullptr, 0.0);
+    if (!r) r = launch_pw(m, PW_FILL, D(s->F[c]), nullptr, 0.0);
+  }
+  if (!r) r = advect_U_convection1(s);
+  for (int c = 0; c < 3 && !r; c++) r = launch_pw(m, PW_ADD_PRODUCT, D(s->F[c]), &D(s->tF3[c]), P.scale_advection_U);
+  if (!r && P.scale_diffusion_U != 0.0) {
+    for (int c = 0; c < 3 && !r; c++) {
+      r = launch_del(m, D(s->tF1[c]), D(s->U[c]), 2, 1, 0, 1);
+      if (!r) r = launch_del(m, D(s->tF1[c]), D(s->U[c]), 2, 2, 0, 2);
+      if (!r) r = launch_del(m, D(s->tF1[c]), D(s->U[c]), 2, 3, 0, 2);
+      if (!r) r = launch_pw(m, PW_ADD_PRODUCT, D(s->F[c]), &D(s->tF1[c]), P.scale_diffusion_U);
+    }
+  }
+  if (!r && P.induction != MOONS_IND_OFF) {
+    for (int c = 0; c < 3 && !r; c++) {
+      if (s->same) r = copy(m, s->tF1[c], s->jxb[c]);
+      else r = embed_extract(m, s->tF1[c], s->jxb[c], P.ind_offset, false);
+      if (!r) r = mask_ghost_XPeriodic(m, D(s->tF1[c]), nullptr);
+      if (!r) r = launch_pw(m, PW_ADD_PRODUCT, D(s->F[c]), &D(s->tF1[c]), 1.0);
+    }
+  }
+  if (r) return r;
+  // ---- solve_momentum (method 6)
+  r = euler_ab2(s, m, s->pcgU, s->pcgP, P.isp_U, P.isp_p, s->U, s->Ustar, s->Unm1, s->p, s->F, s->Fnm1, s->L, s->tF1,
+                s->tCC, P.coeff_implicit_U, &s->coefU, 0, 1, &s->res_p);
+  if (r) return r;
+  for (int c = 0; c < 3 && !r; c++) r = launch_interp(m, D(s->UCC[c]), D(s->U[c]), c + 1);
+  if (!r) r = face2edge_nd(m, s->UE, s->U);
+  if (r) return r;
+  // ---- induction
+  moons_mesh* mi = s->mi;
+  if (P.induction == MOONS_IND_B) {
+    for (int c = 0; c < 3 && !r; c++) {
+      r = copy(mi, s->Fnm1i[c], s->Fi[c]);
+      if (!r) r = launch_pw(mi, PW_FILL, D(s->Li[c]), nullptr, 0.0);
+      if (!r) r = launch_pw(mi, PW_FILL, D(s->Fi[c]), nullptr, 0.0);
+    }
+    for (int c = 0; c < 3 && !r; c++)
+      for (int l = 0; l < 3 && !r; l++)
+        if (c != l) {
+          if (s->same) r = copy(mi, s->UEi[c][l], s->UE[c][l]);
+          else r = embed_extract(mi, s->UEi[c][l], s->UE[c][l], P.ind_offset, true);
+        }
+    if (!r) r = face2edge_nd(mi, s->BE, s->Btot);
+    if (!r) r = launch_cross3(mi, s->tE, s->UEi, s->BE);
+    if (!r) r = curl3(mi, s->curlUxB, s->tE);
+    for (int c = 0; c < 3 && !r; c++)
+      r = launch_pw(mi, PW_ADD_PRODUCT, D(s->Fi[c]), &D(s->curlUxB[c]), P.scale_advection_B);
+    if (!r && P.scale_diffusion_B != 0.0) {
+      for (int c = 0; c < 3 && !r; c++) {
+        r = copy(mi, s->tE[c], s->J[c]);
+        if (!r) r = launch_pw(mi, PW_MUL, D(s->tE[c]), &D(s->sig[c]), 0.0);
+      }
+      if (!r) r = curl3(mi, s->tFi2, s->tE);
+      for (int c = 0; c < 3 && !r; c++)
+        r = launch_pw(mi, PW_ADD_PRODUCT, D(s->Fi[c]), &D(s->tFi2[c]), P.scale_diffusion_B);
+    }
+    if (r) return r;
+    r = euler_ab2(s, mi, s->pcgB, s->pcgPhi, P.isp_B, P.isp_phi, s->B, s->Bstar, s->Bnm1, s->phi, s->Fi, s->Fnm1i,
+                  s->Li, s->tFi1, s->tCCi, P.coeff_implicit_B, &s->coefB, 2, 3, &s->res_phi);
+    if (!r) r = compute_J(s);
+    if (!r) r = compute_Btot(s);
+    if (!r) r = compute_JxB(s);
+  } else if (P.induction == MOONS_IND_POTENTIAL) {
+    r = compute_Btot(s);
+    if (!r) r = potential_solve(s);
+    if (!r) r = compute_JxB(s);
+  }
+  return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm, moons_mhd** out) {
+  if (!mm || !mi || !prm || !out) {
+    set_error("moons_mhd_create: null pointer");
+    return MOONS_ERR_ARG;
+  }
+  if (mm->device != mi->device) {
+    set_error("moons_mhd_create: meshes on different devices");
+    return MOONS_ERR_ARG;
+  }
+  if (prm->induction < MOONS_IND_OFF || prm->induction > MOONS_IND_POTENTIAL || !(prm->dt > 0)) {
+    set_error("moons_mhd_create: bad induction mode or dt");
+    return MOONS_ERR_ARG;
+  }
+  auto* s = new moons_mhd();
+  s->mm = mm;
+  s->mi = mi;
+  s->same = (mm == mi);
+  s->P = *prm;
+  if (!s->same) {
+    for (int d = 0; d < 3; d++)
+      if (prm->ind_offset[d] < 0 || mm->sn[d] + prm->ind_offset[d] > mi->sn[d]) {
+        delete s;
+        set_error("moons_mhd_create: fluid mesh does not fit inside the induction mesh at ind_offset");
+        return MOONS_ERR_SHAPE;
+      }
+    // one stream for both meshes: the induction step reads what the momentum
+    // step wrote (embed/extract), so the two must not overlap
+    s->mi_stream_saved = mi->stream;
+    mi->stream = mm->stream;
+  } else {
+    for (int d = 0; d < 3; d++) s->P.ind_offset[d] = 0;
+  }
+  int r = MOONS_OK;
+  auto F = [&](moons_mesh* m, int dl, moons_sf** o) {
+    if (!r) r = mk(s, m, dl, o);
+  };
+  for (int c = 0; c < 3; c++) {
+    for (moons_sf** f : {&s->U[c], &s->Ustar[c], &s->Unm1[c], &s->F[c], &s->Fnm1[c], &s->L[c], &s->tF1[c], &s->tF2[c],
+                         &s->tF3[c]})
+      F(mm, MOONS_FX + c, f);
+    F(mm, MOONS_CC, &s->UCC[c]);
+    for (int l = 0; l < 3; l++) {
+      s->UE[c][l] = s->UEi[c][l] = s->BE[c][l] = s->TF1[c][l] = s->TF2[c][l] = nullptr;
+      if (c != l) {
+        F(mm, MOONS_EX + l, &s->UE[c][l]);
+        F(mi, MOONS_EX + l, &s->UEi[c][l]);
+        F(mi, MOONS_EX + l, &s->BE[c][l]);
+        F(mi, MOONS_FX + l, &s->TF1[c][l]);
+        F(mi, MOONS_FX + l, &s->TF2[c][l]);
+      }
+    }
+  }
+  F(mm, MOONS_CC, &s->tCC);
+  F(mm, MOONS_CC, &s->p);
+  F(mm, MOONS_CC, &s->divU);
+  bool pot = prm->induction == MOONS_IND_POTENTIAL;
+  for (int c = 0; c < 3; c++) {
+    for (moons_sf** f : {&s->B[c], &s->Bstar[c], &s->Bnm1[c], &s->B0[c], &s->Btot[c], &s->Fi[c], &s->Fnm1i[c],
+                         &s->Li[c], &s->jxb[c], &s->tFi1[c], &s->tFi2[c], &s->curlUxB[c], &s->Ui[c], &s->E[c]})
+      F(mi, MOONS_FX + c, f);
+    F(mi, pot ? MOONS_FX + c : MOONS_EX + c, &s->J[c]);
+    F(mi, pot ? MOONS_FX + c : MOONS_EX + c, &s->sig[c]);
+    F(mi, MOONS_EX + c, &s->tE[c]);
+  }
+  F(mi, MOONS_CC, &s->phi);
+  F(mi, MOONS_CC, &s->tCCi);
+  F(mi, MOONS_CC, &s->divB);
+  // BCs
+  for (int c = 0; c < 3 && !r; c++) {
+    r = set_bcs_from(s->U[c], prm->bc_U[c]);
+    if (!r) {
+      s->Ustar[c]->bc = s->U[c]->bc;
+      if (prm->prescribed_Ustar)
+        for (int f = 1; f <= 6; f++) {
+          int d = (f + 1) / 2;
+          int sz = D(s->U[c]).s(d);
+          bool many = n_along(D(s->U[c]).dl, d) ? sz > 4 : sz > 3;
+          if (many) s->Ustar[c]->bc.prescribed[f] = 1;
+        }
+    }
+  }
+  if (!r) r = set_bcs_from(s->p, prm->bc_p);
+  if (!r && prm->induction != MOONS_IND_OFF) {
+    for (int c = 0; c < 3 && !r; c++) {
+      r = set_bcs_from(s->B[c], prm->bc_B[c]);
+      if (!r) {
+        s->Bstar[c]->bc = s->B[c]->bc;
+        for (int f = 1; f <= 6; f++) {
+          s->Bstar[c]->bc.value[f] = 0.0;  // set_BCs_homogeneous
+          int d = (f + 1) / 2;
+          int sz = D(s->B[c]).s(d);
+          bool many = n_along(D(s->B[c]).dl, d) ? sz > 4 : sz > 3;
+          if (prm->prescribed_Bstar && many) s->Bstar[c]->bc.prescribed[f] = 1;
+        }
+      }
+    }
+    if (!r) r = set_bcs_from(s->phi, prm->bc_phi);
+  }
+  if (!r && cudaMalloc((void**)&s->d_red, 2 * sizeof(double)) != cudaSuccess) r = MOONS_ERR_NOMEM;
+  if (r) {
+    moons_mhd_destroy(s);
+    return r;
+  }
+  *out = s;
+  return MOONS_OK;
+}
+
+int moons_mhd_destroy(moons_mhd* s) {
+  if (!s) return MOONS_OK;
+  for (moons_pcg* p : {s->pcgU, s->pcgP, s->pcgB, s->pcgPhi})
+    if (p) moons_pcg_destroy(p);
+  for (moons_sf* f : s->owned) moons_sf_destroy(f);
+  if (s->d_red) cudaFree(s->d_red);
+  if (s->mi_stream_saved) s->mi->stream = s->mi_stream_saved;
+  delete s;
+  return MOONS_OK;
+}
+
+int moons_mhd_field(moons_mhd* s, int which, int comp, moons_sf** out) {
+  if (!s || !out || comp < 0 || comp > 2) {
+    set_error("moons_mhd_field: bad argument");
+    return MOONS_ERR_ARG;
+  }
+  moons_sf* f = nullptr;
+  switch (which) {
+    case MOONS_MHD_U: f = s->U[comp]; break;
+    case MOONS_MHD_P: f = s->p; break;
+    case MOONS_MHD_B: f = s->B[comp]; break;
+    case MOONS_MHD_B0: f = s->B0[comp]; break;
+    case MOONS_MHD_PHI: f = s->phi; break;
+    case MOONS_MHD_J: f = s->J[comp]; break;
+    case MOONS_MHD_SIGMA_INV: f = s->sig[comp]; break;
+    case MOONS_MHD_JXB: f = s->jxb[comp]; break;
+    case MOONS_MHD_DIVU: f = s->divU; break;
+    case MOONS_MHD_DIVB: f = s->divB; break;
+    default:
+      set_error("moons_mhd_field: unknown field");
+      return MOONS_ERR_ARG;
+  }
+  *out = f;
+  return MOONS_OK;
+}
+
+int moons_mhd_init(moons_mhd* s) {
+  if (!s) {
+    set_error("null mhd");
+    return MOONS_ERR_ARG;
+  }
+  moons_mesh* m = s->mm;
+  cudaSetDevice(m->device);
+  int r = launch_bcs(m, D(s->p), s->p->bc, false);
+  for (int c = 0; c < 3 && !r; c++) {
+    r = launch_bcs(m, D(s->U[c]), s->U[c]->bc, false);
+    if (!r) r = copy(m, s->Unm1[c], s->U[c]);
+    if (!r) r = copy(m, s->Ustar[c], s->U[c]);
+  }
+  if (r) return r;
+  MG_CUDA(cudaStreamSynchronize(m->stream));
+  // solvers (init_mom :160-169, init_induction :203-215)
+  if (!s->pcgU) {
+    moons_sf* xbu[3] = {s->U[0], s->U[1], s->U[2]};
+    if ((r = moons_pcg_create(m, MOONS_OP_MOM_DIFFUSION, MOONS_PREC_MOM, 3, s->Ustar, xbu, nullptr, &s->pcgU))) return r;
+    moons_sf* xp[1] = {s->p};
+    if ((r = moons_pcg_create(m, MOONS_OP_LAP_UNIFORM, MOONS_PREC_LAP, 1, xp, xp, nullptr, &s->pcgP))) return r;
+    if (s->P.induction == MOONS_IND_B) {
+      if ((r = moons_pcg_create(s->mi, MOONS_OP_IND_DIFFUSION, MOONS_PREC_IND, 3, s->Bstar, s->B, s->sig, &s->pcgB)))
+        return r;
+      moons_sf* xf[1] = {s->phi};
+      if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_UNIFORM, MOONS_PREC_LAP, 1, xf, xf, nullptr, &s->pcgPhi))) return r;
+    } else if (s->P.induction == MOONS_IND_POTENTIAL) {
+      moons_sf* xf[1] = {s->phi};
+      if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_PROPS, MOONS_PREC_LAP, 1, xf, xf, s->sig, &s->pcgPhi))) return r;
+    }
+  }
+  moons_mesh* mi = s->mi;
+  if (s->P.induction == MOONS_IND_B) {
+    for (int c = 0; c < 3 && !r; c++) {
+      r = copy(mi, s->Bnm1[c], s->B[c]);
+      if (!r) r = launch_bcs(mi, D(s->B[c]), s->B[c]->bc, false);
+      if (!r) r = copy(mi, s->Bstar[c], s->B[c]);
+    }
+    if (!r) r = compute_J(s);
+    if (!r) r = compute_Btot(s);
+    if (!r) r = compute_JxB(s);
+    if (!r) r = compute_J(s);
+  }
+  for (int c = 0; c < 3 && !r; c++) r = launch_interp(m, D(s->UCC[c]), D(s->U[c]), c + 1);
+  if (!r) r = face2edge_nd(m, s->UE, s->U);
+  if (!r && s->P.induction == MOONS_IND_POTENTIAL) {
+    r = compute_Btot(s);
+    if (!r) r = potential_solve(s);
+    if (!r) r = compute_JxB(s);
+  }
+  if (r) return r;
+  MG_CUDA(cudaStreamSynchronize(m->stream));
+  if (mi != m) MG_CUDA(cudaStreamSynchronize(mi->stream));
+  return MOONS_OK;
+}
+
+int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
+  if (!s || nsteps < 0) {
+    set_error("moons_mhd_step: bad argument");
+    return MOONS_ERR_ARG;
+  }
+  if (!s->pcgU) {
+    set_error("moons_mhd_step: call moons_mhd_init first");
+    return MOONS_ERR_STATE;
+  }
+  moons_mesh* m = s->mm;
+  cudaSetDevice(m->device);
+  for (int k = 0; k < 4; k++) s->iters[k] = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, m->stream);
+  int r = MOONS_OK;
+  for (int n = 0; n < nsteps && !r; n++) {
+    r = step_once(s);
+  }
+  cudaEventRecord(e1, m->stream);
+  cudaError_t e = cudaStreamSynchronize(m->stream);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  MG_CUDA(e);
+  if (info) {
+    info->steps = nsteps;
+    info->iters_U = s->iters[0];
+    info->iters_p = s->iters[1];
+    info->iters_B = s->iters[2];
+    info->iters_phi = s->iters[3];
+    info->res_p = s->res_p;
+    info->res_phi = s->res_phi;
+    info->ms = ms;
+  }
+  return MOONS_OK;
+}
+
+int moons_mhd_divergence(moons_mhd* s, double* du, double* db) {
+  if (!s || !du || !db) {
+    set_error("moons_mhd_divergence: null pointer");
+    return MOONS_ERR_ARG;
+  }
+  moons_mesh* m = s->mm;
+  int r = div3(m, s->divU, s->U);
+  if (r) return r;
+  MG_LAUNCH(k_sumsq, std::min<unsigned>(kRedBlocks, nblocks(D(s->divU).n())), kBlock, m->stream, 
+      D(s->divU), m->d_partial, m->d_ticket, s->d_red);
+  MG_CUDA(cudaStreamSynchronize(m->stream));
+  double h[2] = {0, 0};
+  if (s->P.induction == MOONS_IND_B) {
+    moons_mesh* mi = s->mi;
+    if ((r = div3(mi, s->divB, s->B))) return r;
+    MG_LAUNCH(k_sumsq, std::min<unsigned>(kRedBlocks, nblocks(D(s->divB).n())), kBlock, mi->stream, 
+        D(s->divB), mi->d_partial, mi->d_ticket, s->d_red + 1);
+    MG_CUDA(cudaStreamSynchronize(mi->stream));
+  } else {
+    MG_CUDA(cudaMemsetAsync(s->d_red + 1, 0, sizeof(double), m->stream));
+  }
+  MG_CUDA(cudaMemcpy(h, s->d_red, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  *du = h[0];
+  *db = h[1];
+  return MOONS_OK;
+}
+
+}  // extern "C"

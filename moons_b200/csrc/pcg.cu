@@ -315,6 +315,7 @@ struct moons_pcg {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double* gx[3] = {nullptr, nullptr, nullptr};
+  long long body_launches = 0;  // kernels per execution of the loop body
 };
 
 namespace {
@@ -423,7 +424,7 @@ int compute_prec(moons_pcg* s) {
       set_error("moons_pcg: prec_ind needs the induction operator's sigma^-1 edge fields");
       return MOONS_ERR_ARG;
     }
-    k_prec<<<nblocks(s->Minv[c].n()), kBlock, 0, m->stream>>>(s->Minv[c], m->dg, mode, s->coeff, c, sx, sy, sz);
+    MG_LAUNCH(k_prec, nblocks(s->Minv[c].n()), kBlock, m->stream, s->Minv[c], m->dg, mode, s->coeff, c, sx, sy, sz);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
@@ -447,12 +448,12 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
     dw[c] = dirichlet_wall_bits(s->x_bc[c].defined ? &s->x_bc[c] : nullptr, s->x_dl[c]);
   }
   unsigned G = red_grid(s->Ax, s->nc);
-  k_pcg_ap<<<G, kBlock, 0, m->stream>>>(c3(s->Ax, s->nc), c3(s->p, s->nc), c3(s->vol, s->nc), wm[0], wm[1], wm[2],
+  MG_LAUNCH(k_pcg_ap, G, kBlock, m->stream, c3(s->Ax, s->nc), c3(s->p, s->nc), c3(s->vol, s->nc), wm[0], wm[1], wm[2],
                                         dw[0], dw[1], dw[2], s->S, m->d_partial, m->d_ticket);
-  k_pcg_update<<<G, kBlock, 0, m->stream>>>(c3(x, s->nc), c3(s->p, s->nc), c3(s->r, s->nc), c3(s->Ax, s->nc),
+  MG_LAUNCH(k_pcg_update, G, kBlock, m->stream, c3(x, s->nc), c3(s->p, s->nc), c3(s->r, s->nc), c3(s->Ax, s->nc),
                                             c3(s->z, s->nc), c3(s->Minv, s->nc), dw[0], dw[1], dw[2], s->S,
                                             m->d_partial + 2 * kRedBlocks, m->d_ticket + 1);
-  k_pcg_p<<<G, kBlock, 0, m->stream>>>(c3(s->p, s->nc), c3(s->z, s->nc), s->S);
+  MG_LAUNCH(k_pcg_p, G, kBlock, m->stream, c3(s->p, s->nc), c3(s->z, s->nc), s->S);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
@@ -479,8 +480,11 @@ int build_graph(moons_pcg* s, DF* x) {
   MG_CUDA(cudaGraphAddNode(&node, s->graph, nullptr, 0, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   MG_CUDA(cudaStreamBeginCaptureToGraph(m->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  long long before = g_launch_count;  // captured launches run later, once per body execution
   int r = enqueue_iteration(s, x);
-  k_set_cond<<<1, 1, 0, m->stream>>>(h, s->S);
+  MG_LAUNCH(k_set_cond, 1, 1, m->stream, h, s->S);
+  s->body_launches = g_launch_count - before;
+  g_launch_count = before;
   cudaGraph_t captured = nullptr;
   cudaError_t e = cudaStreamEndCapture(m->stream, &captured);
   if (r) return r;
@@ -564,7 +568,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     else if (!r) s->hS = (PcgScalars*)p;
   }
   if (!r) {
-    for (int c = 0; c < nc; c++) k_volume<<<nblocks(s->vol[c].n()), kBlock, 0, m->stream>>>(s->vol[c], m->dg);
+    for (int c = 0; c < nc; c++) MG_LAUNCH(k_volume, nblocks(s->vol[c].n()), kBlock, m->stream, s->vol[c], m->dg);
     // coeff_implicit is not known here; Lap needs none and mom/ind set it through update_mfp
     r = compute_prec(s);
   }
@@ -654,9 +658,9 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   for (int c = 0; c < nc && !r; c++) r = launch_pw(m, PW_COPY, s->r[c], &B[c], 0.0);
   if (!r && s->all_neumann) {
     // tempx = r*vol; mean = sum(tempx,1)/vol%vol; r -= mean; assign_ghost_XPeriodic(r,0)
-    k_reduce<<<red_grid(&s->r[0], 1), kBlock, 0, m->stream>>>(c3(&s->r[0], 1), c3(&s->vol[0], 1), 2, 0, 0, 0,
+    MG_LAUNCH(k_reduce, red_grid(&s->r[0], 1), kBlock, m->stream, c3(&s->r[0], 1), c3(&s->vol[0], 1), 2, 0, 0, 0,
                                                                m->d_scal, m->d_partial, m->d_ticket);
-    k_sub_mean<<<nblocks(s->r[0].n()), kBlock, 0, m->stream>>>(s->r[0], m->d_scal, s->volsum[0]);
+    MG_LAUNCH(k_sub_mean, nblocks(s->r[0].n()), kBlock, m->stream, s->r[0], m->d_scal, s->volsum[0]);
     r = mask_ghost_XPeriodic(m, s->r[0], nullptr);
   }
   for (int c = 0; c < nc && !r; c++) {
@@ -692,7 +696,7 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   *s->hS = h;
   MG_CUDA(cudaMemcpyAsync(s->S, s->hS, sizeof(PcgScalars), cudaMemcpyHostToDevice, m->stream));
   // res0 = sqrt(sum r^2) whole array
-  k_reduce<<<red_grid(s->r, nc), kBlock, 0, m->stream>>>(c3(s->r, nc), c3(s->r, nc), 1, 0, 0, 0, &s->S->res0,
+  MG_LAUNCH(k_reduce, red_grid(s->r, nc), kBlock, m->stream, c3(s->r, nc), c3(s->r, nc), 1, 0, 0, 0, &s->S->res0,
                                                          m->d_partial, m->d_ticket);
   // z = Minv r ; p = z ; rhok = dot(r,z)
   for (int c = 0; c < nc; c++) {
@@ -702,9 +706,9 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   }
   int dw[3] = {0, 0, 0};
   for (int c = 0; c < nc; c++) dw[c] = dirichlet_wall_bits(s->x_bc[c].defined ? &s->x_bc[c] : nullptr, s->x_dl[c]);
-  k_reduce<<<red_grid(s->r, nc), kBlock, 0, m->stream>>>(c3(s->r, nc), c3(s->z, nc), 0, dw[0], dw[1], dw[2],
+  MG_LAUNCH(k_reduce, red_grid(s->r, nc), kBlock, m->stream, c3(s->r, nc), c3(s->z, nc), 0, dw[0], dw[1], dw[2],
                                                          &s->S->rhok, m->d_partial, m->d_ticket);
-  k_pcg_start<<<1, 1, 0, m->stream>>>(s->S);
+  MG_LAUNCH(k_pcg_start, 1, 1, m->stream, s->S);
   MG_CUDA(cudaGetLastError());
   // ---- the loop: one graph launch (WHILE node) unless the solve is trivial
   bool need_graph = !s->exec;
@@ -727,6 +731,7 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   const PcgScalars& H = *s->hS;
+  g_launch_count += s->body_launches * (long long)H.body_runs;
   if (info) {
     info->iterations = H.iter;
     info->res0 = H.res0;

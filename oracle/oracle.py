@@ -17,7 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libmoons_oracle.so")
 
-from moons_b200.capi import BCSpec, ISP, SolveInfo  # noqa: E402  (plain ctypes structs)
+from moons_b200.capi import BCSpec, ISP, SolveInfo, MHDParams, StepInfo  # noqa: E402  (plain ctypes structs)
 
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
@@ -25,7 +25,7 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("moons_oracle.cpp", "moons_oracle.hpp", "oracle_capi.cpp", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("moons_oracle.cpp", "moons_oracle.hpp", "oracle_capi.cpp", "moons_oracle_mhd.cpp", "Makefile")]
     stale = not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs)
     if force or stale:
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
@@ -62,6 +62,14 @@ def lib():
             "or_pcg_destroy": (None, [_P]),
             "or_pcg_update_mfp": (C.c_int, [_P, C.c_double, C.c_int]),
             "or_pcg_solve": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(ISP), C.POINTER(SolveInfo)]),
+            "or_mhd_create": (_P, [_P, _P, C.POINTER(MHDParams)]),
+            "or_mhd_destroy": (None, [_P]),
+            "or_mhd_upload": (C.c_int, [_P, C.c_int, C.c_int, _D, C.c_longlong]),
+            "or_mhd_download": (C.c_int, [_P, C.c_int, C.c_int, _D, C.c_longlong]),
+            "or_mhd_shape": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+            "or_mhd_init": (C.c_int, [_P]),
+            "or_mhd_step": (C.c_int, [_P, C.c_int, C.POINTER(StepInfo)]),
+            "or_mhd_divergence": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         }
         for n, (rt, at) in sig.items():
             f = getattr(L, n)
@@ -210,6 +218,53 @@ class PCG:
         try:
             if self.h:
                 lib().or_pcg_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class MHD:
+    """The oracle's MHD time step, same surface as moons_b200.capi.MHD."""
+
+    def __init__(self, mesh_mom, mesh_ind, params):
+        self.meshes = (mesh_mom, mesh_ind)
+        self.params = params
+        self.h = lib().or_mhd_create(mesh_mom.h, mesh_ind.h, C.byref(params))
+
+    def shape(self, which, comp=0):
+        s = (C.c_int * 3)()
+        _check(lib().or_mhd_shape(self.h, which, comp, s))
+        return (s[0], s[1], s[2])
+
+    def upload(self, which, comp, a):
+        a = np.asarray(a, dtype=np.float64)
+        assert a.shape == self.shape(which, comp)
+        flat = np.ascontiguousarray(a.ravel(order="F"))
+        _check(lib().or_mhd_upload(self.h, which, comp, flat.ctypes.data_as(_D), flat.size))
+
+    def download(self, which, comp=0):
+        shp = self.shape(which, comp)
+        flat = np.empty(shp[0] * shp[1] * shp[2])
+        _check(lib().or_mhd_download(self.h, which, comp, flat.ctypes.data_as(_D), flat.size))
+        return flat.reshape(shp, order="F")
+
+    def init(self):
+        _check(lib().or_mhd_init(self.h))
+
+    def step(self, n=1):
+        info = StepInfo()
+        _check(lib().or_mhd_step(self.h, int(n), C.byref(info)))
+        return info.as_dict()
+
+    def divergence(self):
+        a, b = C.c_double(), C.c_double()
+        _check(lib().or_mhd_divergence(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().or_mhd_destroy(self.h)
                 self.h = None
         except Exception:
             pass
