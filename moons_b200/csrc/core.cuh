@@ -96,11 +96,14 @@ constexpr int kBlock = 256;
 inline unsigned nblocks(size_t n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }
 
 // index -> (i,j,k) 1-based
+// (fields are < 2^32 points: 32-bit division only)
 __device__ __forceinline__ void ijk_of(size_t idx, const DF& a, int& i, int& j, int& k) {
-  i = (int)(idx % a.s0) + 1;
-  size_t r = idx / a.s0;
-  j = (int)(r % a.s1) + 1;
-  k = (int)(r / a.s1) + 1;
+  unsigned u = (unsigned)idx, s0 = (unsigned)a.s0, s1 = (unsigned)a.s1;
+  unsigned q = u / s0;
+  i = (int)(u - q * s0) + 1;
+  unsigned kk = q / s1;
+  j = (int)(q - kk * s1) + 1;
+  k = (int)kk + 1;
 }
 __device__ __forceinline__ int pick(int d, int i, int j, int k) { return d == 1 ? i : (d == 2 ? j : k); }
 

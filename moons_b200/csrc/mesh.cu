@@ -294,6 +294,11 @@ int moons_mesh_create(moons_mesh** out, const double* hx, int sx, const double* 
                       int sz, int device) {
   if (!out || !hx || !hy || !hz) return arg_fail("moons_mesh_create: null pointer");
   if (sx < 4 || sy < 4 || sz < 4) return arg_fail("moons_mesh_create: need at least 4 nodes per axis");
+  // kernels index points with 32-bit integers and put z on gridDim.y
+  if ((double)sx * sy * sz >= 2147483647.0 || sz > 65535) {
+    g_err = "moons_mesh_create: mesh beyond 2^31 points or 65535 z-nodes";
+    return MOONS_ERR_LIMIT;
+  }
   auto* m = new moons_mesh();
   int dev = device;
   if (dev < 0) {

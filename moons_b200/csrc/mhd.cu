@@ -193,12 +193,16 @@ int copy(moons_mesh* m, moons_sf* dst, moons_sf* src) {
   return MOONS_OK;
 }
 
+// solves are enqueued without a host sync; iteration counts, NaN flags and
+// the last residual are read once per moons_mhd_step (mg_pcg_totals)
 int solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp& isp, int* iters, double* rel) {
-  moons_solve_info info{};
-  int r = moons_pcg_solve(s, x, b, &isp, &info);
-  *iters += info.iterations;
-  if (rel) *rel = info.rel;
-  return r;
+  (void)iters;
+  (void)rel;
+  if (isp.n_skip_check_res < 1) {
+    set_error("moons_mhd: n_skip_check_res must be >= 1");
+    return MOONS_ERR_ARG;
+  }
+  return mg_pcg_enqueue(s, x, b, &isp);
 }
 
 // Euler_time_AB2_sources + clean_div_PCG (time_marching_methods.f90:117-150,
@@ -612,6 +616,9 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
   moons_mesh* m = s->mm;
   cudaSetDevice(m->device);
   for (int k = 0; k < 4; k++) s->iters[k] = 0;
+  moons_pcg* solvers[4] = {s->pcgU, s->pcgP, s->pcgB, s->pcgPhi};
+  for (moons_pcg* p : solvers)
+    if (p) mg_pcg_clear_totals(p);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -628,6 +635,21 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
   cudaEventDestroy(e1);
   if (r) return r;
   MG_CUDA(e);
+  int nan = 0;
+  for (int k = 0; k < 4; k++) {
+    if (!solvers[k]) continue;
+    int it = 0, na = 0;
+    double rel = 0;
+    if ((r = mg_pcg_totals(solvers[k], &it, &na, &rel))) return r;
+    s->iters[k] = it;
+    nan |= na;
+    if (k == 1) s->res_p = rel;
+    if (k == 3) s->res_phi = rel;
+  }
+  if (nan) {
+    set_error("moons_mhd_step: NaN in a solver's residual norms");
+    return MOONS_ERR_NAN;
+  }
   if (info) {
     info->steps = nsteps;
     info->iters_U = s->iters[0];

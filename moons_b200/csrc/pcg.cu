@@ -1,192 +1,50 @@
 // pcg.cu -- matrix-free Jacobi-PCG (PCG_solver_algorithm.f90:37-179) with
 // every scalar of the recurrence kept on the device.
 //
-// One iteration is a fixed sequence of launches (implicit BCs of p, the
-// operator, a fused mask*vol + dot(p,Ap) kernel whose last block forms
-// alpha, a fused x/r/z update + dot(r,r) + dot(z,r) kernel whose last block
-// runs the exit test of update_exit_loop and forms beta, and p = beta p + z).
-// The whole loop is captured once into a CUDA graph whose WHILE node repeats
-// the body until the device-side exit flag is set; the flag also comes up
-// when the iteration count reaches iter_max, so the loop always ends.
+// modify_RHS (PCG_aux.f90:30-79) runs once per solve with the generic
+// kernels.  The iteration body is the fused K1/K2/K3 of fused.cuh (K1 is two
+// kernels for the curl-curl operator).  The whole loop is captured once into
+// a CUDA graph whose WHILE node repeats the body until the device-side exit
+// flag is set; the flag also comes up when the iteration count reaches
+// iter_max, and the node stops after iter_max+2 body runs in any case, so the
+// loop always ends.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 
-#include "kernels.cuh"
+#include "fused.cuh"
 #include "runtime.cuh"
 
 namespace mg {
-
-struct PcgScalars {
-  double rhok, alpha, res, res0, beta, pap, rr, zr, mean;
-  int iter, done, exit_reason, nan;
-  int iter_max, nskip;
-  double tol_rel, tol_abs;
-  int body_runs;  // executions of the loop body (second bound on the loop)
-};
-
-struct WallMask {  // masks applied to Ap, from the BCs of x_BC (PCG_solver_algorithm.f90:72-75)
-  int neu, dir, per;  // face bits (Neumann x0.5, Dirichlet =0); dir bits for periodic_single
-};
 
 struct Comp3 {
   DF a[3];
   int nc;
 };
 
-// ---------------------------------------------------------------------------
-// kernels
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double wall_factor(const DF& a, int i, int j, int k, const WallMask& w, bool& zero) {
-  // multiply_wall_Neumann(0.5) then assign_wall_Dirichlet(0) then assign_wall_Periodic_single(0)
-  double f = 1.0;
-  zero = false;
-  int t[4] = {0, i, j, k};
-  for (int d = 1; d <= 3; d++) {
-    int s = a.s(d);
-    if ((w.neu >> (2 * d - 2)) & 1 && t[d] == 2) f *= 0.5;
-    if ((w.neu >> (2 * d - 1)) & 1 && t[d] == s - 1) f *= 0.5;
-    if ((w.dir >> (2 * d - 2)) & 1 && t[d] == 2) zero = true;
-    if ((w.dir >> (2 * d - 1)) & 1 && t[d] == s - 1) zero = true;
-    if ((w.per >> (d - 1)) & 1 && t[d] == s - 1) zero = true;
-  }
-  return f;
-}
-
-// Ap <- mask(Ap)*vol ; pap = dot(p,Ap) over the interior minus Dirichlet walls of x;
-// last block: alpha = rhok/pap
-__global__ void k_pcg_ap(Comp3 Ap, Comp3 p, Comp3 vol, WallMask wm0, WallMask wm1, WallMask wm2, int dw0, int dw1,
-                         int dw2, PcgScalars* S, double* partial, unsigned* ticket) {
-  if (S->done) return;
-  const WallMask wm[3] = {wm0, wm1, wm2};
-  const int dw[3] = {dw0, dw1, dw2};
-  double acc = 0.0;
-  size_t off = 0;
-  for (int c = 0; c < Ap.nc; c++) {
-    const DF& A = Ap.a[c];
-    size_t n = A.n();
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
-      int i, j, k;
-      ijk_of(idx, A, i, j, k);
-      bool zero;
-      double f = wall_factor(A, i, j, k, wm[c], zero);
-      double v = A.f[idx];
-      if (f != 1.0) v = v * f;
-      if (zero) v = 0.0;
-      v = v * vol.a[c].f[idx];
-      A.f[idx] = v;
-      if (dot_keep(A, i, j, k, dw[c])) acc += p.a[c].f[idx] * v;
-    }
-    off += n;
-  }
-  double bs = block_sum(acc);
-  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
-  if (last_block(ticket)) {
-    double tot = sum_partials(partial, gridDim.x);
-    if (threadIdx.x == 0) {
-      S->pap = tot;
-      S->alpha = S->rhok / tot;
-      *ticket = 0;
-    }
-  }
-}
-
-// x += alpha p ; r -= alpha Ap ; z = Minv r ; rr = dot(r,r), zr = dot(z,r);
-// last block: iteration count, exit test, beta
-__global__ void k_pcg_update(Comp3 x, Comp3 p, Comp3 r, Comp3 Ap, Comp3 z, Comp3 Minv, int dw0, int dw1, int dw2,
-                             PcgScalars* S, double* partial, unsigned* ticket) {
-  if (S->done) return;
-  const int dw[3] = {dw0, dw1, dw2};
-  double alpha = S->alpha;
-  double arr = 0.0, azr = 0.0;
-  for (int c = 0; c < x.nc; c++) {
-    const DF& X = x.a[c];
-    size_t n = X.n();
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
-      X.f[idx] = X.f[idx] + p.a[c].f[idx] * alpha;
-      double rv = r.a[c].f[idx] + Ap.a[c].f[idx] * (-alpha);
-      r.a[c].f[idx] = rv;
-      double zv = Minv.a[c].f[idx] * rv;
-      z.a[c].f[idx] = zv;
-      int i, j, k;
-      ijk_of(idx, X, i, j, k);
-      if (dot_keep(X, i, j, k, dw[c])) {
-        arr += rv * rv;
-        azr += zv * rv;
-      }
-    }
-  }
-  double b1 = block_sum(arr);
-  double b2 = block_sum(azr);
-  if (threadIdx.x == 0) {
-    partial[blockIdx.x] = b1;
-    partial[kRedBlocks + blockIdx.x] = b2;
-  }
-  if (last_block(ticket)) {
-    double rr = sum_partials(partial, gridDim.x);
-    double zr = sum_partials(partial + kRedBlocks, gridDim.x);
-    if (threadIdx.x == 0) {
-      *ticket = 0;
-      S->rr = rr;
-      S->zr = zr;
-      S->iter += 1;
-      bool stop = false;
-      if (S->iter % S->nskip == 0) {
-        double res = sqrt(fabs(rr));
-        S->res = res;
-        bool e1 = res / S->res0 < S->tol_rel;
-        bool e2 = res < S->tol_abs;
-        bool e3 = S->iter >= S->iter_max;
-        if (e1 || e2 || e3) {
-          stop = true;
-          S->exit_reason = e1 ? 1 : (e2 ? 2 : 3);
-        }
-        if (isnan(res)) {
-          S->nan = 1;
-          stop = true;
-        }
-      }
-      if (!stop) {
-        S->beta = zr / S->rhok;
-        S->rhok = zr;
-        if (S->iter >= S->iter_max) {
-          stop = true;
-          S->exit_reason = 3;
-        }
-      }
-      S->done = stop ? 1 : 0;
-    }
-  }
-}
-
-// p = p*beta + z  (product_add)
-__global__ void k_pcg_p(Comp3 p, Comp3 z, PcgScalars* S) {
-  if (S->done) return;
-  double beta = S->beta;
-  for (int c = 0; c < p.nc; c++) {
-    size_t n = p.a[c].n();
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x)
-      p.a[c].f[idx] = p.a[c].f[idx] * beta + z.a[c].f[idx];
-  }
-}
-
 // generic two-level reduction: mode 0 dot(a,b) masked interior, 1 sum(a^2) whole array,
 // 2 sum(a*b) over interior pad 1 (no wall mask)
 __global__ void k_reduce(Comp3 a, Comp3 b, int mode, int dw0, int dw1, int dw2, double* out, double* partial,
                          unsigned* ticket) {
-  const int dw[3] = {dw0, dw1, dw2};
   double acc = 0.0;
-  for (int c = 0; c < a.nc; c++) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (c >= a.nc) break;
     const DF& A = a.a[c];
-    size_t n = A.n();
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const DF& Bf = b.a[c];
+    int dw = c == 0 ? dw0 : (c == 1 ? dw1 : dw2);
+    unsigned n = (unsigned)A.n();
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
       if (mode == 1) {
         double v = A.f[idx];
         acc += v * v;
       } else {
-        int i, j, k;
-        ijk_of(idx, A, i, j, k);
-        if (dot_keep(A, i, j, k, mode == 0 ? dw[c] : 0)) acc += A.f[idx] * b.a[c].f[idx];
+        unsigned q = idx / (unsigned)A.s0;
+        int i = (int)(idx - q * (unsigned)A.s0) + 1;
+        unsigned kk = q / (unsigned)A.s1;
+        int j = (int)(q - kk * (unsigned)A.s1) + 1;
+        int k = (int)kk + 1;
+        if (dot_keep(A, i, j, k, mode == 0 ? dw : 0)) acc += A.f[idx] * Bf.f[idx];
       }
     }
   }
@@ -208,13 +66,23 @@ __global__ void k_pcg_start(PcgScalars* S) {
   S->iter = 0;
   S->body_runs = 0;
   S->nan = isnan(S->res0) ? 1 : 0;
+  if (S->nan) S->nan_any = 1;
   S->exit_reason = 0;
   bool e2 = S->res < S->tol_abs;  // only exit_loop(2) skips the loop (PCG_solver_algorithm.f90:68)
   S->done = (e2 || S->iter_max <= 0 || S->nan) ? 1 : 0;
   if (e2) {
     S->exit_reason = 2;
     S->iter = 1;  // update_iter in the else branch
+    S->iter_total += 1;
   }
+}
+
+// host-side parameters of the next solve (the accumulators are kept)
+__global__ void k_pcg_params(PcgScalars* S, int iter_max, int nskip, double tol_rel, double tol_abs) {
+  S->iter_max = iter_max;
+  S->nskip = nskip;
+  S->tol_rel = tol_rel;
+  S->tol_abs = tol_abs;
 }
 
 // r -= mean, mean = sum(r*vol, pad 1)/vol%vol (subtract_phys_mean_vol_SF)
@@ -227,66 +95,51 @@ __global__ void k_sub_mean(DF r, const double* sum, double volsum) {
 
 // volume_DL_GF (GF_distributions.f90:61-88)
 __global__ void k_volume(DF u, DGrid g) {
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= u.n()) return;
   int i, j, k;
-  ijk_of(idx, u, i, j, k);
-  if (i < 2 || i > u.s0 - 1 || j < 2 || j > u.s1 - 1 || k < 2 || k > u.s2 - 1) {
-    u.f[idx] = 0.0;
-    return;
-  }
-  int ex = n_along(u.dl, 1), ey = n_along(u.dl, 2), ez = n_along(u.dl, 3);
-  double hx = ex ? g.c[0].dhc[i - 1] : g.c[0].dhn[i];
-  double hy = ey ? g.c[1].dhc[j - 1] : g.c[1].dhn[j];
-  double hz = ez ? g.c[2].dhc[k - 1] : g.c[2].dhn[k];
-  u.f[idx] = hx * hy * hz;
+  if (!point_of(u, i, j, k)) return;
+  bool ghost = (i == 1 || i == u.s0 || j == 1 || j == u.s1 || k == 1 || k == u.s2);
+  u(i, j, k) = ghost ? 0.0 : vol_at(g, u.dl, i, j, k);
 }
 
 // Jacobi preconditioners (preconditioners.f90:55-129, GF_diagonals.f90:15-71):
-// mode 1 Lap: 1/(diag*vol); 2 mom: 1/((diag*c+1)*vol); 3 ind: 1/((cc_diag*c+1)*vol);
-// ghost planes 0 (Minv carries no BCs, so assign_ghost_XPeriodic zeroes all six).
+// mode 0 identity (1 everywhere); 1 Lap: 1/(diag*vol); 2 mom: 1/((diag*c+1)*vol);
+// 3 ind: 1/((cc_diag*c+1)*vol); ghost planes 0 (Minv carries no BCs, so
+// assign_ghost_XPeriodic zeroes all six).
 __global__ void k_prec(DF M, DGrid g, int mode, double coeff, int comp, DF sx, DF sy, DF sz) {
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= M.n()) return;
   int i, j, k;
-  ijk_of(idx, M, i, j, k);
-  bool ghost = (i == 1 || i == M.s0 || j == 1 || j == M.s1 || k == 1 || k == M.s2);
-  if (mode == 0) {  // prec_Identity_SF: assign(Minv,1)
-    M.f[idx] = 1.0;
+  if (!point_of(M, i, j, k)) return;
+  if (mode == 0) {
+    M(i, j, k) = 1.0;
     return;
   }
+  bool ghost = (i == 1 || i == M.s0 || j == 1 || j == M.s1 || k == 1 || k == M.s2);
   if (ghost) {
-    M.f[idx] = 0.0;
+    M(i, j, k) = 0.0;
+    return;
+  }
+  if (mode != 3) {
+    M(i, j, k) = minv_at(mode, g, M, M.dl, i, j, k, false, coeff);
     return;
   }
   const DCoord &c1 = g.c[0], &c2 = g.c[1], &c3 = g.c[2];
   double d;
-  if (mode == 1 || mode == 2) {
-    int px = n_along(M.dl, 1), py = n_along(M.dl, 2), pz = n_along(M.dl, 3);
-    d = c1.n2ccD[i] * c1.cc2nU[i - 1] + c1.n2ccU[i - px] * c1.cc2nD[i - px] + c2.n2ccD[j] * c2.cc2nU[j - 1] +
-        c2.n2ccU[j - py] * c2.cc2nD[j - py] + c3.n2ccD[k] * c3.cc2nU[k - 1] + c3.n2ccU[k - pz] * c3.cc2nD[k - pz];
-  } else {
-    if (comp == 0)
-      d = -c2.n2ccD[j] * sz(i, j, k) * c2.cc2nU[j - 1] - c2.n2ccU[j] * sz(i, j + 1, k) * c2.cc2nD[j] -
-          c3.n2ccD[k] * sy(i, j, k) * c3.cc2nU[k - 1] - c3.n2ccU[k] * sy(i, j, k + 1) * c3.cc2nD[k];
-    else if (comp == 1)
-      d = -c1.n2ccD[i] * sz(i, j, k) * c1.cc2nU[i - 1] - c1.n2ccU[i] * sz(i + 1, j, k) * c1.cc2nD[i] -
-          c3.n2ccD[k] * sx(i, j, k) * c3.cc2nU[k - 1] - c3.n2ccU[k] * sx(i, j, k + 1) * c3.cc2nD[k];
-    else
-      d = -c1.n2ccD[i] * sy(i, j, k) * c1.cc2nU[i - 1] - c1.n2ccU[i] * sy(i + 1, j, k) * c1.cc2nD[i] -
-          c2.n2ccD[j] * sx(i, j, k) * c2.cc2nU[j - 1] - c2.n2ccU[j] * sx(i, j + 1, k) * c2.cc2nD[j];
-  }
-  if (mode >= 2) {
-    d = d * coeff;
-    d = d + 1.0;
-  }
-  int ex = n_along(M.dl, 1), ey = n_along(M.dl, 2), ez = n_along(M.dl, 3);
-  double vol = (ex ? c1.dhc[i - 1] : c1.dhn[i]) * (ey ? c2.dhc[j - 1] : c2.dhn[j]) * (ez ? c3.dhc[k - 1] : c3.dhn[k]);
-  M.f[idx] = 1.0 / (d * vol);
+  if (comp == 0)
+    d = -c2.n2ccD[j] * sz(i, j, k) * c2.cc2nU[j - 1] - c2.n2ccU[j] * sz(i, j + 1, k) * c2.cc2nD[j] -
+        c3.n2ccD[k] * sy(i, j, k) * c3.cc2nU[k - 1] - c3.n2ccU[k] * sy(i, j, k + 1) * c3.cc2nD[k];
+  else if (comp == 1)
+    d = -c1.n2ccD[i] * sz(i, j, k) * c1.cc2nU[i - 1] - c1.n2ccU[i] * sz(i + 1, j, k) * c1.cc2nD[i] -
+        c3.n2ccD[k] * sx(i, j, k) * c3.cc2nU[k - 1] - c3.n2ccU[k] * sx(i, j, k + 1) * c3.cc2nD[k];
+  else
+    d = -c1.n2ccD[i] * sy(i, j, k) * c1.cc2nU[i - 1] - c1.n2ccU[i] * sy(i + 1, j, k) * c1.cc2nD[i] -
+        c2.n2ccD[j] * sx(i, j, k) * c2.cc2nU[j - 1] - c2.n2ccU[j] * sx(i, j + 1, k) * c2.cc2nD[j];
+  d = d * coeff;
+  d = d + 1.0;
+  M(i, j, k) = 1.0 / (d * vol_at(g, M.dl, i, j, k));
 }
 
 __global__ void k_set_cond(cudaGraphConditionalHandle h, PcgScalars* S) {
   S->body_runs += 1;
+  S->runs_total += 1;
   bool go = !S->done && S->body_runs < S->iter_max + 2;
   cudaGraphSetConditional(h, go ? 1u : 0u);
 }
@@ -310,6 +163,9 @@ struct moons_pcg {
   double volsum[3] = {0, 0, 0};
   PcgScalars* S = nullptr;   // device
   PcgScalars* hS = nullptr;  // pinned host
+  double* partial = nullptr; // fused-kernel block partials (2 x max blocks)
+  unsigned* ticket = nullptr;
+  size_t max_blocks = 0;
   std::vector<void*> allocs;
   // graph of the loop (rebuilt when x changes)
   cudaGraph_t graph = nullptr;
@@ -335,28 +191,58 @@ Comp3 c3(const DF* a, int nc) {
   for (int c = 0; c < nc; c++) r.a[c] = a[c];
   return r;
 }
+FComp fc(const DF* a, int nc) {
+  FComp r{};
+  r.nc = nc;
+  for (int c = 0; c < nc; c++) r.f[c] = a[c];
+  for (int c = nc; c < 3; c++) r.f[c] = a[0];
+  return r;
+}
 unsigned red_grid(const DF* a, int nc) {
   size_t n = 0;
   for (int c = 0; c < nc; c++) n += a[c].n();
   return (unsigned)std::min<size_t>(kRedBlocks, std::max<size_t>(1, (n + kBlock - 1) / kBlock));
 }
-WallMask wall_mask_of(const DBC& b, int dl, int s[4]) {
-  WallMask w{0, 0, 0};
-  for (int f = 1; f <= 6; f++) {
-    int d = (f + 1) / 2;
-    if (!n_along(dl, d)) continue;
-    bool def = b.defined != 0;
-    if (def ? b.type[f] == MOONS_BC_NEUMANN : true) w.neu |= 1 << (f - 1);
-    if (def ? b.type[f] == MOONS_BC_DIRICHLET : true) w.dir |= 1 << (f - 1);
+// (plane chunk, k, component) grid covering nc fields
+dim3 fgrid(const DF* a, int nc) {
+  unsigned px = 0, kz = 0;
+  for (int c = 0; c < nc; c++) {
+    px = std::max(px, (unsigned)(((size_t)a[c].s0 * a[c].s1 + kBlock - 1) / kBlock));
+    kz = std::max(kz, (unsigned)a[c].s2);
   }
-  if (b.defined)
-    for (int d = 1; d <= 3; d++)
-      if (n_along(dl, d) && b.type[2 * d - 1] == MOONS_BC_PERIODIC && b.type[2 * d] == MOONS_BC_PERIODIC && s[d] > 4)
-        w.per |= 1 << (d - 1);
-  return w;
+  return dim3(px, kz, nc);
 }
 
-// operator_explicit of matrix_free_operators.f90 on component fields
+// the fused kernels' view of one component's BCs
+FBC fbc_of(const DBC& xb /* x (=p) */, const DBC& xbcb /* x_BC */, int dl, const DF& shape) {
+  FBC f{};
+  f.defined = xb.defined;
+  for (int face = 1; face <= 6; face++) {
+    f.type[face] = xb.defined ? xb.type[face] : 0;
+    double dh = xb.dh[face], nhat = xb.nhat[face], cw = xb.c_w[face];
+    int d = (face + 1) / 2;
+    if (f.type[face] == MOONS_BC_ROBIN)
+      f.rc[face] = n_along(dl, d) ? -2.0 * dh * nhat / cw : (2.0 * cw * nhat / dh - 1.0) / (2.0 * cw * nhat / dh + 1.0);
+  }
+  // masks of Ap come from x_BC's BCs (PCG_solver_algorithm.f90:72-75)
+  for (int face = 1; face <= 6; face++) {
+    int d = (face + 1) / 2;
+    if (!n_along(dl, d)) continue;
+    bool def = xbcb.defined != 0;
+    if (def ? xbcb.type[face] == MOONS_BC_NEUMANN : true) f.wall_neu |= 1 << (face - 1);
+    if (def ? xbcb.type[face] == MOONS_BC_DIRICHLET : true) f.wall_dir |= 1 << (face - 1);
+  }
+  if (xbcb.defined)
+    for (int d = 1; d <= 3; d++)
+      if (n_along(dl, d) && xbcb.type[2 * d - 1] == MOONS_BC_PERIODIC && xbcb.type[2 * d] == MOONS_BC_PERIODIC &&
+          shape.s(d) > 4)
+        f.wall_per |= 1 << (d - 1);
+  f.dot_wall = dirichlet_wall_bits(xb.defined ? &xb : nullptr, dl);
+  return f;
+}
+
+// operator_explicit of matrix_free_operators.f90 on component fields (generic
+// kernels; used by modify_RHS, once per solve)
 int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
   moons_mesh* m = s->m;
   int r = MOONS_OK;
@@ -388,7 +274,6 @@ int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
     } break;
     case MOONS_OP_IND_DIFFUSION: {
       DF* t = s->tempk;
-      // curl(tempk, x): faces -> edges
       if (!r) r = launch_del(m, t[0], x[2], 1, 2, 0, 1);
       if (!r) r = launch_del(m, t[0], x[1], 1, 3, 0, 3);
       if (!r) r = launch_del(m, t[1], x[0], 1, 3, 0, 1);
@@ -396,7 +281,6 @@ int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
       if (!r) r = launch_del(m, t[2], x[1], 1, 1, 0, 1);
       if (!r) r = launch_del(m, t[2], x[0], 1, 2, 0, 3);
       for (int d = 0; d < 3 && !r; d++) r = launch_pw(m, PW_MUL, t[d], &s->k[d], 0.0);
-      // curl(Ax, tempk): edges -> faces
       if (!r) r = launch_del(m, out[0], t[2], 1, 2, 0, 1);
       if (!r) r = launch_del(m, out[0], t[1], 1, 3, 0, 3);
       if (!r) r = launch_del(m, out[1], t[0], 1, 3, 0, 1);
@@ -416,44 +300,66 @@ int compute_prec(moons_pcg* s) {
   moons_mesh* m = s->m;
   int mode = s->prec;
   DF dummy{};
+  if (mode == MOONS_PREC_IND && s->op != MOONS_OP_IND_DIFFUSION) {
+    set_error("moons_pcg: prec_ind needs the induction operator's sigma^-1 edge fields");
+    return MOONS_ERR_ARG;
+  }
   for (int c = 0; c < s->nc; c++) {
     DF sx = s->op == MOONS_OP_IND_DIFFUSION ? s->k[0] : dummy;
     DF sy = s->op == MOONS_OP_IND_DIFFUSION ? s->k[1] : dummy;
     DF sz = s->op == MOONS_OP_IND_DIFFUSION ? s->k[2] : dummy;
-    if (mode == MOONS_PREC_IND && s->op != MOONS_OP_IND_DIFFUSION) {
-      set_error("moons_pcg: prec_ind needs the induction operator's sigma^-1 edge fields");
-      return MOONS_ERR_ARG;
-    }
-    MG_LAUNCH(k_prec, nblocks(s->Minv[c].n()), kBlock, m->stream, s->Minv[c], m->dg, mode, s->coeff, c, sx, sy, sz);
+    MG_LAUNCH(k_prec, fgrid(&s->Minv[c], 1), kBlock, m->stream, s->Minv[c], m->dg, mode, s->coeff, c, sx, sy, sz);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
 
+int minv_mode(const moons_pcg* s) {
+  if (s->prec == MOONS_PREC_LAP) return 1;
+  if (s->prec == MOONS_PREC_MOM) return 2;
+  return 0;
+}
+
 // one PCG iteration (PCG_solver_algorithm.f90:69-96), enqueued on the mesh stream
 int enqueue_iteration(moons_pcg* s, DF* x) {
   moons_mesh* m = s->m;
-  int r = MOONS_OK;
-  for (int c = 0; c < s->nc && !r; c++) r = launch_bcs(m, s->p[c], s->x_bc[c], true);
-  if (!r) r = apply_op_explicit(s, s->Ax, s->p);
-  if (r) return r;
-  int sarr[3][4];
-  WallMask wm[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  FBC b[3];
   int dw[3] = {0, 0, 0};
-  for (int c = 0; c < s->nc; c++) {
-    sarr[c][1] = s->Ax[c].s0;
-    sarr[c][2] = s->Ax[c].s1;
-    sarr[c][3] = s->Ax[c].s2;
-    wm[c] = wall_mask_of(s->xbc_bc[c], s->xbc[c].dl, sarr[c]);
-    dw[c] = dirichlet_wall_bits(s->x_bc[c].defined ? &s->x_bc[c] : nullptr, s->x_dl[c]);
+  for (int c = 0; c < 3; c++) {
+    int cc = c < s->nc ? c : 0;
+    b[c] = fbc_of(s->x_bc[cc], s->xbc_bc[cc], s->x_dl[cc], s->Ax[cc]);
+    dw[c] = b[c].dot_wall;
   }
-  unsigned G = red_grid(s->Ax, s->nc);
-  MG_LAUNCH(k_pcg_ap, G, kBlock, m->stream, c3(s->Ax, s->nc), c3(s->p, s->nc), c3(s->vol, s->nc), wm[0], wm[1], wm[2],
-                                        dw[0], dw[1], dw[2], s->S, m->d_partial, m->d_ticket);
-  MG_LAUNCH(k_pcg_update, G, kBlock, m->stream, c3(x, s->nc), c3(s->p, s->nc), c3(s->r, s->nc), c3(s->Ax, s->nc),
-                                            c3(s->z, s->nc), c3(s->Minv, s->nc), dw[0], dw[1], dw[2], s->S,
-                                            m->d_partial + 2 * kRedBlocks, m->d_ticket + 1);
-  MG_LAUNCH(k_pcg_p, G, kBlock, m->stream, c3(s->p, s->nc), c3(s->z, s->nc), s->S);
+  dim3 G = fgrid(s->Ax, s->nc);
+  unsigned* tA = s->ticket;
+  unsigned* tB = s->ticket + 1;
+  DF z0{};
+  switch (s->op) {
+    case MOONS_OP_LAP_UNIFORM:
+      MG_LAUNCH(k_f_lap_ap<0>, G, kBlock, m->stream, fc(s->Ax, s->nc), fc(s->p, s->nc), m->dg, b[0], b[1], b[2], z0, z0,
+                z0, 0.0, s->S, s->partial, tA);
+      break;
+    case MOONS_OP_LAP_PROPS:
+      MG_LAUNCH(k_f_lap_ap<1>, G, kBlock, m->stream, fc(s->Ax, s->nc), fc(s->p, s->nc), m->dg, b[0], b[1], b[2],
+                s->k[0], s->k[1], s->k[2], 0.0, s->S, s->partial, tA);
+      break;
+    case MOONS_OP_MOM_DIFFUSION:
+      MG_LAUNCH(k_f_lap_ap<2>, G, kBlock, m->stream, fc(s->Ax, s->nc), fc(s->p, s->nc), m->dg, b[0], b[1], b[2], z0, z0,
+                z0, s->coeff, s->S, s->partial, tA);
+      break;
+    case MOONS_OP_IND_DIFFUSION: {
+      dim3 GE = fgrid(s->tempk, 3);
+      MG_LAUNCH(k_f_curl_sig, GE, kBlock, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(s->p, 3), m->dg, b[0],
+                b[1], b[2], s->k[0], s->k[1], s->k[2], s->S);
+      MG_LAUNCH(k_f_curl_ap, G, kBlock, m->stream, fc(s->Ax, 3), fc(s->p, 3), s->tempk[0], s->tempk[1], s->tempk[2],
+                m->dg, b[0], b[1], b[2], s->coeff, s->S, s->partial, tA);
+    } break;
+  }
+  int mm = minv_mode(s);
+  MG_LAUNCH(k_f_update, G, kBlock, m->stream, fc(x, s->nc), fc(s->p, s->nc), fc(s->r, s->nc), fc(s->Ax, s->nc),
+            fc(s->Minv, s->nc), m->dg, mm, s->coeff, dw[0], dw[1], dw[2], s->S, s->partial, tB);
+  MG_LAUNCH(k_f_pupd, G, kBlock, m->stream, fc(s->p, s->nc), fc(s->r, s->nc), fc(s->Minv, s->nc), m->dg, mm, s->coeff,
+            s->S);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
@@ -558,22 +464,42 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     }
   }
   if (!r) {
+    dim3 G = fgrid(s->Ax, nc);
+    size_t nb = (size_t)G.x * G.y * G.z;
+    if (needk) {
+      dim3 GE = fgrid(s->tempk, 3);
+      nb = std::max(nb, (size_t)GE.x * GE.y * GE.z);
+    }
+    s->max_blocks = nb;
     void* p;
     if (cudaMalloc(&p, sizeof(PcgScalars)) != cudaSuccess) r = MOONS_ERR_NOMEM;
     else {
       s->S = (PcgScalars*)p;
       s->allocs.push_back(p);
+      cudaMemsetAsync(p, 0, sizeof(PcgScalars), m->stream);
+    }
+    if (!r && cudaMalloc(&p, sizeof(double) * 2 * nb) != cudaSuccess) r = MOONS_ERR_NOMEM;
+    else if (!r) {
+      s->partial = (double*)p;
+      s->allocs.push_back(p);
+    }
+    if (!r && cudaMalloc(&p, sizeof(unsigned) * 4) != cudaSuccess) r = MOONS_ERR_NOMEM;
+    else if (!r) {
+      s->ticket = (unsigned*)p;
+      s->allocs.push_back(p);
+      cudaMemsetAsync(p, 0, sizeof(unsigned) * 4, m->stream);
     }
     if (!r && cudaMallocHost(&p, sizeof(PcgScalars)) != cudaSuccess) r = MOONS_ERR_NOMEM;
     else if (!r) s->hS = (PcgScalars*)p;
+    if (r) set_error("moons_pcg_create: device allocation failed");
   }
   if (!r) {
-    for (int c = 0; c < nc; c++) MG_LAUNCH(k_volume, nblocks(s->vol[c].n()), kBlock, m->stream, s->vol[c], m->dg);
+    for (int c = 0; c < nc; c++) MG_LAUNCH(k_volume, fgrid(&s->vol[c], 1), kBlock, m->stream, s->vol[c], m->dg);
     // coeff_implicit is not known here; Lap needs none and mom/ind set it through update_mfp
     r = compute_prec(s);
   }
   if (!r) {
-    // plain sums of vol (ghosts are 0, so interior sum == whole sum)
+    // SF%vol: plain sum of the volume field (ghosts are 0)
     for (int c = 0; c < nc; c++) {
       std::vector<double> hv(s->vol[c].n());
       if (cudaMemcpyAsync(hv.data(), s->vol[c].f, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, m->stream) !=
@@ -627,18 +553,38 @@ int moons_pcg_update_mfp(moons_pcg* s, double c, int upd) {
   return MOONS_OK;
 }
 
-int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp* isp,
-                    moons_solve_info* info) {
-  if (!s || !x || !b || !isp) {
-    set_error("moons_pcg_solve: null pointer");
-    return MOONS_ERR_ARG;
-  }
-  if (isp->n_skip_check_res < 1) {
-    set_error("moons_pcg_solve: n_skip_check_res must be >= 1");
-    return MOONS_ERR_ARG;
-  }
+}  // extern "C"
+
+namespace mg {
+__global__ void k_pcg_clear_acc(PcgScalars* S) {
+  S->iter_total = 0;
+  S->runs_total = 0;
+  S->nan_any = 0;
+}
+}  // namespace mg
+
+// zero the accumulators (enqueued)
+int mg_pcg_clear_totals(moons_pcg* s) {
+  MG_LAUNCH(k_pcg_clear_acc, 1, 1, s->m->stream, s->S);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+// read the accumulators after the stream drained (syncs)
+int mg_pcg_totals(moons_pcg* s, int* iters, int* nan_any, double* last_rel) {
   moons_mesh* m = s->m;
-  cudaSetDevice(m->device);
+  MG_CUDA(cudaMemcpyAsync(s->hS, s->S, sizeof(PcgScalars), cudaMemcpyDeviceToHost, m->stream));
+  MG_CUDA(cudaStreamSynchronize(m->stream));
+  const PcgScalars& H = *s->hS;
+  g_launch_count += s->body_launches * (long long)H.runs_total;
+  *iters = H.iter_total;
+  *nan_any = H.nan_any;
+  if (last_rel) *last_rel = (H.res0 == 0.0) ? H.res : H.res / H.res0;
+  return MOONS_OK;
+}
+
+// enqueue a whole solve (modify_RHS + loop + final BCs of x); no host sync
+int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp* isp) {
+  moons_mesh* m = s->m;
   DF X[3], B[3];
   for (int c = 0; c < s->nc; c++) {
     if (!x[c] || !b[c] || x[c]->f.dl != s->x_dl[c] || b[c]->f.n() != x[c]->f.n()) {
@@ -648,10 +594,6 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
     X[c] = x[c]->f;
     B[c] = b[c]->f;
   }
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, m->stream);
   int r = MOONS_OK;
   int nc = s->nc;
   // ---- modify_RHS (PCG_aux.f90:30-79)
@@ -659,7 +601,7 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   if (!r && s->all_neumann) {
     // tempx = r*vol; mean = sum(tempx,1)/vol%vol; r -= mean; assign_ghost_XPeriodic(r,0)
     MG_LAUNCH(k_reduce, red_grid(&s->r[0], 1), kBlock, m->stream, c3(&s->r[0], 1), c3(&s->vol[0], 1), 2, 0, 0, 0,
-                                                               m->d_scal, m->d_partial, m->d_ticket);
+              m->d_scal, m->d_partial, m->d_ticket);
     MG_LAUNCH(k_sub_mean, nblocks(s->r[0].n()), kBlock, m->stream, s->r[0], m->d_scal, s->volsum[0]);
     r = mask_ghost_XPeriodic(m, s->r[0], nullptr);
   }
@@ -688,16 +630,10 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   }
   if (r) return r;
   // ---- scalars
-  PcgScalars h{};
-  h.iter_max = isp->iter_max;
-  h.nskip = isp->n_skip_check_res;
-  h.tol_rel = isp->tol_rel;
-  h.tol_abs = isp->tol_abs;
-  *s->hS = h;
-  MG_CUDA(cudaMemcpyAsync(s->S, s->hS, sizeof(PcgScalars), cudaMemcpyHostToDevice, m->stream));
+  MG_LAUNCH(k_pcg_params, 1, 1, m->stream, s->S, isp->iter_max, isp->n_skip_check_res, isp->tol_rel, isp->tol_abs);
   // res0 = sqrt(sum r^2) whole array
   MG_LAUNCH(k_reduce, red_grid(s->r, nc), kBlock, m->stream, c3(s->r, nc), c3(s->r, nc), 1, 0, 0, 0, &s->S->res0,
-                                                         m->d_partial, m->d_ticket);
+            m->d_partial, m->d_ticket);
   // z = Minv r ; p = z ; rhok = dot(r,z)
   for (int c = 0; c < nc; c++) {
     launch_pw(m, PW_COPY, s->z[c], &s->Minv[c], 0.0);
@@ -707,10 +643,10 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   int dw[3] = {0, 0, 0};
   for (int c = 0; c < nc; c++) dw[c] = dirichlet_wall_bits(s->x_bc[c].defined ? &s->x_bc[c] : nullptr, s->x_dl[c]);
   MG_LAUNCH(k_reduce, red_grid(s->r, nc), kBlock, m->stream, c3(s->r, nc), c3(s->z, nc), 0, dw[0], dw[1], dw[2],
-                                                         &s->S->rhok, m->d_partial, m->d_ticket);
+            &s->S->rhok, m->d_partial, m->d_ticket);
   MG_LAUNCH(k_pcg_start, 1, 1, m->stream, s->S);
   MG_CUDA(cudaGetLastError());
-  // ---- the loop: one graph launch (WHILE node) unless the solve is trivial
+  // ---- the loop: one graph launch (WHILE node)
   bool need_graph = !s->exec;
   for (int c = 0; c < nc; c++)
     if (s->gx[c] != X[c].f) need_graph = true;
@@ -722,14 +658,14 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   // x: apply_BCs (the reference applies them after every update; they only
   // rewrite ghost/boundary entries, which no update reads)
   for (int c = 0; c < nc && !r; c++) r = launch_bcs(m, X[c], s->x_bc[c], false);
-  if (r) return r;
+  return r;
+}
+
+// read back what the last enqueued solve left in the device scalars (syncs)
+int mg_pcg_collect(moons_pcg* s, moons_solve_info* info, float ms) {
+  moons_mesh* m = s->m;
   MG_CUDA(cudaMemcpyAsync(s->hS, s->S, sizeof(PcgScalars), cudaMemcpyDeviceToHost, m->stream));
-  cudaEventRecord(e1, m->stream);
   MG_CUDA(cudaStreamSynchronize(m->stream));
-  float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   const PcgScalars& H = *s->hS;
   g_launch_count += s->body_launches * (long long)H.body_runs;
   if (info) {
@@ -745,6 +681,36 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
     return MOONS_ERR_NAN;
   }
   return MOONS_OK;
+}
+
+extern "C" {
+
+int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp* isp,
+                    moons_solve_info* info) {
+  if (!s || !x || !b || !isp) {
+    set_error("moons_pcg_solve: null pointer");
+    return MOONS_ERR_ARG;
+  }
+  if (isp->n_skip_check_res < 1) {
+    set_error("moons_pcg_solve: n_skip_check_res must be >= 1");
+    return MOONS_ERR_ARG;
+  }
+  moons_mesh* m = s->m;
+  cudaSetDevice(m->device);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, m->stream);
+  int r = mg_pcg_enqueue(s, x, b, isp);
+  cudaEventRecord(e1, m->stream);
+  cudaError_t e = cudaStreamSynchronize(m->stream);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  MG_CUDA(e);
+  return mg_pcg_collect(s, info, ms);
 }
 
 }  // extern "C"

@@ -36,10 +36,15 @@ def test_mhd_steps_match_oracle(name, builder, kw):
     ig = g.step(nsteps)
     io = o.step(nsteps)
     fields = [(G.MHD_U, c) for c in range(3)] + [(G.MHD_P, 0), (G.MHD_JXB, 0), (G.MHD_JXB, 1), (G.MHD_JXB, 2)]
-    if kw.get("induction", G.IND_B) != G.IND_OFF:
-        fields += [(G.MHD_PHI, 0)] + [(G.MHD_J, c) for c in range(3)]
-        if kw.get("induction", G.IND_B) == G.IND_B:
-            fields += [(G.MHD_B, c) for c in range(3)]
+    ind = kw.get("induction", G.IND_B)
+    if ind != G.IND_OFF:
+        fields += [(G.MHD_J, c) for c in range(3)]
+    if ind == G.IND_POTENTIAL:
+        fields += [(G.MHD_PHI, 0)]
+    if ind == G.IND_B:
+        # the cleaning potential of the B form is a Lagrange multiplier at
+        # round-off level (div B* ~ 1e-17), so it is not compared
+        fields += [(G.MHD_B, c) for c in range(3)]
     for which, c in fields:
         a, b = g.download(which, c), o.download(which, c)
         e = rel_l2(a, b)
