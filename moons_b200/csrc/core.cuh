@@ -13,6 +13,8 @@
 
 #include "../../include/moons_gpu.h"
 
+#define MG_HD __host__ __device__ __forceinline__
+
 namespace mg {
 
 // ---- 1-D coordinates and stencil coefficients of one axis --------------
@@ -37,10 +39,10 @@ struct DF {
   int dl;          // data location (MOONS_CC ...)
   __host__ __device__ int s(int d) const { return d == 1 ? s0 : (d == 2 ? s1 : s2); }
   __host__ __device__ size_t n() const { return (size_t)s0 * s1 * s2; }
-  __device__ __forceinline__ size_t at(int i, int j, int k) const {
+  MG_HD size_t at(int i, int j, int k) const {
     return (size_t)(i - 1) + (size_t)s0 * ((size_t)(j - 1) + (size_t)s1 * (size_t)(k - 1));
   }
-  __device__ __forceinline__ double& operator()(int i, int j, int k) const { return f[at(i, j, k)]; }
+  MG_HD double& operator()(int i, int j, int k) const { return f[at(i, j, k)]; }
 };
 
 // node-location eye of a data location: bit d-1 set when N along d
@@ -105,6 +107,6 @@ __device__ __forceinline__ void ijk_of(size_t idx, const DF& a, int& i, int& j, 
   j = (int)(q - kk * s1) + 1;
   k = (int)kk + 1;
 }
-__device__ __forceinline__ int pick(int d, int i, int j, int k) { return d == 1 ? i : (d == 2 ? j : k); }
+MG_HD int pick(int d, int i, int j, int k) { return d == 1 ? i : (d == 2 ? j : k); }
 
 }  // namespace mg

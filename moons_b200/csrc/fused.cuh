@@ -50,11 +50,40 @@ struct FComp {
   int nc;
 };
 
-__device__ __forceinline__ int tget(int d, int i, int j, int k) { return d == 1 ? i : (d == 2 ? j : k); }
+// host: the fused kernels' view of one component's BCs.  xb: BCs of x (copied
+// to p: implicit BCs, dot-product walls); xbcb: BCs of x_BC (masks of Ap,
+// PCG_solver_algorithm.f90:72-75); ext: extents of the field (1-based).
+inline FBC make_fbc(const DBC& xb, const DBC& xbcb, int dl, const int ext[4]) {
+  FBC f{};
+  f.defined = xb.defined;
+  for (int face = 1; face <= 6; face++) {
+    f.type[face] = xb.defined ? xb.type[face] : 0;
+    double dh = xb.dh[face], nhat = xb.nhat[face], cw = xb.c_w[face];
+    int d = (face + 1) / 2;
+    if (f.type[face] == MOONS_BC_ROBIN)
+      f.rc[face] = n_along(dl, d) ? -2.0 * dh * nhat / cw : (2.0 * cw * nhat / dh - 1.0) / (2.0 * cw * nhat / dh + 1.0);
+  }
+  for (int face = 1; face <= 6; face++) {
+    int d = (face + 1) / 2;
+    if (!n_along(dl, d)) continue;
+    bool def = xbcb.defined != 0;
+    if (def ? xbcb.type[face] == MOONS_BC_NEUMANN : true) f.wall_neu |= 1 << (face - 1);
+    if (def ? xbcb.type[face] == MOONS_BC_DIRICHLET : true) f.wall_dir |= 1 << (face - 1);
+    if (xb.defined ? xb.type[face] == MOONS_BC_DIRICHLET : true) f.dot_wall |= 1 << (face - 1);
+  }
+  if (xbcb.defined)
+    for (int d = 1; d <= 3; d++)
+      if (n_along(dl, d) && xbcb.type[2 * d - 1] == MOONS_BC_PERIODIC && xbcb.type[2 * d] == MOONS_BC_PERIODIC &&
+          ext[d] > 4)
+        f.wall_per |= 1 << (d - 1);
+  return f;
+}
+
+MG_HD int tget(int d, int i, int j, int k) { return d == 1 ? i : (d == 2 ? j : k); }
 
 // value of p~ (p after apply_BCs_implicit) at (i,j,k) for points an interior
 // output reads: at most one index is a ghost index.
-__device__ __forceinline__ double pt(const DF& p, const FBC& b, int i, int j, int k) {
+MG_HD double pt(const DF& p, const FBC& b, int i, int j, int k) {
   int I[4] = {0, i, j, k};
   double fac = 1.0;
   bool robin_n = false;
@@ -123,19 +152,19 @@ __device__ __forceinline__ double pt(const DF& p, const FBC& b, int i, int j, in
 }
 
 // laplacian_diagonal (GF_diagonals.f90:15-35) and the cell volume of a point
-__device__ __forceinline__ double lap_diag_at(const DGrid& g, int dl, int i, int j, int k) {
+MG_HD double lap_diag_at(const DGrid& g, int dl, int i, int j, int k) {
   const DCoord &c1 = g.c[0], &c2 = g.c[1], &c3 = g.c[2];
   int px = n_along(dl, 1), py = n_along(dl, 2), pz = n_along(dl, 3);
   return c1.n2ccD[i] * c1.cc2nU[i - 1] + c1.n2ccU[i - px] * c1.cc2nD[i - px] + c2.n2ccD[j] * c2.cc2nU[j - 1] +
          c2.n2ccU[j - py] * c2.cc2nD[j - py] + c3.n2ccD[k] * c3.cc2nU[k - 1] + c3.n2ccU[k - pz] * c3.cc2nD[k - pz];
 }
-__device__ __forceinline__ double vol_at(const DGrid& g, int dl, int i, int j, int k) {
+MG_HD double vol_at(const DGrid& g, int dl, int i, int j, int k) {
   int ex = n_along(dl, 1), ey = n_along(dl, 2), ez = n_along(dl, 3);
   return (ex ? g.c[0].dhc[i - 1] : g.c[0].dhn[i]) * (ey ? g.c[1].dhc[j - 1] : g.c[1].dhn[j]) *
          (ez ? g.c[2].dhc[k - 1] : g.c[2].dhn[k]);
 }
 // Minv at a point: mode 1 prec_Lap, 2 prec_mom (coeff), 0 stored
-__device__ __forceinline__ double minv_at(int mode, const DGrid& g, const DF& M, int dl, int i, int j, int k,
+MG_HD double minv_at(int mode, const DGrid& g, const DF& M, int dl, int i, int j, int k,
                                           bool ghost, double coeff) {
   if (mode == 0) return M(i, j, k);
   if (ghost) return 0.0;
@@ -147,9 +176,9 @@ __device__ __forceinline__ double minv_at(int mode, const DGrid& g, const DF& M,
   return 1.0 / (d * vol_at(g, dl, i, j, k));
 }
 
-__device__ __forceinline__ bool in_dot(const DF& a, int i, int j, int k, int wall) { return dot_keep(a, i, j, k, wall); }
+MG_HD bool in_dot(const DF& a, int i, int j, int k, int wall) { return dot_keep(a, i, j, k, wall); }
 
-__device__ __forceinline__ double wall_fac(const DF& a, const FBC& b, int i, int j, int k, bool& zero) {
+MG_HD double wall_fac(const DF& a, const FBC& b, int i, int j, int k, bool& zero) {
   double f = 1.0;
   zero = false;
   int t[4] = {0, i, j, k};
@@ -197,7 +226,7 @@ __device__ __forceinline__ bool last_block_any(unsigned* ticket) {
 // needed because ghost outputs are multiplied by vol = 0).
 // k_faces: optional face coefficients (Lap_nonuniform_props: grad, *k, div).
 template <bool KF>
-__device__ __forceinline__ double lap_pt(const DF& p, const FBC& b, const DGrid& g, const DF& kx, const DF& ky,
+MG_HD double lap_pt(const DF& p, const FBC& b, const DGrid& g, const DF& kx, const DF& ky,
                                          const DF& kz, int i, int j, int k) {
   double v = 0.0;
 #pragma unroll
@@ -244,13 +273,13 @@ __device__ __forceinline__ void finish_alpha(double acc, PcgScalars* S, double* 
 }
 
 // K1 body of one component: LAP_UNIFORM (MODE 0), LAP_PROPS (1), MOM_DIFFUSION (2)
+// value of Ap at one point and its share of p.Ap (host-callable, for checks)
 template <int MODE>
-__device__ __forceinline__ double lap_ap_body(const DF& A, const DF& p, const FBC& b, const DGrid& g, const DF& kx,
-                                              const DF& ky, const DF& kz, double coeff) {
-  int i, j, k;
-  if (!point_of(A, i, j, k)) return 0.0;
+MG_HD void lap_ap_point(const DF& A, const DF& p, const FBC& b, const DGrid& g, const DF& kx, const DF& ky,
+                        const DF& kz, double coeff, int i, int j, int k, double& v, double& acc) {
   bool ghost = (i == 1 || i == A.s0 || j == 1 || j == A.s1 || k == 1 || k == A.s2);
-  double acc = 0.0, v = 0.0;
+  acc = 0.0;
+  v = 0.0;
   if (!ghost) {
     double lap = lap_pt<MODE == 1>(p, b, g, kx, ky, kz, i, j, k);
     if (MODE == 2) {
@@ -264,6 +293,14 @@ __device__ __forceinline__ double lap_ap_body(const DF& A, const DF& p, const FB
     v = lap * vol_at(g, A.dl, i, j, k);
     if (in_dot(A, i, j, k, b.dot_wall)) acc = p(i, j, k) * v;
   }
+}
+template <int MODE>
+__device__ __forceinline__ double lap_ap_body(const DF& A, const DF& p, const FBC& b, const DGrid& g, const DF& kx,
+                                              const DF& ky, const DF& kz, double coeff) {
+  int i, j, k;
+  if (!point_of(A, i, j, k)) return 0.0;
+  double v, acc;
+  lap_ap_point<MODE>(A, p, b, g, kx, ky, kz, coeff, i, j, k, v, acc);
   A(i, j, k) = v;
   return acc;
 }
@@ -282,7 +319,7 @@ __global__ void k_f_lap_ap(FComp Ap, FComp P, DGrid g, FBC b0, FBC b1, FBC b2, D
 // ---- curl-curl (ind_diffusion) -----------------------------------------------
 // K1a: E_l = sig_l * curl_l(p~) on edges l (curl_SF with del assign/subtract,
 // ops_discrete.f90:184-202; ends of CC->N passes are 0)
-__device__ __forceinline__ double dstag_cc2n(const DF& u, const FBC& b, const DCoord& c, int d, int i, int j, int k,
+MG_HD double dstag_cc2n(const DF& u, const FBC& b, const DCoord& c, int d, int i, int j, int k,
                                              int sout) {
   int t = tget(d, i, j, k);
   if (t == 1 || t == sout) return 0.0;
@@ -291,16 +328,21 @@ __device__ __forceinline__ double dstag_cc2n(const DF& u, const FBC& b, const DC
 }
 // l=0: d/dy(pz) - d/dz(py) ; l=1: d/dz(px) - d/dx(pz) ; l=2: d/dx(py) - d/dy(px)
 template <int L>
-__device__ __forceinline__ void curl_sig_body(const DF& E, const DF& pa, const FBC& ba, const DF& pb, const FBC& bb,
-                                              const DF& sg, const DGrid& g) {
+MG_HD double curl_sig_point(const DF& E, const DF& pa, const FBC& ba, const DF& pb, const FBC& bb, const DF& sg,
+                            const DGrid& g, int i, int j, int k) {
   constexpr int da = L == 0 ? 2 : (L == 1 ? 3 : 1);  // derivative dir of the first term
   constexpr int db = L == 0 ? 3 : (L == 1 ? 1 : 2);  // derivative dir of the subtracted term
-  int i, j, k;
-  if (!point_of(E, i, j, k)) return;
   double v = dstag_cc2n(pa, ba, g.c[da - 1], da, i, j, k, E.s(da));
   int tb = tget(db, i, j, k);
   v = (tb == 1 || tb == E.s(db)) ? 0.0 : v - dstag_cc2n(pb, bb, g.c[db - 1], db, i, j, k, E.s(db));
-  E(i, j, k) = v * sg(i, j, k);
+  return v * sg(i, j, k);
+}
+template <int L>
+__device__ __forceinline__ void curl_sig_body(const DF& E, const DF& pa, const FBC& ba, const DF& pb, const FBC& bb,
+                                              const DF& sg, const DGrid& g) {
+  int i, j, k;
+  if (!point_of(E, i, j, k)) return;
+  E(i, j, k) = curl_sig_point<L>(E, pa, ba, pb, bb, sg, g, i, j, k);
 }
 __global__ void k_f_curl_sig(DF E0, DF E1, DF E2, FComp P, DGrid g, FBC b0, FBC b1, FBC b2, DF s0, DF s1, DF s2,
                              PcgScalars* S) {
@@ -311,15 +353,14 @@ __global__ void k_f_curl_sig(DF E0, DF E1, DF E2, FComp P, DGrid g, FBC b0, FBC 
 }
 // K1b: Ap_c = vol*mask(coeff*curl_c(E) + p~) and p.Ap (edges -> faces: N->CC passes)
 template <int C>
-__device__ __forceinline__ double curl_ap_body(const DF& A, const DF& p, const FBC& b, const DF& Ea, const DF& Eb,
-                                               const DGrid& g, double coeff) {
+MG_HD void curl_ap_point(const DF& A, const DF& p, const FBC& b, const DF& Ea, const DF& Eb, const DGrid& g,
+                         double coeff, int i, int j, int k, double& v, double& acc) {
   // C=0: d/dy(Ez) - d/dz(Ey) ; C=1: d/dz(Ex) - d/dx(Ez) ; C=2: d/dx(Ey) - d/dy(Ex)
   constexpr int da = C == 0 ? 2 : (C == 1 ? 3 : 1);
   constexpr int db = C == 0 ? 3 : (C == 1 ? 1 : 2);
-  int i, j, k;
-  if (!point_of(A, i, j, k)) return 0.0;
   bool ghost = (i == 1 || i == A.s0 || j == 1 || j == A.s1 || k == 1 || k == A.s2);
-  double acc = 0.0, v = 0.0;
+  acc = 0.0;
+  v = 0.0;
   if (!ghost) {
     const DCoord& ca = g.c[da - 1];
     const DCoord& cb = g.c[db - 1];
@@ -335,6 +376,14 @@ __device__ __forceinline__ double curl_ap_body(const DF& A, const DF& p, const F
     v = w * vol_at(g, A.dl, i, j, k);
     if (in_dot(A, i, j, k, b.dot_wall)) acc = p(i, j, k) * v;
   }
+}
+template <int C>
+__device__ __forceinline__ double curl_ap_body(const DF& A, const DF& p, const FBC& b, const DF& Ea, const DF& Eb,
+                                               const DGrid& g, double coeff) {
+  int i, j, k;
+  if (!point_of(A, i, j, k)) return 0.0;
+  double v, acc;
+  curl_ap_point<C>(A, p, b, Ea, Eb, g, coeff, i, j, k, v, acc);
   A(i, j, k) = v;
   return acc;
 }

@@ -372,7 +372,7 @@ __device__ __forceinline__ double sum_partials(const double* partial, int n) {
 
 // interior (pad=1) mask test with Dirichlet-wall planes removed
 // (dot_product_SF: multiply, assign_wall_Dirichlet, sum(.,1))
-__device__ __forceinline__ bool dot_keep(const DF& a, int i, int j, int k, int wallmask) {
+MG_HD bool dot_keep(const DF& a, int i, int j, int k, int wallmask) {
   if (i < 2 || i > a.s0 - 1 || j < 2 || j > a.s1 - 1 || k < 2 || k > a.s2 - 1) return false;
   if (wallmask) {
     if ((wallmask & 1) && i == 2) return false;

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "coeffs.hpp"
 #include "kernels.cuh"
 #include "runtime.cuh"
 
@@ -21,118 +22,8 @@ static int arg_fail(const std::string& m) {
   return MOONS_ERR_ARG;
 }
 
-// ---- 1-D stencil coefficients (HW/grid/derivative_stencils.f90:31-217,
-// HW/grid/interpolation_stencils.f90:12-35), built on the host once per mesh.
-// Arrays are 1-based: a[0] unused.
-namespace {
-struct HostCoord {
-  int sn, sc;
-  std::vector<double> hn, hc, dhn, dhc, cc2nD, cc2nU, n2ccD, n2ccU, thD, thU;
-  std::vector<double> colCC_L[2], colCC_D[2], colCC_U[2], colN_L[2], colN_D[2], colN_U[2];
-};
-
-void build_col(std::vector<double>& L, std::vector<double>& D, std::vector<double>& U,
-               const std::vector<double>& dh, int s, bool cc, int order) {
-  int n = std::max(s - 2, 1);
-  L.assign(n + 1, 0.0);
-  D.assign(n + 1, 0.0);
-  U.assign(n + 1, 0.0);
-  if (cc ? s <= 2 : s <= 3) return;
-  auto h = [&](int i) { return dh[i]; };
-  if (order == 2) {
-    if (cc) {
-      double a = 0.5 * h(1);
-      L[1] = 2.0 / (a * (a + h(2)));
-      D[1] = -2.0 / (a * h(2));
-      U[1] = 2.0 / (h(2) * (a + h(2)));
-    } else {
-      L[1] = 2.0 / (h(2) * (h(3) + h(2)));
-      D[1] = -2.0 / (h(3) * h(2));
-      U[1] = 2.0 / (h(3) * (h(3) + h(2)));
-    }
-    for (int i = 3; i <= s - 2; i++) {
-      L[i - 1] = 2.0 / (h(i - 1) * (h(i - 1) + h(i)));
-      D[i - 1] = cc ? -(2.0 / (h(i - 1) * h(i))) : -2.0 / (h(i - 1) * h(i));
-      U[i - 1] = 2.0 / (h(i) * (h(i - 1) + h(i)));
-    }
-    int i = s - 1;
-    if (cc) {
-      double b = 0.5 * h(i);
-      L[s - 2] = 2.0 / (h(i - 1) * (h(i - 1) + b));
-      D[s - 2] = -2.0 / (h(i - 1) * b);
-      U[s - 2] = 2.0 / (b * (h(i - 1) + b));
-    } else {
-      L[s - 2] = 2.0 / (h(i - 2) * (h(i - 1) + h(i - 2)));
-      D[s - 2] = -2.0 / (h(i - 1) * h(i - 2));
-      U[s - 2] = 2.0 / (h(i - 1) * (h(i - 1) + h(i - 2)));
-    }
-  } else {
-    if (cc) {
-      double a = 0.5 * h(1);
-      L[1] = (-(h(2)) / (a * (a + h(2))));
-      D[1] = ((-a + h(2)) / (a * h(2)));
-      U[1] = (a / (h(2) * (a + h(2))));
-    } else {
-      L[1] = -(h(3) + 2.0 * h(2)) / (h(2) * (h(3) + h(2)));
-      D[1] = (h(3) + h(2)) / (h(3) * h(2));
-      U[1] = -h(2) / (h(3) * (h(3) + h(2)));
-    }
-    for (int i = 3; i <= s - 2; i++) {
-      L[i - 1] = cc ? (-h(i) / (h(i - 1) * (h(i - 1) + h(i)))) : -((h(i) / (h(i - 1) * (h(i - 1) + h(i)))));
-      D[i - 1] = ((-h(i - 1) + h(i)) / (h(i - 1) * h(i)));
-      U[i - 1] = (h(i - 1) / (h(i) * (h(i - 1) + h(i))));
-    }
-    int i = s - 1;
-    if (cc) {
-      double b = 0.5 * h(i);
-      L[s - 2] = (-b / (h(i - 1) * (h(i - 1) + b)));
-      D[s - 2] = ((-h(i - 1) + b) / (h(i - 1) * b));
-      U[s - 2] = (h(i - 1) / (b * (h(i - 1) + b)));
-    } else {
-      L[s - 2] = h(i - 1) / (h(i - 2) * (h(i - 1) + h(i - 2)));
-      D[s - 2] = -(h(i - 1) + h(i - 2)) / (h(i - 1) * h(i - 2));
-      U[s - 2] = (2.0 * h(i - 1) + h(i - 2)) / (h(i - 1) * (h(i - 1) + h(i - 2)));
-    }
-  }
-}
-
-HostCoord build_coord(const double* h, int sn) {
-  HostCoord c;
-  c.sn = sn;
-  c.sc = sn - 1;
-  c.hn.assign(sn + 1, 0.0);
-  for (int i = 1; i <= sn; i++) c.hn[i] = h[i - 1];
-  c.dhn.assign(sn, 0.0);
-  for (int i = 1; i <= sn - 1; i++) c.dhn[i] = c.hn[i + 1] - c.hn[i];
-  c.hc.assign(c.sc + 1, 0.0);
-  for (int i = 1; i <= sn - 1; i++) c.hc[i] = (c.hn[i + 1] + c.hn[i]) / 2.0;
-  c.dhc.assign(c.sc, 0.0);
-  for (int i = 1; i <= c.sc - 1; i++) c.dhc[i] = c.hc[i + 1] - c.hc[i];
-  c.cc2nD.assign(c.sc, 0.0);
-  c.cc2nU.assign(c.sc, 0.0);
-  for (int i = 1; i <= c.sc - 1; i++) {
-    c.cc2nD[i] = -(1.0 / c.dhc[i]);
-    c.cc2nU[i] = 1.0 / c.dhc[i];
-  }
-  c.n2ccD.assign(sn, 0.0);
-  c.n2ccU.assign(sn, 0.0);
-  for (int i = 1; i <= sn - 1; i++) {
-    c.n2ccD[i] = -(1.0 / c.dhn[i]);
-    c.n2ccU[i] = 1.0 / c.dhn[i];
-  }
-  c.thD.assign(c.sc, 0.0);
-  c.thU.assign(c.sc, 0.0);
-  for (int i = 1; i <= c.sc - 1; i++) {
-    c.thD[i] = (c.hn[i + 1] - c.hc[i]) / (c.hc[i + 1] - c.hc[i]);
-    c.thU[i] = 1.0 - c.thD[i];
-  }
-  for (int o = 1; o <= 2; o++) {
-    build_col(c.colCC_L[o - 1], c.colCC_D[o - 1], c.colCC_U[o - 1], c.dhc, c.sc, true, o);
-    build_col(c.colN_L[o - 1], c.colN_D[o - 1], c.colN_U[o - 1], c.dhn, c.sn, false, o);
-  }
-  return c;
-}
-}  // namespace
+using host::HostCoord;
+using host::build_coord;
 
 DF make_df(moons_mesh* m, int dl, double** storage) {
   DF f{};
@@ -370,14 +261,26 @@ nomem:
 
 int moons_mesh_destroy(moons_mesh* m) {
   if (!m) return MOONS_OK;
+  mesh_unref(m);
+  return MOONS_OK;
+}
+
+}  // extern "C"
+
+namespace mg {
+void mesh_ref(moons_mesh* m) { m->refs++; }
+void mesh_unref(moons_mesh* m) {
+  if (--m->refs > 0) return;
   cudaSetDevice(m->device);
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (void* p : m->allocs) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
-  return MOONS_OK;
 }
+}  // namespace mg
+
+extern "C" {
 
 int moons_mesh_sync(moons_mesh* m) {
   if (!m) return arg_fail("null mesh");
@@ -390,10 +293,12 @@ int moons_sf_create(moons_mesh* m, int dl, moons_sf** out) {
   if (dl < 0 || dl > 7) return arg_fail("moons_sf_create: bad data location");
   auto* s = new moons_sf();
   s->m = m;
+  mesh_ref(m);
   s->f = make_df(m, dl, nullptr);
   cudaSetDevice(m->device);
   if (cudaMalloc(&s->f.f, s->f.n() * sizeof(double)) != cudaSuccess) {
     delete s;
+    mesh_unref(m);
     g_err = "moons_sf_create: device allocation failed";
     return MOONS_ERR_NOMEM;
   }
@@ -406,7 +311,9 @@ int moons_sf_destroy(moons_sf* s) {
   cudaSetDevice(s->m->device);
   cudaStreamSynchronize(s->m->stream);
   if (s->owns) cudaFree(s->f.f);
+  moons_mesh* m = s->m;
   delete s;
+  mesh_unref(m);
   return MOONS_OK;
 }
 int moons_sf_shape(const moons_sf* s, int out[3]) {

@@ -421,11 +421,15 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
   auto* s = new moons_mhd();
   s->mm = mm;
   s->mi = mi;
+  mesh_ref(mm);
+  mesh_ref(mi);
   s->same = (mm == mi);
   s->P = *prm;
   if (!s->same) {
     for (int d = 0; d < 3; d++)
       if (prm->ind_offset[d] < 0 || mm->sn[d] + prm->ind_offset[d] > mi->sn[d]) {
+        mesh_unref(mm);
+        mesh_unref(mi);
         delete s;
         set_error("moons_mhd_create: fluid mesh does not fit inside the induction mesh at ind_offset");
         return MOONS_ERR_SHAPE;
@@ -519,7 +523,10 @@ int moons_mhd_destroy(moons_mhd* s) {
   for (moons_sf* f : s->owned) moons_sf_destroy(f);
   if (s->d_red) cudaFree(s->d_red);
   if (s->mi_stream_saved) s->mi->stream = s->mi_stream_saved;
+  moons_mesh *mm = s->mm, *mi = s->mi;
   delete s;
+  mesh_unref(mm);
+  mesh_unref(mi);
   return MOONS_OK;
 }
 

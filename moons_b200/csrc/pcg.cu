@@ -213,32 +213,9 @@ dim3 fgrid(const DF* a, int nc) {
   return dim3(px, kz, nc);
 }
 
-// the fused kernels' view of one component's BCs
-FBC fbc_of(const DBC& xb /* x (=p) */, const DBC& xbcb /* x_BC */, int dl, const DF& shape) {
-  FBC f{};
-  f.defined = xb.defined;
-  for (int face = 1; face <= 6; face++) {
-    f.type[face] = xb.defined ? xb.type[face] : 0;
-    double dh = xb.dh[face], nhat = xb.nhat[face], cw = xb.c_w[face];
-    int d = (face + 1) / 2;
-    if (f.type[face] == MOONS_BC_ROBIN)
-      f.rc[face] = n_along(dl, d) ? -2.0 * dh * nhat / cw : (2.0 * cw * nhat / dh - 1.0) / (2.0 * cw * nhat / dh + 1.0);
-  }
-  // masks of Ap come from x_BC's BCs (PCG_solver_algorithm.f90:72-75)
-  for (int face = 1; face <= 6; face++) {
-    int d = (face + 1) / 2;
-    if (!n_along(dl, d)) continue;
-    bool def = xbcb.defined != 0;
-    if (def ? xbcb.type[face] == MOONS_BC_NEUMANN : true) f.wall_neu |= 1 << (face - 1);
-    if (def ? xbcb.type[face] == MOONS_BC_DIRICHLET : true) f.wall_dir |= 1 << (face - 1);
-  }
-  if (xbcb.defined)
-    for (int d = 1; d <= 3; d++)
-      if (n_along(dl, d) && xbcb.type[2 * d - 1] == MOONS_BC_PERIODIC && xbcb.type[2 * d] == MOONS_BC_PERIODIC &&
-          shape.s(d) > 4)
-        f.wall_per |= 1 << (d - 1);
-  f.dot_wall = dirichlet_wall_bits(xb.defined ? &xb : nullptr, dl);
-  return f;
+FBC fbc_of(const DBC& xb, const DBC& xbcb, int dl, const DF& shape) {
+  int ext[4] = {0, shape.s0, shape.s1, shape.s2};
+  return make_fbc(xb, xbcb, dl, ext);
 }
 
 // operator_explicit of matrix_free_operators.f90 on component fields (generic
@@ -429,6 +406,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
   cudaSetDevice(m->device);
   auto* s = new moons_pcg();
   s->m = m;
+  mesh_ref(m);
   s->op = op;
   s->prec = prec;
   s->nc = nc;
@@ -530,7 +508,9 @@ int moons_pcg_destroy(moons_pcg* s) {
   if (s->graph) cudaGraphDestroy(s->graph);
   for (void* p : s->allocs) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
+  moons_mesh* m = s->m;
   delete s;
+  mesh_unref(m);
   return MOONS_OK;
 }
 

@@ -19,6 +19,9 @@ struct moons_mesh {
   double* d_scal = nullptr;      // kSlots result scalars
   double* h_scal = nullptr;      // pinned host mirror
   static constexpr int kSlots = 16;
+  // lifetime: fields, solvers and MHD objects hold a reference, so the mesh
+  // outlives them whatever order the caller destroys things in
+  int refs = 1;
 };
 
 struct moons_sf {
@@ -30,6 +33,8 @@ struct moons_sf {
 };
 
 namespace mg {
+void mesh_ref(moons_mesh* m);
+void mesh_unref(moons_mesh* m);
 // launch helpers (enqueue on the mesh stream; no sync)
 int launch_del(moons_mesh* m, DF out, DF in, int n, int dir, int pad, int gen);
 int launch_pw(moons_mesh* m, int op, DF a, const DF* b, double c);

@@ -116,6 +116,34 @@ def test_pcg_mom_diffusion_vf():
         assert rel_err(g.download(), o.download()) < 1e-9
 
 
+DUCT_B = [[NEUMANN, NEUMANN, DIRICHLET, DIRICHLET, PERIODIC, PERIODIC],
+          [DIRICHLET, DIRICHLET, NEUMANN, NEUMANN, PERIODIC, PERIODIC],
+          [DIRICHLET, DIRICHLET, DIRICHLET, DIRICHLET, PERIODIC, PERIODIC]]
+
+
+@pytest.mark.parametrize("op", ["mom", "ind"])
+def test_pcg_vf_duct_bcs(op):
+    # per-component BC patterns of the duct (pseudo-vacuum B, periodic streamwise)
+    ms = both(small_mesh_coords())
+    rng = np.random.default_rng(9)
+    dls = [FX, FY, FZ]
+    X = fields(ms, dls, [np.zeros(shape(ms[1], d)) for d in dls])
+    for c, (g, o) in enumerate(X):
+        types = DUCT_B[c] if op == "ind" else [DIRICHLET] * 4 + [PERIODIC] * 2
+        spec = bc(types, prescribed=[0, 0, 0, 0, 1, 1])
+        g.set_bcs(spec)
+        o.set_bcs(spec)
+    R = fields(ms, dls, [rng.standard_normal(shape(ms[1], d)) for d in dls])
+    if op == "ind":
+        sig = fields(ms, [EX, EY, EZ], [1.0 / (10.0 ** rng.uniform(-1, 1, shape(ms[1], d))) for d in (EX, EY, EZ)])
+        ig, io = run_both(ms, OP_IND_DIFFUSION, PREC_IND, X, X, R, isp(800, 1e-12, 1e-15), ks=sig, coeff=0.05)
+    else:
+        ig, io = run_both(ms, OP_MOM_DIFFUSION, PREC_MOM, X, X, R, isp(800, 1e-12, 1e-15), coeff=-0.05)
+    assert abs(ig["iterations"] - io["iterations"]) <= 1, (ig, io)
+    for g, o in X:
+        assert rel_err(g.download(), o.download()) < 1e-8
+
+
 def test_pcg_ind_diffusion_vf():
     ms = both(small_mesh_coords())
     rng = np.random.default_rng(5)
