@@ -39,8 +39,10 @@ struct DF {
   int dl;          // data location (MOONS_CC ...)
   __host__ __device__ int s(int d) const { return d == 1 ? s0 : (d == 2 ? s1 : s2); }
   __host__ __device__ size_t n() const { return (size_t)s0 * s1 * s2; }
+  // fields hold < 2^31 points (moons_mesh_create checks), so the offset is
+  // formed in 32-bit arithmetic
   MG_HD size_t at(int i, int j, int k) const {
-    return (size_t)(i - 1) + (size_t)s0 * ((size_t)(j - 1) + (size_t)s1 * (size_t)(k - 1));
+    return (size_t)((unsigned)(i - 1) + (unsigned)s0 * ((unsigned)(j - 1) + (unsigned)s1 * (unsigned)(k - 1)));
   }
   MG_HD double& operator()(int i, int j, int k) const { return f[at(i, j, k)]; }
 };

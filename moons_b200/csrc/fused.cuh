@@ -84,6 +84,9 @@ MG_HD int tget(int d, int i, int j, int k) { return d == 1 ? i : (d == 2 ? j : k
 // value of p~ (p after apply_BCs_implicit) at (i,j,k) for points an interior
 // output reads: at most one index is a ghost index.
 MG_HD double pt(const DF& p, const FBC& b, int i, int j, int k) {
+  // points two or more away from every boundary are neither ghosts nor
+  // boundary nodes: p~ = p there
+  if (i >= 3 && i <= p.s0 - 2 && j >= 3 && j <= p.s1 - 2 && k >= 3 && k <= p.s2 - 2) return p(i, j, k);
   int I[4] = {0, i, j, k};
   double fac = 1.0;
   bool robin_n = false;
@@ -398,13 +401,32 @@ __global__ void k_f_curl_ap(FComp Ap, FComp P, DF E0, DF E1, DF E2, DGrid g, FBC
 }
 
 // ---- K2: x += alpha p ; r -= alpha Ap ; rr, zr ; exit test ; beta -----------
-__device__ __forceinline__ void update_body(const DF& x, const DF& p, const DF& r, const DF& Ap, const DF& M,
-                                            const DGrid& g, int minv_mode, double coeff, int dw, double alpha,
-                                            double& arr, double& azr) {
+// p~ where it differs from p at a point x is updated on: the periodic
+// boundary node s-1 of a node direction (Periodic_N_implicit copies node 2
+// there).  x keeps that value when its own periodic BCs are prescribed, so
+// the update must add alpha*p~ as the reference does.  (Dirichlet boundary
+// nodes of p are 0 in both; ghost entries of x are rewritten by apply_BCs.)
+MG_HD double p_for_x(const DF& p, const FBC& b, int i, int j, int k, size_t idx) {
+  int t[4] = {0, i, j, k};
+#pragma unroll
+  for (int d = 1; d <= 3; d++) {
+    int s = p.s(d);
+    if (n_along(p.dl, d) && t[d] == s - 1 && s > 4 && b.type[2 * d - 1] == MOONS_BC_PERIODIC &&
+        b.type[2 * d] == MOONS_BC_PERIODIC) {
+      int u[4] = {0, i, j, k};
+      u[d] = 2;
+      return p(u[1], u[2], u[3]);
+    }
+  }
+  return p.f[idx];
+}
+__device__ __forceinline__ void update_body(const DF& x, const DF& p, const FBC& b, const DF& r, const DF& Ap,
+                                            const DF& M, const DGrid& g, int minv_mode, double coeff, int dw,
+                                            double alpha, double& arr, double& azr) {
   int i, j, k;
   if (!point_of(x, i, j, k)) return;
   size_t idx = x.at(i, j, k);
-  x.f[idx] = x.f[idx] + p.f[idx] * alpha;
+  x.f[idx] = x.f[idx] + p_for_x(p, b, i, j, k, idx) * alpha;
   double rv = r.f[idx] + Ap.f[idx] * (-alpha);
   r.f[idx] = rv;
   if (in_dot(x, i, j, k, dw)) {
@@ -414,20 +436,21 @@ __device__ __forceinline__ void update_body(const DF& x, const DF& p, const DF& 
   }
 }
 __global__ void k_f_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, DGrid g, int minv_mode, double coeff,
-                           int dw0, int dw1, int dw2, PcgScalars* S, double* partial, unsigned* ticket) {
+                           FBC b0, FBC b1, FBC b2, PcgScalars* S, double* partial, unsigned* ticket) {
   if (S->done) return;
   double arr = 0.0, azr = 0.0;
   double alpha = S->alpha;
-  if (blockIdx.z == 0) update_body(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], g, minv_mode, coeff, dw0, alpha, arr, azr);
+  if (blockIdx.z == 0)
+    update_body(X.f[0], P.f[0], b0, R.f[0], Ap.f[0], M.f[0], g, minv_mode, coeff, b0.dot_wall, alpha, arr, azr);
   else if (blockIdx.z == 1)
-    update_body(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], g, minv_mode, coeff, dw1, alpha, arr, azr);
-  else update_body(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], g, minv_mode, coeff, dw2, alpha, arr, azr);
-  double b1 = block_sum(arr);
-  double b2 = block_sum(azr);
+    update_body(X.f[1], P.f[1], b1, R.f[1], Ap.f[1], M.f[1], g, minv_mode, coeff, b1.dot_wall, alpha, arr, azr);
+  else update_body(X.f[2], P.f[2], b2, R.f[2], Ap.f[2], M.f[2], g, minv_mode, coeff, b2.dot_wall, alpha, arr, azr);
+  double s_rr = block_sum(arr);
+  double s_zr = block_sum(azr);
   unsigned fb = flat_block(), nb = n_blocks();
   if (threadIdx.x == 0) {
-    partial[fb] = b1;
-    partial[nb + fb] = b2;
+    partial[fb] = s_rr;
+    partial[nb + fb] = s_zr;
   }
   if (last_block_any(ticket)) {
     double rr = sum_partials(partial, nb);

@@ -334,7 +334,7 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
   }
   int mm = minv_mode(s);
   MG_LAUNCH(k_f_update, G, kBlock, m->stream, fc(x, s->nc), fc(s->p, s->nc), fc(s->r, s->nc), fc(s->Ax, s->nc),
-            fc(s->Minv, s->nc), m->dg, mm, s->coeff, dw[0], dw[1], dw[2], s->S, s->partial, tB);
+            fc(s->Minv, s->nc), m->dg, mm, s->coeff, b[0], b[1], b[2], s->S, s->partial, tB);
   MG_LAUNCH(k_f_pupd, G, kBlock, m->stream, fc(s->p, s->nc), fc(s->r, s->nc), fc(s->Minv, s->nc), m->dg, mm, s->coeff,
             s->S);
   MG_CUDA(cudaGetLastError());
