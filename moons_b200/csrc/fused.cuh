@@ -214,8 +214,8 @@ __device__ __forceinline__ unsigned n_blocks() { return gridDim.x * gridDim.y * 
 
 __device__ __forceinline__ bool last_block_any(unsigned* ticket) {
   __shared__ bool amlast;
-  __threadfence();
   if (threadIdx.x == 0) {
+    __threadfence();  // this block's partial (written by thread 0) before its ticket
     unsigned t = atomicAdd(ticket, 1u);
     amlast = (t == n_blocks() - 1);
   }

@@ -353,10 +353,11 @@ __device__ __forceinline__ double block_sum(double v) {
 }
 // returns true in the (single) last block after partials are visible;
 // the caller then sums partial[0..gridDim.x) in order.
+// (call after thread 0 wrote this block's partial; only thread 0 fences)
 __device__ __forceinline__ bool last_block(unsigned* ticket) {
   __shared__ bool amlast;
-  __threadfence();
   if (threadIdx.x == 0) {
+    __threadfence();
     unsigned t = atomicAdd(ticket, 1u);
     amlast = (t == gridDim.x - 1);
   }
