@@ -10,6 +10,7 @@
 // loop always ends.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "fused.cuh"
@@ -626,7 +627,24 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
             &s->S->rhok, m->d_partial, m->d_ticket);
   MG_LAUNCH(k_pcg_start, 1, 1, m->stream, s->S);
   MG_CUDA(cudaGetLastError());
-  // ---- the loop: one graph launch (WHILE node)
+  // ---- the loop.  MOONS_PCG_HOSTLOOP=1 launches the same kernels from the
+  // host in chunks of 32 iterations (kernels skip themselves once the exit
+  // flag is up): profilers cannot see kernels inside conditional graphs.
+  static const bool hostloop = [] {
+    const char* e = getenv("MOONS_PCG_HOSTLOOP");
+    return e && e[0] == '1';
+  }();
+  if (hostloop) {
+    for (int it = 0; it < isp->iter_max + 1; it += 32) {
+      for (int q = 0; q < 32 && !r; q++) r = enqueue_iteration(s, X);
+      if (r) return r;
+      MG_CUDA(cudaMemcpyAsync(s->hS, s->S, sizeof(PcgScalars), cudaMemcpyDeviceToHost, m->stream));
+      MG_CUDA(cudaStreamSynchronize(m->stream));
+      if (s->hS->done) break;
+    }
+    for (int c = 0; c < nc && !r; c++) r = launch_bcs(m, X[c], s->x_bc[c], false);
+    return r;
+  }
   bool need_graph = !s->exec;
   for (int c = 0; c < nc; c++)
     if (s->gx[c] != X[c].f) need_graph = true;
