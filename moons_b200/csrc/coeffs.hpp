@@ -10,7 +10,7 @@ namespace mg {
 namespace host {
 struct HostCoord {
   int sn, sc;
-  std::vector<double> hn, hc, dhn, dhc, cc2nD, cc2nU, n2ccD, n2ccU, thD, thU;
+  std::vector<double> hn, hc, dhn, dhc, cc2nD, cc2nU, n2ccD, n2ccU, thD, thU, diagC, diagN;
   std::vector<double> colCC_L[2], colCC_D[2], colCC_U[2], colN_L[2], colN_D[2], colN_U[2];
 };
 
@@ -113,6 +113,11 @@ inline HostCoord build_coord(const double* h, int sn) {
     build_col(c.colCC_L[o - 1], c.colCC_D[o - 1], c.colCC_U[o - 1], c.dhc, c.sc, true, o);
     build_col(c.colN_L[o - 1], c.colN_D[o - 1], c.colN_U[o - 1], c.dhn, c.sn, false, o);
   }
+  // per-axis share of laplacian_diagonal (GF_diagonals.f90:15-35)
+  c.diagC.assign(c.sc + 1, 0.0);
+  for (int i = 2; i <= c.sc - 1; i++) c.diagC[i] = c.n2ccD[i] * c.cc2nU[i - 1] + c.n2ccU[i] * c.cc2nD[i];
+  c.diagN.assign(c.sn + 1, 0.0);
+  for (int i = 2; i <= c.sn - 1; i++) c.diagN[i] = c.n2ccD[i] * c.cc2nU[i - 1] + c.n2ccU[i - 1] * c.cc2nD[i - 1];
   return c;
 }
 }  // namespace host

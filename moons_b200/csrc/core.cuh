@@ -27,6 +27,9 @@ struct DCoord {
   const double *colCC_L[2], *colCC_D[2], *colCC_U[2];  // size sc-2
   const double *colN_L[2], *colN_D[2], *colN_U[2];     // size sn-2
   const double *thD, *thU;      // interpolation theta, size sc-1
+  // this axis' share of laplacian_diagonal (GF_diagonals.f90:15-35) for data
+  // CC along the axis (diagC, index 2..sc-1) and node-located (diagN, 2..sn-1)
+  const double *diagC, *diagN;
 };
 struct DGrid {
   DCoord c[3];

@@ -154,21 +154,23 @@ MG_HD double pt(const DF& p, const FBC& b, int i, int j, int k) {
   return fac * v;
 }
 
-// laplacian_diagonal (GF_diagonals.f90:15-35) and the cell volume of a point
+// laplacian_diagonal (GF_diagonals.f90:15-35) and the cell volume of a point,
+// formed per axis: diag = (dx + dy) + dz with each axis' two terms from the
+// mesh tables (diagC/diagN), vol = (hx*hy)*hz
 MG_HD double lap_diag_at(const DGrid& g, int dl, int i, int j, int k) {
   const DCoord &c1 = g.c[0], &c2 = g.c[1], &c3 = g.c[2];
-  int px = n_along(dl, 1), py = n_along(dl, 2), pz = n_along(dl, 3);
-  return c1.n2ccD[i] * c1.cc2nU[i - 1] + c1.n2ccU[i - px] * c1.cc2nD[i - px] + c2.n2ccD[j] * c2.cc2nU[j - 1] +
-         c2.n2ccU[j - py] * c2.cc2nD[j - py] + c3.n2ccD[k] * c3.cc2nU[k - 1] + c3.n2ccU[k - pz] * c3.cc2nD[k - pz];
+  double dx = n_along(dl, 1) ? c1.diagN[i] : c1.diagC[i];
+  double dy = n_along(dl, 2) ? c2.diagN[j] : c2.diagC[j];
+  double dz = n_along(dl, 3) ? c3.diagN[k] : c3.diagC[k];
+  return (dx + dy) + dz;
 }
 MG_HD double vol_at(const DGrid& g, int dl, int i, int j, int k) {
   int ex = n_along(dl, 1), ey = n_along(dl, 2), ez = n_along(dl, 3);
-  return (ex ? g.c[0].dhc[i - 1] : g.c[0].dhn[i]) * (ey ? g.c[1].dhc[j - 1] : g.c[1].dhn[j]) *
+  return ((ex ? g.c[0].dhc[i - 1] : g.c[0].dhn[i]) * (ey ? g.c[1].dhc[j - 1] : g.c[1].dhn[j])) *
          (ez ? g.c[2].dhc[k - 1] : g.c[2].dhn[k]);
 }
 // Minv at a point: mode 1 prec_Lap, 2 prec_mom (coeff), 0 stored
-MG_HD double minv_at(int mode, const DGrid& g, const DF& M, int dl, int i, int j, int k,
-                                          bool ghost, double coeff) {
+MG_HD double minv_at(int mode, const DGrid& g, const DF& M, int dl, int i, int j, int k, bool ghost, double coeff) {
   if (mode == 0) return M(i, j, k);
   if (ghost) return 0.0;
   double d = lap_diag_at(g, dl, i, j, k);
@@ -214,7 +216,7 @@ __device__ __forceinline__ unsigned n_blocks() { return gridDim.x * gridDim.y * 
 
 __device__ __forceinline__ bool last_block_any(unsigned* ticket) {
   __shared__ bool amlast;
-  if (threadIdx.x == 0) {
+  if (lin_tid() == 0) {
     __threadfence();  // this block's partial (written by thread 0) before its ticket
     unsigned t = atomicAdd(ticket, 1u);
     amlast = (t == n_blocks() - 1);
@@ -264,10 +266,10 @@ MG_HD double lap_pt(const DF& p, const FBC& b, const DGrid& g, const DF& kx, con
 __device__ __forceinline__ void finish_alpha(double acc, PcgScalars* S, double* partial, unsigned* ticket) {
   double bs = block_sum(acc);
   unsigned fb = flat_block();
-  if (threadIdx.x == 0) partial[fb] = bs;
+  if (lin_tid() == 0) partial[fb] = bs;
   if (last_block_any(ticket)) {
     double tot = sum_partials(partial, n_blocks());
-    if (threadIdx.x == 0) {
+    if (lin_tid() == 0) {
       S->pap = tot;
       S->alpha = S->rhok / tot;
       *ticket = 0;

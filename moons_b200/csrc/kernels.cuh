@@ -339,24 +339,26 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   return v;
 }
+__device__ __forceinline__ unsigned lin_tid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+__device__ __forceinline__ unsigned lin_nthreads() { return blockDim.x * blockDim.y * blockDim.z; }
+// block-wide sum (any block shape, <= 1024 threads); valid in thread 0
 __device__ __forceinline__ double block_sum(double v) {
   __shared__ double sh[32];
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned t = lin_tid();
+  int lane = t & 31, w = t >> 5;
   v = warp_sum(v);
   if (lane == 0) sh[w] = v;
   __syncthreads();
-  int nw = (blockDim.x + 31) >> 5;
-  v = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  unsigned nw = (lin_nthreads() + 31) >> 5;
+  v = (t < nw) ? sh[t] : 0.0;
   if (w == 0) v = warp_sum(v);
   __syncthreads();
-  return v;  // valid in thread 0
+  return v;
 }
-// returns true in the (single) last block after partials are visible;
-// the caller then sums partial[0..gridDim.x) in order.
 // (call after thread 0 wrote this block's partial; only thread 0 fences)
 __device__ __forceinline__ bool last_block(unsigned* ticket) {
   __shared__ bool amlast;
-  if (threadIdx.x == 0) {
+  if (lin_tid() == 0) {
     __threadfence();
     unsigned t = atomicAdd(ticket, 1u);
     amlast = (t == gridDim.x - 1);
@@ -367,7 +369,7 @@ __device__ __forceinline__ bool last_block(unsigned* ticket) {
 __device__ __forceinline__ double sum_partials(const double* partial, int n) {
   // fixed-order: each thread sums a strided set, then a fixed tree
   double v = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) v += ((volatile const double*)partial)[i];
+  for (int i = lin_tid(); i < n; i += lin_nthreads()) v += ((volatile const double*)partial)[i];
   return block_sum(v);
 }
 

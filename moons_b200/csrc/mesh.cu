@@ -228,11 +228,12 @@ int moons_mesh_create(moons_mesh** out, const double* hx, int sx, const double* 
     dc.hn = up(c.hn); dc.hc = up(c.hc); dc.dhn = up(c.dhn); dc.dhc = up(c.dhc);
     dc.cc2nD = up(c.cc2nD); dc.cc2nU = up(c.cc2nU); dc.n2ccD = up(c.n2ccD); dc.n2ccU = up(c.n2ccU);
     dc.thD = up(c.thD); dc.thU = up(c.thU);
+    dc.diagC = up(c.diagC); dc.diagN = up(c.diagN);
     for (int o = 0; o < 2; o++) {
       dc.colCC_L[o] = up(c.colCC_L[o]); dc.colCC_D[o] = up(c.colCC_D[o]); dc.colCC_U[o] = up(c.colCC_U[o]);
       dc.colN_L[o] = up(c.colN_L[o]); dc.colN_D[o] = up(c.colN_D[o]); dc.colN_U[o] = up(c.colN_U[o]);
     }
-    if (!dc.hn || !dc.thU || !dc.colN_U[1]) {
+    if (!dc.hn || !dc.thU || !dc.colN_U[1] || !dc.diagN) {
       moons_mesh_destroy(m);
       g_err = "moons_mesh_create: device allocation failed";
       return MOONS_ERR_NOMEM;

@@ -2,8 +2,8 @@
 // every scalar of the recurrence kept on the device.
 //
 // modify_RHS (PCG_aux.f90:30-79) runs once per solve with the generic
-// kernels.  The iteration body is the fused K1/K2/K3 of fused.cuh (K1 is two
-// kernels for the curl-curl operator).  The whole loop is captured once into
+// kernels.  The iteration body is the lean K1/K2/K3 of lean.cuh (K1 is two
+// kernels for the curl-curl operator), two iterations per body.  The whole loop is captured once into
 // a CUDA graph whose WHILE node repeats the body until the device-side exit
 // flag is set; the flag also comes up when the iteration count reaches
 // iter_max, and the node stops after iter_max+2 body runs in any case, so the
@@ -13,7 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 
-#include "fused.cuh"
+#include "lean.cuh"
 #include "runtime.cuh"
 
 namespace mg {
@@ -156,7 +156,7 @@ struct moons_pcg {
   moons_mesh* m = nullptr;
   int op = 0, prec = 0, nc = 1;
   double coeff = 0.0;
-  DF p[3]{}, xbc[3]{}, r[3]{}, Ax[3]{}, vol[3]{}, z[3]{}, Minv[3]{}, tempx[3]{}, k[3]{}, tempk[3]{};
+  DF p[3]{}, p2[3]{}, xbc[3]{}, r[3]{}, Ax[3]{}, vol[3]{}, z[3]{}, Minv[3]{}, tempx[3]{}, k[3]{}, tempk[3]{};
   DBC xbc_bc[3]{};   // BCs of x_BC
   DBC x_bc[3]{};     // BCs of x, copied to p
   int x_dl[3] = {0, 0, 0};
@@ -203,6 +203,17 @@ unsigned red_grid(const DF* a, int nc) {
   size_t n = 0;
   for (int c = 0; c < nc; c++) n += a[c].n();
   return (unsigned)std::min<size_t>(kRedBlocks, std::max<size_t>(1, (n + kBlock - 1) / kBlock));
+}
+// (i tile, j tile, k chunk x component) grid of the lean kernels
+dim3 lgrid(const DF* a, int nc, int* nkc) {
+  unsigned gx = 0, gy = 0, kz = 0;
+  for (int c = 0; c < nc; c++) {
+    gx = std::max(gx, (unsigned)((a[c].s0 + kTX - 1) / kTX));
+    gy = std::max(gy, (unsigned)((a[c].s1 + kTY - 1) / kTY));
+    kz = std::max(kz, (unsigned)a[c].s2);
+  }
+  *nkc = (int)((kz + kKC - 1) / kKC);
+  return dim3(gx, gy, (unsigned)(*nkc * nc));
 }
 // (plane chunk, k, component) grid covering nc fields
 dim3 fgrid(const DF* a, int nc) {
@@ -302,42 +313,48 @@ int minv_mode(const moons_pcg* s) {
 int enqueue_iteration(moons_pcg* s, DF* x) {
   moons_mesh* m = s->m;
   FBC b[3];
-  int dw[3] = {0, 0, 0};
   for (int c = 0; c < 3; c++) {
     int cc = c < s->nc ? c : 0;
     b[c] = fbc_of(s->x_bc[cc], s->xbc_bc[cc], s->x_dl[cc], s->Ax[cc]);
-    dw[c] = b[c].dot_wall;
   }
-  dim3 G = fgrid(s->Ax, s->nc);
+  int nkc = 0;
+  dim3 G = lgrid(s->Ax, s->nc, &nkc);
   unsigned* tA = s->ticket;
   unsigned* tB = s->ticket + 1;
   DF z0{};
-  switch (s->op) {
-    case MOONS_OP_LAP_UNIFORM:
-      MG_LAUNCH(k_f_lap_ap<0>, G, kBlock, m->stream, fc(s->Ax, s->nc), fc(s->p, s->nc), m->dg, b[0], b[1], b[2], z0, z0,
-                z0, 0.0, s->S, s->partial, tA);
-      break;
-    case MOONS_OP_LAP_PROPS:
-      MG_LAUNCH(k_f_lap_ap<1>, G, kBlock, m->stream, fc(s->Ax, s->nc), fc(s->p, s->nc), m->dg, b[0], b[1], b[2],
-                s->k[0], s->k[1], s->k[2], 0.0, s->S, s->partial, tA);
-      break;
-    case MOONS_OP_MOM_DIFFUSION:
-      MG_LAUNCH(k_f_lap_ap<2>, G, kBlock, m->stream, fc(s->Ax, s->nc), fc(s->p, s->nc), m->dg, b[0], b[1], b[2], z0, z0,
-                z0, s->coeff, s->S, s->partial, tA);
-      break;
-    case MOONS_OP_IND_DIFFUSION: {
-      dim3 GE = fgrid(s->tempk, 3);
-      MG_LAUNCH(k_f_curl_sig, GE, kBlock, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(s->p, 3), m->dg, b[0],
-                b[1], b[2], s->k[0], s->k[1], s->k[2], s->S);
-      MG_LAUNCH(k_f_curl_ap, G, kBlock, m->stream, fc(s->Ax, 3), fc(s->p, 3), s->tempk[0], s->tempk[1], s->tempk[2],
-                m->dg, b[0], b[1], b[2], s->coeff, s->S, s->partial, tA);
-    } break;
-  }
   int mm = minv_mode(s);
-  MG_LAUNCH(k_f_update, G, kBlock, m->stream, fc(x, s->nc), fc(s->p, s->nc), fc(s->r, s->nc), fc(s->Ax, s->nc),
-            fc(s->Minv, s->nc), m->dg, mm, s->coeff, b[0], b[1], b[2], s->S, s->partial, tB);
-  MG_LAUNCH(k_f_pupd, G, kBlock, m->stream, fc(s->p, s->nc), fc(s->r, s->nc), fc(s->Minv, s->nc), m->dg, mm, s->coeff,
-            s->S);
+  const dim3 TB(kTX, kTY, 1);
+  // two iterations: p -> p2 -> p (K3 reads one buffer and writes the other)
+  for (int half = 0; half < 2; half++) {
+    DF* pc = half == 0 ? s->p : s->p2;
+    DF* pn = half == 0 ? s->p2 : s->p;
+    switch (s->op) {
+      case MOONS_OP_LAP_UNIFORM:
+        MG_LAUNCH(k_l_lap<0>, G, TB, m->stream, fc(s->Ax, s->nc), fc(pc, s->nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
+                  0.0, nkc, s->S, s->partial, tA);
+        break;
+      case MOONS_OP_LAP_PROPS:
+        MG_LAUNCH(k_l_lap<1>, G, TB, m->stream, fc(s->Ax, s->nc), fc(pc, s->nc), m->dg, b[0], b[1], b[2], s->k[0],
+                  s->k[1], s->k[2], 0.0, nkc, s->S, s->partial, tA);
+        break;
+      case MOONS_OP_MOM_DIFFUSION:
+        MG_LAUNCH(k_l_lap<2>, G, TB, m->stream, fc(s->Ax, s->nc), fc(pc, s->nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
+                  s->coeff, nkc, s->S, s->partial, tA);
+        break;
+      case MOONS_OP_IND_DIFFUSION: {
+        int nke = 0;
+        dim3 GE = lgrid(s->tempk, 3, &nke);
+        MG_LAUNCH(k_l_curl_sig, GE, TB, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(pc, 3), s->k[0], s->k[1],
+                  s->k[2], m->dg, nke, s->S);
+        MG_LAUNCH(k_l_curl_ap, G, TB, m->stream, fc(s->Ax, 3), fc(pc, 3), s->tempk[0], s->tempk[1], s->tempk[2], m->dg,
+                  b[0], b[1], b[2], s->coeff, nkc, s->S, s->partial, tA);
+      } break;
+    }
+    MG_LAUNCH(k_l_update, G, TB, m->stream, fc(x, s->nc), fc(pc, s->nc), fc(s->r, s->nc), fc(s->Ax, s->nc),
+              fc(s->Minv, s->nc), m->dg, mm, s->coeff, b[0], b[1], b[2], nkc, s->S, s->partial, tB);
+    MG_LAUNCH(k_l_pupd, G, TB, m->stream, fc(pc, s->nc), fc(pn, s->nc), fc(s->r, s->nc), fc(s->Minv, s->nc), m->dg, mm,
+              s->coeff, b[0], b[1], b[2], nkc, s->S);
+  }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
@@ -423,6 +440,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     s->x_bc[c] = x[c]->bc;
     s->xbc_bc[c] = x_bc[c]->bc;
     if (!r) r = alloc_df(s, s->p[c], dl);
+    if (!r) r = alloc_df(s, s->p2[c], dl);
     if (!r) r = alloc_df(s, s->xbc[c], x_bc[c]->f.dl);
     if (!r) r = alloc_df(s, s->r[c], dl);
     if (!r) r = alloc_df(s, s->Ax[c], dl);
@@ -443,10 +461,13 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     }
   }
   if (!r) {
-    dim3 G = fgrid(s->Ax, nc);
+    int nk1 = 0, nk2 = 0;
+    dim3 G = lgrid(s->Ax, nc, &nk1);
     size_t nb = (size_t)G.x * G.y * G.z;
+    dim3 G2 = fgrid(s->Ax, nc);
+    nb = std::max(nb, (size_t)G2.x * G2.y * G2.z);
     if (needk) {
-      dim3 GE = fgrid(s->tempk, 3);
+      dim3 GE = lgrid(s->tempk, 3, &nk2);
       nb = std::max(nb, (size_t)GE.x * GE.y * GE.z);
     }
     s->max_blocks = nb;
@@ -620,6 +641,7 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
     launch_pw(m, PW_COPY, s->z[c], &s->Minv[c], 0.0);
     launch_pw(m, PW_MUL, s->z[c], &s->r[c], 0.0);
     launch_pw(m, PW_COPY, s->p[c], &s->z[c], 0.0);
+    launch_bcs(m, s->p[c], s->x_bc[c], true);  // the iteration kernels read p with its implicit BCs
   }
   int dw[3] = {0, 0, 0};
   for (int c = 0; c < nc; c++) dw[c] = dirichlet_wall_bits(s->x_bc[c].defined ? &s->x_bc[c] : nullptr, s->x_dl[c]);
@@ -636,7 +658,7 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
   }();
   if (hostloop) {
     for (int it = 0; it < isp->iter_max + 1; it += 32) {
-      for (int q = 0; q < 32 && !r; q++) r = enqueue_iteration(s, X);
+      for (int q = 0; q < 16 && !r; q++) r = enqueue_iteration(s, X);  // 2 iterations each
       if (r) return r;
       MG_CUDA(cudaMemcpyAsync(s->hS, s->S, sizeof(PcgScalars), cudaMemcpyDeviceToHost, m->stream));
       MG_CUDA(cudaStreamSynchronize(m->stream));

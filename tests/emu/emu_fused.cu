@@ -51,6 +51,7 @@ static void make_grid(HGrid& G, int nx, int ny, int nz) {
     dc.hn = c.hn.data(); dc.hc = c.hc.data(); dc.dhn = c.dhn.data(); dc.dhc = c.dhc.data();
     dc.cc2nD = c.cc2nD.data(); dc.cc2nU = c.cc2nU.data(); dc.n2ccD = c.n2ccD.data(); dc.n2ccU = c.n2ccU.data();
     dc.thD = c.thD.data(); dc.thU = c.thU.data();
+    dc.diagC = c.diagC.data(); dc.diagN = c.diagN.data();
     for (int o = 0; o < 2; o++) {
       dc.colCC_L[o] = c.colCC_L[o].data(); dc.colCC_D[o] = c.colCC_D[o].data(); dc.colCC_U[o] = c.colCC_U[o].data();
       dc.colN_L[o] = c.colN_L[o].data(); dc.colN_D[o] = c.colN_D[o].data(); dc.colN_U[o] = c.colN_U[o].data();

@@ -94,8 +94,10 @@ def test_pcg_lap_props_sigma():
     (b,) = fields(ms, [CC], [rng.standard_normal(s)])
     ig, io = run_both(ms, OP_LAP_PROPS, PREC_LAP, [phi], [phi], [b], isp(5000, 1e-10, 1e-15), ks=ks)
     # six decades of coefficient contrast: thousands of iterations, whose count
-    # moves by a few with the order of the floating-point sums
-    assert abs(ig["iterations"] - io["iterations"]) <= max(1, 0.01 * io["iterations"]), (ig, io)
+    # moves by a few tens with the order of the floating-point sums (CG loses
+    # orthogonality at this conditioning); both runs must reach the tolerance
+    assert abs(ig["iterations"] - io["iterations"]) <= max(1, 0.02 * io["iterations"]), (ig, io)
+    assert ig["rel"] < 1e-10 and io["rel"] < 1e-10
     assert rel_err(phi[0].download(), phi[1].download()) < 1e-7
 
 
