@@ -3,10 +3,13 @@
 // Same three steps as fused.cuh (K1 op+mask+vol+p.Ap -> alpha, K2 x/r update
 // + r.r, z.r -> exit test and beta, K3 p = beta p + Minv r), organised for
 // the memory system instead of for brevity:
-//  * a block is a 32x4 tile of (i,j) columns marching KC planes in k; every
-//    per-column quantity (stencil coefficients, volumes, wall masks, index
-//    arithmetic) is formed once per column, the centre column rolls its z
-//    neighbours in registers, and x/y neighbours come from L1/L2;
+//  * a thread owns one (i,j) column of a plane and kKC consecutive planes in
+//    k; a block is 256 consecutive columns of the plane's inner set or of
+//    its perimeter ring (coalesced, no tile waste, no BC divergence among
+//    inner columns), the grid is (plane blocks, k chunks, component).  Per-column
+//    quantities (stencil coefficients, volumes, wall masks) are formed once
+//    per column; every load of the kKC planes is issued before the first
+//    result is formed, so each thread keeps several loads in flight;
 //  * K3 also writes p's homogeneous (implicit) BC values -- ghost planes,
 //    Dirichlet boundary nodes (0), periodic boundary nodes (copy of node 2)
 //    -- computing the new value of each source point on the fly, so K1 and
@@ -21,66 +24,190 @@
 
 namespace mg {
 
-constexpr int kTX = 32, kTY = 4, kKC = 16;
+constexpr int kLB = 256;  // threads per block (points of one plane)
+constexpr int kKC = 4;    // planes per thread
 
 struct Col {  // per-column (fixed i,j) data of one component
   int i, j;
   bool ok, gij;  // inside the field; ghost in x or y
 };
 
-__device__ __forceinline__ Col col_of(const DF& a) {
+// The (i,j) columns of a plane are split into the INNER set -- columns that
+// are neither ghosts nor boundary nodes of a node-located direction, where
+// no BC or wall rule applies -- and the PERIMETER ring around it.  Blocks
+// 0..npbI-1 of a plane take 256 inner columns each, the next npbP blocks the
+// perimeter, so the BC-specific code paths never diverge inside a warp of
+// inner columns.
+struct PlaneSplit {
+  int ilo, ihi, jlo, jhi;
+  unsigned wI, nI, nP, npbI, npbP;
+};
+MG_HD PlaneSplit plane_split(int s0, int s1, int dl) {
+  PlaneSplit q;
+  q.ilo = n_along(dl, 1) ? 3 : 2;
+  q.jlo = n_along(dl, 2) ? 3 : 2;
+  q.ihi = s0 + 1 - q.ilo;
+  q.jhi = s1 + 1 - q.jlo;
+  const int w = q.ihi - q.ilo + 1, h = q.jhi - q.jlo + 1;
+  q.wI = w > 0 ? (unsigned)w : 0u;
+  q.nI = (w > 0 && h > 0) ? (unsigned)(w * h) : 0u;
+  q.nP = (unsigned)(s0 * s1) - q.nI;
+  q.npbI = (q.nI + kLB - 1) / kLB;
+  q.npbP = (q.nP + kLB - 1) / kLB;
+  return q;
+}
+
+// pb: index of the 256-column block of the plane
+__device__ __forceinline__ Col col_of(const DF& a, unsigned pb) {
   Col c;
-  c.i = blockIdx.x * kTX + threadIdx.x + 1;
-  c.j = blockIdx.y * kTY + threadIdx.y + 1;
-  c.ok = c.i <= a.s0 && c.j <= a.s1;
+  const PlaneSplit q = plane_split(a.s0, a.s1, a.dl);
+  if (pb < q.npbI) {
+    const unsigned t = pb * kLB + threadIdx.x;
+    const unsigned r = t / q.wI;
+    c.ok = t < q.nI;
+    c.j = q.jlo + (int)r;
+    c.i = q.ilo + (int)(t - r * q.wI);
+  } else {
+    unsigned t = (pb - q.npbI) * kLB + threadIdx.x;
+    c.ok = t < q.nP;
+    const unsigned s0 = (unsigned)a.s0;
+    const unsigned nb = (unsigned)(q.jlo - 1) * s0;            // rows below the inner set
+    const unsigned nt = (unsigned)(a.s1 - q.jhi) * s0;         // rows above it
+    if (t < nb) {
+      const unsigned r = t / s0;
+      c.j = 1 + (int)r;
+      c.i = 1 + (int)(t - r * s0);
+    } else if (t < nb + nt) {
+      t -= nb;
+      const unsigned r = t / s0;
+      c.j = q.jhi + 1 + (int)r;
+      c.i = 1 + (int)(t - r * s0);
+    } else {  // left and right bands of the inner rows
+      t -= nb + nt;
+      const unsigned wl = (unsigned)(q.ilo - 1), ws = wl + (unsigned)(a.s0 - q.ihi);
+      const unsigned r = t / ws, u = t - r * ws;
+      c.j = q.jlo + (int)r;
+      c.i = u < wl ? 1 + (int)u : q.ihi + 1 + (int)(u - wl);
+    }
+  }
+  if (!c.ok) c.i = c.j = 1;
   c.gij = c.i == 1 || c.i == a.s0 || c.j == 1 || c.j == a.s1;
   return c;
 }
+// work item w of a grid-stride loop -> (component, k chunk of KC planes,
+// plane block); consecutive items walk the plane blocks of one chunk
+struct Item {
+  unsigned pb;
+  int c, k0;
+};
+template <int KC>
+__device__ __forceinline__ Item item_of(unsigned w, unsigned npb, unsigned nkc) {
+  Item it;
+  const unsigned per = npb * nkc;
+  it.c = (int)(w / per);
+  const unsigned rem = w - (unsigned)it.c * per;
+  const unsigned kc = rem / npb;
+  it.pb = rem - kc * npb;
+  it.k0 = (int)kc * KC + 1;
+  return it;
+}
+
+// plain (coherent) loads: the persistent solver reads data other blocks
+// wrote earlier in the same launch, after a grid barrier
+__device__ __forceinline__ double ld(const double* p) { return *p; }
 
 // Minv on the fly (per-axis tables, same formula as k_prec's)
 MG_HD double diag_axis(const DCoord& c, bool N, int t) { return N ? c.diagN[t] : c.diagC[t]; }
 MG_HD double vol_axis(const DCoord& c, bool N, int t) { return N ? c.dhc[t - 1] : c.dhn[t]; }
 
+// wall-mask factor and zeroing of the x,y position of a column
+__device__ __forceinline__ void wall_xy(const DF& A, const FBC& b, int i, int j, double& f, bool& zero) {
+  f = 1.0;
+  zero = false;
+  int t[2] = {i, j};
+  int s[2] = {A.s0, A.s1};
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    if (((b.wall_neu >> (2 * d)) & 1) && t[d] == 2) f *= 0.5;
+    if (((b.wall_neu >> (2 * d + 1)) & 1) && t[d] == s[d] - 1) f *= 0.5;
+    if (((b.wall_dir >> (2 * d)) & 1) && t[d] == 2) zero = true;
+    if (((b.wall_dir >> (2 * d + 1)) & 1) && t[d] == s[d] - 1) zero = true;
+    if (((b.wall_per >> d) & 1) && t[d] == s[d] - 1) zero = true;
+  }
+}
+__device__ __forceinline__ void wall_z(const DF& A, const FBC& b, bool Nz, int k, double& f, bool& zero) {
+  if (!Nz) return;
+  if (((b.wall_neu >> 4) & 1) && k == 2) f *= 0.5;
+  if (((b.wall_neu >> 5) & 1) && k == A.s2 - 1) f *= 0.5;
+  if ((((b.wall_dir >> 4) & 1) && k == 2) || (((b.wall_dir >> 5) & 1) && k == A.s2 - 1) ||
+      (((b.wall_per >> 2) & 1) && k == A.s2 - 1))
+    zero = true;
+}
+__device__ __forceinline__ bool dot_xy(const DF& A, const FBC& b, int i, int j) {
+  return !(((b.dot_wall & 1) && i == 2) || ((b.dot_wall & 2) && i == A.s0 - 1) || ((b.dot_wall & 4) && j == 2) ||
+           ((b.dot_wall & 8) && j == A.s1 - 1));
+}
+__device__ __forceinline__ bool dot_z(const DF& A, const FBC& b, int k) {
+  return !(((b.dot_wall & 16) && k == 2) || ((b.dot_wall & 32) && k == A.s2 - 1));
+}
+
+// the 1-D second-difference coefficients of one axis at t: the reference's
+// two-gradient composition part = (pm*a1 + p0*a2)*o1 + (p0*b1 + pp*b2)*o2
+struct Ax6 {
+  double a1, a2, b1, b2, o1, o2;
+};
+__device__ __forceinline__ Ax6 axis_coef(const DCoord& c, bool N, int t) {
+  Ax6 r;
+  if (!N) {
+    r.a1 = c.cc2nD[t - 1]; r.a2 = c.cc2nU[t - 1]; r.b1 = c.cc2nD[t]; r.b2 = c.cc2nU[t];
+    r.o1 = c.n2ccD[t]; r.o2 = c.n2ccU[t];
+  } else {
+    r.a1 = c.n2ccD[t - 1]; r.a2 = c.n2ccU[t - 1]; r.b1 = c.n2ccD[t]; r.b2 = c.n2ccU[t];
+    r.o1 = c.cc2nD[t - 1]; r.o2 = c.cc2nU[t - 1];
+  }
+  return r;
+}
+
 // ---- K1: LAP_UNIFORM (MODE 0), LAP_PROPS (1), MOM_DIFFUSION (2) ---------------
 template <int MODE>
 __device__ __forceinline__ double lap_column(const DF& A, const DF& p, const FBC& b, const DGrid& g, const DF& kx,
-                                             const DF& ky, const DF& kz, double coeff, int k0, int k1) {
-  Col cl = col_of(A);
+                                             const DF& ky, const DF& kz, double coeff, unsigned pb, int k0, int k1) {
+  Col cl = col_of(A, pb);
   if (!cl.ok || k0 > k1) return 0.0;  // k chunks past this component's last plane
   const int i = cl.i, j = cl.j;
-  const bool Nx = n_along(A.dl, 1), Ny = n_along(A.dl, 2), Nz = n_along(A.dl, 3);
-  const DCoord &cx = g.c[0], &cy = g.c[1], &cz = g.c[2];
-  const size_t sx = 1, sy = (size_t)A.s0, sz = (size_t)A.s0 * A.s1;
-  double acc = 0.0;
+  const size_t sy = (size_t)A.s0, sz = (size_t)A.s0 * A.s1;
+  const size_t idx0 = A.at(i, j, k0);
   if (cl.gij) {  // ghost columns: Ap = vol*... = 0
-    for (int k = k0; k <= k1; k++) A(i, j, k) = 0.0;
+#pragma unroll
+    for (int q = 0; q < kKC; q++)
+      if (k0 + q <= k1) A.f[idx0 + q * sz] = 0.0;
     return 0.0;
   }
-  // per-column coefficients (x, y): part = a*pm + b*p0 + c*pp form kept as
-  // the reference's two-gradient composition
-  double xa1, xa2, xb1, xb2, xo1, xo2, ya1, ya2, yb1, yb2, yo1, yo2;
-  if (!Nx) { xa1 = cx.cc2nD[i - 1]; xa2 = cx.cc2nU[i - 1]; xb1 = cx.cc2nD[i]; xb2 = cx.cc2nU[i]; xo1 = cx.n2ccD[i]; xo2 = cx.n2ccU[i]; }
-  else { xa1 = cx.n2ccD[i - 1]; xa2 = cx.n2ccU[i - 1]; xb1 = cx.n2ccD[i]; xb2 = cx.n2ccU[i]; xo1 = cx.cc2nD[i - 1]; xo2 = cx.cc2nU[i - 1]; }
-  if (!Ny) { ya1 = cy.cc2nD[j - 1]; ya2 = cy.cc2nU[j - 1]; yb1 = cy.cc2nD[j]; yb2 = cy.cc2nU[j]; yo1 = cy.n2ccD[j]; yo2 = cy.n2ccU[j]; }
-  else { ya1 = cy.n2ccD[j - 1]; ya2 = cy.n2ccU[j - 1]; yb1 = cy.n2ccD[j]; yb2 = cy.n2ccU[j]; yo1 = cy.cc2nD[j - 1]; yo2 = cy.cc2nU[j - 1]; }
-  const double vxy = vol_axis(cx, Nx, i) * vol_axis(cy, Ny, j);
-  // wall masks along x and y (only node directions have wall planes)
-  double fxy = 1.0;
-  bool zxy = false;
-  {
-    int t[3] = {i, j, 0};
-    int s[3] = {A.s0, A.s1, 0};
-    for (int d = 0; d < 2; d++) {
-      if (((b.wall_neu >> (2 * d)) & 1) && t[d] == 2) fxy *= 0.5;
-      if (((b.wall_neu >> (2 * d + 1)) & 1) && t[d] == s[d] - 1) fxy *= 0.5;
-      if (((b.wall_dir >> (2 * d)) & 1) && t[d] == 2) zxy = true;
-      if (((b.wall_dir >> (2 * d + 1)) & 1) && t[d] == s[d] - 1) zxy = true;
-      if (((b.wall_per >> d) & 1) && t[d] == s[d] - 1) zxy = true;
-    }
+  const bool Nx = n_along(A.dl, 1), Ny = n_along(A.dl, 2), Nz = n_along(A.dl, 3);
+  const double* pbase = p.f + idx0;
+  // loads: p on planes k0-1 .. k1+1, x and y neighbours on k0 .. k1
+  double pc[kKC + 2], xm[kKC], xp[kKC], ym[kKC], yp[kKC];
+#pragma unroll
+  for (int q = 0; q < kKC + 2; q++) {
+    int k = k0 - 1 + q;
+    pc[q] = (k >= 1 && k <= A.s2 && k <= k1 + 1) ? ld(pbase + (ptrdiff_t)(q - 1) * (ptrdiff_t)sz) : 0.0;
   }
-  const bool dot_xy = !(((b.dot_wall & 1) && i == 2) || ((b.dot_wall & 2) && i == A.s0 - 1) ||
-                        ((b.dot_wall & 4) && j == 2) || ((b.dot_wall & 8) && j == A.s1 - 1));
-  size_t idx = A.at(i, j, k0);
+#pragma unroll
+  for (int q = 0; q < kKC; q++) {
+    int k = k0 + q;
+    bool in = k > 1 && k < A.s2 && k <= k1;
+    const double* c = pbase + (size_t)q * sz;
+    xm[q] = in ? ld(c - 1) : 0.0;
+    xp[q] = in ? ld(c + 1) : 0.0;
+    ym[q] = in ? ld(c - sy) : 0.0;
+    yp[q] = in ? ld(c + sy) : 0.0;
+  }
+  const Ax6 X = axis_coef(g.c[0], Nx, i), Y = axis_coef(g.c[1], Ny, j);
+  const double vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
+  double fxy;
+  bool zxy;
+  wall_xy(A, b, i, j, fxy, zxy);
+  const bool dxy = dot_xy(A, b, i, j);
   // coefficient fields have their own (face) extents
   size_t ix = 0, iy = 0, iz = 0, szx = 0, szy = 0, szz = 0;
   if (MODE == 1) {
@@ -91,65 +218,61 @@ __device__ __forceinline__ double lap_column(const DF& A, const DF& p, const FBC
     szy = (size_t)ky.s0 * ky.s1;
     szz = (size_t)kz.s0 * kz.s1;
   }
-  double pm = k0 > 1 ? p.f[idx - sz] : 0.0;
-  double p0 = p.f[idx];
-  for (int k = k0; k <= k1; k++, idx += sz, ix += szx, iy += szy, iz += szz) {
-    double pp = k < A.s2 ? p.f[idx + sz] : 0.0;
+  double acc = 0.0;
+#pragma unroll
+  for (int q = 0; q < kKC; q++) {
+    const int k = k0 + q;
+    if (k > k1) break;
+    const size_t idx = idx0 + (size_t)q * sz;
     if (k == 1 || k == A.s2) {
       A.f[idx] = 0.0;
-    } else {
-      double pxm = p.f[idx - sx], pxp = p.f[idx + sx], pym = p.f[idx - sy], pyp = p.f[idx + sy];
-      double za1, za2, zb1, zb2, zo1, zo2;
-      if (!Nz) { za1 = cz.cc2nD[k - 1]; za2 = cz.cc2nU[k - 1]; zb1 = cz.cc2nD[k]; zb2 = cz.cc2nU[k]; zo1 = cz.n2ccD[k]; zo2 = cz.n2ccU[k]; }
-      else { za1 = cz.n2ccD[k - 1]; za2 = cz.n2ccU[k - 1]; zb1 = cz.n2ccD[k]; zb2 = cz.n2ccU[k]; zo1 = cz.cc2nD[k - 1]; zo2 = cz.cc2nU[k - 1]; }
-      double gl = pxm * xa1 + p0 * xa2, gr = p0 * xb1 + pxp * xb2;
-      if (MODE == 1 && !Nx) { gl = gl * kx.f[ix]; gr = gr * kx.f[ix + 1]; }
-      double v = gl * xo1 + gr * xo2;
-      gl = pym * ya1 + p0 * ya2;
-      gr = p0 * yb1 + pyp * yb2;
-      if (MODE == 1 && !Ny) { gl = gl * ky.f[iy]; gr = gr * ky.f[iy + ky.s0]; }
-      v = v + (gl * yo1 + gr * yo2);
-      gl = pm * za1 + p0 * za2;
-      gr = p0 * zb1 + pp * zb2;
-      if (MODE == 1 && !Nz) { gl = gl * kz.f[iz]; gr = gr * kz.f[iz + szz]; }
-      v = v + (gl * zo1 + gr * zo2);
-      if (MODE == 2) {
-        v = v * coeff;
-        v = v + p0;
-      }
-      double f = fxy;
-      bool zero = zxy;
-      if (Nz) {
-        if (((b.wall_neu >> 4) & 1) && k == 2) f *= 0.5;
-        if (((b.wall_neu >> 5) & 1) && k == A.s2 - 1) f *= 0.5;
-        if ((((b.wall_dir >> 4) & 1) && k == 2) || (((b.wall_dir >> 5) & 1) && k == A.s2 - 1) ||
-            (((b.wall_per >> 2) & 1) && k == A.s2 - 1))
-          zero = true;
-      }
-      if (f != 1.0) v = v * f;
-      if (zero) v = 0.0;
-      v = v * (vxy * vol_axis(cz, Nz, k));
-      A.f[idx] = v;
-      bool in = dot_xy && !(((b.dot_wall & 16) && k == 2) || ((b.dot_wall & 32) && k == A.s2 - 1));
-      if (in) acc += p0 * v;
+      continue;
     }
-    pm = p0;
-    p0 = pp;
+    const double pm = pc[q], p0 = pc[q + 1], pp = pc[q + 2];
+    const Ax6 Z = axis_coef(g.c[2], Nz, k);
+    double gl = xm[q] * X.a1 + p0 * X.a2, gr = p0 * X.b1 + xp[q] * X.b2;
+    if (MODE == 1 && !Nx) { gl = gl * ld(kx.f + ix + q * szx); gr = gr * ld(kx.f + ix + q * szx + 1); }
+    double v = gl * X.o1 + gr * X.o2;
+    gl = ym[q] * Y.a1 + p0 * Y.a2;
+    gr = p0 * Y.b1 + yp[q] * Y.b2;
+    if (MODE == 1 && !Ny) { gl = gl * ld(ky.f + iy + q * szy); gr = gr * ld(ky.f + iy + q * szy + ky.s0); }
+    v = v + (gl * Y.o1 + gr * Y.o2);
+    gl = pm * Z.a1 + p0 * Z.a2;
+    gr = p0 * Z.b1 + pp * Z.b2;
+    if (MODE == 1 && !Nz) { gl = gl * ld(kz.f + iz + q * szz); gr = gr * ld(kz.f + iz + (q + 1) * szz); }
+    v = v + (gl * Z.o1 + gr * Z.o2);
+    if (MODE == 2) {
+      v = v * coeff;
+      v = v + p0;
+    }
+    double f = fxy;
+    bool zero = zxy;
+    wall_z(A, b, Nz, k, f, zero);
+    if (f != 1.0) v = v * f;
+    if (zero) v = 0.0;
+    v = v * (vxy * vol_axis(g.c[2], Nz, k));
+    A.f[idx] = v;
+    if (dxy && dot_z(A, b, k)) acc += p0 * v;
   }
   return acc;
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kTX* kTY) k_l_lap(FComp Ap, FComp P, DGrid g, FBC b0, FBC b1, FBC b2, DF kx, DF ky,
-                                                     DF kz, double coeff, int nkc, PcgScalars* S, double* partial,
-                                                     unsigned* ticket) {
+__global__ void __launch_bounds__(kLB, 2) k_l_lap(FComp Ap, FComp P, DGrid g, FBC b0, FBC b1, FBC b2, DF kx, DF ky,
+                                                DF kz, double coeff, unsigned npb, unsigned nkc, PcgScalars* S,
+                                                double* partial, unsigned* ticket) {
   if (S->done) return;
-  int c = blockIdx.z / nkc;
-  int k0 = (blockIdx.z - c * nkc) * kKC + 1;
+  const unsigned nwork = npb * nkc * (unsigned)Ap.nc;
   double acc = 0.0;
-  if (c == 0) acc = lap_column<MODE>(Ap.f[0], P.f[0], b0, g, kx, ky, kz, coeff, k0, min(k0 + kKC - 1, Ap.f[0].s2));
-  else if (c == 1) acc = lap_column<MODE>(Ap.f[1], P.f[1], b1, g, kx, ky, kz, coeff, k0, min(k0 + kKC - 1, Ap.f[1].s2));
-  else acc = lap_column<MODE>(Ap.f[2], P.f[2], b2, g, kx, ky, kz, coeff, k0, min(k0 + kKC - 1, Ap.f[2].s2));
+  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const Item it = item_of<kKC>(w, npb, nkc);
+    if (it.c == 0)
+      acc += lap_column<MODE>(Ap.f[0], P.f[0], b0, g, kx, ky, kz, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[0].s2));
+    else if (it.c == 1)
+      acc += lap_column<MODE>(Ap.f[1], P.f[1], b1, g, kx, ky, kz, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[1].s2));
+    else
+      acc += lap_column<MODE>(Ap.f[2], P.f[2], b2, g, kx, ky, kz, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[2].s2));
+  }
   finish_alpha(acc, S, partial, ticket);
 }
 
@@ -158,156 +281,212 @@ __global__ void __launch_bounds__(kTX* kTY) k_l_lap(FComp Ap, FComp P, DGrid g, 
 // (curl_SF with del assign/subtract: the CC->N passes are 0 at their end nodes)
 template <int L>
 __device__ __forceinline__ void curl_sig_column(const DF& E, const DF& pa, const DF& pb, const DF& sg, const DGrid& g,
-                                                int k0, int k1) {
+                                                unsigned blk, int k0, int k1) {
   constexpr int da = L == 0 ? 2 : (L == 1 ? 3 : 1);
   constexpr int db = L == 0 ? 3 : (L == 1 ? 1 : 2);
-  Col cl = col_of(E);
+  Col cl = col_of(E, blk);
   if (!cl.ok) return;
   const int i = cl.i, j = cl.j;
   const DCoord& ca = g.c[da - 1];
   const DCoord& cb = g.c[db - 1];
   const size_t stride_a = da == 1 ? 1 : (da == 2 ? (size_t)pa.s0 : (size_t)pa.s0 * pa.s1);
   const size_t stride_b = db == 1 ? 1 : (db == 2 ? (size_t)pb.s0 : (size_t)pb.s0 * pb.s1);
-  for (int k = k0; k <= k1; k++) {
-    int ta = da == 1 ? i : (da == 2 ? j : k);
-    int tb = db == 1 ? i : (db == 2 ? j : k);
-    double v = 0.0;
+  double va[kKC], vb[kKC], sv[kKC];
+#pragma unroll
+  for (int q = 0; q < kKC; q++) {
+    const int k = k0 + q;
+    va[q] = 0.0;
+    vb[q] = 0.0;
+    sv[q] = 0.0;
+    if (k > k1) continue;
+    const int ta = da == 1 ? i : (da == 2 ? j : k);
+    const int tb = db == 1 ? i : (db == 2 ? j : k);
     if (!(ta == 1 || ta == E.s(da))) {
       size_t ia = pa.at(i, j, k);
-      v = pa.f[ia - stride_a] * ca.cc2nD[ta - 1] + pa.f[ia] * ca.cc2nU[ta - 1];
+      va[q] = ld(pa.f + ia - stride_a) * ca.cc2nD[ta - 1] + ld(pa.f + ia) * ca.cc2nU[ta - 1];
     }
-    if (tb == 1 || tb == E.s(db)) v = 0.0;
-    else {
+    if (!(tb == 1 || tb == E.s(db))) {
       size_t ib = pb.at(i, j, k);
-      v = v - (pb.f[ib - stride_b] * cb.cc2nD[tb - 1] + pb.f[ib] * cb.cc2nU[tb - 1]);
+      vb[q] = ld(pb.f + ib - stride_b) * cb.cc2nD[tb - 1] + ld(pb.f + ib) * cb.cc2nU[tb - 1];
     }
-    E(i, j, k) = v * sg(i, j, k);
+    sv[q] = ld(sg.f + sg.at(i, j, k));
+  }
+#pragma unroll
+  for (int q = 0; q < kKC; q++) {
+    const int k = k0 + q;
+    if (k > k1) break;
+    const int tb = db == 1 ? i : (db == 2 ? j : k);
+    double v = (tb == 1 || tb == E.s(db)) ? 0.0 : va[q] - vb[q];
+    E(i, j, k) = v * sv[q];
   }
 }
-__global__ void __launch_bounds__(kTX* kTY) k_l_curl_sig(DF E0, DF E1, DF E2, FComp P, DF s0, DF s1, DF s2, DGrid g,
-                                                          int nkc, PcgScalars* S) {
+__global__ void __launch_bounds__(kLB) k_l_curl_sig(DF E0, DF E1, DF E2, FComp P, DF s0, DF s1, DF s2, DGrid g,
+                                                     unsigned npb, unsigned nkc, PcgScalars* S) {
   if (S->done) return;
-  int l = blockIdx.z / nkc;
-  int k0 = (blockIdx.z - l * nkc) * kKC + 1;
-  if (l == 0) curl_sig_column<0>(E0, P.f[2], P.f[1], s0, g, k0, min(k0 + kKC - 1, E0.s2));
-  else if (l == 1) curl_sig_column<1>(E1, P.f[0], P.f[2], s1, g, k0, min(k0 + kKC - 1, E1.s2));
-  else curl_sig_column<2>(E2, P.f[1], P.f[0], s2, g, k0, min(k0 + kKC - 1, E2.s2));
+  const unsigned nwork = npb * nkc * 3u;
+  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const Item it = item_of<kKC>(w, npb, nkc);
+    if (it.c == 0) curl_sig_column<0>(E0, P.f[2], P.f[1], s0, g, it.pb, it.k0, min(it.k0 + kKC - 1, E0.s2));
+    else if (it.c == 1) curl_sig_column<1>(E1, P.f[0], P.f[2], s1, g, it.pb, it.k0, min(it.k0 + kKC - 1, E1.s2));
+    else curl_sig_column<2>(E2, P.f[1], P.f[0], s2, g, it.pb, it.k0, min(it.k0 + kKC - 1, E2.s2));
+  }
 }
 // Ap_c = vol*mask(coeff*curl_c(E) + p) and p.Ap (edges -> faces: N->CC passes)
 template <int C>
 __device__ __forceinline__ double curl_ap_column(const DF& A, const DF& p, const FBC& b, const DF& Ea, const DF& Eb,
-                                                 const DGrid& g, double coeff, int k0, int k1) {
+                                                 const DGrid& g, double coeff, unsigned pb, int k0, int k1) {
   constexpr int da = C == 0 ? 2 : (C == 1 ? 3 : 1);
   constexpr int db = C == 0 ? 3 : (C == 1 ? 1 : 2);
-  Col cl = col_of(A);
+  Col cl = col_of(A, pb);
   if (!cl.ok) return 0.0;
   const int i = cl.i, j = cl.j;
-  double acc = 0.0;
   const DCoord& ca = g.c[da - 1];
   const DCoord& cb = g.c[db - 1];
   const size_t stride_a = da == 1 ? 1 : (da == 2 ? (size_t)Ea.s0 : (size_t)Ea.s0 * Ea.s1);
   const size_t stride_b = db == 1 ? 1 : (db == 2 ? (size_t)Eb.s0 : (size_t)Eb.s0 * Eb.s1);
   const bool Nx = n_along(A.dl, 1), Ny = n_along(A.dl, 2), Nz = n_along(A.dl, 3);
-  for (int k = k0; k <= k1; k++) {
-    bool ghost = cl.gij || k == 1 || k == A.s2;
+  double e0[kKC], e1[kKC], f0[kKC], f1[kKC], pv[kKC];
+#pragma unroll
+  for (int q = 0; q < kKC; q++) {
+    const int k = k0 + q;
+    const bool in = k <= k1 && !(cl.gij || k == 1 || k == A.s2);
+    e0[q] = e1[q] = f0[q] = f1[q] = pv[q] = 0.0;
+    if (in) {
+      size_t ia = Ea.at(i, j, k), ib = Eb.at(i, j, k);
+      e0[q] = ld(Ea.f + ia);
+      e1[q] = ld(Ea.f + ia + stride_a);
+      f0[q] = ld(Eb.f + ib);
+      f1[q] = ld(Eb.f + ib + stride_b);
+      pv[q] = ld(p.f + p.at(i, j, k));
+    }
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int q = 0; q < kKC; q++) {
+    const int k = k0 + q;
+    if (k > k1) break;
+    const bool ghost = cl.gij || k == 1 || k == A.s2;
     double v = 0.0;
     if (!ghost) {
-      int ta = da == 1 ? i : (da == 2 ? j : k);
-      int tb = db == 1 ? i : (db == 2 ? j : k);
-      size_t ia = Ea.at(i, j, k), ib = Eb.at(i, j, k);
-      double w = Ea.f[ia] * ca.n2ccD[ta] + Ea.f[ia + stride_a] * ca.n2ccU[ta];
-      w = w - (Eb.f[ib] * cb.n2ccD[tb] + Eb.f[ib + stride_b] * cb.n2ccU[tb]);
+      const int ta = da == 1 ? i : (da == 2 ? j : k);
+      const int tb = db == 1 ? i : (db == 2 ? j : k);
+      double w = e0[q] * ca.n2ccD[ta] + e1[q] * ca.n2ccU[ta];
+      w = w - (f0[q] * cb.n2ccD[tb] + f1[q] * cb.n2ccU[tb]);
       w = w * coeff;
-      double p0 = p(i, j, k);
-      w = w + p0;
+      w = w + pv[q];
       bool zero;
       double f = wall_fac(A, b, i, j, k, zero);
       if (f != 1.0) w = w * f;
       if (zero) w = 0.0;
       v = w * ((vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j)) * vol_axis(g.c[2], Nz, k));
-      if (in_dot(A, i, j, k, b.dot_wall)) acc += p0 * v;
+      if (in_dot(A, i, j, k, b.dot_wall)) acc += pv[q] * v;
     }
     A(i, j, k) = v;
   }
   return acc;
 }
-__global__ void __launch_bounds__(kTX* kTY) k_l_curl_ap(FComp Ap, FComp P, DF E0, DF E1, DF E2, DGrid g, FBC b0,
-                                                         FBC b1, FBC b2, double coeff, int nkc, PcgScalars* S,
-                                                         double* partial, unsigned* ticket) {
+__global__ void __launch_bounds__(kLB) k_l_curl_ap(FComp Ap, FComp P, DF E0, DF E1, DF E2, DGrid g, FBC b0, FBC b1,
+                                                    FBC b2, double coeff, unsigned npb, unsigned nkc, PcgScalars* S,
+                                                    double* partial, unsigned* ticket) {
   if (S->done) return;
-  int c = blockIdx.z / nkc;
-  int k0 = (blockIdx.z - c * nkc) * kKC + 1;
-  double acc;
-  if (c == 0) acc = curl_ap_column<0>(Ap.f[0], P.f[0], b0, E2, E1, g, coeff, k0, min(k0 + kKC - 1, Ap.f[0].s2));
-  else if (c == 1) acc = curl_ap_column<1>(Ap.f[1], P.f[1], b1, E0, E2, g, coeff, k0, min(k0 + kKC - 1, Ap.f[1].s2));
-  else acc = curl_ap_column<2>(Ap.f[2], P.f[2], b2, E1, E0, g, coeff, k0, min(k0 + kKC - 1, Ap.f[2].s2));
+  const unsigned nwork = npb * nkc * 3u;
+  double acc = 0.0;
+  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const Item it = item_of<kKC>(w, npb, nkc);
+    if (it.c == 0)
+      acc += curl_ap_column<0>(Ap.f[0], P.f[0], b0, E2, E1, g, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[0].s2));
+    else if (it.c == 1)
+      acc += curl_ap_column<1>(Ap.f[1], P.f[1], b1, E0, E2, g, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[1].s2));
+    else
+      acc += curl_ap_column<2>(Ap.f[2], P.f[2], b2, E1, E0, g, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[2].s2));
+  }
   finish_alpha(acc, S, partial, ticket);
 }
 
 // ---- K2: x += alpha p ; r -= alpha Ap ; r.r, z.r ; exit test ; beta --------------
+// (KC planes per thread: the pointwise steps can afford more loads in flight)
+template <int KC = kKC>
 __device__ __forceinline__ void update_column(const DF& x, const DF& p, const DF& r, const DF& Ap, const DF& M,
                                               const FBC& b, const DGrid& g, int mm, double coeff, double alpha,
-                                              int k0, int k1, double& arr, double& azr) {
-  Col cl = col_of(x);
+                                              unsigned pb, int k0, int k1, double& arr, double& azr) {
+  Col cl = col_of(x, pb);
   if (!cl.ok) return;
   const int i = cl.i, j = cl.j;
   const bool Nx = n_along(x.dl, 1), Ny = n_along(x.dl, 2), Nz = n_along(x.dl, 3);
-  const bool inxy = !cl.gij && !(((b.dot_wall & 1) && i == 2) || ((b.dot_wall & 2) && i == x.s0 - 1) ||
-                                 ((b.dot_wall & 4) && j == 2) || ((b.dot_wall & 8) && j == x.s1 - 1));
+  const bool inxy = !cl.gij && dot_xy(x, b, i, j);
+  const size_t sz = (size_t)x.s0 * x.s1;
+  const size_t idx0 = x.at(i, j, k0);
+  double xv[KC], pv[KC], rv[KC], av[KC], mv[KC];
+#pragma unroll
+  for (int q = 0; q < KC; q++) {
+    const bool in = k0 + q <= k1;
+    const size_t idx = idx0 + (size_t)q * sz;
+    xv[q] = in ? x.f[idx] : 0.0;
+    pv[q] = in ? ld(p.f + idx) : 0.0;
+    rv[q] = in ? r.f[idx] : 0.0;
+    av[q] = in ? ld(Ap.f + idx) : 0.0;
+    mv[q] = (in && mm == 0) ? ld(M.f + idx) : 0.0;
+  }
   double dxy = 0.0, vxy = 0.0;
   if (mm != 0 && !cl.gij) {
     dxy = diag_axis(g.c[0], Nx, i) + diag_axis(g.c[1], Ny, j);
     vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
   }
-  const size_t sz = (size_t)x.s0 * x.s1;
-  size_t idx = x.at(i, j, k0);
-  for (int k = k0; k <= k1; k++, idx += sz) {
-    x.f[idx] = x.f[idx] + p.f[idx] * alpha;
-    double rv = r.f[idx] + Ap.f[idx] * (-alpha);
-    r.f[idx] = rv;
-    bool in = inxy && k != 1 && k != x.s2 && !(((b.dot_wall & 16) && k == 2) || ((b.dot_wall & 32) && k == x.s2 - 1));
-    if (in) {
-      double mv;
-      if (mm == 0) mv = M.f[idx];
-      else {
+#pragma unroll
+  for (int q = 0; q < KC; q++) {
+    const int k = k0 + q;
+    if (k > k1) break;
+    const size_t idx = idx0 + (size_t)q * sz;
+    x.f[idx] = xv[q] + pv[q] * alpha;
+    const double rn = rv[q] + av[q] * (-alpha);
+    r.f[idx] = rn;
+    if (inxy && k != 1 && k != x.s2 && dot_z(x, b, k)) {
+      double m = mv[q];
+      if (mm != 0) {
         double d = dxy + diag_axis(g.c[2], Nz, k);
         if (mm == 2) {
           d = d * coeff;
           d = d + 1.0;
         }
-        mv = 1.0 / (d * (vxy * vol_axis(g.c[2], Nz, k)));
+        m = 1.0 / (d * (vxy * vol_axis(g.c[2], Nz, k)));
       }
-      double zv = mv * rv;
-      arr += rv * rv;
-      azr += zv * rv;
+      const double zv = m * rn;
+      arr += rn * rn;
+      azr += zv * rn;
     }
   }
 }
-__global__ void __launch_bounds__(kTX* kTY) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, DGrid g, int mm,
-                                                        double coeff, FBC b0, FBC b1, FBC b2, int nkc, PcgScalars* S,
-                                                        double* partial, unsigned* ticket) {
+template <int KC>
+__global__ void __launch_bounds__(kLB) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, DGrid g, int mm,
+                                                   double coeff, FBC b0, FBC b1, FBC b2, unsigned npb, unsigned nkc,
+                                                   PcgScalars* S, double* partial, unsigned* ticket) {
   if (S->done) return;
-  int c = blockIdx.z / nkc;
-  int k0 = (blockIdx.z - c * nkc) * kKC + 1;
+  const unsigned nwork = npb * nkc * (unsigned)X.nc;
   double arr = 0.0, azr = 0.0;
-  double alpha = S->alpha;
-  if (c == 0)
-    update_column(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, g, mm, coeff, alpha, k0, min(k0 + kKC - 1, X.f[0].s2), arr, azr);
-  else if (c == 1)
-    update_column(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, g, mm, coeff, alpha, k0, min(k0 + kKC - 1, X.f[1].s2), arr, azr);
-  else
-    update_column(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, g, mm, coeff, alpha, k0, min(k0 + kKC - 1, X.f[2].s2), arr, azr);
-  double s_rr = block_sum(arr);
-  double s_zr = block_sum(azr);
-  unsigned fb = flat_block(), nb = n_blocks();
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
+  const double alpha = S->alpha;
+  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const Item it = item_of<KC>(w, npb, nkc);
+    if (it.c == 0)
+      update_column<KC>(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, g, mm, coeff, alpha, it.pb, it.k0,
+                        min(it.k0 + KC - 1, X.f[0].s2), arr, azr);
+    else if (it.c == 1)
+      update_column<KC>(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, g, mm, coeff, alpha, it.pb, it.k0,
+                        min(it.k0 + KC - 1, X.f[1].s2), arr, azr);
+    else
+      update_column<KC>(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, g, mm, coeff, alpha, it.pb, it.k0,
+                        min(it.k0 + KC - 1, X.f[2].s2), arr, azr);
+  }
+  const double s_rr = block_sum(arr);
+  const double s_zr = block_sum(azr);
+  const unsigned fb = flat_block(), nb = n_blocks();
+  if (threadIdx.x == 0) {
     partial[fb] = s_rr;
     partial[nb + fb] = s_zr;
   }
   if (last_block_any(ticket)) {
-    double rr = sum_partials(partial, nb);
-    double zr = sum_partials(partial + nb, nb);
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const double rr = sum_partials(partial, nb);
+    const double zr = sum_partials(partial + nb, nb);
+    if (threadIdx.x == 0) {
       *ticket = 0;
       S->rr = rr;
       S->zr = zr;
@@ -315,11 +494,11 @@ __global__ void __launch_bounds__(kTX* kTY) k_l_update(FComp X, FComp P, FComp R
       S->iter_total += 1;
       bool stop = false;
       if (S->iter % S->nskip == 0) {
-        double res = sqrt(fabs(rr));
+        const double res = sqrt(fabs(rr));
         S->res = res;
-        bool e1 = res / S->res0 < S->tol_rel;
-        bool e2 = res < S->tol_abs;
-        bool e3 = S->iter >= S->iter_max;
+        const bool e1 = res / S->res0 < S->tol_rel;
+        const bool e2 = res < S->tol_abs;
+        const bool e3 = S->iter >= S->iter_max;
         if (e1 || e2 || e3) {
           stop = true;
           S->exit_reason = e1 ? 1 : (e2 ? 2 : 3);
@@ -437,36 +616,52 @@ __device__ __forceinline__ double pnew_at(const DF& p, const DF& r, const DF& M,
 // The new p of a source point is needed by the BC points that copy it, while
 // that source's own thread overwrites p: the kernel therefore reads p_old
 // from `p` and writes `pn` (the two buffers swap every iteration).
+template <int KC = kKC, bool BC = true>
 __device__ __forceinline__ void pupd_column(const DF& p, const DF& pn, const DF& r, const DF& M, const FBC& b,
-                                            const DGrid& g, int mm, double coeff, double beta, int k0, int k1) {
-  Col cl = col_of(p);
+                                            const DGrid& g, int mm, double coeff, double beta, unsigned pb, int k0,
+                                            int k1) {
+  Col cl = col_of(p, pb);
   if (!cl.ok) return;
   const int i = cl.i, j = cl.j;
   const bool Nx = n_along(p.dl, 1), Ny = n_along(p.dl, 2), Nz = n_along(p.dl, 3);
   // columns next to a boundary (or with special boundary nodes) take the general path
-  bool edge_xy = cl.gij || (Nx && (i == 2 || i == p.s0 - 1)) || (Ny && (j == 2 || j == p.s1 - 1));
+  const bool edge_xy = cl.gij || (Nx && (i == 2 || i == p.s0 - 1)) || (Ny && (j == 2 || j == p.s1 - 1));
+  const size_t sz = (size_t)p.s0 * p.s1;
+  const size_t idx0 = p.at(i, j, k0);
+  double pv[KC], rv[KC], mv[KC];
+#pragma unroll
+  for (int q = 0; q < KC; q++) {
+    const bool in = k0 + q <= k1;
+    const size_t idx = idx0 + (size_t)q * sz;
+    pv[q] = in ? ld(p.f + idx) : 0.0;
+    rv[q] = in ? ld(r.f + idx) : 0.0;
+    mv[q] = (in && mm == 0) ? ld(M.f + idx) : 0.0;
+  }
   double dxy = 0.0, vxy = 0.0;
   if (mm != 0 && !cl.gij) {
     dxy = diag_axis(g.c[0], Nx, i) + diag_axis(g.c[1], Ny, j);
     vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
   }
-  const size_t sz = (size_t)p.s0 * p.s1;
-  size_t idx = p.at(i, j, k0);
-  for (int k = k0; k <= k1; k++, idx += sz) {
-    bool special = edge_xy || k == 1 || k == p.s2 || (Nz && (k == 2 || k == p.s2 - 1));
+#pragma unroll
+  for (int q = 0; q < KC; q++) {
+    const int k = k0 + q;
+    if (k > k1) break;
+    const size_t idx = idx0 + (size_t)q * sz;
+    const bool special = BC && (edge_xy || k == 1 || k == p.s2 || (Nz && (k == 2 || k == p.s2 - 1)));
     if (!special || !b.defined) {
-      double mv;
-      if (mm == 0) mv = M.f[idx];
-      else if (cl.gij || k == 1 || k == p.s2) mv = 0.0;
-      else {
-        double d = dxy + diag_axis(g.c[2], Nz, k);
-        if (mm == 2) {
-          d = d * coeff;
-          d = d + 1.0;
+      double m = mv[q];
+      if (mm != 0) {
+        if (cl.gij || k == 1 || k == p.s2) m = 0.0;
+        else {
+          double d = dxy + diag_axis(g.c[2], Nz, k);
+          if (mm == 2) {
+            d = d * coeff;
+            d = d + 1.0;
+          }
+          m = 1.0 / (d * (vxy * vol_axis(g.c[2], Nz, k)));
         }
-        mv = 1.0 / (d * (vxy * vol_axis(g.c[2], Nz, k)));
       }
-      pn.f[idx] = p.f[idx] * beta + mv * r.f[idx];
+      pn.f[idx] = pv[q] * beta + m * rv[q];
     } else {
       Src s = src_of(p, b, i, j, k);
       double v = 0.0;
@@ -479,15 +674,77 @@ __device__ __forceinline__ void pupd_column(const DF& p, const DF& pn, const DF&
     }
   }
 }
-__global__ void __launch_bounds__(kTX* kTY) k_l_pupd(FComp P, FComp Pn, FComp R, FComp M, DGrid g, int mm,
-                                                      double coeff, FBC b0, FBC b1, FBC b2, int nkc, PcgScalars* S) {
+// K3 without BC values (those come from k_l_bcfill afterwards)
+template <int KC>
+__global__ void __launch_bounds__(kLB) k_l_pupd(FComp P, FComp Pn, FComp R, FComp M, DGrid g, int mm, double coeff,
+                                                 FBC b0, FBC b1, FBC b2, unsigned npb, unsigned nkc, PcgScalars* S) {
   if (S->done) return;
-  int c = blockIdx.z / nkc;
-  int k0 = (blockIdx.z - c * nkc) * kKC + 1;
-  double beta = S->beta;
-  if (c == 0) pupd_column(P.f[0], Pn.f[0], R.f[0], M.f[0], b0, g, mm, coeff, beta, k0, min(k0 + kKC - 1, P.f[0].s2));
-  else if (c == 1) pupd_column(P.f[1], Pn.f[1], R.f[1], M.f[1], b1, g, mm, coeff, beta, k0, min(k0 + kKC - 1, P.f[1].s2));
-  else pupd_column(P.f[2], Pn.f[2], R.f[2], M.f[2], b2, g, mm, coeff, beta, k0, min(k0 + kKC - 1, P.f[2].s2));
+  const unsigned nwork = npb * nkc * (unsigned)P.nc;
+  const double beta = S->beta;
+  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const Item it = item_of<KC>(w, npb, nkc);
+    if (it.c == 0)
+      pupd_column<KC, false>(P.f[0], Pn.f[0], R.f[0], M.f[0], b0, g, mm, coeff, beta, it.pb, it.k0,
+                             min(it.k0 + KC - 1, P.f[0].s2));
+    else if (it.c == 1)
+      pupd_column<KC, false>(P.f[1], Pn.f[1], R.f[1], M.f[1], b1, g, mm, coeff, beta, it.pb, it.k0,
+                             min(it.k0 + KC - 1, P.f[1].s2));
+    else
+      pupd_column<KC, false>(P.f[2], Pn.f[2], R.f[2], M.f[2], b2, g, mm, coeff, beta, it.pb, it.k0,
+                             min(it.k0 + KC - 1, P.f[2].s2));
+  }
+}
+
+// p's implicit BC values (apply_BCs_implicit, PCG_solver_algorithm.f90:70)
+// from the new p at their source points: every perimeter column of a plane
+// and the ghost / boundary-node planes of the inner columns.  Sources are
+// never points this kernel changes, so the order of the writes is free.
+__device__ __forceinline__ void bcfill_point(const DF& p, const FBC& b, int i, int j, int k) {
+  const Src s = src_of(p, b, i, j, k);
+  if (s.zero) {
+    p(i, j, k) = 0.0;
+    return;
+  }
+  if (s.I == i && s.J == j && s.K == k && s.fac == 1.0 && s.rc == 0.0) return;
+  double v = p(s.I, s.J, s.K);
+  if (s.rc != 0.0) v = v + p(s.rI, s.rJ, s.rK) * s.rc;
+  p(i, j, k) = s.fac * v;
+}
+__device__ __forceinline__ void bcfill_item(const DF& p, const FBC& b, unsigned r, unsigned npbP, unsigned nkc) {
+  if (!b.defined) return;
+  const PlaneSplit q = plane_split(p.s0, p.s1, p.dl);
+  const unsigned nPi = npbP * nkc;
+  if (r < nPi) {  // perimeter columns, every plane of one chunk
+    const unsigned kc = r / npbP, pp = r - kc * npbP;
+    if (pp >= q.npbP) return;
+    const Col cl = col_of(p, q.npbI + pp);
+    if (!cl.ok) return;
+    const int k0 = (int)kc * kKC + 1, k1 = min(k0 + kKC - 1, p.s2);
+    for (int k = k0; k <= k1; k++) bcfill_point(p, b, cl.i, cl.j, k);
+  } else {  // inner columns: ghost planes and node-located boundary planes
+    const unsigned pi = r - nPi;
+    if (pi >= q.npbI) return;
+    const Col cl = col_of(p, pi);
+    if (!cl.ok) return;
+    bcfill_point(p, b, cl.i, cl.j, 1);
+    bcfill_point(p, b, cl.i, cl.j, p.s2);
+    if (n_along(p.dl, 3)) {
+      bcfill_point(p, b, cl.i, cl.j, 2);
+      bcfill_point(p, b, cl.i, cl.j, p.s2 - 1);
+    }
+  }
+}
+__global__ void __launch_bounds__(kLB) k_l_bcfill(FComp P, FBC b0, FBC b1, FBC b2, unsigned npbP, unsigned npbI,
+                                                   unsigned nkc, PcgScalars* S) {
+  if (S->done) return;
+  const unsigned per = npbP * nkc + npbI;
+  const unsigned nwork = per * (unsigned)P.nc;
+  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const unsigned c = w / per, r = w - c * per;
+    if (c == 0) bcfill_item(P.f[0], b0, r, npbP, nkc);
+    else if (c == 1) bcfill_item(P.f[1], b1, r, npbP, nkc);
+    else bcfill_item(P.f[2], b2, r, npbP, nkc);
+  }
 }
 
 }  // namespace mg

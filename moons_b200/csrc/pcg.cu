@@ -2,18 +2,20 @@
 // every scalar of the recurrence kept on the device.
 //
 // modify_RHS (PCG_aux.f90:30-79) runs once per solve with the generic
-// kernels.  The iteration body is the lean K1/K2/K3 of lean.cuh (K1 is two
-// kernels for the curl-curl operator), two iterations per body.  The whole loop is captured once into
-// a CUDA graph whose WHILE node repeats the body until the device-side exit
-// flag is set; the flag also comes up when the iteration count reaches
-// iter_max, and the node stops after iter_max+2 body runs in any case, so the
-// loop always ends.
+// kernels.  The iteration is the lean kernels of lean.cuh (grid-stride, one
+// resident wave each); the loop is captured once into a CUDA graph whose
+// WHILE node repeats a two-iteration body until the device-side exit flag is
+// set (the flag also comes up at iter_max, and the node stops after
+// iter_max+2 body runs in any case, so the loop always ends).
+// MOONS_PCG_HOSTLOOP=1 launches the same kernels from the host instead (for
+// profilers); MOONS_PCG_MODE=persistent runs the loop as one cooperative
+// kernel with grid barriers (persist.cuh).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 
-#include "lean.cuh"
+#include "persist.cuh"
 #include "runtime.cuh"
 
 namespace mg {
@@ -138,12 +140,20 @@ __global__ void k_prec(DF M, DGrid g, int mode, double coeff, int comp, DF sx, D
   M(i, j, k) = 1.0 / (d * vol_at(g, M.dl, i, j, k));
 }
 
+
 __global__ void k_set_cond(cudaGraphConditionalHandle h, PcgScalars* S) {
   S->body_runs += 1;
   S->runs_total += 1;
   bool go = !S->done && S->body_runs < S->iter_max + 2;
   cudaGraphSetConditional(h, go ? 1u : 0u);
 }
+
+// grids of the lean kernels
+struct LeanGrids {
+  unsigned npb, nkc, nkcU, npbP, npbI, npbE, nkcE;
+  unsigned gA, gB, gC, gD, gE;
+  bool bc;
+};
 
 }  // namespace mg
 
@@ -168,7 +178,13 @@ struct moons_pcg {
   unsigned* ticket = nullptr;
   size_t max_blocks = 0;
   std::vector<void*> allocs;
-  // graph of the loop (rebuilt when x changes)
+  // persistent solver: grid barrier state, block partials, resident grid
+  GridSync* gs = nullptr;
+  double* ppart = nullptr;
+  unsigned coop_grid = 0;
+  // lean kernels: grids, and the CUDA graph of the loop (rebuilt when x changes)
+  int nsm = 0;
+  LeanGrids lg{};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double* gx[3] = {nullptr, nullptr, nullptr};
@@ -204,16 +220,15 @@ unsigned red_grid(const DF* a, int nc) {
   for (int c = 0; c < nc; c++) n += a[c].n();
   return (unsigned)std::min<size_t>(kRedBlocks, std::max<size_t>(1, (n + kBlock - 1) / kBlock));
 }
-// (i tile, j tile, k chunk x component) grid of the lean kernels
-dim3 lgrid(const DF* a, int nc, int* nkc) {
-  unsigned gx = 0, gy = 0, kz = 0;
+// (plane blocks, k chunks, component) grid of the lean kernels
+dim3 lgrid(const DF* a, int nc) {
+  unsigned npb = 0, kz = 0;
   for (int c = 0; c < nc; c++) {
-    gx = std::max(gx, (unsigned)((a[c].s0 + kTX - 1) / kTX));
-    gy = std::max(gy, (unsigned)((a[c].s1 + kTY - 1) / kTY));
+    const PlaneSplit q = plane_split(a[c].s0, a[c].s1, a[c].dl);
+    npb = std::max(npb, q.npbI + q.npbP);
     kz = std::max(kz, (unsigned)a[c].s2);
   }
-  *nkc = (int)((kz + kKC - 1) / kKC);
-  return dim3(gx, gy, (unsigned)(*nkc * nc));
+  return dim3(npb, (kz + kKC - 1) / kKC, (unsigned)nc);
 }
 // (plane chunk, k, component) grid covering nc fields
 dim3 fgrid(const DF* a, int nc) {
@@ -310,6 +325,18 @@ int minv_mode(const moons_pcg* s) {
 }
 
 // one PCG iteration (PCG_solver_algorithm.f90:69-96), enqueued on the mesh stream
+constexpr int kKCU = kKC;  // planes per thread of the pointwise kernels
+
+// grid of a grid-stride kernel: every block resident, at most one per item
+unsigned resident_grid(const moons_pcg* s, const void* kern, size_t items) {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLB, 0);
+  size_t g = (size_t)std::max(occ, 1) * (size_t)std::max(s->nsm, 1);
+  return (unsigned)std::max<size_t>(1, std::min(g, items));
+}
+
+// one PCG iteration (PCG_solver_algorithm.f90:69-96) as five grid-stride
+// kernels, twice: p -> p2 -> p (K3 reads one buffer and writes the other)
 int enqueue_iteration(moons_pcg* s, DF* x) {
   moons_mesh* m = s->m;
   FBC b[3];
@@ -317,46 +344,81 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
     int cc = c < s->nc ? c : 0;
     b[c] = fbc_of(s->x_bc[cc], s->xbc_bc[cc], s->x_dl[cc], s->Ax[cc]);
   }
-  int nkc = 0;
-  dim3 G = lgrid(s->Ax, s->nc, &nkc);
+  const LeanGrids& L = s->lg;
   unsigned* tA = s->ticket;
   unsigned* tB = s->ticket + 1;
   DF z0{};
   int mm = minv_mode(s);
-  const dim3 TB(kTX, kTY, 1);
-  // two iterations: p -> p2 -> p (K3 reads one buffer and writes the other)
+  const int nc = s->nc;
   for (int half = 0; half < 2; half++) {
     DF* pc = half == 0 ? s->p : s->p2;
     DF* pn = half == 0 ? s->p2 : s->p;
     switch (s->op) {
       case MOONS_OP_LAP_UNIFORM:
-        MG_LAUNCH(k_l_lap<0>, G, TB, m->stream, fc(s->Ax, s->nc), fc(pc, s->nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
-                  0.0, nkc, s->S, s->partial, tA);
+        MG_LAUNCH(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
+                  0.0, L.npb, L.nkc, s->S, s->partial, tA);
         break;
       case MOONS_OP_LAP_PROPS:
-        MG_LAUNCH(k_l_lap<1>, G, TB, m->stream, fc(s->Ax, s->nc), fc(pc, s->nc), m->dg, b[0], b[1], b[2], s->k[0],
-                  s->k[1], s->k[2], 0.0, nkc, s->S, s->partial, tA);
+        MG_LAUNCH(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], s->k[0],
+                  s->k[1], s->k[2], 0.0, L.npb, L.nkc, s->S, s->partial, tA);
         break;
       case MOONS_OP_MOM_DIFFUSION:
-        MG_LAUNCH(k_l_lap<2>, G, TB, m->stream, fc(s->Ax, s->nc), fc(pc, s->nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
-                  s->coeff, nkc, s->S, s->partial, tA);
+        MG_LAUNCH(k_l_lap<2>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
+                  s->coeff, L.npb, L.nkc, s->S, s->partial, tA);
         break;
-      case MOONS_OP_IND_DIFFUSION: {
-        int nke = 0;
-        dim3 GE = lgrid(s->tempk, 3, &nke);
-        MG_LAUNCH(k_l_curl_sig, GE, TB, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(pc, 3), s->k[0], s->k[1],
-                  s->k[2], m->dg, nke, s->S);
-        MG_LAUNCH(k_l_curl_ap, G, TB, m->stream, fc(s->Ax, 3), fc(pc, 3), s->tempk[0], s->tempk[1], s->tempk[2], m->dg,
-                  b[0], b[1], b[2], s->coeff, nkc, s->S, s->partial, tA);
-      } break;
+      case MOONS_OP_IND_DIFFUSION:
+        MG_LAUNCH(k_l_curl_sig, L.gE, kLB, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(pc, 3), s->k[0],
+                  s->k[1], s->k[2], m->dg, L.npbE, L.nkcE, s->S);
+        MG_LAUNCH(k_l_curl_ap, L.gA, kLB, m->stream, fc(s->Ax, 3), fc(pc, 3), s->tempk[0], s->tempk[1], s->tempk[2],
+                  m->dg, b[0], b[1], b[2], s->coeff, L.npb, L.nkc, s->S, s->partial, tA);
+        break;
     }
-    MG_LAUNCH(k_l_update, G, TB, m->stream, fc(x, s->nc), fc(pc, s->nc), fc(s->r, s->nc), fc(s->Ax, s->nc),
-              fc(s->Minv, s->nc), m->dg, mm, s->coeff, b[0], b[1], b[2], nkc, s->S, s->partial, tB);
-    MG_LAUNCH(k_l_pupd, G, TB, m->stream, fc(pc, s->nc), fc(pn, s->nc), fc(s->r, s->nc), fc(s->Minv, s->nc), m->dg, mm,
-              s->coeff, b[0], b[1], b[2], nkc, s->S);
+    MG_LAUNCH(k_l_update<kKCU>, L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc), fc(s->Ax, nc),
+              fc(s->Minv, nc), m->dg, mm, s->coeff, b[0], b[1], b[2], L.npb, L.nkcU, s->S, s->partial, tB);
+    MG_LAUNCH(k_l_pupd<kKCU>, L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc), fc(s->Minv, nc), m->dg, mm,
+              s->coeff, b[0], b[1], b[2], L.npb, L.nkcU, s->S);
+    if (L.bc)
+      MG_LAUNCH(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, nc), b[0], b[1], b[2], L.npbP, L.npbI, L.nkc, s->S);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
+}
+
+// sizes and grids of the lean kernels (set once at create)
+void plan_lean(moons_pcg* s) {
+  LeanGrids& L = s->lg;
+  const int nc = s->nc;
+  dim3 G = lgrid(s->Ax, nc);
+  L.npb = G.x;
+  L.nkc = G.y;
+  unsigned kz = G.y * kKC;
+  L.nkcU = (kz + kKCU - 1) / kKCU;
+  L.npbP = L.npbI = 0;
+  L.bc = false;
+  for (int c = 0; c < nc; c++) {
+    const PlaneSplit q = plane_split(s->Ax[c].s0, s->Ax[c].s1, s->Ax[c].dl);
+    L.npbP = std::max(L.npbP, q.npbP);
+    L.npbI = std::max(L.npbI, q.npbI);
+    if (s->x_bc[c].defined) L.bc = true;
+  }
+  const size_t items = (size_t)L.npb * L.nkc * nc;
+  const size_t itemsU = (size_t)L.npb * L.nkcU * nc;
+  const void* ka = s->op == MOONS_OP_LAP_UNIFORM ? (const void*)k_l_lap<0>
+                   : s->op == MOONS_OP_LAP_PROPS ? (const void*)k_l_lap<1>
+                   : s->op == MOONS_OP_MOM_DIFFUSION ? (const void*)k_l_lap<2>
+                                                    : (const void*)k_l_curl_ap;
+  L.gA = resident_grid(s, ka, items);
+  L.gB = resident_grid(s, (const void*)k_l_update<kKCU>, itemsU);
+  L.gC = resident_grid(s, (const void*)k_l_pupd<kKCU>, itemsU);
+  L.gD = resident_grid(s, (const void*)k_l_bcfill, ((size_t)L.npbP * L.nkc + L.npbI) * nc);
+  L.npbE = L.nkcE = 0;
+  L.gE = 1;
+  if (s->op == MOONS_OP_IND_DIFFUSION) {
+    dim3 GE = lgrid(s->tempk, 3);
+    L.npbE = GE.x;
+    L.nkcE = GE.y;
+    L.gE = resident_grid(s, (const void*)k_l_curl_sig, (size_t)GE.x * GE.y * 3);
+  }
 }
 
 int build_graph(moons_pcg* s, DF* x) {
@@ -394,6 +456,74 @@ int build_graph(moons_pcg* s, DF* x) {
   for (int c = 0; c < s->nc; c++) s->gx[c] = x[c].f;
   return MOONS_OK;
 }
+
+// the persistent kernel instance of an operator
+const void* persist_kernel(int op) {
+  switch (op) {
+    case MOONS_OP_LAP_UNIFORM: return (const void*)k_pcg_persist<0>;
+    case MOONS_OP_LAP_PROPS: return (const void*)k_pcg_persist<1>;
+    case MOONS_OP_MOM_DIFFUSION: return (const void*)k_pcg_persist<2>;
+    default: return (const void*)k_pcg_persist<3>;
+  }
+}
+
+// the whole loop as one cooperative launch (all blocks resident)
+int launch_persistent(moons_pcg* s, DF* x) {
+  moons_mesh* m = s->m;
+  PersistArgs a{};
+  a.X = fc(x, s->nc);
+  a.P0 = fc(s->p, s->nc);
+  a.P1 = fc(s->p2, s->nc);
+  a.R = fc(s->r, s->nc);
+  a.Ap = fc(s->Ax, s->nc);
+  a.M = fc(s->Minv, s->nc);
+  a.g = m->dg;
+  FBC b[3];
+  for (int c = 0; c < 3; c++) {
+    int cc = c < s->nc ? c : 0;
+    b[c] = fbc_of(s->x_bc[cc], s->xbc_bc[cc], s->x_dl[cc], s->Ax[cc]);
+  }
+  a.b0 = b[0];
+  a.b1 = b[1];
+  a.b2 = b[2];
+  a.k0 = s->k[0];
+  a.k1 = s->k[1];
+  a.k2 = s->k[2];
+  a.E0 = s->tempk[0];
+  a.E1 = s->tempk[1];
+  a.E2 = s->tempk[2];
+  a.coeff = s->coeff;
+  a.mm = minv_mode(s);
+  dim3 G = lgrid(s->Ax, s->nc);
+  a.npb = G.x;
+  a.nkc = G.y;
+  a.nkcB = (G.y * kKC + kKCB - 1) / kKCB;
+  a.npbE = a.nkcE = 0;
+  if (s->op == MOONS_OP_IND_DIFFUSION) {
+    dim3 GE = lgrid(s->tempk, 3);
+    a.npbE = GE.x;
+    a.nkcE = GE.y;
+  }
+  a.S = s->S;
+  a.part = s->ppart;
+  a.gs = s->gs;
+  MG_CUDA(cudaMemsetAsync(s->gs, 0, sizeof(GridSync), m->stream));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(s->coop_grid, 1, 1);
+  cfg.blockDim = dim3(kLB, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = m->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {&a};
+  MG_CUDA(cudaLaunchKernelExC(&cfg, persist_kernel(s->op), args));
+  ++g_launch_count;
+  return MOONS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -461,13 +591,12 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     }
   }
   if (!r) {
-    int nk1 = 0, nk2 = 0;
-    dim3 G = lgrid(s->Ax, nc, &nk1);
+    dim3 G = lgrid(s->Ax, nc);
     size_t nb = (size_t)G.x * G.y * G.z;
     dim3 G2 = fgrid(s->Ax, nc);
     nb = std::max(nb, (size_t)G2.x * G2.y * G2.z);
     if (needk) {
-      dim3 GE = lgrid(s->tempk, 3, &nk2);
+      dim3 GE = lgrid(s->tempk, 3);
       nb = std::max(nb, (size_t)GE.x * GE.y * GE.z);
     }
     s->max_blocks = nb;
@@ -488,6 +617,36 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
       s->ticket = (unsigned*)p;
       s->allocs.push_back(p);
       cudaMemsetAsync(p, 0, sizeof(unsigned) * 4, m->stream);
+    }
+    // persistent solver: as many blocks as can be resident, at most one per work item
+    if (!r) {
+      int coop = 0, nsm = 0, occ = 0;
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m->device);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+      s->nsm = nsm;
+      plan_lean(s);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, persist_kernel(op), kLB, 0);
+      size_t items = (size_t)G.x * G.y * G.z;
+      if (needk && op == MOONS_OP_IND_DIFFUSION) {
+        dim3 GE = lgrid(s->tempk, 3);
+        items = std::max(items, (size_t)GE.x * GE.y * GE.z);
+      }
+      if (!coop || occ < 1 || nsm < 1) {
+        set_error("moons_pcg_create: the device cannot run the cooperative PCG kernel");
+        r = MOONS_ERR_CUDA;
+      } else {
+        s->coop_grid = (unsigned)std::min<size_t>((size_t)occ * nsm, items);
+      }
+    }
+    if (!r && cudaMalloc(&p, sizeof(GridSync)) != cudaSuccess) r = MOONS_ERR_NOMEM;
+    else if (!r) {
+      s->gs = (GridSync*)p;
+      s->allocs.push_back(p);
+    }
+    if (!r && cudaMalloc(&p, sizeof(double) * 3 * s->coop_grid) != cudaSuccess) r = MOONS_ERR_NOMEM;
+    else if (!r) {
+      s->ppart = (double*)p;
+      s->allocs.push_back(p);
     }
     if (!r && cudaMallocHost(&p, sizeof(PcgScalars)) != cudaSuccess) r = MOONS_ERR_NOMEM;
     else if (!r) s->hS = (PcgScalars*)p;
@@ -523,11 +682,11 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
 }
 
 int moons_pcg_destroy(moons_pcg* s) {
+  if (s && s->exec) cudaGraphExecDestroy(s->exec);
+  if (s && s->graph) cudaGraphDestroy(s->graph);
   if (!s) return MOONS_OK;
   cudaSetDevice(s->m->device);
   cudaStreamSynchronize(s->m->stream);
-  if (s->exec) cudaGraphExecDestroy(s->exec);
-  if (s->graph) cudaGraphDestroy(s->graph);
   for (void* p : s->allocs) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
   moons_mesh* m = s->m;
@@ -562,6 +721,7 @@ __global__ void k_pcg_clear_acc(PcgScalars* S) {
   S->iter_total = 0;
   S->runs_total = 0;
   S->nan_any = 0;
+  S->sync_err = 0;
 }
 }  // namespace mg
 
@@ -579,6 +739,10 @@ int mg_pcg_totals(moons_pcg* s, int* iters, int* nan_any, double* last_rel) {
   const PcgScalars& H = *s->hS;
   g_launch_count += s->body_launches * (long long)H.runs_total;
   *iters = H.iter_total;
+  if (H.sync_err) {
+    set_error("moons_pcg: a grid barrier of the persistent solver timed out");
+    return MOONS_ERR_CUDA;
+  }
   *nan_any = H.nan_any;
   if (last_rel) *last_rel = (H.res0 == 0.0) ? H.res : H.res / H.res0;
   return MOONS_OK;
@@ -649,9 +813,9 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
             &s->S->rhok, m->d_partial, m->d_ticket);
   MG_LAUNCH(k_pcg_start, 1, 1, m->stream, s->S);
   MG_CUDA(cudaGetLastError());
-  // ---- the loop.  MOONS_PCG_HOSTLOOP=1 launches the same kernels from the
-  // host in chunks of 32 iterations (kernels skip themselves once the exit
-  // flag is up): profilers cannot see kernels inside conditional graphs.
+  // ---- the loop.  MOONS_PCG_HOSTLOOP=1 launches the iteration as separate
+  // kernels from the host in chunks of 32 iterations (kernels skip
+  // themselves once the exit flag is up), so a profiler sees each step.
   static const bool hostloop = [] {
     const char* e = getenv("MOONS_PCG_HOSTLOOP");
     return e && e[0] == '1';
@@ -667,14 +831,23 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
     for (int c = 0; c < nc && !r; c++) r = launch_bcs(m, X[c], s->x_bc[c], false);
     return r;
   }
-  bool need_graph = !s->exec;
-  for (int c = 0; c < nc; c++)
-    if (s->gx[c] != X[c].f) need_graph = true;
-  if (need_graph) {
-    r = build_graph(s, X);
-    if (r) return r;
+  static const bool persist = [] {
+    const char* e = getenv("MOONS_PCG_MODE");
+    return e && strcmp(e, "persistent") == 0;
+  }();
+  if (persist) {
+    r = launch_persistent(s, X);
+  } else {
+    bool need_graph = !s->exec;
+    for (int c = 0; c < nc; c++)
+      if (s->gx[c] != X[c].f) need_graph = true;
+    if (need_graph) r = build_graph(s, X);
+    if (!r) {
+      cudaError_t e = cudaGraphLaunch(s->exec, m->stream);
+      if (e != cudaSuccess) r = cuda_fail(e, "cudaGraphLaunch");
+    }
   }
-  MG_CUDA(cudaGraphLaunch(s->exec, m->stream));
+  if (r) return r;
   // x: apply_BCs (the reference applies them after every update; they only
   // rewrite ghost/boundary entries, which no update reads)
   for (int c = 0; c < nc && !r; c++) r = launch_bcs(m, X[c], s->x_bc[c], false);
@@ -695,6 +868,10 @@ int mg_pcg_collect(moons_pcg* s, moons_solve_info* info, float ms) {
     info->rel = (H.res0 == 0.0) ? H.res : H.res / H.res0;
     info->exit_reason = H.exit_reason;
     info->ms = ms;
+  }
+  if (H.sync_err) {
+    set_error("moons_pcg_solve: a grid barrier of the persistent solver timed out");
+    return MOONS_ERR_CUDA;
   }
   if (H.nan || std::isnan(H.res0) || std::isnan(H.res)) {
     set_error("moons_pcg_solve: NaN in residual norms");
@@ -720,6 +897,7 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  mg_pcg_clear_totals(s);
   cudaEventRecord(e0, m->stream);
   int r = mg_pcg_enqueue(s, x, b, isp);
   cudaEventRecord(e1, m->stream);
