@@ -97,15 +97,22 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.out)}
 
 
-def dist_setup(n):
+def dist_setup(n, backend=None):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo for CPU tests.
+    Ranks are independent replicas: the only collectives are the barrier and
+    the max-over-ranks of the timings."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
+        import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         return rank, world, local, dist
     return rank, world, local, None
 
@@ -114,9 +121,15 @@ def max_over_ranks(v, dist):
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(world, steps, ms_max):
+    """Whole-job steps/s of `world` independent replicas (weak scaling)."""
+    return world * steps / (ms_max / 1e3)
 
 
 def poisson_ms(G, kw):
@@ -229,27 +242,27 @@ def main():
     if dist is not None:
         dist.barrier()
     ms = max_over_ranks(info["ms"], dist)
-    value = world * args.steps / (ms / 1e3)
+    value = replica_rate(world, args.steps, ms)
     du, db = sim.divergence()
 
-    # ---- end to end through the C-ABI with pinned host buffers: each step
-    # uploads the state (U, B) and downloads U.
-    ups = [sim.field(G.MHD_U, c) for c in range(3)] + [sim.field(G.MHD_B, c) for c in range(3)]
-    downs = [sim.field(G.MHD_U, c) for c in range(3)]
-    host_up = [torch.from_numpy(f.download().ravel(order="F").copy()).pin_memory() for f in ups]
-    host_dn = [torch.empty(f.n, dtype=torch.float64).pin_memory() for f in downs]
-    h2d = sum(f.n * 8 for f in ups)
-    d2h = sum(f.n * 8 for f in downs)
+    # ---- end to end through the C-ABI with pinned host buffers, as a host
+    # code driving the time loop: each step uploads the state (U, B) from the
+    # host, advances it, and downloads it back into the same host buffers,
+    # so the steps follow the simulation's own trajectory.
+    state = [sim.field(G.MHD_U, c) for c in range(3)] + [sim.field(G.MHD_B, c) for c in range(3)]
+    host = [torch.from_numpy(f.download().ravel(order="F").copy()).pin_memory() for f in state]
+    h2d = sum(f.n * 8 for f in state)
+    d2h = h2d
     ke = max(2, args.steps)
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(ke):
-        for f, h in zip(ups, host_up):
+        for f, h in zip(state, host):
             f.upload_ptr(h.data_ptr())
         sim.step(1)
-        for f, h in zip(downs, host_dn):
+        for f, h in zip(state, host):
             f.download_ptr(h.data_ptr())
     t_e2e = time.perf_counter() - t0
     t_e2e = max_over_ranks(t_e2e, dist)

@@ -1,0 +1,162 @@
+! moons_gpu_mod.f90 -- ISO_C_BINDING interfaces to include/moons_gpu.h.
+!
+! The module a Fortran host (the reference's solve_MOONS, init_mom,
+! init_induction, Euler_time_*, clean_div_*) uses to call the B200 library.
+! Every function returns an integer status (0 = OK); the caller decides
+! whether to stop, as the reference's own error paths do.  Arrays are passed
+! with c_loc of the contiguous grid_field array f(sx,sy,sz) for the duration
+! of the call only.  Written against the C header; it is not compiled in
+! this repository's build (no Fortran compiler in the image).
+module moons_gpu_mod
+  use, intrinsic :: iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: MOONS_OK = 0
+  integer(c_int), parameter :: MOONS_CC = 0, MOONS_FX = 1, MOONS_FY = 2, MOONS_FZ = 3
+  integer(c_int), parameter :: MOONS_EX = 4, MOONS_EY = 5, MOONS_EZ = 6, MOONS_NODE = 7
+  integer(c_int), parameter :: MOONS_BC_NONE = 0, MOONS_BC_DIRICHLET = 1, MOONS_BC_NEUMANN = 2
+  integer(c_int), parameter :: MOONS_BC_PERIODIC = 3, MOONS_BC_ROBIN = 4
+  integer(c_int), parameter :: MOONS_OP_LAP_UNIFORM = 1, MOONS_OP_LAP_PROPS = 2
+  integer(c_int), parameter :: MOONS_OP_IND_DIFFUSION = 3, MOONS_OP_MOM_DIFFUSION = 4
+  integer(c_int), parameter :: MOONS_PREC_IDENTITY = 0, MOONS_PREC_LAP = 1
+  integer(c_int), parameter :: MOONS_PREC_MOM = 2, MOONS_PREC_IND = 3
+
+  type, bind(C) :: moons_bc_spec
+    integer(c_int) :: type(6)
+    integer(c_int) :: prescribed(6)
+    real(c_double) :: value(6)
+    real(c_double) :: c_w(6)
+    integer(c_int) :: order(6)
+    integer(c_int) :: all_neumann
+  end type
+
+  type, bind(C) :: moons_isp
+    integer(c_int) :: iter_max
+    real(c_double) :: tol_rel
+    real(c_double) :: tol_abs
+    integer(c_int) :: n_skip_check_res
+  end type
+
+  type, bind(C) :: moons_solve_info
+    integer(c_int) :: iterations
+    real(c_double) :: res0, res, rel
+    integer(c_int) :: exit_reason
+    real(c_double) :: ms
+  end type
+
+  interface
+    function moons_last_error() bind(C, name="moons_last_error") result(p)
+      import :: c_ptr
+      type(c_ptr) :: p
+    end function
+
+    function moons_mesh_create(m, hn_x, sn_x, hn_y, sn_y, hn_z, sn_z, device) &
+        bind(C, name="moons_mesh_create") result(st)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr) :: m
+      real(c_double), intent(in) :: hn_x(*), hn_y(*), hn_z(*)
+      integer(c_int), value :: sn_x, sn_y, sn_z, device
+      integer(c_int) :: st
+    end function
+
+    function moons_mesh_destroy(m) bind(C, name="moons_mesh_destroy") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: m
+      integer(c_int) :: st
+    end function
+
+    function moons_sf_create(m, data_loc, f) bind(C, name="moons_sf_create") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: m
+      integer(c_int), value :: data_loc
+      type(c_ptr) :: f
+      integer(c_int) :: st
+    end function
+
+    function moons_sf_destroy(f) bind(C, name="moons_sf_destroy") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: f
+      integer(c_int) :: st
+    end function
+
+    function moons_sf_upload(f, host, n) bind(C, name="moons_sf_upload") result(st)
+      import :: c_ptr, c_int, c_double, c_long_long
+      type(c_ptr), value :: f
+      real(c_double), intent(in) :: host(*)
+      integer(c_long_long), value :: n
+      integer(c_int) :: st
+    end function
+
+    function moons_sf_download(f, host, n) bind(C, name="moons_sf_download") result(st)
+      import :: c_ptr, c_int, c_double, c_long_long
+      type(c_ptr), value :: f
+      real(c_double), intent(out) :: host(*)
+      integer(c_long_long), value :: n
+      integer(c_int) :: st
+    end function
+
+    function moons_sf_set_bcs(f, spec) bind(C, name="moons_sf_set_bcs") result(st)
+      import :: c_ptr, c_int, moons_bc_spec
+      type(c_ptr), value :: f
+      type(moons_bc_spec), intent(in) :: spec
+      integer(c_int) :: st
+    end function
+
+    function moons_apply_bcs(f) bind(C, name="moons_apply_bcs") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: f
+      integer(c_int) :: st
+    end function
+
+    function moons_grad(gx, gy, gz, u) bind(C, name="moons_grad") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: gx, gy, gz, u
+      integer(c_int) :: st
+    end function
+
+    function moons_div(out, ux, uy, uz) bind(C, name="moons_div") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: out, ux, uy, uz
+      integer(c_int) :: st
+    end function
+
+    function moons_curl(ox, oy, oz, ux, uy, uz) bind(C, name="moons_curl") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: ox, oy, oz, ux, uy, uz
+      integer(c_int) :: st
+    end function
+
+    function moons_pcg_create(m, op, prec, ncomp, x, x_bc, k, s) &
+        bind(C, name="moons_pcg_create") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: m
+      integer(c_int), value :: op, prec, ncomp
+      type(c_ptr), intent(in) :: x(*), x_bc(*), k(*)
+      type(c_ptr) :: s
+      integer(c_int) :: st
+    end function
+
+    function moons_pcg_update_mfp(s, coeff, upd) bind(C, name="moons_pcg_update_mfp") result(st)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: s
+      real(c_double), value :: coeff
+      integer(c_int), value :: upd
+      integer(c_int) :: st
+    end function
+
+    function moons_pcg_solve(s, x, b, isp, info) bind(C, name="moons_pcg_solve") result(st)
+      import :: c_ptr, c_int, moons_isp, moons_solve_info
+      type(c_ptr), value :: s
+      type(c_ptr), intent(in) :: x(*), b(*)
+      type(moons_isp), intent(in) :: isp
+      type(moons_solve_info), intent(out) :: info
+      integer(c_int) :: st
+    end function
+
+    function moons_pcg_destroy(s) bind(C, name="moons_pcg_destroy") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s
+      integer(c_int) :: st
+    end function
+  end interface
+end module moons_gpu_mod
