@@ -167,6 +167,24 @@ int moons_lap_var(moons_sf* out, const moons_sf* u, const moons_sf* kx,
  * along dir. */
 int moons_interp(moons_sf* out, const moons_sf* in, int dir);
 
+/* moons_lap_var without device allocation.  No counterpart in the
+ * reference: it exists for host codes that cannot allocate device memory at
+ * the point of the call (their own pool already holds the free memory, or
+ * they keep allocator traffic out of a timed loop).  Same result as
+ * moons_lap_var; the three face temporaries come from one built-in device
+ * array instead of the allocator.
+ *  - each temporary holds at most MOONS_LAP_VAR_NOALLOC_MAX_POINTS doubles;
+ *    larger fields are rejected with MOONS_ERR_LIMIT (use moons_lap_var);
+ *  - the first call on a device looks up the array on that device and does
+ *    nothing else on later calls: make the first call before any stream
+ *    capture;
+ *  - the array needs no initial contents (every element read is written
+ *    earlier in the same call);
+ *  - the array is shared per device: calls that overlap in time race. */
+#define MOONS_LAP_VAR_NOALLOC_MAX_POINTS 131072
+int moons_lap_var_noalloc(moons_sf* out, const moons_sf* u, const moons_sf* kx,
+                          const moons_sf* ky, const moons_sf* kz);
+
 /* ---- PCG (code/handwritten/PCG/PCG_solver_extend.f90:51-291,
  *      code/handwritten/solvers/PCG/PCG_solver_algorithm.f90:37-179) ------ */
 /* ncomp = 1 (SF) or 3 (VF).  x[] are the unknown's fields (their BCs are

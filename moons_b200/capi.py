@@ -183,6 +183,7 @@ def lib() -> C.CDLL:
             "moons_curl": (C.c_int, [_P, _P, _P, _P, _P, _P]),
             "moons_lap_centered": (C.c_int, [_P, _P]),
             "moons_lap_var": (C.c_int, [_P, _P, _P, _P, _P]),
+            "moons_lap_var_noalloc": (C.c_int, [_P, _P, _P, _P, _P]),
             "moons_interp": (C.c_int, [_P, _P, C.c_int]),
             "moons_pcg_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(_P), C.POINTER(_P),
                                            C.POINTER(_P), C.POINTER(_P)]),
@@ -317,6 +318,17 @@ def lap_centered(o: Field, u: Field):
 
 def lap_var(o: Field, u: Field, k: Sequence[Field]):
     _check(lib().moons_lap_var(o.h, u.h, k[0].h, k[1].h, k[2].h))
+
+
+def lap_var_noalloc(o: Field, u: Field, k: Sequence[Field]):
+    """lap_var without device allocation: the face temporaries come from a
+    built-in device array (at most LAP_VAR_NOALLOC_MAX_POINTS points each;
+    larger fields raise MoonsError with MOONS_ERR_LIMIT).  Calls that overlap
+    in time race on that array."""
+    _check(lib().moons_lap_var_noalloc(o.h, u.h, k[0].h, k[1].h, k[2].h))
+
+
+LAP_VAR_NOALLOC_MAX_POINTS = 131072
 
 
 def interp(o: Field, i: Field, d: int):

@@ -3,3 +3,4 @@
 #include "mesh.cu"
 #include "pcg.cu"
 #include "mhd.cu"
+#include "noalloc.cu"
