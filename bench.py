@@ -132,8 +132,10 @@ def replica_rate(world, steps, ms_max):
     return world * steps / (ms_max / 1e3)
 
 
-def poisson_ms(G, kw):
-    """Pressure-Poisson time to 1e-10 on the duct fluid mesh (random RHS)."""
+def poisson_ms(G, kw, prec=None):
+    """Pressure-Poisson time to 1e-10 on the duct fluid mesh (random RHS),
+    best of 3 solves from x = 0, with the given preconditioner (default the
+    reference's Jacobi prec_Lap)."""
     from moons_b200 import configs
     mom, _, prm, _ = configs.duct(**kw)
     m = G.Mesh(*mom)
@@ -141,13 +143,14 @@ def poisson_ms(G, kw):
     p.set_bcs(prm.bc_p)
     b = m.field(G.CC)
     b.upload(np.random.default_rng(7).standard_normal(b.shape))
-    s = G.PCG(m, G.OP_LAP_UNIFORM, G.PREC_LAP, [p], [p])
+    s = G.PCG(m, G.OP_LAP_UNIFORM, G.PREC_LAP if prec is None else prec, [p], [p])
     best = None
     for _ in range(3):
         p.fill(0.0)
         info = s.solve([p], [b], G.isp(200000, 1e-10, 1e-300))
         if best is None or info["ms"] < best["ms"]:
             best = info
+    s.close()
     return best, b.n
 
 
@@ -270,6 +273,8 @@ def main():
 
     # ---- Poisson ms to 1e-10 + roofline of the pressure PCG iteration
     pinfo, ncc = poisson_ms(G, kw)
+    mginfo, _ = poisson_ms(G, kw, G.PREC_MG)
+    mxinfo, _ = poisson_ms(G, kw, G.PREC_MG_MIXED)
     alg_bytes = 88.0 * ncc * pinfo["iterations"]  # 88 B per cell per FP64 PCG iteration (algorithmic)
     achieved = alg_bytes / (pinfo["ms"] / 1e3) / 1e9
     peaks = {}
@@ -303,7 +308,12 @@ def main():
             "per_step": {k: info[k] / max(args.steps, 1) for k in ("iters_U", "iters_p", "iters_B", "iters_phi")},
             "div_U_l2sq": du, "div_B_l2sq": db,
             "poisson": {"ms_to_1e-10": pinfo["ms"], "iterations": pinfo["iterations"], "rel": pinfo["rel"],
-                        "cells": ncc, "solver": "FP64 Jacobi-PCG"},
+                        "cells": ncc, "solver": "FP64 Jacobi-PCG (reference algorithm)",
+                        "mg_fp64": {"ms_to_1e-10": mginfo["ms"], "iterations": mginfo["iterations"],
+                                    "rel": mginfo["rel"], "solver": "CG + FP64 multigrid V(1,1)"},
+                        "mixed": {"ms_to_1e-10": mxinfo["ms"], "iterations": mxinfo["iterations"],
+                                  "rel": mxinfo["rel"], "solver": "FP64 flexible CG + FP32 multigrid V(1,1)"},
+                        "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"]},
             "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (duct fluid mesh)",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -101,7 +101,13 @@ enum {
   MOONS_PREC_IDENTITY = 0,    /* prec_Identity_SF/VF :27-51                  */
   MOONS_PREC_LAP = 1,         /* prec_Lap_SF/VF      :55-82                  */
   MOONS_PREC_MOM = 2,         /* prec_mom_SF/VF      :85-113                 */
-  MOONS_PREC_IND = 3          /* prec_ind_VF         :115-129                */
+  MOONS_PREC_IND = 3,         /* prec_ind_VF         :115-129                */
+  /* Multigrid V-cycle preconditioners (one CC unknown, LAP_UNIFORM or
+   * LAP_PROPS, Dirichlet/Neumann/periodic BCs).  The reference has the
+   * building blocks (GF_restrict.f90, GF_prolongate.f90, SOR.f90) but no
+   * compiled V-cycle (code_not_compiled/9.6.2017/MG/MG.f90:241-396). */
+  MOONS_PREC_MG = 4,          /* FP64 V-cycle inside CG                      */
+  MOONS_PREC_MG_MIXED = 5     /* FP32 V-cycle inside FP64 flexible CG         */
 };
 
 typedef struct moons_mesh moons_mesh;

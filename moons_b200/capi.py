@@ -25,6 +25,7 @@ CC, FX, FY, FZ, EX, EY, EZ, NODE = range(8)
 DIRICHLET, NEUMANN, PERIODIC, ROBIN = 1, 2, 3, 4
 OP_LAP_UNIFORM, OP_LAP_PROPS, OP_IND_DIFFUSION, OP_MOM_DIFFUSION = 1, 2, 3, 4
 PREC_IDENTITY, PREC_LAP, PREC_MOM, PREC_IND = 0, 1, 2, 3
+PREC_MG, PREC_MG_MIXED = 4, 5  # multigrid V-cycle in CG (FP64) / in flexible CG (FP32 V-cycle)
 
 
 class MoonsError(RuntimeError):

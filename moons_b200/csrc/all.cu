@@ -2,5 +2,6 @@
 // live in headers shared by the entry-point files).
 #include "mesh.cu"
 #include "pcg.cu"
+#include "mgpcg.cu"
 #include "mhd.cu"
 #include "noalloc.cu"

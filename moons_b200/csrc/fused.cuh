@@ -32,7 +32,6 @@ struct PcgScalars {
   int body_runs;  // executions of the loop body (second bound on the loop)
   // accumulated over solves until the host clears them
   int iter_total, runs_total, nan_any;
-  int sync_err;  // a grid-barrier wait of the persistent solver gave up (sticky)
 };
 
 // implicit BCs + masks of one unknown component, as the fused kernels see them

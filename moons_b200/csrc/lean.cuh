@@ -3,22 +3,22 @@
 // Same three steps as fused.cuh (K1 op+mask+vol+p.Ap -> alpha, K2 x/r update
 // + r.r, z.r -> exit test and beta, K3 p = beta p + Minv r), organised for
 // the memory system instead of for brevity:
-//  * a thread owns one (i,j) column of a plane and kKC consecutive planes in
-//    k; a block is 256 consecutive columns of the plane's inner set or of
-//    its perimeter ring (coalesced, no tile waste, no BC divergence among
-//    inner columns), the grid is (plane blocks, k chunks, component).  Per-column
-//    quantities (stencil coefficients, volumes, wall masks) are formed once
-//    per column; every load of the kKC planes is issued before the first
-//    result is formed, so each thread keeps several loads in flight;
-//  * K3 also writes p's homogeneous (implicit) BC values -- ghost planes,
+//  * a block owns 256 consecutive columns of the plane's inner set or of its
+//    perimeter ring (coalesced, no tile waste, no BC divergence among inner
+//    columns) and strides over the k chunks of kKC planes: grid = (plane
+//    blocks, k stride, component), sized to one resident wave.  Per-column
+//    quantities (index, stencil coefficients, volumes, wall masks) are
+//    formed once per thread; every load of a chunk is issued before its
+//    first result is formed, so each thread keeps several loads in flight;
+//  * p carries its homogeneous (implicit) BC values: K3 forms the new p at
+//    every point and k_l_bcfill rewrites the BC points -- ghost planes,
 //    Dirichlet boundary nodes (0), periodic boundary nodes (copy of node 2)
-//    -- computing the new value of each source point on the fly, so K1 and
-//    K2 read p raw, exactly as the reference's operator reads p after
-//    apply_BCs_implicit (which only ever writes these points, and only from
-//    one interior point each; edge and corner ghosts, which no interior
-//    stencil reads, are filled in a fixed order);
-//  * Minv of prec_Lap/prec_mom is rebuilt from per-axis tables
-//    (diag = (dx+dy)+dz, vol = (hx*hy)*hz) instead of being read.
+//    -- from their source points, so K1 and K2 read p raw, exactly as the
+//    reference's operator reads p after apply_BCs_implicit (which only ever
+//    writes these points, and only from one interior point each; edge and
+//    corner ghosts, which no interior stencil reads, are composed in a fixed
+//    order);
+//  * Minv is read, as the reference stores it (prec_* fill PCG%Minv once).
 #pragma once
 #include "fused.cuh"
 
@@ -94,30 +94,11 @@ __device__ __forceinline__ Col col_of(const DF& a, unsigned pb) {
   c.gij = c.i == 1 || c.i == a.s0 || c.j == 1 || c.j == a.s1;
   return c;
 }
-// work item w of a grid-stride loop -> (component, k chunk of KC planes,
-// plane block); consecutive items walk the plane blocks of one chunk
-struct Item {
-  unsigned pb;
-  int c, k0;
-};
-template <int KC>
-__device__ __forceinline__ Item item_of(unsigned w, unsigned npb, unsigned nkc) {
-  Item it;
-  const unsigned per = npb * nkc;
-  it.c = (int)(w / per);
-  const unsigned rem = w - (unsigned)it.c * per;
-  const unsigned kc = rem / npb;
-  it.pb = rem - kc * npb;
-  it.k0 = (int)kc * KC + 1;
-  return it;
-}
-
 // plain (coherent) loads: the persistent solver reads data other blocks
 // wrote earlier in the same launch, after a grid barrier
 __device__ __forceinline__ double ld(const double* p) { return *p; }
 
-// Minv on the fly (per-axis tables, same formula as k_prec's)
-MG_HD double diag_axis(const DCoord& c, bool N, int t) { return N ? c.diagN[t] : c.diagC[t]; }
+// cell-volume share of one axis (volume_DL_GF, GF_distributions.f90:61-88)
 MG_HD double vol_axis(const DCoord& c, bool N, int t) { return N ? c.dhc[t - 1] : c.dhn[t]; }
 
 // wall-mask factor and zeroing of the x,y position of a column
@@ -169,110 +150,112 @@ __device__ __forceinline__ Ax6 axis_coef(const DCoord& c, bool N, int t) {
 }
 
 // ---- K1: LAP_UNIFORM (MODE 0), LAP_PROPS (1), MOM_DIFFUSION (2) ---------------
+// all k chunks of this block's columns (blockIdx.y strides over them)
 template <int MODE>
-__device__ __forceinline__ double lap_column(const DF& A, const DF& p, const FBC& b, const DGrid& g, const DF& kx,
-                                             const DF& ky, const DF& kz, double coeff, unsigned pb, int k0, int k1) {
-  Col cl = col_of(A, pb);
-  if (!cl.ok || k0 > k1) return 0.0;  // k chunks past this component's last plane
+__device__ __forceinline__ double lap_col(const DF& A, const DF& p, const FBC& b, const DGrid& g, const DF& kx,
+                                          const DF& ky, const DF& kz, double coeff) {
+  const Col cl = col_of(A, blockIdx.x);
+  if (!cl.ok) return 0.0;
   const int i = cl.i, j = cl.j;
   const size_t sy = (size_t)A.s0, sz = (size_t)A.s0 * A.s1;
-  const size_t idx0 = A.at(i, j, k0);
+  const int nkc = (A.s2 + kKC - 1) / kKC;
   if (cl.gij) {  // ghost columns: Ap = vol*... = 0
+    for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+      const int k0 = kc * kKC + 1;
+      const size_t idx0 = A.at(i, j, k0);
 #pragma unroll
-    for (int q = 0; q < kKC; q++)
-      if (k0 + q <= k1) A.f[idx0 + q * sz] = 0.0;
+      for (int q = 0; q < kKC; q++)
+        if (k0 + q <= A.s2) A.f[idx0 + q * sz] = 0.0;
+    }
     return 0.0;
   }
   const bool Nx = n_along(A.dl, 1), Ny = n_along(A.dl, 2), Nz = n_along(A.dl, 3);
-  const double* pbase = p.f + idx0;
-  // loads: p on planes k0-1 .. k1+1, x and y neighbours on k0 .. k1
-  double pc[kKC + 2], xm[kKC], xp[kKC], ym[kKC], yp[kKC];
-#pragma unroll
-  for (int q = 0; q < kKC + 2; q++) {
-    int k = k0 - 1 + q;
-    pc[q] = (k >= 1 && k <= A.s2 && k <= k1 + 1) ? ld(pbase + (ptrdiff_t)(q - 1) * (ptrdiff_t)sz) : 0.0;
-  }
-#pragma unroll
-  for (int q = 0; q < kKC; q++) {
-    int k = k0 + q;
-    bool in = k > 1 && k < A.s2 && k <= k1;
-    const double* c = pbase + (size_t)q * sz;
-    xm[q] = in ? ld(c - 1) : 0.0;
-    xp[q] = in ? ld(c + 1) : 0.0;
-    ym[q] = in ? ld(c - sy) : 0.0;
-    yp[q] = in ? ld(c + sy) : 0.0;
-  }
   const Ax6 X = axis_coef(g.c[0], Nx, i), Y = axis_coef(g.c[1], Ny, j);
   const double vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
   double fxy;
   bool zxy;
   wall_xy(A, b, i, j, fxy, zxy);
   const bool dxy = dot_xy(A, b, i, j);
-  // coefficient fields have their own (face) extents
-  size_t ix = 0, iy = 0, iz = 0, szx = 0, szy = 0, szz = 0;
-  if (MODE == 1) {
-    ix = kx.at(i, j, k0);
-    iy = ky.at(i, j, k0);
-    iz = kz.at(i, j, k0);
-    szx = (size_t)kx.s0 * kx.s1;
-    szy = (size_t)ky.s0 * ky.s1;
-    szz = (size_t)kz.s0 * kz.s1;
-  }
   double acc = 0.0;
+  for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+    const int k0 = kc * kKC + 1, k1 = min(k0 + kKC - 1, A.s2);
+    const size_t idx0 = A.at(i, j, k0);
+    const double* pbase = p.f + idx0;
+    // loads: p on planes k0-1 .. k1+1, x and y neighbours on k0 .. k1
+    double pc[kKC + 2], xm[kKC], xp[kKC], ym[kKC], yp[kKC];
 #pragma unroll
-  for (int q = 0; q < kKC; q++) {
-    const int k = k0 + q;
-    if (k > k1) break;
-    const size_t idx = idx0 + (size_t)q * sz;
-    if (k == 1 || k == A.s2) {
-      A.f[idx] = 0.0;
-      continue;
+    for (int q = 0; q < kKC + 2; q++) {
+      const int k = k0 - 1 + q;
+      pc[q] = (k >= 1 && k <= k1 + 1 && k <= A.s2) ? ld(pbase + (ptrdiff_t)(q - 1) * (ptrdiff_t)sz) : 0.0;
     }
-    const double pm = pc[q], p0 = pc[q + 1], pp = pc[q + 2];
-    const Ax6 Z = axis_coef(g.c[2], Nz, k);
-    double gl = xm[q] * X.a1 + p0 * X.a2, gr = p0 * X.b1 + xp[q] * X.b2;
-    if (MODE == 1 && !Nx) { gl = gl * ld(kx.f + ix + q * szx); gr = gr * ld(kx.f + ix + q * szx + 1); }
-    double v = gl * X.o1 + gr * X.o2;
-    gl = ym[q] * Y.a1 + p0 * Y.a2;
-    gr = p0 * Y.b1 + yp[q] * Y.b2;
-    if (MODE == 1 && !Ny) { gl = gl * ld(ky.f + iy + q * szy); gr = gr * ld(ky.f + iy + q * szy + ky.s0); }
-    v = v + (gl * Y.o1 + gr * Y.o2);
-    gl = pm * Z.a1 + p0 * Z.a2;
-    gr = p0 * Z.b1 + pp * Z.b2;
-    if (MODE == 1 && !Nz) { gl = gl * ld(kz.f + iz + q * szz); gr = gr * ld(kz.f + iz + (q + 1) * szz); }
-    v = v + (gl * Z.o1 + gr * Z.o2);
-    if (MODE == 2) {
-      v = v * coeff;
-      v = v + p0;
+#pragma unroll
+    for (int q = 0; q < kKC; q++) {
+      const int k = k0 + q;
+      const bool in = k > 1 && k < A.s2 && k <= k1;
+      const double* c = pbase + (size_t)q * sz;
+      xm[q] = in ? ld(c - 1) : 0.0;
+      xp[q] = in ? ld(c + 1) : 0.0;
+      ym[q] = in ? ld(c - sy) : 0.0;
+      yp[q] = in ? ld(c + sy) : 0.0;
     }
-    double f = fxy;
-    bool zero = zxy;
-    wall_z(A, b, Nz, k, f, zero);
-    if (f != 1.0) v = v * f;
-    if (zero) v = 0.0;
-    v = v * (vxy * vol_axis(g.c[2], Nz, k));
-    A.f[idx] = v;
-    if (dxy && dot_z(A, b, k)) acc += p0 * v;
+    // coefficient fields have their own (face) extents
+    size_t ix = 0, iy = 0, iz = 0, szx = 0, szy = 0, szz = 0;
+    if (MODE == 1) {
+      ix = kx.at(i, j, k0);
+      iy = ky.at(i, j, k0);
+      iz = kz.at(i, j, k0);
+      szx = (size_t)kx.s0 * kx.s1;
+      szy = (size_t)ky.s0 * ky.s1;
+      szz = (size_t)kz.s0 * kz.s1;
+    }
+#pragma unroll
+    for (int q = 0; q < kKC; q++) {
+      const int k = k0 + q;
+      if (k > k1) break;
+      const size_t idx = idx0 + (size_t)q * sz;
+      if (k == 1 || k == A.s2) {
+        A.f[idx] = 0.0;
+        continue;
+      }
+      const double pm = pc[q], p0 = pc[q + 1], pp = pc[q + 2];
+      const Ax6 Z = axis_coef(g.c[2], Nz, k);
+      double gl = xm[q] * X.a1 + p0 * X.a2, gr = p0 * X.b1 + xp[q] * X.b2;
+      if (MODE == 1 && !Nx) { gl = gl * ld(kx.f + ix + q * szx); gr = gr * ld(kx.f + ix + q * szx + 1); }
+      double v = gl * X.o1 + gr * X.o2;
+      gl = ym[q] * Y.a1 + p0 * Y.a2;
+      gr = p0 * Y.b1 + yp[q] * Y.b2;
+      if (MODE == 1 && !Ny) { gl = gl * ld(ky.f + iy + q * szy); gr = gr * ld(ky.f + iy + q * szy + ky.s0); }
+      v = v + (gl * Y.o1 + gr * Y.o2);
+      gl = pm * Z.a1 + p0 * Z.a2;
+      gr = p0 * Z.b1 + pp * Z.b2;
+      if (MODE == 1 && !Nz) { gl = gl * ld(kz.f + iz + q * szz); gr = gr * ld(kz.f + iz + (q + 1) * szz); }
+      v = v + (gl * Z.o1 + gr * Z.o2);
+      if (MODE == 2) {
+        v = v * coeff;
+        v = v + p0;
+      }
+      double f = fxy;
+      bool zero = zxy;
+      wall_z(A, b, Nz, k, f, zero);
+      if (f != 1.0) v = v * f;
+      if (zero) v = 0.0;
+      v = v * (vxy * vol_axis(g.c[2], Nz, k));
+      A.f[idx] = v;
+      if (dxy && dot_z(A, b, k)) acc += p0 * v;
+    }
   }
   return acc;
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(kLB, 2) k_l_lap(FComp Ap, FComp P, DGrid g, FBC b0, FBC b1, FBC b2, DF kx, DF ky,
-                                                DF kz, double coeff, unsigned npb, unsigned nkc, PcgScalars* S,
-                                                double* partial, unsigned* ticket) {
+                                                   DF kz, double coeff, PcgScalars* S, double* partial,
+                                                   unsigned* ticket) {
   if (S->done) return;
-  const unsigned nwork = npb * nkc * (unsigned)Ap.nc;
-  double acc = 0.0;
-  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const Item it = item_of<kKC>(w, npb, nkc);
-    if (it.c == 0)
-      acc += lap_column<MODE>(Ap.f[0], P.f[0], b0, g, kx, ky, kz, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[0].s2));
-    else if (it.c == 1)
-      acc += lap_column<MODE>(Ap.f[1], P.f[1], b1, g, kx, ky, kz, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[1].s2));
-    else
-      acc += lap_column<MODE>(Ap.f[2], P.f[2], b2, g, kx, ky, kz, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[2].s2));
-  }
+  double acc;
+  if (blockIdx.z == 0) acc = lap_col<MODE>(Ap.f[0], P.f[0], b0, g, kx, ky, kz, coeff);
+  else if (blockIdx.z == 1) acc = lap_col<MODE>(Ap.f[1], P.f[1], b1, g, kx, ky, kz, coeff);
+  else acc = lap_col<MODE>(Ap.f[2], P.f[2], b2, g, kx, ky, kz, coeff);
   finish_alpha(acc, S, partial, ticket);
 }
 
@@ -280,64 +263,63 @@ __global__ void __launch_bounds__(kLB, 2) k_l_lap(FComp Ap, FComp P, DGrid g, FB
 // l=0: d/dy(pz) - d/dz(py) ; l=1: d/dz(px) - d/dx(pz) ; l=2: d/dx(py) - d/dy(px)
 // (curl_SF with del assign/subtract: the CC->N passes are 0 at their end nodes)
 template <int L>
-__device__ __forceinline__ void curl_sig_column(const DF& E, const DF& pa, const DF& pb, const DF& sg, const DGrid& g,
-                                                unsigned blk, int k0, int k1) {
+__device__ __forceinline__ void curl_sig_col(const DF& E, const DF& pa, const DF& pb, const DF& sg, const DGrid& g) {
   constexpr int da = L == 0 ? 2 : (L == 1 ? 3 : 1);
   constexpr int db = L == 0 ? 3 : (L == 1 ? 1 : 2);
-  Col cl = col_of(E, blk);
+  const Col cl = col_of(E, blockIdx.x);
   if (!cl.ok) return;
   const int i = cl.i, j = cl.j;
   const DCoord& ca = g.c[da - 1];
   const DCoord& cb = g.c[db - 1];
   const size_t stride_a = da == 1 ? 1 : (da == 2 ? (size_t)pa.s0 : (size_t)pa.s0 * pa.s1);
   const size_t stride_b = db == 1 ? 1 : (db == 2 ? (size_t)pb.s0 : (size_t)pb.s0 * pb.s1);
-  double va[kKC], vb[kKC], sv[kKC];
+  const int nkc = (E.s2 + kKC - 1) / kKC;
+  for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+    const int k0 = kc * kKC + 1, k1 = min(k0 + kKC - 1, E.s2);
+    double va[kKC], vb[kKC], sv[kKC];
 #pragma unroll
-  for (int q = 0; q < kKC; q++) {
-    const int k = k0 + q;
-    va[q] = 0.0;
-    vb[q] = 0.0;
-    sv[q] = 0.0;
-    if (k > k1) continue;
-    const int ta = da == 1 ? i : (da == 2 ? j : k);
-    const int tb = db == 1 ? i : (db == 2 ? j : k);
-    if (!(ta == 1 || ta == E.s(da))) {
-      size_t ia = pa.at(i, j, k);
-      va[q] = ld(pa.f + ia - stride_a) * ca.cc2nD[ta - 1] + ld(pa.f + ia) * ca.cc2nU[ta - 1];
+    for (int q = 0; q < kKC; q++) {
+      const int k = k0 + q;
+      va[q] = 0.0;
+      vb[q] = 0.0;
+      sv[q] = 0.0;
+      if (k > k1) continue;
+      const int ta = da == 1 ? i : (da == 2 ? j : k);
+      const int tb = db == 1 ? i : (db == 2 ? j : k);
+      if (!(ta == 1 || ta == E.s(da))) {
+        const size_t ia = pa.at(i, j, k);
+        va[q] = ld(pa.f + ia - stride_a) * ca.cc2nD[ta - 1] + ld(pa.f + ia) * ca.cc2nU[ta - 1];
+      }
+      if (!(tb == 1 || tb == E.s(db))) {
+        const size_t ib = pb.at(i, j, k);
+        vb[q] = ld(pb.f + ib - stride_b) * cb.cc2nD[tb - 1] + ld(pb.f + ib) * cb.cc2nU[tb - 1];
+      }
+      sv[q] = ld(sg.f + sg.at(i, j, k));
     }
-    if (!(tb == 1 || tb == E.s(db))) {
-      size_t ib = pb.at(i, j, k);
-      vb[q] = ld(pb.f + ib - stride_b) * cb.cc2nD[tb - 1] + ld(pb.f + ib) * cb.cc2nU[tb - 1];
-    }
-    sv[q] = ld(sg.f + sg.at(i, j, k));
-  }
 #pragma unroll
-  for (int q = 0; q < kKC; q++) {
-    const int k = k0 + q;
-    if (k > k1) break;
-    const int tb = db == 1 ? i : (db == 2 ? j : k);
-    double v = (tb == 1 || tb == E.s(db)) ? 0.0 : va[q] - vb[q];
-    E(i, j, k) = v * sv[q];
+    for (int q = 0; q < kKC; q++) {
+      const int k = k0 + q;
+      if (k > k1) break;
+      const int tb = db == 1 ? i : (db == 2 ? j : k);
+      const double v = (tb == 1 || tb == E.s(db)) ? 0.0 : va[q] - vb[q];
+      E(i, j, k) = v * sv[q];
+    }
   }
 }
 __global__ void __launch_bounds__(kLB) k_l_curl_sig(DF E0, DF E1, DF E2, FComp P, DF s0, DF s1, DF s2, DGrid g,
-                                                     unsigned npb, unsigned nkc, PcgScalars* S) {
+                                                     PcgScalars* S) {
   if (S->done) return;
-  const unsigned nwork = npb * nkc * 3u;
-  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const Item it = item_of<kKC>(w, npb, nkc);
-    if (it.c == 0) curl_sig_column<0>(E0, P.f[2], P.f[1], s0, g, it.pb, it.k0, min(it.k0 + kKC - 1, E0.s2));
-    else if (it.c == 1) curl_sig_column<1>(E1, P.f[0], P.f[2], s1, g, it.pb, it.k0, min(it.k0 + kKC - 1, E1.s2));
-    else curl_sig_column<2>(E2, P.f[1], P.f[0], s2, g, it.pb, it.k0, min(it.k0 + kKC - 1, E2.s2));
-  }
+  if (blockIdx.z == 0) curl_sig_col<0>(E0, P.f[2], P.f[1], s0, g);
+  else if (blockIdx.z == 1) curl_sig_col<1>(E1, P.f[0], P.f[2], s1, g);
+  else curl_sig_col<2>(E2, P.f[1], P.f[0], s2, g);
 }
 // Ap_c = vol*mask(coeff*curl_c(E) + p) and p.Ap (edges -> faces: N->CC passes)
 template <int C>
-__device__ __forceinline__ double curl_ap_column(const DF& A, const DF& p, const FBC& b, const DF& Ea, const DF& Eb,
-                                                 const DGrid& g, double coeff, unsigned pb, int k0, int k1) {
+__device__ __forceinline__ double curl_ap_col(const DF& A, const DF& p, const FBC& b, const DF& Ea, const DF& Eb,
+                                              const DGrid& g, double coeff) {
   constexpr int da = C == 0 ? 2 : (C == 1 ? 3 : 1);
   constexpr int db = C == 0 ? 3 : (C == 1 ? 1 : 2);
-  Col cl = col_of(A, pb);
+  const Col cl = col_of(A, blockIdx.x);
   if (!cl.ok) return 0.0;
   const int i = cl.i, j = cl.j;
   const DCoord& ca = g.c[da - 1];
@@ -345,137 +327,111 @@ __device__ __forceinline__ double curl_ap_column(const DF& A, const DF& p, const
   const size_t stride_a = da == 1 ? 1 : (da == 2 ? (size_t)Ea.s0 : (size_t)Ea.s0 * Ea.s1);
   const size_t stride_b = db == 1 ? 1 : (db == 2 ? (size_t)Eb.s0 : (size_t)Eb.s0 * Eb.s1);
   const bool Nx = n_along(A.dl, 1), Ny = n_along(A.dl, 2), Nz = n_along(A.dl, 3);
-  double e0[kKC], e1[kKC], f0[kKC], f1[kKC], pv[kKC];
-#pragma unroll
-  for (int q = 0; q < kKC; q++) {
-    const int k = k0 + q;
-    const bool in = k <= k1 && !(cl.gij || k == 1 || k == A.s2);
-    e0[q] = e1[q] = f0[q] = f1[q] = pv[q] = 0.0;
-    if (in) {
-      size_t ia = Ea.at(i, j, k), ib = Eb.at(i, j, k);
-      e0[q] = ld(Ea.f + ia);
-      e1[q] = ld(Ea.f + ia + stride_a);
-      f0[q] = ld(Eb.f + ib);
-      f1[q] = ld(Eb.f + ib + stride_b);
-      pv[q] = ld(p.f + p.at(i, j, k));
-    }
-  }
+  const double vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
+  const int nkc = (A.s2 + kKC - 1) / kKC;
   double acc = 0.0;
+  for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+    const int k0 = kc * kKC + 1, k1 = min(k0 + kKC - 1, A.s2);
+    double e0[kKC], e1[kKC], f0[kKC], f1[kKC], pv[kKC];
 #pragma unroll
-  for (int q = 0; q < kKC; q++) {
-    const int k = k0 + q;
-    if (k > k1) break;
-    const bool ghost = cl.gij || k == 1 || k == A.s2;
-    double v = 0.0;
-    if (!ghost) {
-      const int ta = da == 1 ? i : (da == 2 ? j : k);
-      const int tb = db == 1 ? i : (db == 2 ? j : k);
-      double w = e0[q] * ca.n2ccD[ta] + e1[q] * ca.n2ccU[ta];
-      w = w - (f0[q] * cb.n2ccD[tb] + f1[q] * cb.n2ccU[tb]);
-      w = w * coeff;
-      w = w + pv[q];
-      bool zero;
-      double f = wall_fac(A, b, i, j, k, zero);
-      if (f != 1.0) w = w * f;
-      if (zero) w = 0.0;
-      v = w * ((vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j)) * vol_axis(g.c[2], Nz, k));
-      if (in_dot(A, i, j, k, b.dot_wall)) acc += pv[q] * v;
+    for (int q = 0; q < kKC; q++) {
+      const int k = k0 + q;
+      const bool in = k <= k1 && !(cl.gij || k == 1 || k == A.s2);
+      e0[q] = e1[q] = f0[q] = f1[q] = pv[q] = 0.0;
+      if (in) {
+        const size_t ia = Ea.at(i, j, k), ib = Eb.at(i, j, k);
+        e0[q] = ld(Ea.f + ia);
+        e1[q] = ld(Ea.f + ia + stride_a);
+        f0[q] = ld(Eb.f + ib);
+        f1[q] = ld(Eb.f + ib + stride_b);
+        pv[q] = ld(p.f + p.at(i, j, k));
+      }
     }
-    A(i, j, k) = v;
+#pragma unroll
+    for (int q = 0; q < kKC; q++) {
+      const int k = k0 + q;
+      if (k > k1) break;
+      const bool ghost = cl.gij || k == 1 || k == A.s2;
+      double v = 0.0;
+      if (!ghost) {
+        const int ta = da == 1 ? i : (da == 2 ? j : k);
+        const int tb = db == 1 ? i : (db == 2 ? j : k);
+        double w = e0[q] * ca.n2ccD[ta] + e1[q] * ca.n2ccU[ta];
+        w = w - (f0[q] * cb.n2ccD[tb] + f1[q] * cb.n2ccU[tb]);
+        w = w * coeff;
+        w = w + pv[q];
+        bool zero;
+        const double f = wall_fac(A, b, i, j, k, zero);
+        if (f != 1.0) w = w * f;
+        if (zero) w = 0.0;
+        v = w * (vxy * vol_axis(g.c[2], Nz, k));
+        if (in_dot(A, i, j, k, b.dot_wall)) acc += pv[q] * v;
+      }
+      A(i, j, k) = v;
+    }
   }
   return acc;
 }
 __global__ void __launch_bounds__(kLB) k_l_curl_ap(FComp Ap, FComp P, DF E0, DF E1, DF E2, DGrid g, FBC b0, FBC b1,
-                                                    FBC b2, double coeff, unsigned npb, unsigned nkc, PcgScalars* S,
-                                                    double* partial, unsigned* ticket) {
+                                                    FBC b2, double coeff, PcgScalars* S, double* partial,
+                                                    unsigned* ticket) {
   if (S->done) return;
-  const unsigned nwork = npb * nkc * 3u;
-  double acc = 0.0;
-  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const Item it = item_of<kKC>(w, npb, nkc);
-    if (it.c == 0)
-      acc += curl_ap_column<0>(Ap.f[0], P.f[0], b0, E2, E1, g, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[0].s2));
-    else if (it.c == 1)
-      acc += curl_ap_column<1>(Ap.f[1], P.f[1], b1, E0, E2, g, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[1].s2));
-    else
-      acc += curl_ap_column<2>(Ap.f[2], P.f[2], b2, E1, E0, g, coeff, it.pb, it.k0, min(it.k0 + kKC - 1, Ap.f[2].s2));
-  }
+  double acc;
+  if (blockIdx.z == 0) acc = curl_ap_col<0>(Ap.f[0], P.f[0], b0, E2, E1, g, coeff);
+  else if (blockIdx.z == 1) acc = curl_ap_col<1>(Ap.f[1], P.f[1], b1, E0, E2, g, coeff);
+  else acc = curl_ap_col<2>(Ap.f[2], P.f[2], b2, E1, E0, g, coeff);
   finish_alpha(acc, S, partial, ticket);
 }
 
-// ---- K2: x += alpha p ; r -= alpha Ap ; r.r, z.r ; exit test ; beta --------------
-// (KC planes per thread: the pointwise steps can afford more loads in flight)
-template <int KC = kKC>
-__device__ __forceinline__ void update_column(const DF& x, const DF& p, const DF& r, const DF& Ap, const DF& M,
-                                              const FBC& b, const DGrid& g, int mm, double coeff, double alpha,
-                                              unsigned pb, int k0, int k1, double& arr, double& azr) {
-  Col cl = col_of(x, pb);
+// ---- K2: x += alpha p ; r -= alpha Ap ; z = Minv r ; r.r, z.r ; exit test ; beta ----
+template <int KC>
+__device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r, const DF& Ap, const DF& M,
+                                           const FBC& b, double alpha, double& arr, double& azr) {
+  const Col cl = col_of(x, blockIdx.x);
   if (!cl.ok) return;
   const int i = cl.i, j = cl.j;
-  const bool Nx = n_along(x.dl, 1), Ny = n_along(x.dl, 2), Nz = n_along(x.dl, 3);
   const bool inxy = !cl.gij && dot_xy(x, b, i, j);
   const size_t sz = (size_t)x.s0 * x.s1;
-  const size_t idx0 = x.at(i, j, k0);
-  double xv[KC], pv[KC], rv[KC], av[KC], mv[KC];
+  const int nkc = (x.s2 + KC - 1) / KC;
+  for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+    const int k0 = kc * KC + 1, k1 = min(k0 + KC - 1, x.s2);
+    const size_t idx0 = x.at(i, j, k0);
+    double xv[KC], pv[KC], rv[KC], av[KC], mv[KC];
 #pragma unroll
-  for (int q = 0; q < KC; q++) {
-    const bool in = k0 + q <= k1;
-    const size_t idx = idx0 + (size_t)q * sz;
-    xv[q] = in ? x.f[idx] : 0.0;
-    pv[q] = in ? ld(p.f + idx) : 0.0;
-    rv[q] = in ? r.f[idx] : 0.0;
-    av[q] = in ? ld(Ap.f + idx) : 0.0;
-    mv[q] = (in && mm == 0) ? ld(M.f + idx) : 0.0;
-  }
-  double dxy = 0.0, vxy = 0.0;
-  if (mm != 0 && !cl.gij) {
-    dxy = diag_axis(g.c[0], Nx, i) + diag_axis(g.c[1], Ny, j);
-    vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
-  }
+    for (int q = 0; q < KC; q++) {
+      const bool in = k0 + q <= k1;
+      const size_t idx = idx0 + (size_t)q * sz;
+      xv[q] = in ? x.f[idx] : 0.0;
+      pv[q] = in ? ld(p.f + idx) : 0.0;
+      rv[q] = in ? r.f[idx] : 0.0;
+      av[q] = in ? ld(Ap.f + idx) : 0.0;
+      mv[q] = in ? ld(M.f + idx) : 0.0;
+    }
 #pragma unroll
-  for (int q = 0; q < KC; q++) {
-    const int k = k0 + q;
-    if (k > k1) break;
-    const size_t idx = idx0 + (size_t)q * sz;
-    x.f[idx] = xv[q] + pv[q] * alpha;
-    const double rn = rv[q] + av[q] * (-alpha);
-    r.f[idx] = rn;
-    if (inxy && k != 1 && k != x.s2 && dot_z(x, b, k)) {
-      double m = mv[q];
-      if (mm != 0) {
-        double d = dxy + diag_axis(g.c[2], Nz, k);
-        if (mm == 2) {
-          d = d * coeff;
-          d = d + 1.0;
-        }
-        m = 1.0 / (d * (vxy * vol_axis(g.c[2], Nz, k)));
+    for (int q = 0; q < KC; q++) {
+      const int k = k0 + q;
+      if (k > k1) break;
+      const size_t idx = idx0 + (size_t)q * sz;
+      x.f[idx] = xv[q] + pv[q] * alpha;
+      const double rn = rv[q] + av[q] * (-alpha);
+      r.f[idx] = rn;
+      if (inxy && k != 1 && k != x.s2 && dot_z(x, b, k)) {
+        const double zv = mv[q] * rn;
+        arr += rn * rn;
+        azr += zv * rn;
       }
-      const double zv = m * rn;
-      arr += rn * rn;
-      azr += zv * rn;
     }
   }
 }
 template <int KC>
-__global__ void __launch_bounds__(kLB) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, DGrid g, int mm,
-                                                   double coeff, FBC b0, FBC b1, FBC b2, unsigned npb, unsigned nkc,
-                                                   PcgScalars* S, double* partial, unsigned* ticket) {
+__global__ void __launch_bounds__(kLB) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, FBC b0, FBC b1,
+                                                   FBC b2, PcgScalars* S, double* partial, unsigned* ticket) {
   if (S->done) return;
-  const unsigned nwork = npb * nkc * (unsigned)X.nc;
   double arr = 0.0, azr = 0.0;
   const double alpha = S->alpha;
-  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const Item it = item_of<KC>(w, npb, nkc);
-    if (it.c == 0)
-      update_column<KC>(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, g, mm, coeff, alpha, it.pb, it.k0,
-                        min(it.k0 + KC - 1, X.f[0].s2), arr, azr);
-    else if (it.c == 1)
-      update_column<KC>(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, g, mm, coeff, alpha, it.pb, it.k0,
-                        min(it.k0 + KC - 1, X.f[1].s2), arr, azr);
-    else
-      update_column<KC>(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, g, mm, coeff, alpha, it.pb, it.k0,
-                        min(it.k0 + KC - 1, X.f[2].s2), arr, azr);
-  }
+  if (blockIdx.z == 0) update_col<KC>(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, alpha, arr, azr);
+  else if (blockIdx.z == 1) update_col<KC>(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, alpha, arr, azr);
+  else update_col<KC>(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, alpha, arr, azr);
   const double s_rr = block_sum(arr);
   const double s_zr = block_sum(azr);
   const unsigned fb = flat_block(), nb = n_blocks();
@@ -522,7 +478,40 @@ __global__ void __launch_bounds__(kLB) k_l_update(FComp X, FComp P, FComp R, FCo
   }
 }
 
-// ---- K3: p = p*beta + Minv r, plus p's implicit BC values ------------------------
+// ---- K3: p' = p*beta + Minv r at every point (BC points: k_l_bcfill) -------------
+template <int KC>
+__device__ __forceinline__ void pupd_col(const DF& p, const DF& pn, const DF& r, const DF& M, double beta) {
+  const Col cl = col_of(p, blockIdx.x);
+  if (!cl.ok) return;
+  const size_t sz = (size_t)p.s0 * p.s1;
+  const int nkc = (p.s2 + KC - 1) / KC;
+  for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+    const int k0 = kc * KC + 1, k1 = min(k0 + KC - 1, p.s2);
+    const size_t idx0 = p.at(cl.i, cl.j, k0);
+    double pv[KC], rv[KC], mv[KC];
+#pragma unroll
+    for (int q = 0; q < KC; q++) {
+      const bool in = k0 + q <= k1;
+      const size_t idx = idx0 + (size_t)q * sz;
+      pv[q] = in ? ld(p.f + idx) : 0.0;
+      rv[q] = in ? ld(r.f + idx) : 0.0;
+      mv[q] = in ? ld(M.f + idx) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < KC; q++)
+      if (k0 + q <= k1) pn.f[idx0 + (size_t)q * sz] = pv[q] * beta + mv[q] * rv[q];
+  }
+}
+template <int KC>
+__global__ void __launch_bounds__(kLB) k_l_pupd(FComp P, FComp Pn, FComp R, FComp M, PcgScalars* S) {
+  if (S->done) return;
+  const double beta = S->beta;
+  if (blockIdx.z == 0) pupd_col<KC>(P.f[0], Pn.f[0], R.f[0], M.f[0], beta);
+  else if (blockIdx.z == 1) pupd_col<KC>(P.f[1], Pn.f[1], R.f[1], M.f[1], beta);
+  else pupd_col<KC>(P.f[2], Pn.f[2], R.f[2], M.f[2], beta);
+}
+
+// ---- p's implicit BC values (apply_BCs_implicit, PCG_solver_algorithm.f90:70) ----
 // where p~ at (i,j,k) comes from: source point, factor, and an optional second
 // (Robin_N) term; interior points map to themselves.  Resolves every ghost
 // direction in turn (edge/corner ghosts, which no stencil reads, get the
@@ -542,30 +531,31 @@ MG_HD Src src_of(const DF& p, const FBC& b, int i, int j, int k) {
   s.rc = 0.0;
   int rd = 0, rb = 0;
   if (b.defined) {
+#pragma unroll
     for (int d = 1; d <= 3; d++) {
-      int t = I[d], n = p.s(d);
-      bool N = n_along(p.dl, d);
-      int fmin = 2 * d - 1, fmax = 2 * d;
+      const int t = I[d], n = p.s(d);
+      const bool N = n_along(p.dl, d);
+      const int fmin = 2 * d - 1, fmax = 2 * d;
       if (!N) {
         if (t == 1 || t == n) {
-          int ty = b.type[t == 1 ? fmin : fmax];
-          int in = t == 1 ? 2 : n - 1;
+          const int ty = b.type[t == 1 ? fmin : fmax];
+          const int in = t == 1 ? 2 : n - 1;
           if (ty == MOONS_BC_DIRICHLET) { I[d] = in; s.fac = -s.fac; }
           else if (ty == MOONS_BC_NEUMANN) I[d] = in;
           else if (ty == MOONS_BC_PERIODIC) I[d] = t == 1 ? n - 1 : 2;
           else if (ty == MOONS_BC_ROBIN) { I[d] = in; s.fac *= b.rc[t == 1 ? fmin : fmax]; }
         }
       } else {
-        bool many = n > 4;
-        bool per = b.type[fmin] == MOONS_BC_PERIODIC && b.type[fmax] == MOONS_BC_PERIODIC;
+        const bool many = n > 4;
+        const bool per = b.type[fmin] == MOONS_BC_PERIODIC && b.type[fmax] == MOONS_BC_PERIODIC;
         if (t == 1) {
-          int ty = b.type[fmin];
+          const int ty = b.type[fmin];
           if (ty == MOONS_BC_DIRICHLET) { I[d] = 3; s.fac = -s.fac; }
           else if (ty == MOONS_BC_NEUMANN) I[d] = 3;
           else if (ty == MOONS_BC_PERIODIC) I[d] = n - 2;
           else if (ty == MOONS_BC_ROBIN) { I[d] = 3; rd = d; rb = 2; s.rc = b.rc[fmin]; }
         } else if (t == n) {
-          int ty = b.type[fmax];
+          const int ty = b.type[fmax];
           if (ty == MOONS_BC_DIRICHLET) { I[d] = n - 2; s.fac = -s.fac; }
           else if (ty == MOONS_BC_NEUMANN) I[d] = n - 2;
           else if (ty == MOONS_BC_PERIODIC) { if (!many) I[d] = 3; }
@@ -577,9 +567,10 @@ MG_HD Src src_of(const DF& p, const FBC& b, int i, int j, int k) {
         }
       }
     }
+#pragma unroll
     for (int d = 1; d <= 3; d++) {  // a source on a Dirichlet boundary plane is 0
       if (!n_along(p.dl, d)) continue;
-      int n = p.s(d);
+      const int n = p.s(d);
       if ((I[d] == 2 && b.type[2 * d - 1] == MOONS_BC_DIRICHLET) || (I[d] == n - 1 && b.type[2 * d] == MOONS_BC_DIRICHLET))
         s.zero = true;
     }
@@ -587,118 +578,14 @@ MG_HD Src src_of(const DF& p, const FBC& b, int i, int j, int k) {
   s.I = I[1];
   s.J = I[2];
   s.K = I[3];
-  int R[4] = {0, I[1], I[2], I[3]};
-  if (rd) R[rd] = rb;
-  s.rI = R[1];
-  s.rJ = R[2];
-  s.rK = R[3];
+  s.rI = rd == 1 ? rb : I[1];
+  s.rJ = rd == 2 ? rb : I[2];
+  s.rK = rd == 3 ? rb : I[3];
   return s;
 }
 
-__device__ __forceinline__ double pnew_at(const DF& p, const DF& r, const DF& M, const DGrid& g, int mm, double coeff,
-                                          double beta, int i, int j, int k) {
-  double mv;
-  bool ghost = i == 1 || i == p.s0 || j == 1 || j == p.s1 || k == 1 || k == p.s2;
-  if (mm == 0) mv = M(i, j, k);
-  else if (ghost) mv = 0.0;
-  else {
-    const bool Nx = n_along(p.dl, 1), Ny = n_along(p.dl, 2), Nz = n_along(p.dl, 3);
-    double d = (diag_axis(g.c[0], Nx, i) + diag_axis(g.c[1], Ny, j)) + diag_axis(g.c[2], Nz, k);
-    if (mm == 2) {
-      d = d * coeff;
-      d = d + 1.0;
-    }
-    mv = 1.0 / (d * ((vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j)) * vol_axis(g.c[2], Nz, k)));
-  }
-  return p(i, j, k) * beta + mv * r(i, j, k);
-}
-
-// The new p of a source point is needed by the BC points that copy it, while
-// that source's own thread overwrites p: the kernel therefore reads p_old
-// from `p` and writes `pn` (the two buffers swap every iteration).
-template <int KC = kKC, bool BC = true>
-__device__ __forceinline__ void pupd_column(const DF& p, const DF& pn, const DF& r, const DF& M, const FBC& b,
-                                            const DGrid& g, int mm, double coeff, double beta, unsigned pb, int k0,
-                                            int k1) {
-  Col cl = col_of(p, pb);
-  if (!cl.ok) return;
-  const int i = cl.i, j = cl.j;
-  const bool Nx = n_along(p.dl, 1), Ny = n_along(p.dl, 2), Nz = n_along(p.dl, 3);
-  // columns next to a boundary (or with special boundary nodes) take the general path
-  const bool edge_xy = cl.gij || (Nx && (i == 2 || i == p.s0 - 1)) || (Ny && (j == 2 || j == p.s1 - 1));
-  const size_t sz = (size_t)p.s0 * p.s1;
-  const size_t idx0 = p.at(i, j, k0);
-  double pv[KC], rv[KC], mv[KC];
-#pragma unroll
-  for (int q = 0; q < KC; q++) {
-    const bool in = k0 + q <= k1;
-    const size_t idx = idx0 + (size_t)q * sz;
-    pv[q] = in ? ld(p.f + idx) : 0.0;
-    rv[q] = in ? ld(r.f + idx) : 0.0;
-    mv[q] = (in && mm == 0) ? ld(M.f + idx) : 0.0;
-  }
-  double dxy = 0.0, vxy = 0.0;
-  if (mm != 0 && !cl.gij) {
-    dxy = diag_axis(g.c[0], Nx, i) + diag_axis(g.c[1], Ny, j);
-    vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
-  }
-#pragma unroll
-  for (int q = 0; q < KC; q++) {
-    const int k = k0 + q;
-    if (k > k1) break;
-    const size_t idx = idx0 + (size_t)q * sz;
-    const bool special = BC && (edge_xy || k == 1 || k == p.s2 || (Nz && (k == 2 || k == p.s2 - 1)));
-    if (!special || !b.defined) {
-      double m = mv[q];
-      if (mm != 0) {
-        if (cl.gij || k == 1 || k == p.s2) m = 0.0;
-        else {
-          double d = dxy + diag_axis(g.c[2], Nz, k);
-          if (mm == 2) {
-            d = d * coeff;
-            d = d + 1.0;
-          }
-          m = 1.0 / (d * (vxy * vol_axis(g.c[2], Nz, k)));
-        }
-      }
-      pn.f[idx] = pv[q] * beta + m * rv[q];
-    } else {
-      Src s = src_of(p, b, i, j, k);
-      double v = 0.0;
-      if (!s.zero) {
-        v = pnew_at(p, r, M, g, mm, coeff, beta, s.I, s.J, s.K);
-        if (s.rc != 0.0) v = v + pnew_at(p, r, M, g, mm, coeff, beta, s.rI, s.rJ, s.rK) * s.rc;
-        v = s.fac * v;
-      }
-      pn.f[idx] = v;
-    }
-  }
-}
-// K3 without BC values (those come from k_l_bcfill afterwards)
-template <int KC>
-__global__ void __launch_bounds__(kLB) k_l_pupd(FComp P, FComp Pn, FComp R, FComp M, DGrid g, int mm, double coeff,
-                                                 FBC b0, FBC b1, FBC b2, unsigned npb, unsigned nkc, PcgScalars* S) {
-  if (S->done) return;
-  const unsigned nwork = npb * nkc * (unsigned)P.nc;
-  const double beta = S->beta;
-  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const Item it = item_of<KC>(w, npb, nkc);
-    if (it.c == 0)
-      pupd_column<KC, false>(P.f[0], Pn.f[0], R.f[0], M.f[0], b0, g, mm, coeff, beta, it.pb, it.k0,
-                             min(it.k0 + KC - 1, P.f[0].s2));
-    else if (it.c == 1)
-      pupd_column<KC, false>(P.f[1], Pn.f[1], R.f[1], M.f[1], b1, g, mm, coeff, beta, it.pb, it.k0,
-                             min(it.k0 + KC - 1, P.f[1].s2));
-    else
-      pupd_column<KC, false>(P.f[2], Pn.f[2], R.f[2], M.f[2], b2, g, mm, coeff, beta, it.pb, it.k0,
-                             min(it.k0 + KC - 1, P.f[2].s2));
-  }
-}
-
-// p's implicit BC values (apply_BCs_implicit, PCG_solver_algorithm.f90:70)
-// from the new p at their source points: every perimeter column of a plane
-// and the ghost / boundary-node planes of the inner columns.  Sources are
-// never points this kernel changes, so the order of the writes is free.
+// rewrite one BC point from its source(s); sources are never points this
+// kernel changes, so the order of the writes is free
 __device__ __forceinline__ void bcfill_point(const DF& p, const FBC& b, int i, int j, int k) {
   const Src s = src_of(p, b, i, j, k);
   if (s.zero) {
@@ -710,20 +597,20 @@ __device__ __forceinline__ void bcfill_point(const DF& p, const FBC& b, int i, i
   if (s.rc != 0.0) v = v + p(s.rI, s.rJ, s.rK) * s.rc;
   p(i, j, k) = s.fac * v;
 }
-__device__ __forceinline__ void bcfill_item(const DF& p, const FBC& b, unsigned r, unsigned npbP, unsigned nkc) {
+// block x < npbP: perimeter columns, every plane (strided over blockIdx.y);
+// block x >= npbP: inner columns, ghost planes and node-located boundary
+// planes (blockIdx.y = 0 only)
+__device__ __forceinline__ void bcfill_col(const DF& p, const FBC& b, unsigned npbP) {
   if (!b.defined) return;
   const PlaneSplit q = plane_split(p.s0, p.s1, p.dl);
-  const unsigned nPi = npbP * nkc;
-  if (r < nPi) {  // perimeter columns, every plane of one chunk
-    const unsigned kc = r / npbP, pp = r - kc * npbP;
-    if (pp >= q.npbP) return;
-    const Col cl = col_of(p, q.npbI + pp);
+  if (blockIdx.x < npbP) {
+    if (blockIdx.x >= q.npbP) return;
+    const Col cl = col_of(p, q.npbI + blockIdx.x);
     if (!cl.ok) return;
-    const int k0 = (int)kc * kKC + 1, k1 = min(k0 + kKC - 1, p.s2);
-    for (int k = k0; k <= k1; k++) bcfill_point(p, b, cl.i, cl.j, k);
-  } else {  // inner columns: ghost planes and node-located boundary planes
-    const unsigned pi = r - nPi;
-    if (pi >= q.npbI) return;
+    for (int k = blockIdx.y + 1; k <= p.s2; k += gridDim.y) bcfill_point(p, b, cl.i, cl.j, k);
+  } else {
+    const unsigned pi = blockIdx.x - npbP;
+    if (pi >= q.npbI || blockIdx.y != 0) return;
     const Col cl = col_of(p, pi);
     if (!cl.ok) return;
     bcfill_point(p, b, cl.i, cl.j, 1);
@@ -734,17 +621,11 @@ __device__ __forceinline__ void bcfill_item(const DF& p, const FBC& b, unsigned 
     }
   }
 }
-__global__ void __launch_bounds__(kLB) k_l_bcfill(FComp P, FBC b0, FBC b1, FBC b2, unsigned npbP, unsigned npbI,
-                                                   unsigned nkc, PcgScalars* S) {
+__global__ void __launch_bounds__(kLB) k_l_bcfill(FComp P, FBC b0, FBC b1, FBC b2, unsigned npbP, PcgScalars* S) {
   if (S->done) return;
-  const unsigned per = npbP * nkc + npbI;
-  const unsigned nwork = per * (unsigned)P.nc;
-  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const unsigned c = w / per, r = w - c * per;
-    if (c == 0) bcfill_item(P.f[0], b0, r, npbP, nkc);
-    else if (c == 1) bcfill_item(P.f[1], b1, r, npbP, nkc);
-    else bcfill_item(P.f[2], b2, r, npbP, nkc);
-  }
+  if (blockIdx.z == 0) bcfill_col(P.f[0], b0, npbP);
+  else if (blockIdx.z == 1) bcfill_col(P.f[1], b1, npbP);
+  else bcfill_col(P.f[2], b2, npbP);
 }
 
 }  // namespace mg

@@ -1,0 +1,470 @@
+// mgpcg.cu -- multigrid-preconditioned CG for cell-centred Poisson problems
+// (MOONS_PREC_MG: FP64 V-cycle inside CG; MOONS_PREC_MG_MIXED: FP32 V-cycle
+// inside an FP64 flexible CG).
+//
+// The outer iteration is the reference's PCG (PCG_solver_algorithm.f90:69-96)
+// with z = Minv r replaced by z = V(r): the residual, the CG inner products,
+// alpha/beta and the exit tests stay FP64 in both variants.  The mixed
+// variant uses the flexible (Polak-Ribiere) beta = z.(r - r_prev) / rho, so
+// the FP32 rounding inside the V-cycle cannot stall the recurrence.
+// Supported: one CC unknown (pressure, potential) with LAP_UNIFORM or
+// LAP_PROPS and Dirichlet / Neumann / periodic BCs, on meshes whose interior
+// cell counts are even (coarsening stops at the first odd count or at 2).
+#include <array>
+
+#include "mgrid.cuh"
+#include "runtime.cuh"
+
+using namespace mg;
+
+// ---------------------------------------------------------------------------
+// the hierarchy
+// ---------------------------------------------------------------------------
+struct MGHier {
+  bool mixed = false;
+  int nl = 0;
+  int sweeps_coarse = 24;
+  std::vector<std::array<int, 3>> s;  // CC extents per level
+  std::vector<MGLev<double>> Ld;
+  std::vector<MGLev<float>> Lf;
+  std::vector<std::array<MGProl<double>, 3>> Pd;  // [l]: fine level l-1 from coarse level l
+  std::vector<std::array<MGProl<float>, 3>> Pf;
+  std::vector<std::array<MGRest<double>, 3>> Rd;
+  std::vector<std::array<MGRest<float>, 3>> Rf;
+  double* rprev = nullptr;  // flexible CG: previous residual
+  // coarsest level: dense inverse (direct solve) when small enough
+  int ncoarse = 0;
+  double* cinv_d = nullptr;
+  float* cinv_f = nullptr;
+  std::vector<void*> allocs;
+  ~MGHier() {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+namespace {
+
+template <typename T>
+T* dev_copy(MGHier* h, const std::vector<T>& v, cudaStream_t st) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(1, v.size()) * sizeof(T)) != cudaSuccess) return nullptr;
+  h->allocs.push_back(p);
+  if (!v.empty()) cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+  return (T*)p;
+}
+template <typename T>
+T* dev_zeros(MGHier* h, size_t n, cudaStream_t st) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T)) != cudaSuccess) return nullptr;
+  h->allocs.push_back(p);
+  cudaMemsetAsync(p, 0, std::max<size_t>(1, n) * sizeof(T), st);
+  return (T*)p;
+}
+template <typename T>
+std::vector<T> conv(const std::vector<double>& v) {
+  return std::vector<T>(v.begin(), v.end());
+}
+
+// coarse node coordinates (with ghost nodes) keeping every other fine node
+std::vector<double> coarsen_nodes(const std::vector<double>& hn) {
+  const int sn = (int)hn.size();
+  std::vector<double> c;
+  c.push_back(0.0);
+  for (int i = 1; i <= sn - 2; i += 2) c.push_back(hn[i]);
+  c.push_back(0.0);
+  const int m = (int)c.size();
+  c[0] = c[1] - (c[2] - c[1]);
+  c[m - 1] = c[m - 2] + (c[m - 2] - c[m - 3]);
+  return c;
+}
+
+struct Axis1D {
+  // prolongation of one axis (fine f = 1..scf, only 2..scf-1 used)
+  std::vector<int> i0, i1;
+  std::vector<double> w0, w1;
+  // restriction = transpose, CSR over coarse I = 1..scc
+  std::vector<int> off, fi;
+  std::vector<double> fw;
+};
+
+// coarse index -> (interior index, sign) through the homogeneous BC of the face
+void resolve(int& I, double& w, int scc, int tlo, int thi) {
+  if (I == 1) {
+    if (tlo == MOONS_BC_PERIODIC) I = scc - 1;
+    else {
+      I = 2;
+      if (tlo == MOONS_BC_DIRICHLET) w = -w;
+    }
+  } else if (I == scc) {
+    if (thi == MOONS_BC_PERIODIC) I = 2;
+    else {
+      I = scc - 1;
+      if (thi == MOONS_BC_DIRICHLET) w = -w;
+    }
+  }
+}
+
+Axis1D build_axis(const host::HostCoord& cc, int scf, int tlo, int thi) {
+  Axis1D a;
+  const int scc = cc.sc;
+  a.i0.assign(scf + 1, 2);
+  a.i1.assign(scf + 1, 2);
+  a.w0.assign(scf + 1, 0.0);
+  a.w1.assign(scf + 1, 0.0);
+  std::vector<std::vector<std::pair<int, double>>> cols(scc + 1);
+  for (int f = 2; f <= scf - 1; f++) {
+    const int I = (f + 2) / 2;
+    int nb;
+    double wp, wn;
+    if ((f & 1) == 0) {  // left child: face I-1|I
+      wp = 0.5 + 0.5 * cc.thD[I - 1];
+      wn = 0.5 * cc.thU[I - 1];
+      nb = I - 1;
+    } else {  // right child: face I|I+1
+      wp = 0.5 + 0.5 * cc.thU[I];
+      wn = 0.5 * cc.thD[I];
+      nb = I + 1;
+    }
+    resolve(nb, wn, scc, tlo, thi);
+    a.i0[f] = I;
+    a.w0[f] = wp;
+    a.i1[f] = nb;
+    a.w1[f] = wn;
+    cols[I].push_back({f, wp});
+    cols[nb].push_back({f, wn});
+  }
+  a.off.assign(scc + 2, 0);
+  for (int I = 1; I <= scc; I++) {
+    a.off[I + 1] = a.off[I] + (int)cols[I].size();
+    for (auto& e : cols[I]) {
+      a.fi.push_back(e.first);
+      a.fw.push_back(e.second);
+    }
+  }
+  a.off[0] = 0;
+  return a;
+}
+
+template <typename T>
+MGAxis<T> axis_tables(MGHier* h, const host::HostCoord& c, cudaStream_t st) {
+  MGAxis<T> a{};
+  a.cD = dev_copy(h, conv<T>(c.cc2nD), st);
+  a.cU = dev_copy(h, conv<T>(c.cc2nU), st);
+  a.nD = dev_copy(h, conv<T>(c.n2ccD), st);
+  a.nU = dev_copy(h, conv<T>(c.n2ccU), st);
+  a.dg = dev_copy(h, conv<T>(c.diagC), st);
+  a.hv = dev_copy(h, conv<T>(c.dhn), st);
+  return a;
+}
+
+// area-weighted mean of the fine faces covering each coarse face of axis d
+std::vector<double> coarsen_faces(const std::vector<double>& kf, int d, const std::array<int, 3>& sf,
+                                  const std::array<int, 3>& sc, const host::HostCoord* cf) {
+  std::array<int, 3> ef = sf, ec = sc;
+  ef[d] += 1;
+  ec[d] += 1;
+  std::vector<double> kc((size_t)ec[0] * ec[1] * ec[2], 1.0);
+  auto fid = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)ef[0] * ((j - 1) + (size_t)ef[1] * (k - 1)); };
+  auto cid = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)ec[0] * ((j - 1) + (size_t)ec[1] * (k - 1)); };
+  const int a = d == 0 ? 1 : 0, b = d == 2 ? 1 : 2;  // transverse axes
+  for (int K = 1; K <= ec[2]; K++)
+    for (int J = 1; J <= ec[1]; J++)
+      for (int I = 1; I <= ec[0]; I++) {
+        int C[3] = {I, J, K};
+        // interior coarse cells along the transverse axes, physical nodes along d
+        bool inner = true;
+        for (int q = 0; q < 3; q++) {
+          const int lo = 2, hi = q == d ? ec[q] - 1 : ec[q] - 1;
+          if (C[q] < lo || C[q] > hi) inner = false;
+        }
+        if (!inner) continue;
+        int F[3];
+        F[d] = 2 * C[d] - 2;  // coincident fine node
+        double num = 0.0, den = 0.0;
+        for (int u = 0; u < 2; u++)
+          for (int v = 0; v < 2; v++) {
+            F[a] = 2 * C[a] - 2 + u;
+            F[b] = 2 * C[b] - 2 + v;
+            const double w = cf[a].dhn[F[a]] * cf[b].dhn[F[b]];
+            num += w * kf[fid(F[0], F[1], F[2])];
+            den += w;
+          }
+        kc[cid(I, J, K)] = num / den;
+      }
+  return kc;
+}
+
+// dense operator of one level over its interior cells (the same arithmetic
+// as apply_A, with ghost neighbours resolved through the homogeneous BCs)
+std::vector<double> dense_operator(const host::HostCoord* c, const std::array<int, 3>& s, const int* bt,
+                                   const std::array<std::vector<double>, 3>* K) {
+  const int nx = s[0] - 2, ny = s[1] - 2, nz = s[2] - 2;
+  const int n = nx * ny * nz;
+  std::vector<double> A((size_t)n * n, 0.0);
+  auto row_of = [&](int i, int j, int k) { return (i - 2) + nx * ((j - 2) + ny * (k - 2)); };
+  for (int k = 2; k <= s[2] - 1; k++)
+    for (int j = 2; j <= s[1] - 1; j++)
+      for (int i = 2; i <= s[0] - 1; i++) {
+        const int row = row_of(i, j, k);
+        const int ii[3] = {i, j, k};
+        const double vol = (c[0].dhn[i] * c[1].dhn[j]) * c[2].dhn[k];
+        for (int d = 0; d < 3; d++) {
+          const int t = ii[d];
+          double kl = 1.0, kr = 1.0;
+          if (K) {
+            std::array<int, 3> e = s;
+            e[d] += 1;
+            auto fid = [&](int a, int b, int cc) { return (size_t)(a - 1) + (size_t)e[0] * ((b - 1) + (size_t)e[1] * (cc - 1)); };
+            int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+            hi[d] += 1;
+            kl = (*K)[d][fid(lo[0], lo[1], lo[2])];
+            kr = (*K)[d][fid(hi[0], hi[1], hi[2])];
+          }
+          const double cm = c[d].cc2nD[t - 1] * kl * c[d].n2ccD[t];
+          const double c0 = c[d].cc2nU[t - 1] * kl * c[d].n2ccD[t] + c[d].cc2nD[t] * kr * c[d].n2ccU[t];
+          const double cp = c[d].cc2nU[t] * kr * c[d].n2ccU[t];
+          A[(size_t)row * n + row] += c0 * vol;
+          for (int side = 0; side < 2; side++) {
+            int nb[3] = {i, j, k};
+            nb[d] += side == 0 ? -1 : 1;
+            double w = (side == 0 ? cm : cp) * vol;
+            if (nb[d] == 1) {
+              if (bt[2 * d + 1] == MOONS_BC_PERIODIC) nb[d] = s[d] - 1;
+              else {
+                nb[d] = 2;
+                if (bt[2 * d + 1] == MOONS_BC_DIRICHLET) w = -w;
+              }
+            } else if (nb[d] == s[d]) {
+              if (bt[2 * d + 2] == MOONS_BC_PERIODIC) nb[d] = 2;
+              else {
+                nb[d] = s[d] - 1;
+                if (bt[2 * d + 2] == MOONS_BC_DIRICHLET) w = -w;
+              }
+            }
+            A[(size_t)row * n + row_of(nb[0], nb[1], nb[2])] += w;
+          }
+        }
+      }
+  return A;
+}
+
+// inverse by Gauss-Jordan with partial pivoting; false if singular
+bool invert(std::vector<double> A, int n, std::vector<double>& inv) {
+  inv.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
+  for (int col = 0; col < n; col++) {
+    int piv = col;
+    for (int r = col + 1; r < n; r++)
+      if (std::fabs(A[(size_t)r * n + col]) > std::fabs(A[(size_t)piv * n + col])) piv = r;
+    if (A[(size_t)piv * n + col] == 0.0) return false;
+    if (piv != col)
+      for (int c = 0; c < n; c++) {
+        std::swap(A[(size_t)piv * n + c], A[(size_t)col * n + c]);
+        std::swap(inv[(size_t)piv * n + c], inv[(size_t)col * n + c]);
+      }
+    const double d = 1.0 / A[(size_t)col * n + col];
+    for (int c = 0; c < n; c++) {
+      A[(size_t)col * n + c] *= d;
+      inv[(size_t)col * n + c] *= d;
+    }
+    for (int r = 0; r < n; r++) {
+      if (r == col) continue;
+      const double f = A[(size_t)r * n + col];
+      if (f == 0.0) continue;
+      for (int c = 0; c < n; c++) {
+        A[(size_t)r * n + c] -= f * A[(size_t)col * n + c];
+        inv[(size_t)r * n + c] -= f * inv[(size_t)col * n + c];
+      }
+    }
+  }
+  return true;
+}
+
+}  // namespace
+
+// build the hierarchy for a PCG object (CC, one component)
+int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf, MGHier** out) {
+  *out = nullptr;
+  auto h = std::make_unique<MGHier>();
+  h->mixed = mixed != 0;
+  cudaStream_t st = m->stream;
+  std::vector<host::HostCoord> C[3];
+  std::array<int, 3> s0 = {m->sn[0] - 1, m->sn[1] - 1, m->sn[2] - 1};
+  for (int d = 0; d < 3; d++) C[d].push_back(host::build_coord(m->hn[d].data(), m->sn[d]));
+  h->s.push_back(s0);
+  for (;;) {
+    const auto& sl = h->s.back();
+    bool can = true;
+    for (int d = 0; d < 3; d++) {
+      const int N = sl[d] - 2;
+      if (N < 4 || (N & 1)) can = false;
+    }
+    if (!can || h->s.size() >= 12) break;
+    std::array<int, 3> sc{};
+    for (int d = 0; d < 3; d++) {
+      const std::vector<double>& hf = C[d].back().hn;  // 1-based
+      std::vector<double> hc = coarsen_nodes(std::vector<double>(hf.begin() + 1, hf.end()));
+      C[d].push_back(host::build_coord(hc.data(), (int)hc.size()));
+      sc[d] = (int)hc.size() - 1;
+    }
+    h->s.push_back(sc);
+  }
+  h->nl = (int)h->s.size();
+  int bt[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int f = 1; f <= 6; f++) bt[f] = bc.defined ? bc.type[f] : MOONS_BC_NEUMANN;
+  // face coefficients per level (LAP_PROPS)
+  std::vector<std::array<std::vector<double>, 3>> K(h->nl);
+  if (kf) {
+    for (int d = 0; d < 3; d++) {
+      K[0][d].resize(kf[d].n());
+      cudaMemcpy(K[0][d].data(), kf[d].f, kf[d].n() * sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    for (int l = 1; l < h->nl; l++)
+      for (int d = 0; d < 3; d++) {
+        const host::HostCoord cf[3] = {C[0][l - 1], C[1][l - 1], C[2][l - 1]};
+        K[l][d] = coarsen_faces(K[l - 1][d], d, h->s[l - 1], h->s[l], cf);
+      }
+  }
+  for (int l = 0; l < h->nl; l++) {
+    const size_t n = (size_t)h->s[l][0] * h->s[l][1] * h->s[l][2];
+    MGLev<double> Ld{};
+    MGLev<float> Lf{};
+    for (int f = 0; f < 7; f++) Ld.bt[f] = Lf.bt[f] = bt[f];
+    Ld.s0 = Lf.s0 = h->s[l][0];
+    Ld.s1 = Lf.s1 = h->s[l][1];
+    Ld.s2 = Lf.s2 = h->s[l][2];
+    if (!h->mixed) {
+      for (int d = 0; d < 3; d++) Ld.ax[d] = axis_tables<double>(h.get(), C[d][l], st);
+      Ld.e = l == 0 ? s->z[0].f : dev_zeros<double>(h.get(), n, st);
+      Ld.r = l == 0 ? s->r[0].f : dev_zeros<double>(h.get(), n, st);
+      Ld.t = dev_zeros<double>(h.get(), n, st);
+      if (kf) {
+        Ld.kx = dev_copy(h.get(), K[l][0], st);
+        Ld.ky = dev_copy(h.get(), K[l][1], st);
+        Ld.kz = dev_copy(h.get(), K[l][2], st);
+      }
+      if (!Ld.t || !Ld.e || !Ld.r) return MOONS_ERR_NOMEM;
+    } else {
+      for (int d = 0; d < 3; d++) Lf.ax[d] = axis_tables<float>(h.get(), C[d][l], st);
+      Lf.e = dev_zeros<float>(h.get(), n, st);
+      Lf.r = dev_zeros<float>(h.get(), n, st);
+      Lf.t = dev_zeros<float>(h.get(), n, st);
+      if (kf) {
+        Lf.kx = dev_copy(h.get(), conv<float>(K[l][0]), st);
+        Lf.ky = dev_copy(h.get(), conv<float>(K[l][1]), st);
+        Lf.kz = dev_copy(h.get(), conv<float>(K[l][2]), st);
+      }
+      if (!Lf.t || !Lf.e || !Lf.r) return MOONS_ERR_NOMEM;
+    }
+    h->Ld.push_back(Ld);
+    h->Lf.push_back(Lf);
+    std::array<MGProl<double>, 3> Pd{};
+    std::array<MGProl<float>, 3> Pf{};
+    std::array<MGRest<double>, 3> Rd{};
+    std::array<MGRest<float>, 3> Rf{};
+    if (l > 0) {
+      for (int d = 0; d < 3; d++) {
+        Axis1D A = build_axis(C[d][l], h->s[l - 1][d], bt[2 * d + 1], bt[2 * d + 2]);
+        const int* i0 = dev_copy(h.get(), A.i0, st);
+        const int* i1 = dev_copy(h.get(), A.i1, st);
+        const int* off = dev_copy(h.get(), A.off, st);
+        const int* fi = dev_copy(h.get(), A.fi, st);
+        if (!h->mixed) {
+          Pd[d] = MGProl<double>{i0, i1, dev_copy(h.get(), A.w0, st), dev_copy(h.get(), A.w1, st)};
+          Rd[d] = MGRest<double>{off, fi, dev_copy(h.get(), A.fw, st)};
+        } else {
+          Pf[d] = MGProl<float>{i0, i1, dev_copy(h.get(), conv<float>(A.w0), st),
+                                dev_copy(h.get(), conv<float>(A.w1), st)};
+          Rf[d] = MGRest<float>{off, fi, dev_copy(h.get(), conv<float>(A.fw), st)};
+        }
+      }
+    }
+    h->Pd.push_back(Pd);
+    h->Pf.push_back(Pf);
+    h->Rd.push_back(Rd);
+    h->Rf.push_back(Rf);
+  }
+  if (h->mixed) {
+    h->rprev = dev_zeros<double>(h.get(), (size_t)s0[0] * s0[1] * s0[2], st);
+    if (!h->rprev) return MOONS_ERR_NOMEM;
+  }
+  {  // coarsest level: dense inverse, regularised on the constants when singular
+    const int l = h->nl - 1;
+    const auto& sc = h->s[l];
+    const int n = (sc[0] - 2) * (sc[1] - 2) * (sc[2] - 2);
+    if (n <= 1024) {
+      const host::HostCoord cc[3] = {C[0][l], C[1][l], C[2][l]};
+      std::vector<double> A = dense_operator(cc, sc, bt, kf ? &K[l] : nullptr);
+      bool dir = false;
+      for (int f = 1; f <= 6; f++) dir = dir || bt[f] == MOONS_BC_DIRICHLET;
+      if (!dir) {
+        double avg = 0.0;
+        for (int i = 0; i < n; i++) avg += A[(size_t)i * n + i];
+        avg /= n;
+        for (size_t q = 0; q < A.size(); q++) A[q] += avg / n;
+      }
+      std::vector<double> inv;
+      if (invert(A, n, inv)) {
+        h->ncoarse = n;
+        if (!h->mixed) h->cinv_d = dev_copy(h.get(), inv, st);
+        else h->cinv_f = dev_copy(h.get(), conv<float>(inv), st);
+      }
+    }
+  }
+  MG_CUDA(cudaStreamSynchronize(st));
+  *out = h.release();
+  return MOONS_OK;
+}
+
+void mg_free(MGHier* h) { delete h; }
+double* mg_rprev(MGHier* h) { return h->rprev; }
+
+namespace {
+unsigned vgrid(size_t n) { return (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 8)); }
+
+template <typename T>
+const T* coarse_inv(const MGHier* h);
+template <>
+const double* coarse_inv<double>(const MGHier* h) { return h->cinv_d; }
+template <>
+const float* coarse_inv<float>(const MGHier* h) { return h->cinv_f; }
+
+template <typename T>
+int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::array<MGProl<T>, 3>>& P,
+             const std::vector<std::array<MGRest<T>, 3>>& R, cudaStream_t st, const PcgScalars* S) {
+  const int nl = h->nl;
+  auto npts = [&](int l) { return (size_t)(L[l].s0 - 2) * (L[l].s1 - 2) * (L[l].s2 - 2); };
+  for (int l = 0; l < nl - 1; l++) {  // down: pre-smooth, residual, restrict
+    const unsigned g = vgrid(npts(l) / 2 + 1);
+    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, 1, S);
+    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, S);
+    MG_LAUNCH(k_mg_resid<T>, vgrid(npts(l)), 256, st, L[l], S);
+    MG_LAUNCH(k_mg_restrict<T>, vgrid(npts(l + 1)), 256, st, L[l], L[l + 1], R[l + 1][0], R[l + 1][1], R[l + 1][2], S);
+  }
+  if (h->ncoarse > 0)
+    MG_LAUNCH(k_mg_direct<T>, (unsigned)((h->ncoarse + 255) / 256), 256, st, L[nl - 1], coarse_inv<T>(h), h->ncoarse,
+              S);
+  else
+    MG_LAUNCH(k_mg_coarse<T>, 1, 256, st, L[nl - 1], h->sweeps_coarse, S);
+  for (int l = nl - 2; l >= 0; l--) {  // up: prolong + correct, post-smooth (reverse colours)
+    const unsigned g = vgrid(npts(l) / 2 + 1);
+    MG_LAUNCH(k_mg_prolong<T>, vgrid(npts(l)), 256, st, L[l], L[l + 1], P[l + 1][0], P[l + 1][1], P[l + 1][2], S);
+    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, S);
+    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, 0, S);
+  }
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+}  // namespace
+
+// z = V(r) on the PCG's fine level (z, r: FP64 PCG arrays)
+int mg_vcycle(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
+  if (!h->mixed) return vcycle_t<double>(h, h->Ld, h->Pd, h->Rd, st, S);
+  const size_t n = r.n();
+  MG_LAUNCH((k_mg_cast<float, double>), vgrid(n), 256, st, h->Lf[0].r, (const double*)r.f, n, S);
+  int rc = vcycle_t<float>(h, h->Lf, h->Pf, h->Rf, st, S);
+  if (rc) return rc;
+  MG_LAUNCH((k_mg_cast<double, float>), vgrid(n), 256, st, z.f, (const float*)h->Lf[0].e, n, S);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}

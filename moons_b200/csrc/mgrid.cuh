@@ -1,0 +1,427 @@
+// mgrid.cuh -- geometric multigrid V-cycle for cell-centred Poisson
+// problems, used as the preconditioner of (flexible) CG.
+//
+// Building blocks follow the reference's multigrid pieces
+// (code/handwritten/grid_field/GF_MG/GF_restrict.f90:22-82,
+// GF_MG/GF_prolongate.f90:22-106, coordinates_extend.f90:336-391 restrict_c,
+// solvers/SOR/SOR.f90:234-314 redBlack/init_r) and the V-cycle design of
+// code_not_compiled/9.6.2017/MG/MG.f90:241-396 (not compiled in the
+// reference):
+//  * coarse grids keep every other node of the fine grid (stretching kept);
+//  * prolongation is the reference's prolongate_C: each fine cell takes the
+//    mean of its parent's value and the theta-interpolated value at the
+//    parent's face nearest to it (linear interpolation on stretched grids);
+//  * restriction is the exact transpose of that prolongation (built from the
+//    same 1-D weights on the host), so the V-cycle is a symmetric operator
+//    and plain CG may use it (the reference's restrict_C is the
+//    volume-weighted average; its index expressions for the transverse
+//    directions read `i` where `j`/`k` are meant, GF_restrict.f90:38-39);
+//  * smoothing is red-black Gauss-Seidel (redBlack with omega = 1) on the
+//    volume-weighted operator, forward (red, black) before the coarse
+//    correction and backward (black, red) after it;
+//  * ghost values are never stored: a neighbour index on a ghost plane is
+//    resolved through the level's homogeneous BCs (Dirichlet -u, Neumann u,
+//    periodic opposite side), exactly as apply_BCs_implicit fills them;
+//  * the coarsest level is solved by a fixed number of symmetric
+//    red-black sweeps inside one block.
+// Everything is templated on the arithmetic type: T = double for the plain
+// path, T = float for the mixed-precision path (V-cycle in FP32 inside an
+// FP64 flexible CG).
+#pragma once
+#include "lean.cuh"
+
+namespace mg {
+
+template <typename T>
+struct MGAxis {
+  const T *cD, *cU;  // stagCC2N D/U (index 1..sc-1)
+  const T *nD, *nU;  // stagN2CC D/U (index 1..sn-1)
+  const T* dg;       // laplacian diagonal share of CC data (index 2..sc-1)
+  const T* hv;       // cell widths dhn (index 1..sc)
+};
+
+template <typename T>
+struct MGLev {
+  T *e, *r, *t;      // correction, right-hand side, residual (CC, with ghosts)
+  int s0, s1, s2;
+  MGAxis<T> ax[3];
+  const T* kx;       // face coefficients (LAP_PROPS) or null
+  const T* ky;
+  const T* kz;
+  int bt[7];         // BC type per face (MOONS_BC_*)
+};
+
+// prolongation tables of one axis: for fine index f, two coarse interior
+// indices (ghosts already resolved) and their weights
+template <typename T>
+struct MGProl {
+  const int* i0;
+  const int* i1;
+  const T* w0;
+  const T* w1;
+};
+// restriction (transpose) tables of one axis: for coarse interior index I,
+// entries off[I] .. off[I+1]-1 of (fi, fw)
+template <typename T>
+struct MGRest {
+  const int* off;
+  const int* fi;
+  const T* fw;
+};
+
+template <typename T>
+__device__ __forceinline__ size_t lidx(const MGLev<T>& L, int i, int j, int k) {
+  return (size_t)((unsigned)(i - 1) + (unsigned)L.s0 * ((unsigned)(j - 1) + (unsigned)L.s1 * (unsigned)(k - 1)));
+}
+
+// value at (i,j,k) of a field whose ghost entries are implied by the level's
+// homogeneous BCs
+template <typename T>
+__device__ __forceinline__ T ev(const MGLev<T>& L, const T* e, int i, int j, int k) {
+  T fac = T(1);
+  int I[3] = {i, j, k};
+  const int s[3] = {L.s0, L.s1, L.s2};
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (I[d] == 1) {
+      const int ty = L.bt[2 * d + 1];
+      if (ty == MOONS_BC_PERIODIC) I[d] = s[d] - 1;
+      else {
+        I[d] = 2;
+        if (ty == MOONS_BC_DIRICHLET) fac = -fac;
+      }
+    } else if (I[d] == s[d]) {
+      const int ty = L.bt[2 * d + 2];
+      if (ty == MOONS_BC_PERIODIC) I[d] = 2;
+      else {
+        I[d] = s[d] - 1;
+        if (ty == MOONS_BC_DIRICHLET) fac = -fac;
+      }
+    }
+  }
+  return fac * e[lidx(L, I[0], I[1], I[2])];
+}
+
+// index of face (i,j,k) of a face-`d` array on the level's grid (the face
+// array has one more entry along d)
+template <typename T>
+__device__ __forceinline__ size_t fidx(const MGLev<T>& L, int d, int i, int j, int k) {
+  const unsigned f0 = (unsigned)L.s0 + (d == 0), f1 = (unsigned)L.s1 + (d == 1);
+  return (size_t)((unsigned)(i - 1) + f0 * ((unsigned)(j - 1) + f1 * (unsigned)(k - 1)));
+}
+
+// (A e)(i,j,k) = vol * div(k grad e) at an interior point (k = 1 without
+// face coefficients), and its diagonal D (the smoother's divisor)
+template <typename T>
+__device__ __forceinline__ T apply_A(const MGLev<T>& L, const T* e, int i, int j, int k, T& D) {
+  const size_t id = lidx(L, i, j, k);
+  const T e0 = e[id];
+  const int ii[3] = {i, j, k};
+  // points two or more away from every boundary read no ghost value
+  const bool inner = i > 2 && i < L.s0 - 1 && j > 2 && j < L.s1 - 1 && k > 2 && k < L.s2 - 1;
+  const size_t st[3] = {1, (size_t)L.s0, (size_t)L.s0 * L.s1};
+  T v = T(0);
+  T dg = T(0);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const MGAxis<T>& A = L.ax[d];
+    const int t = ii[d];
+    const int di = d == 0, dj = d == 1, dk = d == 2;
+    const T em = inner ? e[id - st[d]] : ev(L, e, i - di, j - dj, k - dk);
+    const T ep = inner ? e[id + st[d]] : ev(L, e, i + di, j + dj, k + dk);
+    T gl = em * A.cD[t - 1] + e0 * A.cU[t - 1];
+    T gr = e0 * A.cD[t] + ep * A.cU[t];
+    T dgl = A.cU[t - 1], dgr = A.cD[t];
+    const T* kf = d == 0 ? L.kx : (d == 1 ? L.ky : L.kz);
+    if (kf) {
+      const T kl = kf[fidx(L, d, i, j, k)], kr = kf[fidx(L, d, i + di, j + dj, k + dk)];
+      gl = gl * kl;
+      gr = gr * kr;
+      dgl = dgl * kl;
+      dgr = dgr * kr;
+    }
+    v = v + (gl * A.nD[t] + gr * A.nU[t]);
+    dg = dg + (dgl * A.nD[t] + dgr * A.nU[t]);
+  }
+  const T vol = (L.ax[0].hv[i] * L.ax[1].hv[j]) * L.ax[2].hv[k];
+  D = dg * vol;
+  return v * vol;
+}
+
+// the diagonal D alone
+template <typename T>
+__device__ __forceinline__ T diag_A(const MGLev<T>& L, int i, int j, int k) {
+  const int ii[3] = {i, j, k};
+  T dg = T(0);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const MGAxis<T>& A = L.ax[d];
+    const int t = ii[d];
+    const int di = d == 0, dj = d == 1, dk = d == 2;
+    T dgl = A.cU[t - 1], dgr = A.cD[t];
+    const T* kf = d == 0 ? L.kx : (d == 1 ? L.ky : L.kz);
+    if (kf) {
+      dgl = dgl * kf[fidx(L, d, i, j, k)];
+      dgr = dgr * kf[fidx(L, d, i + di, j + dj, k + dk)];
+    }
+    dg = dg + (dgl * A.nD[t] + dgr * A.nU[t]);
+  }
+  return dg * ((L.ax[0].hv[i] * L.ax[1].hv[j]) * L.ax[2].hv[k]);
+}
+
+// one red-black half sweep of colour `color` (points with (i+j+k)&1 == color).
+// first != 0: e starts at zero (both colours are written).
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int first, const PcgScalars* S) {
+  if (S && S->done) return;
+  const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
+  const int nxh = (nx + 1) / 2;
+  const unsigned n = (unsigned)nxh * (unsigned)ny * (unsigned)nz;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / (unsigned)nxh;
+    const int ih = (int)(t - q * (unsigned)nxh);
+    const unsigned kk = q / (unsigned)ny;
+    const int j = (int)(q - kk * (unsigned)ny) + 2, k = (int)kk + 2;
+    const int i0 = 2 + ((color + j + k) & 1);
+    const int i = i0 + 2 * ih;
+    if (first) {  // the other colour of this pair starts at zero
+      const int io = 2 + ((color + 1 + j + k) & 1) + 2 * ih;
+      if (io <= L.s0 - 1) L.e[lidx(L, io, j, k)] = T(0);
+    }
+    if (i > L.s0 - 1) continue;
+    const size_t id = lidx(L, i, j, k);
+    if (first) {
+      // e = 0 everywhere before this sweep, so A e = 0 and e = r / D
+      L.e[id] = L.r[id] / diag_A<T>(L, i, j, k);
+    } else {
+      T D;
+      const T Ae = apply_A<T>(L, L.e, i, j, k, D);
+      L.e[id] = L.e[id] + (L.r[id] - Ae) / D;
+    }
+  }
+}
+
+// t = r - A e at interior points
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_resid(MGLev<T> L, const PcgScalars* S) {
+  if (S && S->done) return;
+  const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
+  const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / (unsigned)nx;
+    const int i = (int)(t - q * (unsigned)nx) + 2;
+    const unsigned kk = q / (unsigned)ny;
+    const int j = (int)(q - kk * (unsigned)ny) + 2, k = (int)kk + 2;
+    T D;
+    const T Ae = apply_A<T>(L, L.e, i, j, k, D);
+    const size_t id = lidx(L, i, j, k);
+    L.t[id] = L.r[id] - Ae;
+  }
+}
+
+// coarse r = R (fine t), R the transpose of the prolongation
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_restrict(MGLev<T> F, MGLev<T> C, MGRest<T> Rx, MGRest<T> Ry,
+                                                     MGRest<T> Rz, const PcgScalars* S) {
+  if (S && S->done) return;
+  const int nx = C.s0 - 2, ny = C.s1 - 2, nz = C.s2 - 2;
+  const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / (unsigned)nx;
+    const int I = (int)(t - q * (unsigned)nx) + 2;
+    const unsigned kk = q / (unsigned)ny;
+    const int J = (int)(q - kk * (unsigned)ny) + 2, K = (int)kk + 2;
+    T acc = T(0);
+    for (int c = Rz.off[K]; c < Rz.off[K + 1]; c++) {
+      const int fk = Rz.fi[c];
+      const T wz = Rz.fw[c];
+      for (int b = Ry.off[J]; b < Ry.off[J + 1]; b++) {
+        const int fj = Ry.fi[b];
+        const T wyz = Ry.fw[b] * wz;
+        T row = T(0);
+        for (int a = Rx.off[I]; a < Rx.off[I + 1]; a++) row = row + Rx.fw[a] * F.t[lidx(F, Rx.fi[a], fj, fk)];
+        acc = acc + wyz * row;
+      }
+    }
+    C.r[lidx(C, I, J, K)] = acc;
+  }
+}
+
+// fine e += P (coarse e)
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_prolong(MGLev<T> F, MGLev<T> C, MGProl<T> Px, MGProl<T> Py,
+                                                    MGProl<T> Pz, const PcgScalars* S) {
+  if (S && S->done) return;
+  const int nx = F.s0 - 2, ny = F.s1 - 2, nz = F.s2 - 2;
+  const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / (unsigned)nx;
+    const int i = (int)(t - q * (unsigned)nx) + 2;
+    const unsigned kk = q / (unsigned)ny;
+    const int j = (int)(q - kk * (unsigned)ny) + 2, k = (int)kk + 2;
+    const int ix[2] = {Px.i0[i], Px.i1[i]}, jy[2] = {Py.i0[j], Py.i1[j]}, kz[2] = {Pz.i0[k], Pz.i1[k]};
+    const T wx[2] = {Px.w0[i], Px.w1[i]}, wy[2] = {Py.w0[j], Py.w1[j]}, wz[2] = {Pz.w0[k], Pz.w1[k]};
+    T acc = T(0);
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int b = 0; b < 2; b++) {
+        const T w = wy[b] * wz[c];
+        acc = acc + w * (wx[0] * C.e[lidx(C, ix[0], jy[b], kz[c])] + wx[1] * C.e[lidx(C, ix[1], jy[b], kz[c])]);
+      }
+    const size_t id = lidx(F, i, j, k);
+    F.e[id] = F.e[id] + acc;
+  }
+}
+
+// coarsest level: e = 0, then `sweeps` forward red-black sweeps and as many
+// backward ones (symmetric), all inside one block
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_coarse(MGLev<T> L, int sweeps, const PcgScalars* S) {
+  if (S && S->done) return;
+  const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
+  const int n = nx * ny * nz;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int i = t % nx + 2, q = t / nx, j = q % ny + 2, k = q / ny + 2;
+    L.e[lidx(L, i, j, k)] = T(0);
+  }
+  __syncthreads();
+  for (int s = 0; s < 4 * sweeps; s++) {
+    // forward: colours 0,1,0,1,... ; backward: 1,0,1,0,...
+    const int color = s < 2 * sweeps ? (s & 1) : 1 - (s & 1);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      const int i = t % nx + 2, q = t / nx, j = q % ny + 2, k = q / ny + 2;
+      if (((i + j + k) & 1) != color) continue;
+      T D;
+      const T Ae = apply_A<T>(L, L.e, i, j, k, D);
+      const size_t id = lidx(L, i, j, k);
+      L.e[id] = L.e[id] + (L.r[id] - Ae) / D;
+    }
+    __syncthreads();
+  }
+}
+
+// coarsest level solved directly: e = Minv r over the n interior cells
+// (Minv: the inverse of the level's operator, regularised on the constant
+// mode when no face is Dirichlet; built on the host)
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_direct(MGLev<T> L, const T* Minv, int n, const PcgScalars* S) {
+  if (S && S->done) return;
+  const int nx = L.s0 - 2, ny = L.s1 - 2;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    T acc = T(0);
+    for (int c = 0; c < n; c++) {
+      const int i = c % nx + 2, q = c / nx, j = q % ny + 2, k = q / ny + 2;
+      acc = acc + Minv[(size_t)row * n + c] * L.r[lidx(L, i, j, k)];
+    }
+    const int i = row % nx + 2, q = row / nx, j = q % ny + 2, k = q / ny + 2;
+    L.e[lidx(L, i, j, k)] = acc;
+  }
+}
+
+// dst = (Tdst) src over n entries
+template <typename Td, typename Ts>
+__global__ void k_mg_cast(Td* dst, const Ts* src, size_t n, const PcgScalars* S) {
+  if (S && S->done) return;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (Td)src[i];
+}
+
+// ---- the outer (flexible) CG around the V-cycle (mgpcg.cu) ----------------
+
+// x += alpha p ; r -= alpha Ap ; r_prev = old r (flexible) ; r.r over the
+// interior; the last block runs update_exit_loop
+__global__ void __launch_bounds__(kLB) k_m_update(DF x, DF p, DF r, DF Ap, double* rprev, PcgScalars* S,
+                                                  double* partial, unsigned* ticket) {
+  if (S->done) return;
+  const double alpha = S->alpha;
+  double arr = 0.0;
+  const unsigned n = (unsigned)x.n();
+  for (unsigned id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+    const double rv = r.f[id];
+    if (rprev) rprev[id] = rv;
+    x.f[id] = x.f[id] + p.f[id] * alpha;
+    const double rn = rv + Ap.f[id] * (-alpha);
+    r.f[id] = rn;
+    int i, j, k;
+    ijk_of(id, x, i, j, k);
+    if (i > 1 && i < x.s0 && j > 1 && j < x.s1 && k > 1 && k < x.s2) arr += rn * rn;
+  }
+  const double s_rr = block_sum(arr);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s_rr;
+  if (last_block(ticket)) {
+    const double rr = sum_partials(partial, gridDim.x);
+    if (threadIdx.x == 0) {
+      *ticket = 0;
+      S->rr = rr;
+      S->iter += 1;
+      S->iter_total += 1;
+      bool stop = false;
+      if (S->iter % S->nskip == 0) {
+        const double res = sqrt(fabs(rr));
+        S->res = res;
+        const bool e1 = res / S->res0 < S->tol_rel;
+        const bool e2 = res < S->tol_abs;
+        const bool e3 = S->iter >= S->iter_max;
+        if (e1 || e2 || e3) {
+          stop = true;
+          S->exit_reason = e1 ? 1 : (e2 ? 2 : 3);
+        }
+        if (isnan(res)) {
+          S->nan = 1;
+          S->nan_any = 1;
+          stop = true;
+        }
+      }
+      if (!stop && S->iter >= S->iter_max) {
+        stop = true;
+        S->exit_reason = 3;
+      }
+      S->done = stop ? 1 : 0;
+    }
+  }
+}
+
+// rho' = z.r (interior), flexible: minus z.r_prev; beta = that / rho
+__global__ void __launch_bounds__(kLB) k_m_beta(DF z, DF r, const double* rprev, PcgScalars* S, double* partial,
+                                                unsigned* ticket) {
+  if (S->done) return;
+  double azr = 0.0, azp = 0.0;
+  const unsigned n = (unsigned)z.n();
+  for (unsigned id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+    int i, j, k;
+    ijk_of(id, z, i, j, k);
+    if (i > 1 && i < z.s0 && j > 1 && j < z.s1 && k > 1 && k < z.s2) {
+      const double zv = z.f[id];
+      azr += zv * r.f[id];
+      if (rprev) azp += zv * rprev[id];
+    }
+  }
+  const double s1 = block_sum(azr);
+  const double s2 = block_sum(azp);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = s1;
+    partial[gridDim.x + blockIdx.x] = s2;
+  }
+  if (last_block(ticket)) {
+    const double zr = sum_partials(partial, gridDim.x);
+    const double zp = sum_partials(partial + gridDim.x, gridDim.x);
+    if (threadIdx.x == 0) {
+      *ticket = 0;
+      S->zr = zr;
+      S->beta = (rprev ? zr - zp : zr) / S->rhok;
+      S->rhok = zr;
+    }
+  }
+}
+
+// p' = z + beta p (every point; BC points are rewritten by k_l_bcfill)
+__global__ void __launch_bounds__(kLB) k_m_pupd(DF pn, DF p, DF z, const PcgScalars* S) {
+  if (S->done) return;
+  const double beta = S->beta;
+  const unsigned n = (unsigned)p.n();
+  for (unsigned id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x)
+    pn.f[id] = z.f[id] + p.f[id] * beta;
+}
+
+}  // namespace mg

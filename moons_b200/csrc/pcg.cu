@@ -8,14 +8,13 @@
 // set (the flag also comes up at iter_max, and the node stops after
 // iter_max+2 body runs in any case, so the loop always ends).
 // MOONS_PCG_HOSTLOOP=1 launches the same kernels from the host instead (for
-// profilers); MOONS_PCG_MODE=persistent runs the loop as one cooperative
-// kernel with grid barriers (persist.cuh).
+// profilers).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 
-#include "persist.cuh"
+#include "mgrid.cuh"
 #include "runtime.cuh"
 
 namespace mg {
@@ -148,16 +147,24 @@ __global__ void k_set_cond(cudaGraphConditionalHandle h, PcgScalars* S) {
   cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
-// grids of the lean kernels
+// grids of the lean kernels: (plane blocks, k stride, component)
 struct LeanGrids {
-  unsigned npb, nkc, nkcU, npbP, npbI, npbE, nkcE;
-  unsigned gA, gB, gC, gD, gE;
+  dim3 gA, gB, gC, gD, gE;  // K1 (op), K2 (update), K3 (p update), BC fill, curl-curl edge pass
+  unsigned npbP;            // perimeter plane blocks (BC fill)
   bool bc;
 };
 
 }  // namespace mg
 
 using namespace mg;
+
+// multigrid preconditioner (mgpcg.cu)
+struct MGHier;
+struct moons_pcg;
+int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const mg::DBC& bc, const mg::DF* kf, MGHier** out);
+void mg_free(MGHier* h);
+int mg_vcycle(MGHier* h, mg::DF z, mg::DF r, cudaStream_t st, const mg::PcgScalars* S);
+double* mg_rprev(MGHier* h);
 
 // ---------------------------------------------------------------------------
 // the PCG object
@@ -178,10 +185,6 @@ struct moons_pcg {
   unsigned* ticket = nullptr;
   size_t max_blocks = 0;
   std::vector<void*> allocs;
-  // persistent solver: grid barrier state, block partials, resident grid
-  GridSync* gs = nullptr;
-  double* ppart = nullptr;
-  unsigned coop_grid = 0;
   // lean kernels: grids, and the CUDA graph of the loop (rebuilt when x changes)
   int nsm = 0;
   LeanGrids lg{};
@@ -189,6 +192,7 @@ struct moons_pcg {
   cudaGraphExec_t exec = nullptr;
   double* gx[3] = {nullptr, nullptr, nullptr};
   long long body_launches = 0;  // kernels per execution of the loop body
+  MGHier* mgh = nullptr;        // MOONS_PREC_MG / MG_MIXED: the V-cycle hierarchy
 };
 
 namespace {
@@ -219,16 +223,6 @@ unsigned red_grid(const DF* a, int nc) {
   size_t n = 0;
   for (int c = 0; c < nc; c++) n += a[c].n();
   return (unsigned)std::min<size_t>(kRedBlocks, std::max<size_t>(1, (n + kBlock - 1) / kBlock));
-}
-// (plane blocks, k chunks, component) grid of the lean kernels
-dim3 lgrid(const DF* a, int nc) {
-  unsigned npb = 0, kz = 0;
-  for (int c = 0; c < nc; c++) {
-    const PlaneSplit q = plane_split(a[c].s0, a[c].s1, a[c].dl);
-    npb = std::max(npb, q.npbI + q.npbP);
-    kz = std::max(kz, (unsigned)a[c].s2);
-  }
-  return dim3(npb, (kz + kKC - 1) / kKC, (unsigned)nc);
 }
 // (plane chunk, k, component) grid covering nc fields
 dim3 fgrid(const DF* a, int nc) {
@@ -303,6 +297,7 @@ int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
 int compute_prec(moons_pcg* s) {
   moons_mesh* m = s->m;
   int mode = s->prec;
+  if (mode == MOONS_PREC_MG || mode == MOONS_PREC_MG_MIXED) mode = MOONS_PREC_IDENTITY;  // Minv unused
   DF dummy{};
   if (mode == MOONS_PREC_IND && s->op != MOONS_OP_IND_DIFFUSION) {
     set_error("moons_pcg: prec_ind needs the induction operator's sigma^-1 edge fields");
@@ -318,11 +313,6 @@ int compute_prec(moons_pcg* s) {
   return MOONS_OK;
 }
 
-int minv_mode(const moons_pcg* s) {
-  if (s->prec == MOONS_PREC_LAP) return 1;
-  if (s->prec == MOONS_PREC_MOM) return 2;
-  return 0;
-}
 
 // one PCG iteration (PCG_solver_algorithm.f90:69-96), enqueued on the mesh stream
 constexpr int kKCU = kKC;  // planes per thread of the pointwise kernels
@@ -337,7 +327,10 @@ unsigned resident_grid(const moons_pcg* s, const void* kern, size_t items) {
 
 // one PCG iteration (PCG_solver_algorithm.f90:69-96) as five grid-stride
 // kernels, twice: p -> p2 -> p (K3 reads one buffer and writes the other)
+int enqueue_mg_iteration(moons_pcg* s, DF* x);
+
 int enqueue_iteration(moons_pcg* s, DF* x) {
+  if (s->mgh) return enqueue_mg_iteration(s, x);
   moons_mesh* m = s->m;
   FBC b[3];
   for (int c = 0; c < 3; c++) {
@@ -348,7 +341,6 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
   unsigned* tA = s->ticket;
   unsigned* tB = s->ticket + 1;
   DF z0{};
-  int mm = minv_mode(s);
   const int nc = s->nc;
   for (int half = 0; half < 2; half++) {
     DF* pc = half == 0 ? s->p : s->p2;
@@ -356,69 +348,106 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
     switch (s->op) {
       case MOONS_OP_LAP_UNIFORM:
         MG_LAUNCH(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
-                  0.0, L.npb, L.nkc, s->S, s->partial, tA);
+                  0.0, s->S, s->partial, tA);
         break;
       case MOONS_OP_LAP_PROPS:
         MG_LAUNCH(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], s->k[0],
-                  s->k[1], s->k[2], 0.0, L.npb, L.nkc, s->S, s->partial, tA);
+                  s->k[1], s->k[2], 0.0, s->S, s->partial, tA);
         break;
       case MOONS_OP_MOM_DIFFUSION:
         MG_LAUNCH(k_l_lap<2>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
-                  s->coeff, L.npb, L.nkc, s->S, s->partial, tA);
+                  s->coeff, s->S, s->partial, tA);
         break;
       case MOONS_OP_IND_DIFFUSION:
         MG_LAUNCH(k_l_curl_sig, L.gE, kLB, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(pc, 3), s->k[0],
-                  s->k[1], s->k[2], m->dg, L.npbE, L.nkcE, s->S);
+                  s->k[1], s->k[2], m->dg, s->S);
         MG_LAUNCH(k_l_curl_ap, L.gA, kLB, m->stream, fc(s->Ax, 3), fc(pc, 3), s->tempk[0], s->tempk[1], s->tempk[2],
-                  m->dg, b[0], b[1], b[2], s->coeff, L.npb, L.nkc, s->S, s->partial, tA);
+                  m->dg, b[0], b[1], b[2], s->coeff, s->S, s->partial, tA);
         break;
     }
     MG_LAUNCH(k_l_update<kKCU>, L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc), fc(s->Ax, nc),
-              fc(s->Minv, nc), m->dg, mm, s->coeff, b[0], b[1], b[2], L.npb, L.nkcU, s->S, s->partial, tB);
-    MG_LAUNCH(k_l_pupd<kKCU>, L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc), fc(s->Minv, nc), m->dg, mm,
-              s->coeff, b[0], b[1], b[2], L.npb, L.nkcU, s->S);
-    if (L.bc)
-      MG_LAUNCH(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, nc), b[0], b[1], b[2], L.npbP, L.npbI, L.nkc, s->S);
+              fc(s->Minv, nc), b[0], b[1], b[2], s->S, s->partial, tB);
+    MG_LAUNCH(k_l_pupd<kKCU>, L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc), fc(s->Minv, nc), s->S);
+    if (L.bc) MG_LAUNCH(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, nc), b[0], b[1], b[2], L.npbP, s->S);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
 
-// sizes and grids of the lean kernels (set once at create)
+// one multigrid-preconditioned CG iteration, twice (p -> p2 -> p)
+int enqueue_mg_iteration(moons_pcg* s, DF* x) {
+  moons_mesh* m = s->m;
+  FBC b[3];
+  for (int c = 0; c < 3; c++) b[c] = fbc_of(s->x_bc[0], s->xbc_bc[0], s->x_dl[0], s->Ax[0]);
+  const LeanGrids& L = s->lg;
+  unsigned* tA = s->ticket;
+  unsigned* tB = s->ticket + 1;
+  DF z0{};
+  const unsigned gF = resident_grid(s, (const void*)k_m_update, nblocks(s->r[0].n()));
+  double* rprev = mg_rprev(s->mgh);
+  for (int half = 0; half < 2; half++) {
+    DF* pc = half == 0 ? s->p : s->p2;
+    DF* pn = half == 0 ? s->p2 : s->p;
+    if (s->op == MOONS_OP_LAP_PROPS)
+      MG_LAUNCH(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], s->k[0], s->k[1],
+                s->k[2], 0.0, s->S, s->partial, tA);
+    else
+      MG_LAUNCH(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], z0, z0, z0, 0.0,
+                s->S, s->partial, tA);
+    MG_LAUNCH(k_m_update, gF, kLB, m->stream, x[0], pc[0], s->r[0], s->Ax[0], rprev, s->S, s->partial, tB);
+    int r = mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, s->S);
+    if (r) return r;
+    MG_LAUNCH(k_m_beta, gF, kLB, m->stream, s->z[0], s->r[0], rprev, s->S, s->partial, tA);
+    MG_LAUNCH(k_m_pupd, gF, kLB, m->stream, pn[0], pc[0], s->z[0], s->S);
+    if (L.bc) MG_LAUNCH(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, 1), b[0], b[1], b[2], L.npbP, s->S);
+  }
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+// (plane blocks, k stride, component) grid of a lean kernel over fields a[0..nc):
+// the k stride fills one resident wave (SMs x occupancy)
+dim3 lean_grid(const moons_pcg* s, const void* kern, const DF* a, int nc, int kc) {
+  unsigned npb = 0, nkc = 0;
+  for (int c = 0; c < nc; c++) {
+    const PlaneSplit q = plane_split(a[c].s0, a[c].s1, a[c].dl);
+    npb = std::max(npb, q.npbI + q.npbP);
+    nkc = std::max(nkc, (unsigned)((a[c].s2 + kc - 1) / kc));
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLB, 0);
+  const size_t wave = (size_t)std::max(occ, 1) * (size_t)std::max(s->nsm, 1);
+  const size_t per = (size_t)npb * nc;
+  const unsigned gy = (unsigned)std::max<size_t>(1, std::min<size_t>(nkc, (wave + per - 1) / per));
+  return dim3(npb, gy, (unsigned)nc);
+}
+
+// grids of the lean kernels (set once at create)
 void plan_lean(moons_pcg* s) {
   LeanGrids& L = s->lg;
   const int nc = s->nc;
-  dim3 G = lgrid(s->Ax, nc);
-  L.npb = G.x;
-  L.nkc = G.y;
-  unsigned kz = G.y * kKC;
-  L.nkcU = (kz + kKCU - 1) / kKCU;
-  L.npbP = L.npbI = 0;
-  L.bc = false;
-  for (int c = 0; c < nc; c++) {
-    const PlaneSplit q = plane_split(s->Ax[c].s0, s->Ax[c].s1, s->Ax[c].dl);
-    L.npbP = std::max(L.npbP, q.npbP);
-    L.npbI = std::max(L.npbI, q.npbI);
-    if (s->x_bc[c].defined) L.bc = true;
-  }
-  const size_t items = (size_t)L.npb * L.nkc * nc;
-  const size_t itemsU = (size_t)L.npb * L.nkcU * nc;
   const void* ka = s->op == MOONS_OP_LAP_UNIFORM ? (const void*)k_l_lap<0>
                    : s->op == MOONS_OP_LAP_PROPS ? (const void*)k_l_lap<1>
                    : s->op == MOONS_OP_MOM_DIFFUSION ? (const void*)k_l_lap<2>
                                                     : (const void*)k_l_curl_ap;
-  L.gA = resident_grid(s, ka, items);
-  L.gB = resident_grid(s, (const void*)k_l_update<kKCU>, itemsU);
-  L.gC = resident_grid(s, (const void*)k_l_pupd<kKCU>, itemsU);
-  L.gD = resident_grid(s, (const void*)k_l_bcfill, ((size_t)L.npbP * L.nkc + L.npbI) * nc);
-  L.npbE = L.nkcE = 0;
-  L.gE = 1;
-  if (s->op == MOONS_OP_IND_DIFFUSION) {
-    dim3 GE = lgrid(s->tempk, 3);
-    L.npbE = GE.x;
-    L.nkcE = GE.y;
-    L.gE = resident_grid(s, (const void*)k_l_curl_sig, (size_t)GE.x * GE.y * 3);
+  L.gA = lean_grid(s, ka, s->Ax, nc, kKC);
+  L.gB = lean_grid(s, (const void*)k_l_update<kKCU>, s->Ax, nc, kKCU);
+  L.gC = lean_grid(s, (const void*)k_l_pupd<kKCU>, s->Ax, nc, kKCU);
+  L.gE = dim3(1, 1, 1);
+  if (s->op == MOONS_OP_IND_DIFFUSION) L.gE = lean_grid(s, (const void*)k_l_curl_sig, s->tempk, 3, kKC);
+  // BC fill: perimeter blocks over every plane, then inner blocks (ghost planes)
+  unsigned npbP = 0, npbI = 0, smax = 0;
+  L.bc = false;
+  for (int c = 0; c < nc; c++) {
+    const PlaneSplit q = plane_split(s->Ax[c].s0, s->Ax[c].s1, s->Ax[c].dl);
+    npbP = std::max(npbP, q.npbP);
+    npbI = std::max(npbI, q.npbI);
+    smax = std::max(smax, (unsigned)s->Ax[c].s2);
+    if (s->x_bc[c].defined) L.bc = true;
   }
+  L.npbP = npbP;
+  const unsigned gyD = std::max(1u, std::min(smax, (unsigned)(2 * std::max(s->nsm, 1)) / std::max(1u, npbP * nc)));
+  L.gD = dim3(npbP + npbI, gyD, (unsigned)nc);
 }
 
 int build_graph(moons_pcg* s, DF* x) {
@@ -457,72 +486,6 @@ int build_graph(moons_pcg* s, DF* x) {
   return MOONS_OK;
 }
 
-// the persistent kernel instance of an operator
-const void* persist_kernel(int op) {
-  switch (op) {
-    case MOONS_OP_LAP_UNIFORM: return (const void*)k_pcg_persist<0>;
-    case MOONS_OP_LAP_PROPS: return (const void*)k_pcg_persist<1>;
-    case MOONS_OP_MOM_DIFFUSION: return (const void*)k_pcg_persist<2>;
-    default: return (const void*)k_pcg_persist<3>;
-  }
-}
-
-// the whole loop as one cooperative launch (all blocks resident)
-int launch_persistent(moons_pcg* s, DF* x) {
-  moons_mesh* m = s->m;
-  PersistArgs a{};
-  a.X = fc(x, s->nc);
-  a.P0 = fc(s->p, s->nc);
-  a.P1 = fc(s->p2, s->nc);
-  a.R = fc(s->r, s->nc);
-  a.Ap = fc(s->Ax, s->nc);
-  a.M = fc(s->Minv, s->nc);
-  a.g = m->dg;
-  FBC b[3];
-  for (int c = 0; c < 3; c++) {
-    int cc = c < s->nc ? c : 0;
-    b[c] = fbc_of(s->x_bc[cc], s->xbc_bc[cc], s->x_dl[cc], s->Ax[cc]);
-  }
-  a.b0 = b[0];
-  a.b1 = b[1];
-  a.b2 = b[2];
-  a.k0 = s->k[0];
-  a.k1 = s->k[1];
-  a.k2 = s->k[2];
-  a.E0 = s->tempk[0];
-  a.E1 = s->tempk[1];
-  a.E2 = s->tempk[2];
-  a.coeff = s->coeff;
-  a.mm = minv_mode(s);
-  dim3 G = lgrid(s->Ax, s->nc);
-  a.npb = G.x;
-  a.nkc = G.y;
-  a.nkcB = (G.y * kKC + kKCB - 1) / kKCB;
-  a.npbE = a.nkcE = 0;
-  if (s->op == MOONS_OP_IND_DIFFUSION) {
-    dim3 GE = lgrid(s->tempk, 3);
-    a.npbE = GE.x;
-    a.nkcE = GE.y;
-  }
-  a.S = s->S;
-  a.part = s->ppart;
-  a.gs = s->gs;
-  MG_CUDA(cudaMemsetAsync(s->gs, 0, sizeof(GridSync), m->stream));
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(s->coop_grid, 1, 1);
-  cfg.blockDim = dim3(kLB, 1, 1);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = m->stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  void* args[] = {&a};
-  MG_CUDA(cudaLaunchKernelExC(&cfg, persist_kernel(s->op), args));
-  ++g_launch_count;
-  return MOONS_OK;
-}
 
 }  // namespace
 
@@ -538,7 +501,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: ncomp must be 1 or 3");
     return MOONS_ERR_ARG;
   }
-  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_MOM_DIFFUSION || prec < 0 || prec > MOONS_PREC_IND) {
+  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_MOM_DIFFUSION || prec < 0 || prec > MOONS_PREC_MG_MIXED) {
     set_error("moons_pcg_create: bad operator/preconditioner");
     return MOONS_ERR_ARG;
   }
@@ -550,6 +513,21 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
   if (needk && (!k || !k[0] || !k[1] || !k[2])) {
     set_error("moons_pcg_create: operator needs three coefficient fields");
     return MOONS_ERR_ARG;
+  }
+  const bool use_mg = prec == MOONS_PREC_MG || prec == MOONS_PREC_MG_MIXED;
+  if (use_mg) {
+    bool ok = nc == 1 && (op == MOONS_OP_LAP_UNIFORM || op == MOONS_OP_LAP_PROPS) && x[0] &&
+              x[0]->f.dl == MOONS_CC;
+    if (ok && x[0]->bc.defined)
+      for (int f = 1; f <= 6; f++) {
+        const int t = x[0]->bc.type[f];
+        if (t != MOONS_BC_DIRICHLET && t != MOONS_BC_NEUMANN && t != MOONS_BC_PERIODIC) ok = false;
+      }
+    if (!ok) {
+      set_error("moons_pcg_create: multigrid needs one CC unknown, LAP_UNIFORM or LAP_PROPS, and "
+                "Dirichlet/Neumann/periodic BCs");
+      return MOONS_ERR_ARG;
+    }
   }
   cudaSetDevice(m->device);
   auto* s = new moons_pcg();
@@ -591,14 +569,15 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     }
   }
   if (!r) {
-    dim3 G = lgrid(s->Ax, nc);
-    size_t nb = (size_t)G.x * G.y * G.z;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    s->nsm = nsm;
+    plan_lean(s);
+    const LeanGrids& L = s->lg;
     dim3 G2 = fgrid(s->Ax, nc);
-    nb = std::max(nb, (size_t)G2.x * G2.y * G2.z);
-    if (needk) {
-      dim3 GE = lgrid(s->tempk, 3);
-      nb = std::max(nb, (size_t)GE.x * GE.y * GE.z);
-    }
+    size_t nb = (size_t)G2.x * G2.y * G2.z;
+    for (const dim3& g : {L.gA, L.gB, L.gC, L.gD, L.gE}) nb = std::max(nb, (size_t)g.x * g.y * g.z);
+    nb = std::max<size_t>(nb, kRedBlocks);
     s->max_blocks = nb;
     void* p;
     if (cudaMalloc(&p, sizeof(PcgScalars)) != cudaSuccess) r = MOONS_ERR_NOMEM;
@@ -617,36 +596,6 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
       s->ticket = (unsigned*)p;
       s->allocs.push_back(p);
       cudaMemsetAsync(p, 0, sizeof(unsigned) * 4, m->stream);
-    }
-    // persistent solver: as many blocks as can be resident, at most one per work item
-    if (!r) {
-      int coop = 0, nsm = 0, occ = 0;
-      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m->device);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-      s->nsm = nsm;
-      plan_lean(s);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, persist_kernel(op), kLB, 0);
-      size_t items = (size_t)G.x * G.y * G.z;
-      if (needk && op == MOONS_OP_IND_DIFFUSION) {
-        dim3 GE = lgrid(s->tempk, 3);
-        items = std::max(items, (size_t)GE.x * GE.y * GE.z);
-      }
-      if (!coop || occ < 1 || nsm < 1) {
-        set_error("moons_pcg_create: the device cannot run the cooperative PCG kernel");
-        r = MOONS_ERR_CUDA;
-      } else {
-        s->coop_grid = (unsigned)std::min<size_t>((size_t)occ * nsm, items);
-      }
-    }
-    if (!r && cudaMalloc(&p, sizeof(GridSync)) != cudaSuccess) r = MOONS_ERR_NOMEM;
-    else if (!r) {
-      s->gs = (GridSync*)p;
-      s->allocs.push_back(p);
-    }
-    if (!r && cudaMalloc(&p, sizeof(double) * 3 * s->coop_grid) != cudaSuccess) r = MOONS_ERR_NOMEM;
-    else if (!r) {
-      s->ppart = (double*)p;
-      s->allocs.push_back(p);
     }
     if (!r && cudaMallocHost(&p, sizeof(PcgScalars)) != cudaSuccess) r = MOONS_ERR_NOMEM;
     else if (!r) s->hS = (PcgScalars*)p;
@@ -672,6 +621,10 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
       s->volsum[c] = t;
     }
   }
+  if (!r && use_mg) {
+    r = mg_build(s, m, prec == MOONS_PREC_MG_MIXED, s->x_bc[0], op == MOONS_OP_LAP_PROPS ? s->k : nullptr, &s->mgh);
+    if (r == MOONS_ERR_NOMEM) set_error("moons_pcg_create: device allocation failed (multigrid levels)");
+  }
   if (!r && cudaStreamSynchronize(m->stream) != cudaSuccess) r = cuda_fail(cudaGetLastError(), "pcg create");
   if (r) {
     moons_pcg_destroy(s);
@@ -687,6 +640,7 @@ int moons_pcg_destroy(moons_pcg* s) {
   if (!s) return MOONS_OK;
   cudaSetDevice(s->m->device);
   cudaStreamSynchronize(s->m->stream);
+  if (s->mgh) mg_free(s->mgh);
   for (void* p : s->allocs) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
   moons_mesh* m = s->m;
@@ -721,7 +675,6 @@ __global__ void k_pcg_clear_acc(PcgScalars* S) {
   S->iter_total = 0;
   S->runs_total = 0;
   S->nan_any = 0;
-  S->sync_err = 0;
 }
 }  // namespace mg
 
@@ -739,10 +692,6 @@ int mg_pcg_totals(moons_pcg* s, int* iters, int* nan_any, double* last_rel) {
   const PcgScalars& H = *s->hS;
   g_launch_count += s->body_launches * (long long)H.runs_total;
   *iters = H.iter_total;
-  if (H.sync_err) {
-    set_error("moons_pcg: a grid barrier of the persistent solver timed out");
-    return MOONS_ERR_CUDA;
-  }
   *nan_any = H.nan_any;
   if (last_rel) *last_rel = (H.res0 == 0.0) ? H.res : H.res / H.res0;
   return MOONS_OK;
@@ -801,9 +750,15 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
   MG_LAUNCH(k_reduce, red_grid(s->r, nc), kBlock, m->stream, c3(s->r, nc), c3(s->r, nc), 1, 0, 0, 0, &s->S->res0,
             m->d_partial, m->d_ticket);
   // z = Minv r ; p = z ; rhok = dot(r,z)
+  if (s->mgh) {
+    r = mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, nullptr);
+    if (r) return r;
+  }
   for (int c = 0; c < nc; c++) {
-    launch_pw(m, PW_COPY, s->z[c], &s->Minv[c], 0.0);
-    launch_pw(m, PW_MUL, s->z[c], &s->r[c], 0.0);
+    if (!s->mgh) {
+      launch_pw(m, PW_COPY, s->z[c], &s->Minv[c], 0.0);
+      launch_pw(m, PW_MUL, s->z[c], &s->r[c], 0.0);
+    }
     launch_pw(m, PW_COPY, s->p[c], &s->z[c], 0.0);
     launch_bcs(m, s->p[c], s->x_bc[c], true);  // the iteration kernels read p with its implicit BCs
   }
@@ -831,21 +786,13 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
     for (int c = 0; c < nc && !r; c++) r = launch_bcs(m, X[c], s->x_bc[c], false);
     return r;
   }
-  static const bool persist = [] {
-    const char* e = getenv("MOONS_PCG_MODE");
-    return e && strcmp(e, "persistent") == 0;
-  }();
-  if (persist) {
-    r = launch_persistent(s, X);
-  } else {
-    bool need_graph = !s->exec;
-    for (int c = 0; c < nc; c++)
-      if (s->gx[c] != X[c].f) need_graph = true;
-    if (need_graph) r = build_graph(s, X);
-    if (!r) {
-      cudaError_t e = cudaGraphLaunch(s->exec, m->stream);
-      if (e != cudaSuccess) r = cuda_fail(e, "cudaGraphLaunch");
-    }
+  bool need_graph = !s->exec;
+  for (int c = 0; c < nc; c++)
+    if (s->gx[c] != X[c].f) need_graph = true;
+  if (need_graph) r = build_graph(s, X);
+  if (!r) {
+    cudaError_t e = cudaGraphLaunch(s->exec, m->stream);
+    if (e != cudaSuccess) r = cuda_fail(e, "cudaGraphLaunch");
   }
   if (r) return r;
   // x: apply_BCs (the reference applies them after every update; they only
@@ -868,10 +815,6 @@ int mg_pcg_collect(moons_pcg* s, moons_solve_info* info, float ms) {
     info->rel = (H.res0 == 0.0) ? H.res : H.res / H.res0;
     info->exit_reason = H.exit_reason;
     info->ms = ms;
-  }
-  if (H.sync_err) {
-    set_error("moons_pcg_solve: a grid barrier of the persistent solver timed out");
-    return MOONS_ERR_CUDA;
   }
   if (H.nan || std::isnan(H.res0) || std::isnan(H.res)) {
     set_error("moons_pcg_solve: NaN in residual norms");
