@@ -42,7 +42,32 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="moons", choices=["moons", "reference"])
     ap.add_argument("--small", action="store_true", help="small mesh (debug only)")
+    ap.add_argument("--profile", choices=["step", "jacobi", "mg", "mixed"], default=None,
+                    help="profiling run for ncu launch lists: one duct step, or one duct pressure solve with the "
+                         "given preconditioner capped at --profile-iters iterations; prints what ran, no bench line")
+    ap.add_argument("--profile-iters", type=int, default=40)
     return ap.parse_args()
+
+
+def run_profile(args):
+    from moons_b200 import capi as G, configs
+    kw = duct_kw(args.small)
+    if args.profile == "step":
+        sim = configs.make(G, configs.duct, seed=0, **kw)
+        info = sim.step(1)
+        print(json.dumps({"profile": "step", "workload": WORKLOAD, "info": info}), flush=True)
+        return
+    prec = {"jacobi": G.PREC_LAP, "mg": G.PREC_MG, "mixed": G.PREC_MG_MIXED}[args.profile]
+    mom, _, prm, _ = configs.duct(**kw)
+    m = G.Mesh(*mom)
+    p = m.field(G.CC)
+    p.set_bcs(prm.bc_p)
+    b = m.field(G.CC)
+    b.upload(np.random.default_rng(7).standard_normal(b.shape))
+    s = G.PCG(m, G.OP_LAP_UNIFORM, prec, [p], [p])
+    info = s.solve([p], [b], G.isp(args.profile_iters, 1e-10, 1e-300))
+    print(json.dumps({"profile": args.profile, "workload": "duct pressure Poisson " + str(list(b.shape)),
+                      "info": info}), flush=True)
 
 
 def duct_kw(small):
@@ -223,6 +248,9 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.profile:
+        run_profile(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -310,9 +338,9 @@ def main():
             "poisson": {"ms_to_1e-10": pinfo["ms"], "iterations": pinfo["iterations"], "rel": pinfo["rel"],
                         "cells": ncc, "solver": "FP64 Jacobi-PCG (reference algorithm)",
                         "mg_fp64": {"ms_to_1e-10": mginfo["ms"], "iterations": mginfo["iterations"],
-                                    "rel": mginfo["rel"], "solver": "CG + FP64 multigrid V(1,1)"},
+                                    "rel": mginfo["rel"], "solver": "CG + FP64 multigrid V(2,2), red-black SOR 1.15"},
                         "mixed": {"ms_to_1e-10": mxinfo["ms"], "iterations": mxinfo["iterations"],
-                                  "rel": mxinfo["rel"], "solver": "FP64 flexible CG + FP32 multigrid V(1,1)"},
+                                  "rel": mxinfo["rel"], "solver": "FP64 flexible CG + FP32 multigrid V(2,2), red-black SOR 1.15"},
                         "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"]},
             "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (duct fluid mesh)",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",

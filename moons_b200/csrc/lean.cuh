@@ -598,8 +598,8 @@ __device__ __forceinline__ void bcfill_point(const DF& p, const FBC& b, int i, i
   p(i, j, k) = s.fac * v;
 }
 // block x < npbP: perimeter columns, every plane (strided over blockIdx.y);
-// block x >= npbP: inner columns, ghost planes and node-located boundary
-// planes (blockIdx.y = 0 only)
+// block x >= npbP: inner columns, one ghost plane or node-located boundary
+// plane per blockIdx.y = 0..3
 __device__ __forceinline__ void bcfill_col(const DF& p, const FBC& b, unsigned npbP) {
   if (!b.defined) return;
   const PlaneSplit q = plane_split(p.s0, p.s1, p.dl);
@@ -610,15 +610,12 @@ __device__ __forceinline__ void bcfill_col(const DF& p, const FBC& b, unsigned n
     for (int k = blockIdx.y + 1; k <= p.s2; k += gridDim.y) bcfill_point(p, b, cl.i, cl.j, k);
   } else {
     const unsigned pi = blockIdx.x - npbP;
-    if (pi >= q.npbI || blockIdx.y != 0) return;
+    const bool Nz = n_along(p.dl, 3);
+    if (pi >= q.npbI || blockIdx.y >= (Nz ? 4u : 2u)) return;
     const Col cl = col_of(p, pi);
     if (!cl.ok) return;
-    bcfill_point(p, b, cl.i, cl.j, 1);
-    bcfill_point(p, b, cl.i, cl.j, p.s2);
-    if (n_along(p.dl, 3)) {
-      bcfill_point(p, b, cl.i, cl.j, 2);
-      bcfill_point(p, b, cl.i, cl.j, p.s2 - 1);
-    }
+    const int k = blockIdx.y == 0 ? 1 : (blockIdx.y == 1 ? p.s2 : (blockIdx.y == 2 ? 2 : p.s2 - 1));
+    bcfill_point(p, b, cl.i, cl.j, k);
   }
 }
 __global__ void __launch_bounds__(kLB) k_l_bcfill(FComp P, FBC b0, FBC b1, FBC b2, unsigned npbP, PcgScalars* S) {

@@ -23,7 +23,11 @@ using namespace mg;
 struct MGHier {
   bool mixed = false;
   int nl = 0;
-  int sweeps_coarse = 24;
+  int sweeps_coarse = 24;  // coarsest level without a dense inverse
+  int nu = 2;              // red-black sweeps before and after the coarse correction
+  double omega = 1.15;     // over-relaxation of the sweeps
+  int nsm = 148;
+  int occ[4] = {1, 1, 1, 1};  // resident blocks per SM: smooth, resid, restrict, prolong
   std::vector<std::array<int, 3>> s;  // CC extents per level
   std::vector<MGLev<double>> Ld;
   std::vector<MGLev<float>> Lf;
@@ -411,6 +415,20 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
       }
     }
   }
+  {
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    h->nsm = std::max(nsm, 1);
+    const void* ks[2][4] = {{(const void*)k_mg_smooth<double>, (const void*)k_mg_resid<double>,
+                             (const void*)k_mg_restrict<double>, (const void*)k_mg_prolong<double>},
+                            {(const void*)k_mg_smooth<float>, (const void*)k_mg_resid<float>,
+                             (const void*)k_mg_restrict<float>, (const void*)k_mg_prolong<float>}};
+    for (int q = 0; q < 4; q++) {
+      int occ = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ks[h->mixed ? 1 : 0][q], 256, 0);
+      h->occ[q] = std::max(occ, 1);
+    }
+  }
   MG_CUDA(cudaStreamSynchronize(st));
   *out = h.release();
   return MOONS_OK;
@@ -420,7 +438,10 @@ void mg_free(MGHier* h) { delete h; }
 double* mg_rprev(MGHier* h) { return h->rprev; }
 
 namespace {
-unsigned vgrid(size_t n) { return (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 8)); }
+// grid-stride kernels: at most one resident wave
+unsigned vgrid(size_t n, int occ = 8, int nsm = 148) {
+  return (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)occ * nsm));
+}
 
 template <typename T>
 const T* coarse_inv(const MGHier* h);
@@ -434,12 +455,16 @@ int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::a
              const std::vector<std::array<MGRest<T>, 3>>& R, cudaStream_t st, const PcgScalars* S) {
   const int nl = h->nl;
   auto npts = [&](int l) { return (size_t)(L[l].s0 - 2) * (L[l].s1 - 2) * (L[l].s2 - 2); };
+  const T om = (T)h->omega;
   for (int l = 0; l < nl - 1; l++) {  // down: pre-smooth, residual, restrict
-    const unsigned g = vgrid(npts(l) / 2 + 1);
-    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, 1, S);
-    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, S);
-    MG_LAUNCH(k_mg_resid<T>, vgrid(npts(l)), 256, st, L[l], S);
-    MG_LAUNCH(k_mg_restrict<T>, vgrid(npts(l + 1)), 256, st, L[l], L[l + 1], R[l + 1][0], R[l + 1][1], R[l + 1][2], S);
+    const unsigned g = vgrid(npts(l) / 2 + 1, h->occ[0], h->nsm);
+    for (int q = 0; q < h->nu; q++) {
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, q == 0 ? 1 : 0, om, S);
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, om, S);
+    }
+    MG_LAUNCH(k_mg_resid<T>, vgrid(npts(l), h->occ[1], h->nsm), 256, st, L[l], S);
+    MG_LAUNCH(k_mg_restrict<T>, vgrid(npts(l + 1), h->occ[2], h->nsm), 256, st, L[l], L[l + 1], R[l + 1][0],
+              R[l + 1][1], R[l + 1][2], S);
   }
   if (h->ncoarse > 0)
     MG_LAUNCH(k_mg_direct<T>, (unsigned)((h->ncoarse + 255) / 256), 256, st, L[nl - 1], coarse_inv<T>(h), h->ncoarse,
@@ -447,10 +472,13 @@ int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::a
   else
     MG_LAUNCH(k_mg_coarse<T>, 1, 256, st, L[nl - 1], h->sweeps_coarse, S);
   for (int l = nl - 2; l >= 0; l--) {  // up: prolong + correct, post-smooth (reverse colours)
-    const unsigned g = vgrid(npts(l) / 2 + 1);
-    MG_LAUNCH(k_mg_prolong<T>, vgrid(npts(l)), 256, st, L[l], L[l + 1], P[l + 1][0], P[l + 1][1], P[l + 1][2], S);
-    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, S);
-    MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, 0, S);
+    const unsigned g = vgrid(npts(l) / 2 + 1, h->occ[0], h->nsm);
+    MG_LAUNCH(k_mg_prolong<T>, vgrid(npts(l), h->occ[3], h->nsm), 256, st, L[l], L[l + 1], P[l + 1][0], P[l + 1][1],
+              P[l + 1][2], S);
+    for (int q = 0; q < h->nu; q++) {
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, om, S);
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, 0, om, S);
+    }
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;

@@ -16,14 +16,15 @@
 //    and plain CG may use it (the reference's restrict_C is the
 //    volume-weighted average; its index expressions for the transverse
 //    directions read `i` where `j`/`k` are meant, GF_restrict.f90:38-39);
-//  * smoothing is red-black Gauss-Seidel (redBlack with omega = 1) on the
-//    volume-weighted operator, forward (red, black) before the coarse
-//    correction and backward (black, red) after it;
+//  * smoothing is red-black SOR (redBlack, omega = 1.15) on the
+//    volume-weighted operator, two forward sweeps (red, black) before the
+//    coarse correction and two backward ones (black, red) after it;
 //  * ghost values are never stored: a neighbour index on a ghost plane is
 //    resolved through the level's homogeneous BCs (Dirichlet -u, Neumann u,
 //    periodic opposite side), exactly as apply_BCs_implicit fills them;
-//  * the coarsest level is solved by a fixed number of symmetric
-//    red-black sweeps inside one block.
+//  * the coarsest level is solved directly (dense inverse built on the host,
+//    regularised on the constants when no face is Dirichlet), or by a fixed
+//    number of symmetric red-black sweeps inside one block when too large.
 // Everything is templated on the arithmetic type: T = double for the plain
 // path, T = float for the mixed-precision path (V-cycle in FP32 inside an
 // FP64 flexible CG).
@@ -102,6 +103,18 @@ __device__ __forceinline__ T ev(const MGLev<T>& L, const T* e, int i, int j, int
   return fac * e[lidx(L, I[0], I[1], I[2])];
 }
 
+// factor by which the ghost neighbour on side `hi` of axis d (index t of the
+// point) repeats the point itself (Neumann +1, Dirichlet -1), 0 otherwise:
+// that share belongs to the operator's true diagonal
+template <typename T>
+__device__ __forceinline__ T self_ghost(const MGLev<T>& L, int d, bool hi, int t) {
+  const int s = d == 0 ? L.s0 : (d == 1 ? L.s1 : L.s2);
+  if (hi ? t != s - 1 : t != 2) return T(0);
+  const int ty = L.bt[2 * d + (hi ? 2 : 1)];
+  if (ty == MOONS_BC_PERIODIC) return T(0);
+  return ty == MOONS_BC_DIRICHLET ? T(-1) : T(1);
+}
+
 // index of face (i,j,k) of a face-`d` array on the level's grid (the face
 // array has one more entry along d)
 template <typename T>
@@ -110,8 +123,23 @@ __device__ __forceinline__ size_t fidx(const MGLev<T>& L, int d, int i, int j, i
   return (size_t)((unsigned)(i - 1) + f0 * ((unsigned)(j - 1) + f1 * (unsigned)(k - 1)));
 }
 
+// diagonal share of the ghost neighbours that repeat the point (per unit volume)
+template <typename T>
+__device__ __forceinline__ T diag_self(const MGLev<T>& L, const MGAxis<T>& A, const T* kf, int d, int i, int j, int k,
+                                       int t) {
+  const T flo = self_ghost(L, d, false, t), fhi = self_ghost(L, d, true, t);
+  if (flo == T(0) && fhi == T(0)) return T(0);
+  const int di = d == 0, dj = d == 1, dk = d == 2;
+  T kl = T(1), kr = T(1);
+  if (kf) {
+    kl = kf[fidx(L, d, i, j, k)];
+    kr = kf[fidx(L, d, i + di, j + dj, k + dk)];
+  }
+  return flo * (A.cD[t - 1] * kl) * A.nD[t] + fhi * (A.cU[t] * kr) * A.nU[t];
+}
+
 // (A e)(i,j,k) = vol * div(k grad e) at an interior point (k = 1 without
-// face coefficients), and its diagonal D (the smoother's divisor)
+// face coefficients), and its true diagonal D (the smoother's divisor)
 template <typename T>
 __device__ __forceinline__ T apply_A(const MGLev<T>& L, const T* e, int i, int j, int k, T& D) {
   const size_t id = lidx(L, i, j, k);
@@ -142,6 +170,7 @@ __device__ __forceinline__ T apply_A(const MGLev<T>& L, const T* e, int i, int j
     }
     v = v + (gl * A.nD[t] + gr * A.nU[t]);
     dg = dg + (dgl * A.nD[t] + dgr * A.nU[t]);
+    if (!inner) dg = dg + diag_self<T>(L, A, kf, d, i, j, k, t);
   }
   const T vol = (L.ax[0].hv[i] * L.ax[1].hv[j]) * L.ax[2].hv[k];
   D = dg * vol;
@@ -165,6 +194,7 @@ __device__ __forceinline__ T diag_A(const MGLev<T>& L, int i, int j, int k) {
       dgr = dgr * kf[fidx(L, d, i + di, j + dj, k + dk)];
     }
     dg = dg + (dgl * A.nD[t] + dgr * A.nU[t]);
+    dg = dg + diag_self<T>(L, A, kf, d, i, j, k, t);
   }
   return dg * ((L.ax[0].hv[i] * L.ax[1].hv[j]) * L.ax[2].hv[k]);
 }
@@ -172,7 +202,7 @@ __device__ __forceinline__ T diag_A(const MGLev<T>& L, int i, int j, int k) {
 // one red-black half sweep of colour `color` (points with (i+j+k)&1 == color).
 // first != 0: e starts at zero (both colours are written).
 template <typename T>
-__global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int first, const PcgScalars* S) {
+__global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int first, T omega, const PcgScalars* S) {
   if (S && S->done) return;
   const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
   const int nxh = (nx + 1) / 2;
@@ -192,11 +222,11 @@ __global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int fi
     const size_t id = lidx(L, i, j, k);
     if (first) {
       // e = 0 everywhere before this sweep, so A e = 0 and e = r / D
-      L.e[id] = L.r[id] / diag_A<T>(L, i, j, k);
+      L.e[id] = omega * L.r[id] / diag_A<T>(L, i, j, k);
     } else {
       T D;
       const T Ae = apply_A<T>(L, L.e, i, j, k, D);
-      L.e[id] = L.e[id] + (L.r[id] - Ae) / D;
+      L.e[id] = L.e[id] + omega * (L.r[id] - Ae) / D;
     }
   }
 }

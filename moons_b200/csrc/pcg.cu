@@ -418,7 +418,7 @@ dim3 lean_grid(const moons_pcg* s, const void* kern, const DF* a, int nc, int kc
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLB, 0);
   const size_t wave = (size_t)std::max(occ, 1) * (size_t)std::max(s->nsm, 1);
   const size_t per = (size_t)npb * nc;
-  const unsigned gy = (unsigned)std::max<size_t>(1, std::min<size_t>(nkc, (wave + per - 1) / per));
+  const unsigned gy = (unsigned)std::max<size_t>(1, std::min<size_t>(nkc, wave / per));  // never a partial 2nd wave
   return dim3(npb, gy, (unsigned)nc);
 }
 
@@ -446,7 +446,7 @@ void plan_lean(moons_pcg* s) {
     if (s->x_bc[c].defined) L.bc = true;
   }
   L.npbP = npbP;
-  const unsigned gyD = std::max(1u, std::min(smax, (unsigned)(2 * std::max(s->nsm, 1)) / std::max(1u, npbP * nc)));
+  const unsigned gyD = std::max(4u, std::min(smax, (unsigned)(2 * std::max(s->nsm, 1)) / std::max(1u, npbP * nc)));
   L.gD = dim3(npbP + npbI, gyD, (unsigned)nc);
 }
 
