@@ -245,6 +245,11 @@ typedef struct {
   int prescribed_Ustar;     /* SP%VS%U%SS%prescribed_BCs: Ustar gets prescribed
                                BCs (set_prescribed_BCs, block_field_extend.f90:810-821) */
   int prescribed_Bstar;     /* SP%VS%B%SS%prescribed_BCs                      */
+  int prec_poisson;         /* preconditioner of the pressure and potential
+                               solves: 0 (default) = the reference's prec_Lap,
+                               or MOONS_PREC_MG / MOONS_PREC_MG_MIXED (no
+                               reference counterpart: same system, same exit
+                               tests, far fewer iterations)                   */
 } moons_mhd_params;
 
 typedef struct {

@@ -98,6 +98,7 @@ class MHDParams(C.Structure):
         ("ind_offset", C.c_int * 3),
         ("prescribed_Ustar", C.c_int),
         ("prescribed_Bstar", C.c_int),
+        ("prec_poisson", C.c_int),
     ]
 
 

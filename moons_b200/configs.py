@@ -148,10 +148,13 @@ def duct(nx: int = 64, ny: int = 64, nz: int = 256, Re: float = 1000.0, Ha: floa
     return mom, ind, prm, init
 
 
-def make(backend, builder, *args, seed: int = 0, **kw):
+def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, **kw):
     """Create meshes + the MHD object on ``backend`` (moons_b200.capi or the
-    oracle module) from a builder, upload the seeded initial state and init."""
+    oracle module) from a builder, upload the seeded initial state and init.
+    ``prec_poisson`` selects the pressure/potential preconditioner (0: the
+    reference's Jacobi prec_Lap; capi.PREC_MG / PREC_MG_MIXED: multigrid)."""
     mom, ind, prm, init = builder(*args, **kw)
+    prm.prec_poisson = prec_poisson
     mm = backend.Mesh(*mom)
     mi = mm if ind is mom else backend.Mesh(*ind)
     sim = backend.MHD(mm, mi, prm)

@@ -8,8 +8,9 @@
 // variant uses the flexible (Polak-Ribiere) beta = z.(r - r_prev) / rho, so
 // the FP32 rounding inside the V-cycle cannot stall the recurrence.
 // Supported: one CC unknown (pressure, potential) with LAP_UNIFORM or
-// LAP_PROPS and Dirichlet / Neumann / periodic BCs, on meshes whose interior
-// cell counts are even (coarsening stops at the first odd count or at 2).
+// LAP_PROPS and Dirichlet / Neumann / periodic BCs.  Each level halves every
+// axis whose interior cell count is even and >= 4 and keeps the others
+// (semi-coarsening), until no axis can be halved.
 #include <array>
 
 #include "mgrid.cuh"
@@ -108,7 +109,7 @@ void resolve(int& I, double& w, int scc, int tlo, int thi) {
   }
 }
 
-Axis1D build_axis(const host::HostCoord& cc, int scf, int tlo, int thi) {
+Axis1D build_axis(const host::HostCoord& cc, int scf, int tlo, int thi, bool coarsened) {
   Axis1D a;
   const int scc = cc.sc;
   a.i0.assign(scf + 1, 2);
@@ -116,7 +117,12 @@ Axis1D build_axis(const host::HostCoord& cc, int scf, int tlo, int thi) {
   a.w0.assign(scf + 1, 0.0);
   a.w1.assign(scf + 1, 0.0);
   std::vector<std::vector<std::pair<int, double>>> cols(scc + 1);
-  for (int f = 2; f <= scf - 1; f++) {
+  for (int f = 2; f <= scf - 1 && !coarsened; f++) {  // axis kept: identity
+    a.i0[f] = a.i1[f] = f;
+    a.w0[f] = 1.0;
+    cols[f].push_back({f, 1.0});
+  }
+  for (int f = 2; f <= scf - 1 && coarsened; f++) {
     const int I = (f + 2) / 2;
     int nb;
     double wp, wn;
@@ -163,7 +169,7 @@ MGAxis<T> axis_tables(MGHier* h, const host::HostCoord& c, cudaStream_t st) {
 
 // area-weighted mean of the fine faces covering each coarse face of axis d
 std::vector<double> coarsen_faces(const std::vector<double>& kf, int d, const std::array<int, 3>& sf,
-                                  const std::array<int, 3>& sc, const host::HostCoord* cf) {
+                                  const std::array<int, 3>& sc, const host::HostCoord* cf, const bool* cz) {
   std::array<int, 3> ef = sf, ec = sc;
   ef[d] += 1;
   ec[d] += 1;
@@ -183,12 +189,12 @@ std::vector<double> coarsen_faces(const std::vector<double>& kf, int d, const st
         }
         if (!inner) continue;
         int F[3];
-        F[d] = 2 * C[d] - 2;  // coincident fine node
+        F[d] = cz[d] ? 2 * C[d] - 2 : C[d];  // coincident fine node
         double num = 0.0, den = 0.0;
-        for (int u = 0; u < 2; u++)
-          for (int v = 0; v < 2; v++) {
-            F[a] = 2 * C[a] - 2 + u;
-            F[b] = 2 * C[b] - 2 + v;
+        for (int u = 0; u < (cz[a] ? 2 : 1); u++)
+          for (int v = 0; v < (cz[b] ? 2 : 1); v++) {
+            F[a] = cz[a] ? 2 * C[a] - 2 + u : C[a];
+            F[b] = cz[b] ? 2 * C[b] - 2 + v : C[b];
             const double w = cf[a].dhn[F[a]] * cf[b].dhn[F[b]];
             num += w * kf[fid(F[0], F[1], F[2])];
             den += w;
@@ -296,22 +302,31 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
   std::array<int, 3> s0 = {m->sn[0] - 1, m->sn[1] - 1, m->sn[2] - 1};
   for (int d = 0; d < 3; d++) C[d].push_back(host::build_coord(m->hn[d].data(), m->sn[d]));
   h->s.push_back(s0);
+  // each level halves every axis whose interior count is even and >= 4 (the
+  // others are kept), until no axis can be halved
+  std::vector<std::array<bool, 3>> coarsened(1, std::array<bool, 3>{false, false, false});
   for (;;) {
     const auto& sl = h->s.back();
-    bool can = true;
+    std::array<bool, 3> cz{};
+    bool any = false;
     for (int d = 0; d < 3; d++) {
       const int N = sl[d] - 2;
-      if (N < 4 || (N & 1)) can = false;
+      cz[d] = N >= 4 && (N & 1) == 0;
+      any = any || cz[d];
     }
-    if (!can || h->s.size() >= 12) break;
+    // small enough for the dense direct solve: stop
+    if ((long)(sl[0] - 2) * (sl[1] - 2) * (sl[2] - 2) <= 512) any = false;
+    if (!any || h->s.size() >= 16) break;
     std::array<int, 3> sc{};
     for (int d = 0; d < 3; d++) {
       const std::vector<double>& hf = C[d].back().hn;  // 1-based
-      std::vector<double> hc = coarsen_nodes(std::vector<double>(hf.begin() + 1, hf.end()));
+      std::vector<double> h0(hf.begin() + 1, hf.end());
+      std::vector<double> hc = cz[d] ? coarsen_nodes(h0) : h0;
       C[d].push_back(host::build_coord(hc.data(), (int)hc.size()));
       sc[d] = (int)hc.size() - 1;
     }
     h->s.push_back(sc);
+    coarsened.push_back(cz);
   }
   h->nl = (int)h->s.size();
   int bt[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -326,7 +341,7 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
     for (int l = 1; l < h->nl; l++)
       for (int d = 0; d < 3; d++) {
         const host::HostCoord cf[3] = {C[0][l - 1], C[1][l - 1], C[2][l - 1]};
-        K[l][d] = coarsen_faces(K[l - 1][d], d, h->s[l - 1], h->s[l], cf);
+        K[l][d] = coarsen_faces(K[l - 1][d], d, h->s[l - 1], h->s[l], cf, coarsened[l].data());
       }
   }
   for (int l = 0; l < h->nl; l++) {
@@ -368,7 +383,7 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
     std::array<MGRest<float>, 3> Rf{};
     if (l > 0) {
       for (int d = 0; d < 3; d++) {
-        Axis1D A = build_axis(C[d][l], h->s[l - 1][d], bt[2 * d + 1], bt[2 * d + 2]);
+        Axis1D A = build_axis(C[d][l], h->s[l - 1][d], bt[2 * d + 1], bt[2 * d + 2], coarsened[l][d]);
         const int* i0 = dev_copy(h.get(), A.i0, st);
         const int* i1 = dev_copy(h.get(), A.i1, st);
         const int* off = dev_copy(h.get(), A.off, st);

@@ -7,7 +7,8 @@
 // solvers/SOR/SOR.f90:234-314 redBlack/init_r) and the V-cycle design of
 // code_not_compiled/9.6.2017/MG/MG.f90:241-396 (not compiled in the
 // reference):
-//  * coarse grids keep every other node of the fine grid (stretching kept);
+//  * coarse grids keep every other node of the fine grid along each axis
+//    whose interior count is even (stretching kept; other axes unchanged);
 //  * prolongation is the reference's prolongate_C: each fine cell takes the
 //    mean of its parent's value and the theta-interpolated value at the
 //    parent's face nearest to it (linear interpolation on stretched grids);
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(256) k_mg_direct(MGLev<T> L, const T* Minv, in
     T acc = T(0);
     for (int c = 0; c < n; c++) {
       const int i = c % nx + 2, q = c / nx, j = q % ny + 2, k = q / ny + 2;
-      acc = acc + Minv[(size_t)row * n + c] * L.r[lidx(L, i, j, k)];
+      acc = acc + Minv[(size_t)c * n + row] * L.r[lidx(L, i, j, k)];  // symmetric: coalesced over rows
     }
     const int i = row % nx + 2, q = row / nx, j = q % ny + 2, k = q / ny + 2;
     L.e[lidx(L, i, j, k)] = acc;
