@@ -315,7 +315,7 @@ int compute_prec(moons_pcg* s) {
 
 
 // one PCG iteration (PCG_solver_algorithm.f90:69-96), enqueued on the mesh stream
-constexpr int kKCU = kKC;  // planes per thread of the pointwise kernels
+constexpr int kKCU = 2;  // planes per thread of the pointwise kernels (measured best)
 
 // grid of a grid-stride kernel: every block resident, at most one per item
 unsigned resident_grid(const moons_pcg* s, const void* kern, size_t items) {
