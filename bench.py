@@ -179,6 +179,60 @@ def poisson_ms(G, kw, prec=None):
     return best, b.n
 
 
+def sigma_shell_poisson(G, n=128, shell=4, seeds_plain=4, seeds_mg=64):
+    """Mixed-precision Poisson case: div(sigma grad phi) = div(u x B) on a
+    128^3 grid with a 10^U(-3,3) wall shell, to 1e-10 relative residual.
+    Mean solve time of the reference's Jacobi-PCG (FP64) over `seeds_plain`
+    seeds, and of multigrid-CG (FP64 V-cycle) and flexible CG with an FP32
+    V-cycle over `seeds_mg` seeds; error of the mixed solution against the
+    FP64 multigrid one (constant removed, all-Neumann)."""
+    from moons_b200 import configs
+    out = {}
+    err = None
+    for name, prec, ns in (("plain_fp64_jacobi", G.PREC_LAP, seeds_plain), ("mg_fp64", G.PREC_MG, seeds_mg),
+                           ("mixed_fp32_vcycle", G.PREC_MG_MIXED, seeds_mg)):
+        ms, its, rel = [], [], []
+        for seed in range(ns):
+            coords, sig, E = configs.sigma_shell(n, shell, seed)
+            m = G.Mesh(*coords)
+            phi = m.field(G.CC)
+            phi.set_bcs(G.bc_spec([G.NEUMANN] * 6, all_neumann=True))
+            ks, es = [], []
+            for d, dl in enumerate((G.FX, G.FY, G.FZ)):
+                k = m.field(dl)
+                k.upload(sig[d])
+                ks.append(k)
+                e = m.field(dl)
+                e.upload(E[d])
+                es.append(e)
+            rhs = m.field(G.CC)
+            G.div(rhs, *es)
+            s = G.PCG(m, G.OP_LAP_PROPS, prec, [phi], [phi], ks)
+            par = G.isp(400000, 1e-10, 1e-300)
+            phi.fill(0.0)
+            s.solve([phi], [rhs], par)  # warm-up (graph build)
+            phi.fill(0.0)
+            info = s.solve([phi], [rhs], par)
+            ms.append(info["ms"])
+            its.append(info["iterations"])
+            rel.append(info["rel"])
+            if seed == 0 and name != "plain_fp64_jacobi":
+                x = phi.download()[1:-1, 1:-1, 1:-1]
+                x = x - x.mean()
+                if name == "mg_fp64":
+                    ref0 = x
+                else:
+                    err = float(np.abs(x - ref0).max() / np.abs(ref0).max())
+            s.close()
+        out[name] = {"ms_mean": float(np.mean(ms)), "iterations_mean": float(np.mean(its)),
+                     "rel_max": float(np.max(rel)), "seeds": ns}
+    out["speedup_mixed_vs_plain"] = out["plain_fp64_jacobi"]["ms_mean"] / out["mixed_fp32_vcycle"]["ms_mean"]
+    out["speedup_mixed_vs_mg_fp64"] = out["mg_fp64"]["ms_mean"] / out["mixed_fp32_vcycle"]["ms_mean"]
+    out["mixed_vs_fp64_solution_max_rel_err_seed0"] = err
+    out["workload"] = f"sigma-weighted Poisson {n}^3 cells, 4-cell wall shell sigma=10^U(-3,3), RHS div(u x B)"
+    return out
+
+
 def cpu_sample(kw, gpu_iters=None):
     """Bounded CPU sample: the oracle (single thread) on the full-size duct.
     It times init + one step with every PCG capped at a few iterations, and
@@ -311,6 +365,8 @@ def main():
     # ---- Poisson ms to 1e-10 + roofline of the pressure PCG iteration
     pinfo, ncc = poisson_ms(G, kw)
     mginfo, _ = poisson_ms(G, kw, G.PREC_MG)
+    shell = sigma_shell_poisson(G, n=32 if args.small else 128, seeds_plain=1 if args.small else 4,
+                                seeds_mg=2 if args.small else 16)
     mxinfo, _ = poisson_ms(G, kw, G.PREC_MG_MIXED)
     alg_bytes = 88.0 * ncc * pinfo["iterations"]  # 88 B per cell per FP64 PCG iteration (algorithmic)
     achieved = alg_bytes / (pinfo["ms"] / 1e3) / 1e9
@@ -354,6 +410,7 @@ def main():
                         "mixed": {"ms_to_1e-10": mxinfo["ms"], "iterations": mxinfo["iterations"],
                                   "rel": mxinfo["rel"], "solver": "FP64 flexible CG + FP32 multigrid V(2,2), red-black SOR 1.15"},
                         "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"]},
+            "poisson_sigma_shell": shell,
             "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (duct fluid mesh)",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -161,3 +161,77 @@ def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, **kw):
     init(sim, np.random.default_rng(seed))
     sim.init()
     return sim
+
+
+def sigma_shell(n: int = 128, shell: int = 4, seed: int = 0):
+    """Mixed-precision Poisson case: div(sigma grad phi) = div(u x B) on the
+    uniform unit cube with n^3 cells, sigma = 1 inside and one seeded draw of
+    10^U(-3,3) in a `shell`-cell layer along every wall; u and B i.i.d.
+    N(0,1) per face; insulating walls (Neumann everywhere), so the solver
+    removes the right-hand side's mean (all_neumann).
+
+    Returns (coords, sigma_faces, E_faces): node coordinates with ghosts,
+    sigma on the x/y/z faces (mean of the two adjacent cells, the reference's
+    cell-to-face interpolation), and E = u x B on the faces (the other
+    components of u and B brought to each face by the mean of the four
+    surrounding faces, face2Face_no_diag), all as Fortran-layout arrays with
+    ghosts.  div(E) is formed by the library's own divergence."""
+    rng = np.random.default_rng(seed)
+    h = mg.add_ghost_nodes(mg.uniform(0.0, 1.0, n))
+    coords = (h, h.copy(), h.copy())
+    sc = n + 2
+    sig_c = np.ones((sc, sc, sc))
+    s_wall = 10.0 ** rng.uniform(-3.0, 3.0)
+    idx = np.arange(sc)
+    inner = (idx >= 1 + shell) & (idx <= n - shell)
+    ins = inner[:, None, None] & inner[None, :, None] & inner[None, None, :]
+    sig_c[~ins] = s_wall
+    sig_f = []
+    for d in range(3):
+        shp = [sc, sc, sc]
+        shp[d] = sc + 1
+        f = np.ones(shp)
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        mid = [slice(None)] * 3
+        lo[d] = slice(0, sc - 1)
+        hi[d] = slice(1, sc)
+        mid[d] = slice(1, sc)
+        f[tuple(mid)] = 0.5 * (sig_c[tuple(lo)] + sig_c[tuple(hi)])
+        sig_f.append(f)
+    # u, B on faces
+    def faces():
+        out = []
+        for d in range(3):
+            shp = [sc, sc, sc]
+            shp[d] = sc + 1
+            out.append(rng.standard_normal(shp))
+        return out
+    u, B = faces(), faces()
+
+    def to_face(a, src, dst):
+        # mean of the four src-faces around each dst-face (interior entries)
+        shp = [sc, sc, sc]
+        shp[dst] = sc + 1
+        out = np.zeros(shp)
+        # cell-centre value of the src component: mean of its two faces
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[src] = slice(0, sc)
+        hi[src] = slice(1, sc + 1)
+        cc = 0.5 * (a[tuple(lo)] + a[tuple(hi)])
+        # cell centre -> dst faces: mean of the two neighbouring cells
+        l2 = [slice(None)] * 3
+        h2 = [slice(None)] * 3
+        m2 = [slice(None)] * 3
+        l2[dst] = slice(0, sc - 1)
+        h2[dst] = slice(1, sc)
+        m2[dst] = slice(1, sc)
+        out[tuple(m2)] = 0.5 * (cc[tuple(l2)] + cc[tuple(h2)])
+        return out
+
+    E = []
+    for d in range(3):
+        a, b = (d + 1) % 3, (d + 2) % 3
+        E.append(to_face(u[a], a, d) * to_face(B[b], b, d) - to_face(u[b], b, d) * to_face(B[a], a, d))
+    return coords, sig_f, E
