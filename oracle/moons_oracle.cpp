@@ -1,3 +1,9 @@
+#include <tuple>
+#include <map>
+#include <cstdlib>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 // moons_oracle.cpp -- CPU restatement of the MOONS hot path (TEST ORACLE).
 // See moons_oracle.hpp for scope and parity status.  Citations are paths
 // inside the reference project; HW = code/handwritten.
@@ -8,6 +14,126 @@
 #include <functional>
 
 namespace mo {
+
+// ---------------------------------------------------------------------------
+// fixed-chunk thread pool (CPU baseline only; see moons_oracle.hpp)
+// ---------------------------------------------------------------------------
+namespace {
+constexpr long kChunks = 64;
+thread_local bool t_in_par = false;  // a loop nested in a parallel loop runs serially
+struct Pool {
+  std::mutex mu;
+  std::condition_variable cv, done_cv;
+  std::vector<std::thread> workers;
+  const std::function<void(long, long, int)>* job = nullptr;
+  long n = 0, next = 0, finished = 0;
+  unsigned gen = 0;
+  bool quit = false;
+  int nthreads = 0;
+  void run_chunks() {
+    for (;;) {
+      long c;
+      {
+        std::lock_guard<std::mutex> l(mu);
+        if (next >= kChunks) return;
+        c = next++;
+      }
+      const long b = n * c / kChunks, e = n * (c + 1) / kChunks;
+      if (b < e) {
+        t_in_par = true;
+        (*job)(b, e, (int)c);
+        t_in_par = false;
+      }
+      std::lock_guard<std::mutex> l(mu);
+      if (++finished == kChunks) done_cv.notify_all();
+    }
+  }
+  void start(int t) {
+    nthreads = t;
+    for (int w = 1; w < t; w++)
+      workers.emplace_back([this] {
+        unsigned seen = 0;
+        for (;;) {
+          {
+            std::unique_lock<std::mutex> l(mu);
+            cv.wait(l, [&] { return quit || gen != seen; });
+            if (quit) return;
+            seen = gen;
+          }
+          run_chunks();
+        }
+      });
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> l(mu);
+      quit = true;
+    }
+    cv.notify_all();
+    for (auto& w : workers) w.join();
+  }
+};
+Pool* g_pool = nullptr;
+int g_threads = 0;
+std::mutex g_pool_mu;
+}  // namespace
+
+int oracle_threads() {
+  if (g_threads > 0) return g_threads;
+  const char* e = getenv("MOONS_ORACLE_THREADS");
+  int n = e ? atoi(e) : (int)std::thread::hardware_concurrency();
+  return std::max(1, n);
+}
+void set_oracle_threads(int n) {
+  std::lock_guard<std::mutex> l(g_pool_mu);
+  delete g_pool;
+  g_pool = nullptr;
+  g_threads = std::max(1, n);
+}
+// fn(begin, end, chunk) over the kChunks fixed chunks of [0, n); serial
+// below `min_parallel` units
+void par_chunks_i(long n, long min_parallel, const std::function<void(long, long, int)>& fn) {
+  const int t = oracle_threads();
+  if (t <= 1 || n < min_parallel || t_in_par) {
+    for (long c = 0; c < kChunks; c++) {
+      const long b = n * c / kChunks, e = n * (c + 1) / kChunks;
+      if (b < e) fn(b, e, (int)c);
+    }
+    return;
+  }
+  std::lock_guard<std::mutex> l(g_pool_mu);  // one parallel loop at a time
+  if (!g_pool || g_pool->nthreads != t) {
+    delete g_pool;
+    g_pool = new Pool();
+    g_pool->start(t);
+  }
+  Pool& P = *g_pool;
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.job = &fn;
+    P.n = n;
+    P.next = 0;
+    P.finished = 0;
+    P.gen++;
+  }
+  P.cv.notify_all();
+  P.run_chunks();
+  std::unique_lock<std::mutex> lk(P.mu);
+  P.done_cv.wait(lk, [&] { return P.finished == kChunks; });
+  P.job = nullptr;
+}
+void par_chunks(long n, const std::function<void(long, long)>& fn) {
+  par_chunks_i(n, 4096, [&](long b, long e, int) { fn(b, e); });
+}
+// sum of f(b, e) over the fixed chunks of [0, n), added in chunk order
+static double par_sum(long n, long min_parallel, const std::function<double(long, long)>& f) {
+  std::vector<double> part(kChunks, 0.0);
+  par_chunks_i(n, min_parallel, [&](long b, long e, int c) { part[c] = f(b, e); });
+  double s = 0.0;
+  for (double v : part) s += v;
+  return s;
+}
+
 
 // ---------------------------------------------------------------------------
 // coordinates: HW/grid/coordinates_extend.f90:78-173 (init_c),
@@ -187,32 +313,54 @@ void set_bcs(SF& u, const Grid& g, const int type[6], const int prescribed[6],
 // pointwise ops (HW/grid_field/GF_3D/*)
 // ---------------------------------------------------------------------------
 void assign(SF& a, double v) { std::fill(a.f.begin(), a.f.end(), v); }
-void assign(SF& a, const SF& b) { a.f = b.f; }
+void assign(SF& a, const SF& b) {
+  if (a.f.size() != b.f.size()) {
+    a.f = b.f;
+    return;
+  }
+  par_chunks((long)a.n(), [&](long s, long e) { std::copy(b.f.begin() + s, b.f.begin() + e, a.f.begin() + s); });
+}
 void add(SF& a, const SF& b) {
-  for (size_t i = 0; i < a.n(); i++) a.f[i] += b.f[i];
+  par_chunks((long)a.n(), [&](long s, long e) {
+    for (long i = s; i < e; i++) a.f[i] += b.f[i];
+  });
 }
 void subtract(SF& a, const SF& b) {
-  for (size_t i = 0; i < a.n(); i++) a.f[i] -= b.f[i];
+  par_chunks((long)a.n(), [&](long s, long e) {
+    for (long i = s; i < e; i++) a.f[i] -= b.f[i];
+  });
 }
 void multiply(SF& a, const SF& b) {
-  for (size_t i = 0; i < a.n(); i++) a.f[i] *= b.f[i];
+  par_chunks((long)a.n(), [&](long s, long e) {
+    for (long i = s; i < e; i++) a.f[i] *= b.f[i];
+  });
 }
 void multiply(SF& a, double c) {
-  for (auto& v : a.f) v *= c;
+  par_chunks((long)a.n(), [&](long s, long e) {
+    for (long i = s; i < e; i++) a.f[i] *= c;
+  });
 }
 void add_product(SF& a, const SF& b, double c) {  // GF_add_product.f90:13-30
-  for (size_t i = 0; i < a.n(); i++) a.f[i] = a.f[i] + b.f[i] * c;
+  par_chunks((long)a.n(), [&](long s, long e) {
+    for (long i = s; i < e; i++) a.f[i] = a.f[i] + b.f[i] * c;
+  });
 }
 void product_add(SF& a, double c, const SF& b) {  // GF_product_add.f90:14-30
-  for (size_t i = 0; i < a.n(); i++) a.f[i] = a.f[i] * c + b.f[i];
+  par_chunks((long)a.n(), [&](long s, long e) {
+    for (long i = s; i < e; i++) a.f[i] = a.f[i] * c + b.f[i];
+  });
 }
-// sum_GF_pad (GF_aux.f90:140-160, _PARALLELIZE_GF_ branch: 1+pad..s-pad)
+// sum_GF_pad (GF_aux.f90:140-160, _PARALLELIZE_GF_ branch: 1+pad..s-pad);
+// plane sums added in k order (fixed chunks of planes)
 double sum_pad(const SF& a, int pad) {
-  double m = 0;
-  for (int k = 1 + pad; k <= a.s[3] - pad; k++)
-    for (int j = 1 + pad; j <= a.s[2] - pad; j++)
-      for (int i = 1 + pad; i <= a.s[1] - pad; i++) m += a(i, j, k);
-  return m;
+  const int k0 = 1 + pad, nk = a.s[3] - 2 * pad;
+  return par_sum(std::max(nk, 0), 8, [&](long b, long e) {
+    double m = 0;
+    for (int k = k0 + (int)b; k < k0 + (int)e; k++)
+      for (int j = 1 + pad; j <= a.s[2] - pad; j++)
+        for (int i = 1 + pad; i <= a.s[1] - pad; i++) m += a(i, j, k);
+    return m;
+  });
 }
 
 // volume_DL_GF (GF_distributions.f90:61-88) + volume_SF (SF_extend.f90:571-581)
@@ -429,9 +577,12 @@ static void pencil_ops(SF& out, const SF& in, int dir, int pad,
                        const std::function<void(std::vector<double>&, const std::vector<double>&)>& op) {
   int a = dir == 1 ? 2 : 1, b = dir == 3 ? 2 : 3;
   int sin_ = in.s[dir], sout = out.s[dir];
+  // loops over the input's transverse extents (diff_stag/diff_col use f%s);
+  // pencils are independent, so they are cut into chunks of y
+  const int y0 = 1 + pad, ny = in.s[b] - 2 * pad;
+  par_chunks_i(std::max(ny, 0), 8, [&](long cb, long ce, int) {
   std::vector<double> pin(sin_ + 1), pout(sout + 1);
-  // loops over the input's transverse extents (diff_stag/diff_col use f%s)
-  for (int y = 1 + pad; y <= in.s[b] - pad; y++)
+  for (int y = y0 + (int)cb; y < y0 + (int)ce; y++) {
     for (int x = 1 + pad; x <= in.s[a] - pad; x++) {
       int ia[4];
       ia[a] = x;
@@ -450,6 +601,8 @@ static void pencil_ops(SF& out, const SF& in, int dir, int pad,
         out(ia[1], ia[2], ia[3]) = pout[t];
       }
     }
+  }
+  });
 }
 
 void del(SF& out, const SF& in, const Grid& g, int n, int dir, int pad, int gen) {
@@ -547,20 +700,32 @@ static int dl_after_diff(int dl, int dir) {  // flip location along dir
 // lap_centered_VF_new applies per component).  Both are div(grad) through
 // staggered temporaries; div_SF's ghost zeroing applies only to the SF_new
 // (CC) form.
+// operator temporaries kept between calls (every entry that the second
+// pass reads was written by the first, a del "assign", in the same call)
+static SF& temp_sf(const Grid& g, int dl, int slot) {
+  static thread_local std::map<std::tuple<const Grid*, int, int>, SF> cache;
+  SF& t = cache[std::make_tuple(&g, dl, slot)];
+  auto e = dl_eye(dl);
+  bool same = !t.f.empty() && t.dl == dl;
+  for (int d = 0; d < 3 && same; d++) same = t.s[d + 1] == (e[d] ? g.c[d].sn : g.c[d].sc);
+  if (!same) t.init(g, dl);
+  return t;
+}
+
 void lap_centered(SF& out, const SF& u, const Grid& g) {
-  const Grid* gp = &g;
-  SF t[3];
-  for (int d = 1; d <= 3; d++) t[d - 1].init(*gp, dl_after_diff(u.dl, d));
+  SF& t0 = temp_sf(g, dl_after_diff(u.dl, 1), 1);
+  SF& t1 = temp_sf(g, dl_after_diff(u.dl, 2), 2);
+  SF& t2 = temp_sf(g, dl_after_diff(u.dl, 3), 3);
   if (u.dl == 0) {
-    grad(t[0], t[1], t[2], u, g);
-    div(out, t[0], t[1], t[2], g);
+    grad(t0, t1, t2, u, g);
+    div(out, t0, t1, t2, g);
   } else {
-    del(t[0], u, g, 1, 1, 0, 1);
-    del(out, t[0], g, 1, 1, 0, 1);
-    del(t[1], u, g, 1, 2, 0, 1);
-    del(out, t[1], g, 1, 2, 0, 2);
-    del(t[2], u, g, 1, 3, 0, 1);
-    del(out, t[2], g, 1, 3, 0, 2);
+    del(t0, u, g, 1, 1, 0, 1);
+    del(out, t0, g, 1, 1, 0, 1);
+    del(t1, u, g, 1, 2, 0, 1);
+    del(out, t1, g, 1, 2, 0, 2);
+    del(t2, u, g, 1, 3, 0, 1);
+    del(out, t2, g, 1, 3, 0, 2);
   }
 }
 // lapUniformCoeff_SF (ops_discrete.f90:101-110)
@@ -571,13 +736,14 @@ void lap_uniform_coeff(SF& out, const SF& u, const Grid& g) {
 }
 // lapVarCoeff_VF (ops_discrete.f90:275-285)
 void lap_var(SF& out, const SF& u, const SF& kx, const SF& ky, const SF& kz, const Grid& g) {
-  SF t[3];
-  for (int d = 1; d <= 3; d++) t[d - 1].init(g, dl_after_diff(u.dl, d));
-  grad(t[0], t[1], t[2], u, g);
-  multiply(t[0], kx);
-  multiply(t[1], ky);
-  multiply(t[2], kz);
-  div(out, t[0], t[1], t[2], g);
+  SF& t0 = temp_sf(g, dl_after_diff(u.dl, 1), 4);
+  SF& t1 = temp_sf(g, dl_after_diff(u.dl, 2), 5);
+  SF& t2 = temp_sf(g, dl_after_diff(u.dl, 3), 6);
+  grad(t0, t1, t2, u, g);
+  multiply(t0, kx);
+  multiply(t1, ky);
+  multiply(t2, kz);
+  div(out, t0, t1, t2, g);
 }
 
 // interpO2_SF (ops_interp.f90:190-220) -> interp_C2N_GF / interp_N2C_GF
@@ -786,8 +952,10 @@ static double dotp(const std::vector<SF>& A, const std::vector<SF>& B, SF* const
   // dot_product_SF/VF (ops_aux.f90:199-216)
   double d = 0;
   for (size_t c = 0; c < A.size(); c++) {
-    tmp[c].f = A[c].f;
-    multiply(tmp[c], B[c]);
+    if (tmp[c].f.size() != A[c].f.size()) tmp[c].f = A[c].f;
+    par_chunks((long)A[c].n(), [&](long s, long e) {
+      for (long i = s; i < e; i++) tmp[c].f[i] = A[c].f[i] * B[c].f[i];
+    });
     assign_wall_Dirichlet(tmp[c], 0.0, x[c]);
     d += sum_pad(tmp[c], 1);
   }

@@ -16,6 +16,7 @@
 // All loops use 1-based indices exactly as the cited Fortran does.
 #pragma once
 #include <array>
+#include <functional>
 #include <cmath>
 #include <cstdint>
 #include <memory>
@@ -24,6 +25,14 @@
 #include <vector>
 
 namespace mo {
+
+// Host threads of the oracle (CPU baseline): loops are cut into a fixed
+// number of chunks whatever the thread count, and reductions add the chunk
+// sums in chunk order, so results do not depend on the number of threads.
+// MOONS_ORACLE_THREADS sets the count (default: all hardware threads).
+int oracle_threads();
+void set_oracle_threads(int n);
+void par_chunks(long n, const std::function<void(long, long)>& fn);
 
 using Vec = std::vector<double>;
 

@@ -83,6 +83,13 @@ class OracleError(RuntimeError):
     pass
 
 
+def threads() -> int:
+    """Host threads the oracle's loops run on (MOONS_ORACLE_THREADS, default all)."""
+    f = lib().or_threads
+    f.restype = C.c_int
+    return int(f())
+
+
 def _check(code):
     if code != 0:
         raise OracleError(f"oracle error {code}: {lib().or_last_error().decode()}")

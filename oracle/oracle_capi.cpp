@@ -37,6 +37,9 @@ int fail(const std::string& m) {
 
 extern "C" {
 
+// host threads the oracle's loops use (MOONS_ORACLE_THREADS or all)
+int or_threads() { return mo::oracle_threads(); }
+
 const char* or_last_error(void) { return g_err.c_str(); }
 
 void* or_mesh_create(const double* hx, int sx, const double* hy, int sy, const double* hz, int sz) {
