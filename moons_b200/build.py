@@ -61,8 +61,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if verbose:
         sys.stderr.write(r.stderr)
     os.replace(tmp, LIB)
+    # register / spill / shared-memory report; compile times vary per build
+    report = "".join(l for l in r.stderr.splitlines(True) if "Compile time" not in l)
     with open(os.path.join(LIBDIR, "ptxas.txt"), "w") as f:
-        f.write(r.stderr)
+        f.write(report)
     return LIB
 
 
