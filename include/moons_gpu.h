@@ -287,6 +287,47 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info);
  * divU/divB probes export) */
 int moons_mhd_divergence(moons_mhd* s, double* l2_divU, double* l2_divB);
 
+/* ---- learned preconditioner: 3-D U-Net -------------------------------------
+ * No reference counterpart (the reference's preconditioners are the Jacobi
+ * family of code/handwritten/solvers/preconditioners/preconditioners.f90:
+ * 55-129).  A network on a mesh's cell-centred interior (cell counts
+ * multiples of 8): z = M(r) ~ A^-1 r, inputs r / rms(r) and one per-cell
+ * feature of the operator's coefficients, BF16 activations and weights,
+ * FP32 accumulation on the tensor cores (tcgen05).  It is trained on
+ * (r, e) pairs with A e = r by moons_unet_train_step (forward, backward and
+ * Adam on the GPU) and used inside flexible CG through moons_pcg_set_unet.
+ * Parameters: one flat FP32 array; per convolution W[co][ci][dz][dy][dx]
+ * then b[co] (layers enc0a 8->16, enc0b 16->16, enc1a 16->32, enc1b 32->32,
+ * enc2a 32->64, enc2b 64->64, enc3a 64->128, enc3b 128->128,
+ * dec2a 192->64, dec2b 64->64, dec1a 96->32, dec1b 32->32, dec0a 48->16,
+ * dec0b 16->16), then the 1x1 head w[16], b. */
+typedef struct moons_unet moons_unet;
+int moons_unet_create(moons_mesh* m, unsigned long long seed, moons_unet** out);
+int moons_unet_destroy(moons_unet* u);
+int moons_unet_nparams(const moons_unet* u, long long* n);
+int moons_unet_get_params(moons_unet* u, float* host, long long n);
+int moons_unet_set_params(moons_unet* u, const float* host, long long n);  /* resets Adam */
+/* z = out_scale * rms(r) * y: the scale c of the network's output */
+int moons_unet_set_out_scale(moons_unet* u, double c);
+int moons_unet_get_out_scale(const moons_unet* u, double* c);
+/* per-cell feature (ghosts included, cell-centred layout), e.g.
+ * log10(mean face coefficient) / 3 */
+int moons_unet_set_feature(moons_unet* u, const float* host, long long n);
+/* z = M(r); r, z cell-centred fields of the net's mesh (z's ghosts = 0) */
+int moons_unet_apply(moons_unet* u, moons_sf* z, const moons_sf* r);
+/* loss = |y - t|^2 / |t|^2 with t = e / (out_scale * rms(r)) and its
+ * gradient (grads_host may be null; n = nparams) */
+int moons_unet_loss_grad(moons_unet* u, const moons_sf* r, const moons_sf* e, float* loss, float* grads_host,
+                         long long n);
+/* one Adam step (beta 0.9 / 0.999) on one (r, e) pair; loss may be null */
+int moons_unet_train_step(moons_unet* u, const moons_sf* r, const moons_sf* e, float lr, float* loss);
+/* kernel self-check of one layer on host data ([C][Z][Y][X] FP32, interior,
+ * rounded to BF16 on upload): op 0 out = conv(in) (+bias, ReLU if relu);
+ * op 1 out = transposed conv of dout (gradient w.r.t. the input); op 2 out =
+ * weight gradient [cout][cin][27] followed by the bias gradient [cout] */
+int moons_unet_layer_check(int op, int X, int Y, int Z, int cinA, int cinB, int cout, const float* in,
+                           const float* dout, const float* W, const float* bias, int relu, float* out);
+
 #ifdef __cplusplus
 }
 #endif

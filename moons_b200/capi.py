@@ -138,6 +138,7 @@ def isp(iter_max: int, tol_rel: float, tol_abs: float, n_skip_check_res: int = 1
 
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
 
 
 class _Lib:
@@ -199,6 +200,19 @@ def lib() -> C.CDLL:
             "moons_mhd_step": (C.c_int, [_P, C.c_int, C.POINTER(StepInfo)]),
             "moons_mhd_divergence": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             "moons_kernel_launches": (C.c_longlong, []),
+            "moons_unet_create": (C.c_int, [_P, C.c_ulonglong, C.POINTER(_P)]),
+            "moons_unet_destroy": (C.c_int, [_P]),
+            "moons_unet_nparams": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+            "moons_unet_get_params": (C.c_int, [_P, _F, C.c_longlong]),
+            "moons_unet_set_params": (C.c_int, [_P, _F, C.c_longlong]),
+            "moons_unet_set_out_scale": (C.c_int, [_P, C.c_double]),
+            "moons_unet_get_out_scale": (C.c_int, [_P, C.POINTER(C.c_double)]),
+            "moons_unet_set_feature": (C.c_int, [_P, _F, C.c_longlong]),
+            "moons_unet_apply": (C.c_int, [_P, _P, _P]),
+            "moons_unet_loss_grad": (C.c_int, [_P, _P, _P, _F, _F, C.c_longlong]),
+            "moons_unet_train_step": (C.c_int, [_P, _P, _P, C.c_float, _F]),
+            "moons_unet_layer_check": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                 _F, _F, _F, _F, C.c_int, _F]),
         }
         for name, (rt, at) in sig.items():
             f = getattr(L, name)
@@ -454,3 +468,82 @@ def kernel_launches() -> int:
     """Kernels this process launched through the library (host launches plus
     the launches executed inside the solver's device-side loop)."""
     return int(lib().moons_kernel_launches())
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(_F)
+
+
+class UNet:
+    """The learned preconditioner (3-D U-Net) on a mesh's cell-centred
+    interior; see moons_unet_* in include/moons_gpu.h."""
+
+    def __init__(self, mesh: Mesh, seed: int = 0):
+        self.mesh = mesh
+        h = _P()
+        _check(lib().moons_unet_create(mesh.h, int(seed), C.byref(h)))
+        self.h = h
+        n = C.c_longlong()
+        _check(lib().moons_unet_nparams(h, C.byref(n)))
+        self.nparams = int(n.value)
+
+    def get_params(self) -> np.ndarray:
+        a = np.empty(self.nparams, dtype=np.float32)
+        _check(lib().moons_unet_get_params(self.h, _fp(a), self.nparams))
+        return a
+
+    def set_params(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        _check(lib().moons_unet_set_params(self.h, _fp(a), a.size))
+
+    @property
+    def out_scale(self) -> float:
+        c = C.c_double()
+        _check(lib().moons_unet_get_out_scale(self.h, C.byref(c)))
+        return c.value
+
+    @out_scale.setter
+    def out_scale(self, c: float):
+        _check(lib().moons_unet_set_out_scale(self.h, float(c)))
+
+    def set_feature(self, feat):
+        a = np.ascontiguousarray(np.asarray(feat, dtype=np.float32).ravel(order="F"))
+        _check(lib().moons_unet_set_feature(self.h, _fp(a), a.size))
+
+    def apply(self, z: Field, r: Field):
+        _check(lib().moons_unet_apply(self.h, z.h, r.h))
+
+    def loss_grad(self, r: Field, e: Field, want_grads: bool = True):
+        loss = np.zeros(1, dtype=np.float32)
+        g = np.empty(self.nparams, dtype=np.float32) if want_grads else None
+        _check(lib().moons_unet_loss_grad(self.h, r.h, e.h, _fp(loss), _fp(g), self.nparams if want_grads else 0))
+        return float(loss[0]), g
+
+    def train_step(self, r: Field, e: Field, lr: float) -> float:
+        loss = np.zeros(1, dtype=np.float32)
+        _check(lib().moons_unet_train_step(self.h, r.h, e.h, float(lr), _fp(loss)))
+        return float(loss[0])
+
+    def close(self):
+        if self.h:
+            lib().moons_unet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def unet_layer_check(op: int, X: int, Y: int, Z: int, cinA: int, cinB: int, cout: int, inp=None, dout=None,
+                     W=None, bias=None, relu: bool = True) -> np.ndarray:
+    """Run one U-Net layer kernel on host data (see moons_unet_layer_check)."""
+    cin = cinA + cinB
+    f32 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+    inp, dout, W, bias = f32(inp), f32(dout), f32(W), f32(bias)
+    n = {0: cout * X * Y * Z, 1: cin * X * Y * Z, 2: cout * cin * 27 + cout}[op]
+    out = np.empty(n, dtype=np.float32)
+    _check(lib().moons_unet_layer_check(op, X, Y, Z, cinA, cinB, cout, _fp(inp), _fp(dout), _fp(W), _fp(bias),
+                                        int(relu), _fp(out)))
+    return out

@@ -5,3 +5,4 @@
 #include "mgpcg.cu"
 #include "mhd.cu"
 #include "noalloc.cu"
+#include "unet.cu"

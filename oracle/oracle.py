@@ -21,11 +21,12 @@ from moons_b200.capi import BCSpec, ISP, SolveInfo, MHDParams, StepInfo  # noqa:
 
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
 _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("moons_oracle.cpp", "moons_oracle.hpp", "oracle_capi.cpp", "moons_oracle_mhd.cpp", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("moons_oracle.cpp", "moons_oracle.hpp", "oracle_capi.cpp", "moons_oracle_mhd.cpp", "unet_oracle.cpp", "Makefile")]
     stale = not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs)
     if force or stale:
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
@@ -70,6 +71,12 @@ def lib():
             "or_mhd_init": (C.c_int, [_P]),
             "or_mhd_step": (C.c_int, [_P, C.c_int, C.POINTER(StepInfo)]),
             "or_mhd_divergence": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+            "or_unet_layer": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        _F, _F, _F, _F, C.c_int, _F]),
+            "or_unet_nparams": (C.c_longlong, []),
+            "or_unet_set_exact": (None, [C.c_int]),
+            "or_unet_forward": (C.c_int, [C.c_int, C.c_int, C.c_int, _F, C.c_double, _D, _F, _D]),
+            "or_unet_loss_grad": (C.c_int, [C.c_int, C.c_int, C.c_int, _F, C.c_double, _D, _F, _D, _D, _F]),
         }
         for n, (rt, at) in sig.items():
             f = getattr(L, n)
@@ -275,3 +282,59 @@ class MHD:
                 self.h = None
         except Exception:
             pass
+
+
+# ---- learned preconditioner (U-Net) restatement ------------------------------
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fptr(a):
+    return None if a is None else a.ctypes.data_as(_F)
+
+
+def unet_layer(op, X, Y, Z, cinA, cinB, cout, inp=None, dout=None, W=None, bias=None, relu=True):
+    """One U-Net layer on the CPU (same contract as capi.unet_layer_check)."""
+    cin = cinA + cinB
+    inp, dout, W, bias = _f32(inp), _f32(dout), _f32(W), _f32(bias)
+    n = {0: cout * X * Y * Z, 1: cin * X * Y * Z, 2: cout * cin * 27 + cout}[op]
+    out = np.empty(n, dtype=np.float32)
+    _check(lib().or_unet_layer(op, X, Y, Z, cinA, cinB, cout, _fptr(inp), _fptr(dout), _fptr(W), _fptr(bias),
+                               int(relu), _fptr(out)))
+    return out
+
+
+def unet_set_exact(on: bool):
+    """Exact arithmetic (no BF16 rounding) in the U-Net restatement."""
+    lib().or_unet_set_exact(int(bool(on)))
+
+
+def unet_nparams() -> int:
+    return int(lib().or_unet_nparams())
+
+
+def _cc(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+
+
+def unet_forward(X, Y, Z, params, out_scale, r, feat=None):
+    """z = M(r) of the network with the given flat parameters; r, feat and
+    the result are cell-centred arrays with ghosts (Fortran order)."""
+    p = _f32(params)
+    rr = _cc(r)
+    ff = None if feat is None else np.ascontiguousarray(np.asarray(feat, dtype=np.float32).ravel(order="F"))
+    z = np.zeros_like(rr)
+    _check(lib().or_unet_forward(X, Y, Z, _fptr(p), float(out_scale), rr.ctypes.data_as(_D), _fptr(ff),
+                                 z.ctypes.data_as(_D)))
+    return z.reshape((X + 2, Y + 2, Z + 2), order="F")
+
+
+def unet_loss_grad(X, Y, Z, params, out_scale, r, e, feat=None):
+    p = _f32(params)
+    rr, ee = _cc(r), _cc(e)
+    ff = None if feat is None else np.ascontiguousarray(np.asarray(feat, dtype=np.float32).ravel(order="F"))
+    loss = np.zeros(1, dtype=np.float64)
+    g = np.zeros(p.size, dtype=np.float32)
+    _check(lib().or_unet_loss_grad(X, Y, Z, _fptr(p), float(out_scale), rr.ctypes.data_as(_D), _fptr(ff),
+                                   ee.ctypes.data_as(_D), loss.ctypes.data_as(_D), _fptr(g)))
+    return float(loss[0]), g

@@ -1,0 +1,148 @@
+"""The learned preconditioner's CUDA path against the oracle's U-Net
+restatement: single layers (tcgen05 implicit-GEMM convolution, transposed
+convolution, weight gradient), the whole network's output, the loss and every
+parameter's gradient, and a few Adam steps that lower the loss.
+
+Tolerances: the GPU stores activations and their gradients in BF16 (8-bit
+mantissa) and accumulates in FP32 in another order than the oracle (double),
+so single layers agree to BF16 rounding and whole-network quantities to a few
+BF16 steps."""
+import numpy as np
+import pytest
+
+import oracle.oracle as O
+from moons_b200 import capi as G
+from moons_b200.capi import CC
+from tests.common import coords
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# (X, Y, Z): several tiles per plane with a partial last tile, a row longer
+# than one 128-voxel tile, and a single plane
+SIZES = [(16, 12, 8), (130, 3, 2), (8, 8, 1)]
+
+
+@pytest.mark.parametrize("X,Y,Z", SIZES)
+@pytest.mark.parametrize("cinA,cinB,cout", [(8, 0, 16), (16, 0, 32), (32, 16, 16), (64, 0, 128), (128, 64, 64)])
+def test_conv_forward_matches_oracle(X, Y, Z, cinA, cinB, cout):
+    rng = np.random.default_rng(X * 1000 + cinA + cout)
+    cin = cinA + cinB
+    x = bf16(rng.standard_normal((cin, Z, Y, X)))
+    W = rng.standard_normal((cout, cin, 27)).astype(np.float32) * np.sqrt(2.0 / (27 * cin))
+    b = rng.standard_normal(cout).astype(np.float32) * 0.1
+    got = G.unet_layer_check(0, X, Y, Z, cinA, cinB, cout, inp=x, W=W, bias=b, relu=True)
+    ref = O.unet_layer(0, X, Y, Z, cinA, cinB, cout, inp=x, W=W, bias=b, relu=True)
+    # BF16 output rounding: at most half a BF16 step of each value, plus the
+    # FP32-vs-double accumulation difference
+    assert np.all(np.abs(got - ref) <= 2 ** -8 * np.abs(ref) + 1e-4 * np.abs(ref).max() + 1e-6)
+    assert rel_l2(got, ref) < 4e-3
+
+
+@pytest.mark.parametrize("X,Y,Z", SIZES)
+@pytest.mark.parametrize("cin,cout", [(16, 16), (48, 16), (96, 32), (192, 64), (64, 128)])
+def test_conv_transpose_matches_oracle(X, Y, Z, cin, cout):
+    rng = np.random.default_rng(X * 100 + cin + cout)
+    g = bf16(rng.standard_normal((cout, Z, Y, X)))
+    W = rng.standard_normal((cout, cin, 27)).astype(np.float32) * 0.05
+    got = G.unet_layer_check(1, X, Y, Z, cin, 0, cout, dout=g, W=W)
+    ref = O.unet_layer(1, X, Y, Z, cin, 0, cout, dout=g, W=W)
+    assert np.all(np.abs(got - ref) <= 2 ** -8 * np.abs(ref) + 1e-4 * np.abs(ref).max() + 1e-6)
+    assert rel_l2(got, ref) < 4e-3
+
+
+@pytest.mark.parametrize("X,Y,Z", SIZES)
+@pytest.mark.parametrize("cinA,cinB,cout", [(8, 0, 16), (16, 0, 16), (32, 0, 64), (48, 0, 16), (96, 0, 32),
+                                            (128, 0, 128), (128, 64, 64), (32, 16, 16)])
+def test_weight_gradient_matches_oracle(X, Y, Z, cinA, cinB, cout):
+    rng = np.random.default_rng(X * 10 + cinA + cinB + cout)
+    cin = cinA + cinB
+    x = bf16(rng.standard_normal((cin, Z, Y, X)))
+    g = bf16(rng.standard_normal((cout, Z, Y, X)))
+    got = G.unet_layer_check(2, X, Y, Z, cinA, cinB, cout, inp=x, dout=g)
+    ref = O.unet_layer(2, X, Y, Z, cinA, cinB, cout, inp=x, dout=g)
+    nw = cout * cin * 27
+    assert rel_l2(got[:nw], ref[:nw]) < 1e-5
+    assert rel_l2(got[nw:], ref[nw:]) < 1e-5
+
+
+def _problem(X, Y, Z, seed):
+    """A net on an X x Y x Z cell mesh and a smooth-plus-rough (r, e) pair."""
+    hx, hy, hz = (coords("uniform", n) for n in (X, Y, Z))
+    m = G.Mesh(hx, hy, hz)
+    rng = np.random.default_rng(seed)
+    shp = (X + 2, Y + 2, Z + 2)
+    r = np.zeros(shp)
+    e = np.zeros(shp)
+    xs = np.linspace(0, np.pi, X)[:, None, None]
+    r[1:-1, 1:-1, 1:-1] = rng.standard_normal((X, Y, Z)) + 2 * np.sin(xs) * np.ones((1, Y, Z))
+    e[1:-1, 1:-1, 1:-1] = 0.3 * rng.standard_normal((X, Y, Z)) + np.sin(xs) * np.ones((1, Y, Z))
+    feat = np.zeros(shp, dtype=np.float32)
+    feat[1:-1, 1:-1, 1:-1] = rng.uniform(-1, 1, (X, Y, Z))
+    fr, fe = m.field(CC), m.field(CC)
+    fr.upload(r)
+    fe.upload(e)
+    return m, fr, fe, r, e, feat
+
+
+@pytest.mark.parametrize("X,Y,Z", [(16, 16, 16), (24, 16, 8)])
+def test_network_forward_matches_oracle(X, Y, Z):
+    m, fr, fe, r, e, feat = _problem(X, Y, Z, 3)
+    net = G.UNet(m, seed=7)
+    net.out_scale = 0.5
+    net.set_feature(feat)
+    z = m.field(CC)
+    net.apply(z, fr)
+    got = z.download()
+    ref = O.unet_forward(X, Y, Z, net.get_params(), 0.5, r, feat)
+    assert np.all(got[0] == 0) and np.all(got[-1] == 0)  # ghosts untouched
+    assert rel_l2(got, ref) < 2e-2
+
+
+@pytest.mark.parametrize("X,Y,Z", [(16, 16, 16), (24, 16, 8)])
+def test_loss_and_gradients_match_oracle(X, Y, Z):
+    m, fr, fe, r, e, feat = _problem(X, Y, Z, 4)
+    net = G.UNet(m, seed=11)
+    net.out_scale = 0.8
+    net.set_feature(feat)
+    loss, g = net.loss_grad(fr, fe)
+    p = net.get_params()
+    lref, gref = O.unet_loss_grad(X, Y, Z, p, 0.8, r, e, feat)
+    assert abs(loss - lref) <= 2e-2 * lref
+    io = [(8, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 128), (128, 128), (192, 64), (64, 64),
+          (96, 32), (32, 32), (48, 16), (16, 16)]
+    # the single-layer tests pin the kernels; here a wiring error would show
+    # as an O(1) mismatch, while BF16 rounding flips move the gradients of the
+    # coarsest level (a few voxels) by several per cent
+    assert rel_l2(g, gref) < 3e-2
+    o = 0
+    for li, (cin, cout) in enumerate(io):
+        nw = cin * cout * 27
+        assert rel_l2(g[o:o + nw], gref[o:o + nw]) < 0.15, ("weights", li)
+        assert rel_l2(g[o + nw:o + nw + cout], gref[o + nw:o + nw + cout]) < 0.15, ("bias", li)
+        o += nw + cout
+    assert rel_l2(g[o:], gref[o:]) < 2e-2
+
+
+def test_adam_steps_lower_the_loss():
+    X, Y, Z = 16, 16, 16
+    m, fr, fe, r, e, feat = _problem(X, Y, Z, 5)
+    net = G.UNet(m, seed=1)
+    net.set_feature(feat)
+    first = net.train_step(fr, fe, 1e-3)
+    for _ in range(40):
+        last = net.train_step(fr, fe, 1e-3)
+    assert np.isfinite(last) and last < 0.5 * first

@@ -1,0 +1,114 @@
+"""The U-Net restatement in the oracle pinned on the CPU: the transposed
+convolution is the adjoint of the convolution, the weight gradient is the
+derivative of <conv(x; W), g> in W, and the full backward pass (exact mode,
+no BF16 rounding) matches central finite differences of the loss."""
+import numpy as np
+import pytest
+
+import oracle.oracle as O
+
+
+def bf16(a):
+    """Round float32 values to BF16 (nearest even), as the kernels store them."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("cin,cout", [(8, 16), (16, 32), (48, 16)])
+def test_conv_transpose_is_adjoint(cin, cout):
+    rng = np.random.default_rng(cin * 7 + cout)
+    X, Y, Z = 6, 5, 4
+    x = bf16(rng.standard_normal((cin, Z, Y, X)))
+    g = bf16(rng.standard_normal((cout, Z, Y, X)))
+    W = bf16(rng.standard_normal((cout, cin, 27)) * 0.1)
+    y = O.unet_layer(0, X, Y, Z, cin, 0, cout, inp=x, W=W, relu=False)
+    xt = O.unet_layer(1, X, Y, Z, cin, 0, cout, dout=g, W=W)
+    lhs = float(np.dot(y.astype(np.float64), g.ravel().astype(np.float64)))
+    rhs = float(np.dot(x.ravel().astype(np.float64), xt.astype(np.float64)))
+    assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), 1.0)
+
+
+def test_weight_gradient_is_derivative_of_pairing():
+    rng = np.random.default_rng(3)
+    X, Y, Z, cin, cout = 5, 6, 4, 16, 16
+    x = bf16(rng.standard_normal((cin, Z, Y, X)))
+    g = bf16(rng.standard_normal((cout, Z, Y, X)))
+    V = bf16(rng.standard_normal((cout, cin, 27)))
+    dW = O.unet_layer(2, X, Y, Z, cin, 0, cout, inp=x, dout=g)
+    gw, gb = dW[: cout * cin * 27], dW[cout * cin * 27:]
+    # <conv(x; V), g> is linear in V with gradient dW
+    y = O.unet_layer(0, X, Y, Z, cin, 0, cout, inp=x, W=V, relu=False)
+    lhs = float(np.dot(gw.astype(np.float64), V.ravel().astype(np.float64)))
+    rhs = float(np.dot(y.astype(np.float64), g.ravel().astype(np.float64)))
+    assert abs(lhs - rhs) <= 1e-4 * max(abs(rhs), 1.0)
+    assert np.allclose(gb, g.reshape(cout, -1).sum(axis=1), rtol=1e-5, atol=1e-4)
+
+
+def _pair(X, Y, Z, seed):
+    rng = np.random.default_rng(seed)
+    r = np.zeros((X + 2, Y + 2, Z + 2))
+    e = np.zeros((X + 2, Y + 2, Z + 2))
+    r[1:-1, 1:-1, 1:-1] = rng.standard_normal((X, Y, Z))
+    e[1:-1, 1:-1, 1:-1] = 0.5 * rng.standard_normal((X, Y, Z))
+    feat = np.zeros((X + 2, Y + 2, Z + 2), dtype=np.float32)
+    feat[1:-1, 1:-1, 1:-1] = rng.uniform(-1, 1, (X, Y, Z))
+    return r, e, feat
+
+
+def _params(seed):
+    rng = np.random.default_rng(seed)
+    n = O.unet_nparams()
+    p = np.zeros(n, dtype=np.float32)
+    io = [(8, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 128), (128, 128), (192, 64), (64, 64),
+          (96, 32), (32, 32), (48, 16), (16, 16)]
+    o = 0
+    for cin, cout in io:
+        nw = cin * cout * 27
+        p[o:o + nw] = rng.uniform(-1, 1, nw) * np.sqrt(6.0 / (cin * 27))
+        o += nw
+        p[o:o + cout] = rng.uniform(0.0, 0.1, cout)
+        o += cout
+    p[o:o + 16] = rng.uniform(-0.5, 0.5, 16)
+    p[o + 16] = 0.1
+    return p
+
+
+def test_backward_matches_finite_differences():
+    X, Y, Z = 8, 8, 8
+    r, e, feat = _pair(X, Y, Z, 1)
+    p = _params(2)
+    O.unet_set_exact(True)
+    try:
+        loss, g = O.unet_loss_grad(X, Y, Z, p, 0.7, r, e, feat)
+        assert np.isfinite(loss) and loss > 0
+        rng = np.random.default_rng(5)
+        # probe a few parameters of every layer (weights and biases) and the head
+        io = [(8, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 128), (128, 128), (192, 64),
+              (64, 64), (96, 32), (32, 32), (48, 16), (16, 16)]
+        idx, o = [], 0
+        for cin, cout in io:
+            nw = cin * cout * 27
+            w = o + rng.integers(0, nw, 40)
+            idx += [int(i) for i in w[np.argsort(-np.abs(g[w]))[:2]]]
+            idx.append(o + nw + int(np.argmax(np.abs(g[o + nw:o + nw + cout]))))
+            o += nw + cout
+        idx += [o + 3, o + 16]
+        # ReLU kinks make single steps unreliable: take the best of three
+        worst = 0.0
+        for i in idx:
+            best = np.inf
+            for hh in (3e-3, 1e-3, 3e-4):
+                h = hh * max(1.0, abs(float(p[i])))
+                pp, pm = p.copy(), p.copy()
+                pp[i] += h
+                pm[i] -= h
+                lp, _ = O.unet_loss_grad(X, Y, Z, pp, 0.7, r, e, feat)
+                lm, _ = O.unet_loss_grad(X, Y, Z, pm, 0.7, r, e, feat)
+                fd = (lp - lm) / (float(pp[i]) - float(pm[i]))  # the step as stored in FP32
+                best = min(best, abs(fd - g[i]) / max(abs(g[i]), abs(fd), 1e-2 * np.abs(g).max()))
+            worst = max(worst, best)
+        assert worst < 2e-2, worst
+    finally:
+        O.unet_set_exact(False)
