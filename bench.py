@@ -233,6 +233,98 @@ def sigma_shell_poisson(G, n=128, shell=4, seeds_plain=4, seeds_mg=64):
     return out
 
 
+def unet_flops(n):
+    """Algorithmic FLOPs of one U-Net forward on an n^3 grid: 2 * 27 * Cin *
+    Cout per voxel and 3x3x3 convolution (real input channels; the head and
+    the pooling are negligible)."""
+    layers = [(2, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 128, 3),
+              (128, 128, 3), (192, 64, 2), (64, 64, 2), (96, 32, 1), (32, 32, 1), (48, 16, 0), (16, 16, 0)]
+    return sum(2 * 27 * ci * co * (n >> lv) ** 3 for ci, co, lv in layers)
+
+
+def learned_poisson(G, n=128, shell=4, ntrain=8, held=(1000, 1001, 1002), epochs=(15, 8)):
+    """Learned preconditioner on the sigma-shell case: the U-Net is trained on
+    the GPU (forward, backward, Adam in the library's kernels) on pairs the
+    solver generates from `ntrain` seeded draws -- Jacobi-PCG iterates, then
+    the learned solve's own iterates -- and then solves held-out draws to
+    1e-10 in flexible CG (multigrid fallback on stagnation).  Reports its
+    solve time and iterations next to the reference's Jacobi-PCG and the
+    FP32-V-cycle flexible CG, the training cost, and the U-Net forward rate."""
+    from moons_b200 import learned as L
+    import torch
+    t0 = time.perf_counter()
+    mesh = L.shell_mesh(n)
+    cases = [L.ShellCase.build(mesh, n, shell, s) for s in range(ntrain)]
+    pairs = L.make_pairs(cases, iterates=(0, 2, 8, 32, 128))
+    net = G.UNet(mesh, seed=0)
+    net.out_scale = L.output_scale(pairs)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    h0 = L.train(net, cases, pairs, epochs=epochs[0], lr=1e-3, lr_min=1e-4)
+    n0 = len(pairs)
+    pairs += L.make_pairs_learned(cases, net, iterates=(1, 2, 4, 8, 16))
+    h1 = L.train(net, cases, pairs, epochs=epochs[1], lr=5e-4, lr_min=5e-5, seed=1)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    steps = epochs[0] * n0 + epochs[1] * len(pairs)
+
+    def solve(case, prec):
+        s = case.solver(prec)
+        if prec == G.PREC_UNET:
+            net.set_coeff(case.k)
+            s.set_unet(net)
+        par = G.isp(20000, 1e-10, 1e-300)
+        case.phi.fill(0.0)
+        s.solve([case.phi], [case.rhs], par)  # warm-up (graph build)
+        case.phi.fill(0.0)
+        info = s.solve([case.phi], [case.rhs], par)
+        s.close()
+        return info
+
+    per = []
+    for i, sd in enumerate(held):
+        c = L.ShellCase.build(mesh, n, shell, sd)
+        row = {"seed": sd}
+        for name, prec in (("learned", G.PREC_UNET), ("mixed_fp32_vcycle", G.PREC_MG_MIXED)) + (
+                (("plain_fp64_jacobi", G.PREC_LAP),) if i == 0 else ()):
+            info = solve(c, prec)
+            row[name] = {"ms": info["ms"], "iterations": info["iterations"], "exit_reason": info["exit_reason"],
+                         "rel": info["rel"]}
+        per.append(row)
+    # U-Net forward rate (host-synchronised applies on one draw)
+    z = mesh.field(G.CC)
+    r = pairs[0].r
+    net.set_coeff(cases[0].k)
+    for _ in range(3):
+        net.apply(z, r)
+    reps = 10
+    t2 = time.perf_counter()
+    for _ in range(reps):
+        net.apply(z, r)
+    fwd_ms = (time.perf_counter() - t2) / reps * 1e3
+    fl = unet_flops(n)
+    lm = float(np.mean([p["learned"]["ms"] for p in per]))
+    mm = float(np.mean([p["mixed_fp32_vcycle"]["ms"] for p in per]))
+    jm = per[0]["plain_fp64_jacobi"]["ms"]
+    return {
+        "workload": f"sigma-weighted Poisson {n}^3, {shell}-cell wall shell sigma=10^U(-3,3), RHS div(u x B); "
+                    f"trained on {ntrain} seeded draws, evaluated on held-out seeds {list(held)}",
+        "train": {"pairs": len(pairs), "adam_steps": steps, "seconds": t_train,
+                  "ms_per_step": t_train / max(steps, 1) * 1e3,
+                  "loss_first_last": [h0[0], h1[-1]], "loss": "energy-norm cosine (kind 2)",
+                  "data_seconds": t1 - t0},
+        "held_out": per,
+        "learned_ms_mean": lm, "mixed_ms_mean": mm, "plain_ms_seed0": jm,
+        "speedup_learned_vs_plain": jm / per[0]["learned"]["ms"],
+        "speedup_learned_vs_mixed": mm / lm,
+        "iterations_learned_vs_plain_seed0": [per[0]["learned"]["iterations"],
+                                               per[0]["plain_fp64_jacobi"]["iterations"]],
+        "unet_forward": {"ms_host_synced": fwd_ms, "gflop": fl / 1e9, "tflops": fl / (fwd_ms / 1e3) / 1e12},
+        "note": "exit_reason 11: the learned phase stagnated (10 iterations without halving the residual) and "
+                "the FP32 V-cycle finished the solve; iterations and ms include both phases",
+    }
+
+
 def cpu_sample(kw, gpu_iters=None):
     """Bounded CPU sample: the oracle (single thread) on the full-size duct.
     It times init + one step with every PCG capped at a few iterations, and
@@ -371,6 +463,8 @@ def main():
     shell = sigma_shell_poisson(G, n=32 if args.small else 128, seeds_plain=1 if args.small else 4,
                                 seeds_mg=2 if args.small else 16)
     mxinfo, _ = poisson_ms(G, kw, G.PREC_MG_MIXED)
+    learned = learned_poisson(G, n=32 if args.small else 128, shell=2 if args.small else 4,
+                              ntrain=4 if args.small else 8, held=(1000,) if args.small else (1000, 1001, 1002))
     alg_bytes = 88.0 * ncc * pinfo["iterations"]  # 88 B per cell per FP64 PCG iteration (algorithmic)
     achieved = alg_bytes / (pinfo["ms"] / 1e3) / 1e9
     peaks = {}
@@ -416,6 +510,7 @@ def main():
                                   "rel": mxinfo["rel"], "solver": "FP64 flexible CG + FP32 multigrid V(2,2), red-black SOR 1.15"},
                         "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"]},
             "poisson_sigma_shell": shell,
+            "poisson_learned": learned,
             "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (duct fluid mesh)",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -85,7 +85,9 @@ typedef struct {
   double res0;         /* L2 of the modified RHS over the whole array        */
   double res;          /* sqrt|dot(r,r)| at exit                             */
   double rel;          /* res/res0 (res when res0 == 0)                      */
-  int exit_reason;     /* 1 tol_rel, 2 tol_abs, 3 iter_max                   */
+  int exit_reason;     /* 1 tol_rel, 2 tol_abs, 3 iter_max; 11/12/13: the same
+                          reached by the multigrid fallback after the learned
+                          preconditioner stagnated (MOONS_PREC_UNET)        */
   double ms;           /* device time of the solve, CUDA events              */
 } moons_solve_info;
 
@@ -107,7 +109,10 @@ enum {
    * building blocks (GF_restrict.f90, GF_prolongate.f90, SOR.f90) but no
    * compiled V-cycle (code_not_compiled/9.6.2017/MG/MG.f90:241-396). */
   MOONS_PREC_MG = 4,          /* FP64 V-cycle inside CG                      */
-  MOONS_PREC_MG_MIXED = 5     /* FP32 V-cycle inside FP64 flexible CG         */
+  MOONS_PREC_MG_MIXED = 5,    /* FP32 V-cycle inside FP64 flexible CG         */
+  MOONS_PREC_UNET = 6         /* learned: the U-Net (moons_pcg_set_unet) inside
+                                 FP64 flexible CG, FP32 V-cycle as the fallback
+                                 when 10 iterations fail to halve the residual */
 };
 
 typedef struct moons_mesh moons_mesh;
@@ -315,12 +320,29 @@ int moons_unet_get_out_scale(const moons_unet* u, double* c);
 int moons_unet_set_feature(moons_unet* u, const float* host, long long n);
 /* z = M(r); r, z cell-centred fields of the net's mesh (z's ghosts = 0) */
 int moons_unet_apply(moons_unet* u, moons_sf* z, const moons_sf* r);
-/* loss = |y - t|^2 / |t|^2 with t = e / (out_scale * rms(r)) and its
- * gradient (grads_host may be null; n = nparams) */
+/* training loss: kind 0 relative L2, |y - t|^2 / |t|^2 with
+ * t = e / (out_scale * rms(r)); kind 1 (default) cosine, 1 - y.t / (|y| |t|),
+ * invariant to a positive scale of the output, as flexible CG is; */
+int moons_unet_set_loss(moons_unet* u, int kind);
+/* kind 2: cosine in the energy norm of the solver's operator A (the norm CG
+ * minimises), 1 - y.A e / sqrt(y.A y  e.A e) with A e = r; the operator is
+ * the FP32 finest multigrid level of a MOONS_PREC_MG_MIXED / MOONS_PREC_UNET
+ * solver on the net's mesh, set (per case) by moons_unet_set_operator */
+int moons_unet_set_operator(moons_unet* u, moons_pcg* s);
+/* the training loss and its gradient (grads_host may be null; n = nparams) */
 int moons_unet_loss_grad(moons_unet* u, const moons_sf* r, const moons_sf* e, float* loss, float* grads_host,
                          long long n);
 /* one Adam step (beta 0.9 / 0.999) on one (r, e) pair; loss may be null */
 int moons_unet_train_step(moons_unet* u, const moons_sf* r, const moons_sf* e, float lr, float* loss);
+/* per-cell feature from face coefficients: log10(mean of the six faces)/3 */
+int moons_unet_set_coeff(moons_unet* u, const moons_sf* kx, const moons_sf* ky, const moons_sf* kz);
+/* the solver's own residual for the iterate x (modify_RHS + the initial
+ * residual of PCG_solver_algorithm.f90:55-66): r = vol*(b - A x_BC - A x),
+ * mean removed for all-Neumann problems; what a preconditioner is applied to */
+int moons_pcg_residual(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, moons_sf* const* r);
+/* attach a network to a solver created with MOONS_PREC_UNET (same mesh; the
+ * solver does not own it and reads its current weights at every solve) */
+int moons_pcg_set_unet(moons_pcg* s, moons_unet* u);
 /* kernel self-check of one layer on host data ([C][Z][Y][X] FP32, interior,
  * rounded to BF16 on upload): op 0 out = conv(in) (+bias, ReLU if relu);
  * op 1 out = transposed conv of dout (gradient w.r.t. the input); op 2 out =

@@ -26,6 +26,7 @@ DIRICHLET, NEUMANN, PERIODIC, ROBIN = 1, 2, 3, 4
 OP_LAP_UNIFORM, OP_LAP_PROPS, OP_IND_DIFFUSION, OP_MOM_DIFFUSION = 1, 2, 3, 4
 PREC_IDENTITY, PREC_LAP, PREC_MOM, PREC_IND = 0, 1, 2, 3
 PREC_MG, PREC_MG_MIXED = 4, 5  # multigrid V-cycle in CG (FP64) / in flexible CG (FP32 V-cycle)
+PREC_UNET = 6  # learned U-Net in flexible CG, FP32 V-cycle fallback (PCG.set_unet)
 
 
 class MoonsError(RuntimeError):
@@ -209,6 +210,11 @@ def lib() -> C.CDLL:
             "moons_unet_get_out_scale": (C.c_int, [_P, C.POINTER(C.c_double)]),
             "moons_unet_set_feature": (C.c_int, [_P, _F, C.c_longlong]),
             "moons_unet_apply": (C.c_int, [_P, _P, _P]),
+            "moons_unet_set_coeff": (C.c_int, [_P, _P, _P, _P]),
+            "moons_unet_set_loss": (C.c_int, [_P, C.c_int]),
+            "moons_unet_set_operator": (C.c_int, [_P, _P]),
+            "moons_pcg_set_unet": (C.c_int, [_P, _P]),
+            "moons_pcg_residual": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
             "moons_unet_loss_grad": (C.c_int, [_P, _P, _P, _F, _F, C.c_longlong]),
             "moons_unet_train_step": (C.c_int, [_P, _P, _P, C.c_float, _F]),
             "moons_unet_layer_check": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -447,6 +453,15 @@ class PCG:
     def update_mfp(self, coeff: float, update_prec: bool = True):
         _check(lib().moons_pcg_update_mfp(self.h, float(coeff), 1 if update_prec else 0))
 
+    def residual(self, x: Sequence[Field], b: Sequence[Field], out: Sequence[Field]):
+        """The solver's internal residual vol*(b - A x) for the iterate x."""
+        _check(lib().moons_pcg_residual(self.h, _ptrs(x), _ptrs(b), _ptrs(out)))
+
+    def set_unet(self, net: "UNet"):
+        """Attach the network of a PREC_UNET solver (kept alive by the solver)."""
+        _check(lib().moons_pcg_set_unet(self.h, net.h))
+        self.net = net
+
     def solve(self, x: Sequence[Field], b: Sequence[Field], params: ISP) -> dict:
         info = SolveInfo()
         _check(lib().moons_pcg_solve(self.h, _ptrs(x), _ptrs(b), C.byref(params), C.byref(info)))
@@ -509,6 +524,19 @@ class UNet:
     def set_feature(self, feat):
         a = np.ascontiguousarray(np.asarray(feat, dtype=np.float32).ravel(order="F"))
         _check(lib().moons_unet_set_feature(self.h, _fp(a), a.size))
+
+    def set_loss(self, kind: int):
+        """Training loss: 0 relative L2, 1 cosine (scale-invariant, default),
+        2 cosine in the energy norm of the operator set by set_operator."""
+        _check(lib().moons_unet_set_loss(self.h, int(kind)))
+
+    def set_operator(self, solver: "PCG"):
+        """The operator of the energy-norm loss (an MG_MIXED / UNET solver)."""
+        _check(lib().moons_unet_set_operator(self.h, solver.h))
+
+    def set_coeff(self, k: Sequence[Field]):
+        """Feature from the face coefficients of a LAP_PROPS operator."""
+        _check(lib().moons_unet_set_coeff(self.h, k[0].h, k[1].h, k[2].h))
 
     def apply(self, z: Field, r: Field):
         _check(lib().moons_unet_apply(self.h, z.h, r.h))

@@ -32,6 +32,11 @@ struct PcgScalars {
   int body_runs;  // executions of the loop body (second bound on the loop)
   // accumulated over solves until the host clears them
   int iter_total, runs_total, nan_any;
+  // stagnation test of flexible CG with a learned preconditioner: every
+  // stag_window iterations, stop (exit_reason 4) unless the residual fell
+  // below stag_factor times its value stag_window iterations before
+  int stag_window;
+  double stag_factor, stag_ref;
 };
 
 // implicit BCs + masks of one unknown component, as the fused kernels see them

@@ -450,6 +450,95 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
 }
 
 void mg_free(MGHier* h) { delete h; }
+
+namespace mg {
+// out = (volume-weighted operator) in, on the finest FP32 level (interior;
+// ghost values of `in` are implied by the BCs, never read)
+__global__ void __launch_bounds__(256) k_mg_apply_f32(MGLev<float> L, const float* in, float* out) {
+  const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
+  const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / (unsigned)nx;
+    const int i = (int)(t - q * (unsigned)nx) + 2;
+    const unsigned kk = q / (unsigned)ny;
+    const int j = (int)(q - kk * (unsigned)ny) + 2, k = (int)kk + 2;
+    float D;
+    out[lidx(L, i, j, k)] = apply_A<float>(L, in, i, j, k, D);
+  }
+}
+
+int mg_apply_fine_f32(MGHier* h, const float* in, float* out, cudaStream_t st) {
+  if (!h || !h->mixed || h->Lf.empty()) {
+    set_error("multigrid: no FP32 finest level");
+    return MOONS_ERR_STATE;
+  }
+  const MGLev<float>& L = h->Lf[0];
+  const size_t n = (size_t)(L.s0 - 2) * (L.s1 - 2) * (L.s2 - 2);
+  MG_LAUNCH(k_mg_apply_f32, (unsigned)std::min<size_t>((n + 255) / 256, (size_t)h->nsm * 8), 256, st, L, in, out);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+// block partials of y.(A y) over the interior, the operator evaluated and
+// summed in FP64 from the FP32 level (the sum cancels heavily where the
+// coefficients are large, which FP32 accumulation cannot carry)
+__global__ void __launch_bounds__(256) k_mg_energy_f64(MGLev<float> L, const float* y, double* partial) {
+  const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
+  const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
+  double acc = 0.0;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / (unsigned)nx;
+    const int i = (int)(t - q * (unsigned)nx) + 2;
+    const unsigned kk = q / (unsigned)ny;
+    const int j = (int)(q - kk * (unsigned)ny) + 2, k = (int)kk + 2;
+    const size_t id = lidx(L, i, j, k);
+    const double e0 = y[id];
+    const int ii[3] = {i, j, k};
+    const size_t st[3] = {1, (size_t)L.s0, (size_t)L.s0 * L.s1};
+    const bool inner = i > 2 && i < L.s0 - 1 && j > 2 && j < L.s1 - 1 && k > 2 && k < L.s2 - 1;
+    double v = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const MGAxis<float>& A = L.ax[d];
+      const int tt = ii[d];
+      const int di = d == 0, dj = d == 1, dk = d == 2;
+      const double em = inner ? y[id - st[d]] : ev(L, y, i - di, j - dj, k - dk);
+      const double ep = inner ? y[id + st[d]] : ev(L, y, i + di, j + dj, k + dk);
+      double gl = em * (double)A.cD[tt - 1] + e0 * (double)A.cU[tt - 1];
+      double gr = e0 * (double)A.cD[tt] + ep * (double)A.cU[tt];
+      const float* kf = d == 0 ? L.kx : (d == 1 ? L.ky : L.kz);
+      if (kf) {
+        gl *= (double)kf[fidx(L, d, i, j, k)];
+        gr *= (double)kf[fidx(L, d, i + di, j + dj, k + dk)];
+      }
+      v += gl * (double)A.nD[tt] + gr * (double)A.nU[tt];
+    }
+    const double vol = ((double)L.ax[0].hv[i] * (double)L.ax[1].hv[j]) * (double)L.ax[2].hv[k];
+    acc += e0 * v * vol;
+  }
+  __shared__ double sh[8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sh[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+int mg_energy_fine_f64(MGHier* h, const float* y, double* partial, int nblocks, cudaStream_t st) {
+  if (!h || !h->mixed || h->Lf.empty()) {
+    set_error("multigrid: no FP32 finest level");
+    return MOONS_ERR_STATE;
+  }
+  MG_LAUNCH(k_mg_energy_f64, (unsigned)nblocks, 256, st, h->Lf[0], y, partial);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+bool mg_is_mixed(const MGHier* h) { return h && h->mixed; }
+}  // namespace mg
 double* mg_rprev(MGHier* h) { return h->rprev; }
 
 namespace {

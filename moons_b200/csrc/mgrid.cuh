@@ -366,6 +366,18 @@ __global__ void __launch_bounds__(kLB) k_m_update(DF x, DF p, DF r, DF Ap, doubl
                                                   double* partial, unsigned* ticket) {
   if (S->done) return;
   const double alpha = S->alpha;
+  if (S->stag_window > 0 && !(isfinite(alpha) && alpha > 0.0)) {
+    // learned preconditioner broke down: alpha = z.r / p.Ap must be positive
+    // and finite (z.r and p.Ap share the operator's sign when the
+    // preconditioner is definite like the operator).  Leave x and r as they
+    // are and hand over to the fallback (exit_reason 4); every block sees
+    // the same alpha and returns here
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      S->exit_reason = 4;
+      S->done = 1;
+    }
+    return;
+  }
   double arr = 0.0;
   const unsigned n = (unsigned)x.n();
   for (unsigned id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
@@ -407,6 +419,15 @@ __global__ void __launch_bounds__(kLB) k_m_update(DF x, DF p, DF r, DF Ap, doubl
       if (!stop && S->iter >= S->iter_max) {
         stop = true;
         S->exit_reason = 3;
+      }
+      if (!stop && S->stag_window > 0 && S->iter % S->stag_window == 0) {
+        const double res = sqrt(fabs(rr));
+        if (res > S->stag_factor * S->stag_ref) {
+          stop = true;
+          S->res = res;
+          S->exit_reason = 4;
+        }
+        S->stag_ref = res;
       }
       S->done = stop ? 1 : 0;
     }

@@ -64,7 +64,21 @@ __global__ void k_reduce(Comp3 a, Comp3 b, int mode, int dw0, int dw1, int dw2, 
 // start of the solve, after res0 (=sum r^2) and rhok (=dot(r,z)) were reduced
 __global__ void k_pcg_start(PcgScalars* S) {
   S->res0 = sqrt(S->res0);
+  S->stag_ref = S->res0;
   S->res = sqrt(fabs(S->rhok));
+  if (S->stag_window > 0 && !(fabs(S->rhok) > 0.0) && S->res0 > 0.0) {
+    // learned preconditioner: z.r = 0 (or NaN) gives no search direction;
+    // hand over to the fallback (exit_reason 4) before the first iteration.
+    // (Its sign is not tested: the Laplacians are negative definite, and a
+    // good preconditioner then has z.r < 0, as the Jacobi one does.)
+    S->iter = 0;
+    S->body_runs = 0;
+    S->nan = 0;
+    S->res = S->res0;
+    S->exit_reason = 4;
+    S->done = 1;
+    return;
+  }
   S->iter = 0;
   S->body_runs = 0;
   S->nan = isnan(S->res0) ? 1 : 0;
@@ -80,6 +94,12 @@ __global__ void k_pcg_start(PcgScalars* S) {
 }
 
 // host-side parameters of the next solve (the accumulators are kept)
+// stagnation test of the learned preconditioner (window 0 = off)
+__global__ void k_stag_params(PcgScalars* S, int window, double factor) {
+  S->stag_window = window;
+  S->stag_factor = factor;
+}
+
 __global__ void k_pcg_params(PcgScalars* S, int iter_max, int nskip, double tol_rel, double tol_abs) {
   S->iter_max = iter_max;
   S->nskip = nskip;
@@ -160,7 +180,17 @@ using namespace mg;
 
 // multigrid preconditioner (mgpcg.cu)
 struct MGHier;
+// flexible CG with the learned preconditioner stops (and the multigrid
+// fallback takes over) when 10 iterations fail to halve the residual
+constexpr int kStagWindow = 10;
+constexpr double kStagFactor = 0.5;
+
 struct moons_pcg;
+namespace mg {
+int unet_apply_dev(moons_unet* u, double* z, const double* r, const int* skip);
+int unet_prepare(moons_unet* u);
+moons_mesh* unet_mesh(moons_unet* u);
+}  // namespace mg
 int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const mg::DBC& bc, const mg::DF* kf, MGHier** out);
 void mg_free(MGHier* h);
 int mg_vcycle(MGHier* h, mg::DF z, mg::DF r, cudaStream_t st, const mg::PcgScalars* S);
@@ -192,7 +222,16 @@ struct moons_pcg {
   cudaGraphExec_t exec = nullptr;
   double* gx[3] = {nullptr, nullptr, nullptr};
   long long body_launches = 0;  // kernels per execution of the loop body
-  MGHier* mgh = nullptr;        // MOONS_PREC_MG / MG_MIXED: the V-cycle hierarchy
+  MGHier* mgh = nullptr;        // MOONS_PREC_MG / MG_MIXED / UNET: the V-cycle hierarchy
+  // MOONS_PREC_UNET: the network (not owned) and the multigrid fallback mode
+  moons_unet* unet = nullptr;
+  bool learned = false;
+  bool fb = false;              // true while the fallback (FP32 V-cycle) runs
+  // the other mode's loop graph (swapped in and out with the fields above)
+  cudaGraph_t graph_alt = nullptr;
+  cudaGraphExec_t exec_alt = nullptr;
+  double* gx_alt[3] = {nullptr, nullptr, nullptr};
+  long long body_launches_alt = 0;
 };
 
 namespace {
@@ -297,7 +336,8 @@ int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
 int compute_prec(moons_pcg* s) {
   moons_mesh* m = s->m;
   int mode = s->prec;
-  if (mode == MOONS_PREC_MG || mode == MOONS_PREC_MG_MIXED) mode = MOONS_PREC_IDENTITY;  // Minv unused
+  if (mode == MOONS_PREC_MG || mode == MOONS_PREC_MG_MIXED || mode == MOONS_PREC_UNET)
+    mode = MOONS_PREC_IDENTITY;  // Minv unused
   DF dummy{};
   if (mode == MOONS_PREC_IND && s->op != MOONS_OP_IND_DIFFUSION) {
     set_error("moons_pcg: prec_ind needs the induction operator's sigma^-1 edge fields");
@@ -395,7 +435,8 @@ int enqueue_mg_iteration(moons_pcg* s, DF* x) {
       MG_LAUNCH(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], z0, z0, z0, 0.0,
                 s->S, s->partial, tA);
     MG_LAUNCH(k_m_update, gF, kLB, m->stream, x[0], pc[0], s->r[0], s->Ax[0], rprev, s->S, s->partial, tB);
-    int r = mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, s->S);
+    int r = (s->learned && !s->fb) ? unet_apply_dev(s->unet, s->z[0].f, s->r[0].f, &s->S->done)
+                                   : mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, s->S);
     if (r) return r;
     MG_LAUNCH(k_m_beta, gF, kLB, m->stream, s->z[0], s->r[0], rprev, s->S, s->partial, tA);
     MG_LAUNCH(k_m_pupd, gF, kLB, m->stream, pn[0], pc[0], s->z[0], s->S);
@@ -450,6 +491,28 @@ void plan_lean(moons_pcg* s) {
   L.gD = dim3(npbP + npbI, gyD, (unsigned)nc);
 }
 
+// destroy both loop graphs (they are rebuilt on the next solve)
+void drop_graphs(moons_pcg* s) {
+  if (s->exec) cudaGraphExecDestroy(s->exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  if (s->exec_alt) cudaGraphExecDestroy(s->exec_alt);
+  if (s->graph_alt) cudaGraphDestroy(s->graph_alt);
+  s->exec = s->exec_alt = nullptr;
+  s->graph = s->graph_alt = nullptr;
+  for (int c = 0; c < 3; c++) s->gx[c] = s->gx_alt[c] = nullptr;
+}
+
+// switch between the learned and the fallback preconditioner (each mode
+// keeps its own loop graph)
+void set_fallback(moons_pcg* s, bool fb) {
+  if (s->fb == fb) return;
+  std::swap(s->graph, s->graph_alt);
+  std::swap(s->exec, s->exec_alt);
+  for (int c = 0; c < 3; c++) std::swap(s->gx[c], s->gx_alt[c]);
+  std::swap(s->body_launches, s->body_launches_alt);
+  s->fb = fb;
+}
+
 int build_graph(moons_pcg* s, DF* x) {
   moons_mesh* m = s->m;
   if (s->exec) {
@@ -501,7 +564,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: ncomp must be 1 or 3");
     return MOONS_ERR_ARG;
   }
-  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_MOM_DIFFUSION || prec < 0 || prec > MOONS_PREC_MG_MIXED) {
+  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_MOM_DIFFUSION || prec < 0 || prec > MOONS_PREC_UNET) {
     set_error("moons_pcg_create: bad operator/preconditioner");
     return MOONS_ERR_ARG;
   }
@@ -514,7 +577,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: operator needs three coefficient fields");
     return MOONS_ERR_ARG;
   }
-  const bool use_mg = prec == MOONS_PREC_MG || prec == MOONS_PREC_MG_MIXED;
+  const bool use_mg = prec == MOONS_PREC_MG || prec == MOONS_PREC_MG_MIXED || prec == MOONS_PREC_UNET;
   if (use_mg) {
     bool ok = nc == 1 && (op == MOONS_OP_LAP_UNIFORM || op == MOONS_OP_LAP_PROPS) && x[0] &&
               x[0]->f.dl == MOONS_CC;
@@ -622,7 +685,8 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     }
   }
   if (!r && use_mg) {
-    r = mg_build(s, m, prec == MOONS_PREC_MG_MIXED, s->x_bc[0], op == MOONS_OP_LAP_PROPS ? s->k : nullptr, &s->mgh);
+    r = mg_build(s, m, prec != MOONS_PREC_MG, s->x_bc[0], op == MOONS_OP_LAP_PROPS ? s->k : nullptr, &s->mgh);
+    s->learned = prec == MOONS_PREC_UNET;
     if (r == MOONS_ERR_NOMEM) set_error("moons_pcg_create: device allocation failed (multigrid levels)");
   }
   if (!r && cudaStreamSynchronize(m->stream) != cudaSuccess) r = cuda_fail(cudaGetLastError(), "pcg create");
@@ -637,6 +701,8 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
 int moons_pcg_destroy(moons_pcg* s) {
   if (s && s->exec) cudaGraphExecDestroy(s->exec);
   if (s && s->graph) cudaGraphDestroy(s->graph);
+  if (s && s->exec_alt) cudaGraphExecDestroy(s->exec_alt);
+  if (s && s->graph_alt) cudaGraphDestroy(s->graph_alt);
   if (!s) return MOONS_OK;
   cudaSetDevice(s->m->device);
   cudaStreamSynchronize(s->m->stream);
@@ -655,12 +721,7 @@ int moons_pcg_update_mfp(moons_pcg* s, double c, int upd) {
     return MOONS_ERR_ARG;
   }
   s->coeff = c;
-  if (s->exec) {  // the coefficient is baked into the captured launches
-    cudaGraphExecDestroy(s->exec);
-    s->exec = nullptr;
-    cudaGraphDestroy(s->graph);
-    s->graph = nullptr;
-  }
+  drop_graphs(s);  // the coefficient is baked into the captured launches
   if (upd) {
     int r = compute_prec(s);
     if (r) return r;
@@ -697,21 +758,16 @@ int mg_pcg_totals(moons_pcg* s, int* iters, int* nan_any, double* last_rel) {
   return MOONS_OK;
 }
 
-// enqueue a whole solve (modify_RHS + loop + final BCs of x); no host sync
-int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp* isp) {
+int modify_rhs(moons_pcg* s, DF* X, DF* B);
+
+// modify_RHS (PCG_aux.f90:30-79) and the initial residual of
+// PCG_solver_algorithm.f90:55-66: s->r = vol * (b - A x_BC - A x), the mean
+// removed for an all-Neumann problem, wall masks applied; x gets its
+// implicit BCs.  Enqueued, no host sync.
+int modify_rhs(moons_pcg* s, DF* X, DF* B) {
   moons_mesh* m = s->m;
-  DF X[3], B[3];
-  for (int c = 0; c < s->nc; c++) {
-    if (!x[c] || !b[c] || x[c]->f.dl != s->x_dl[c] || b[c]->f.n() != x[c]->f.n()) {
-      set_error("moons_pcg_solve: field does not match the solver");
-      return MOONS_ERR_SHAPE;
-    }
-    X[c] = x[c]->f;
-    B[c] = b[c]->f;
-  }
+  const int nc = s->nc;
   int r = MOONS_OK;
-  int nc = s->nc;
-  // ---- modify_RHS (PCG_aux.f90:30-79)
   for (int c = 0; c < nc && !r; c++) r = launch_pw(m, PW_COPY, s->r[c], &B[c], 0.0);
   if (!r && s->all_neumann) {
     // tempx = r*vol; mean = sum(tempx,1)/vol%vol; r -= mean; assign_ghost_XPeriodic(r,0)
@@ -744,13 +800,40 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
     }
   }
   if (r) return r;
+  return r;
+}
+
+// enqueue a whole solve (modify_RHS + loop + final BCs of x); no host sync
+int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp* isp) {
+  moons_mesh* m = s->m;
+  DF X[3], B[3];
+  for (int c = 0; c < s->nc; c++) {
+    if (!x[c] || !b[c] || x[c]->f.dl != s->x_dl[c] || b[c]->f.n() != x[c]->f.n()) {
+      set_error("moons_pcg_solve: field does not match the solver");
+      return MOONS_ERR_SHAPE;
+    }
+    X[c] = x[c]->f;
+    B[c] = b[c]->f;
+  }
+  int nc = s->nc;
+  int r = modify_rhs(s, X, B);
+  if (r) return r;
   // ---- scalars
   MG_LAUNCH(k_pcg_params, 1, 1, m->stream, s->S, isp->iter_max, isp->n_skip_check_res, isp->tol_rel, isp->tol_abs);
   // res0 = sqrt(sum r^2) whole array
   MG_LAUNCH(k_reduce, red_grid(s->r, nc), kBlock, m->stream, c3(s->r, nc), c3(s->r, nc), 1, 0, 0, 0, &s->S->res0,
             m->d_partial, m->d_ticket);
+  const bool learned = s->learned && !s->fb;
+  MG_LAUNCH(k_stag_params, 1, 1, m->stream, s->S, learned ? kStagWindow : 0, kStagFactor);
   // z = Minv r ; p = z ; rhok = dot(r,z)
-  if (s->mgh) {
+  if (learned) {
+    if (!s->unet) {
+      set_error("moons_pcg_solve: MOONS_PREC_UNET needs a network (moons_pcg_set_unet)");
+      return MOONS_ERR_STATE;
+    }
+    r = unet_apply_dev(s->unet, s->z[0].f, s->r[0].f, nullptr);
+    if (r) return r;
+  } else if (s->mgh) {
     r = mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, nullptr);
     if (r) return r;
   }
@@ -841,17 +924,95 @@ int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const 
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   mg_pcg_clear_totals(s);
+  set_fallback(s, false);
   cudaEventRecord(e0, m->stream);
   int r = mg_pcg_enqueue(s, x, b, isp);
   cudaEventRecord(e1, m->stream);
   cudaError_t e = cudaStreamSynchronize(m->stream);
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
+  if (!r) r = e == cudaSuccess ? MOONS_OK : cuda_fail(e, "moons_pcg_solve");
+  moons_solve_info i1{};
+  if (!r) r = mg_pcg_collect(s, &i1, ms);
+  if (!r && s->learned && i1.exit_reason == 4) {
+    // the learned preconditioner stagnated: continue from the current x with
+    // the FP32 V-cycle, to the original target (relative to the first res0)
+    moons_isp isp2 = *isp;
+    isp2.iter_max = std::max(0, isp->iter_max - i1.iterations);
+    const double target = isp->tol_rel * i1.res0;
+    isp2.tol_rel = i1.res > 0.0 ? target / i1.res : isp->tol_rel;
+    set_fallback(s, true);
+    cudaEventRecord(e0, m->stream);
+    r = mg_pcg_enqueue(s, x, b, &isp2);
+    cudaEventRecord(e1, m->stream);
+    e = cudaStreamSynchronize(m->stream);
+    float ms2 = 0;
+    cudaEventElapsedTime(&ms2, e0, e1);
+    if (!r) r = e == cudaSuccess ? MOONS_OK : cuda_fail(e, "moons_pcg_solve (fallback)");
+    moons_solve_info i2{};
+    if (!r) r = mg_pcg_collect(s, &i2, ms2);
+    set_fallback(s, false);
+    if (!r) {
+      i2.iterations += i1.iterations;
+      i2.res0 = i1.res0;
+      i2.rel = i1.res0 == 0.0 ? i2.res : i2.res / i1.res0;
+      i2.exit_reason += 10;
+      i2.ms += i1.ms;
+      i1 = i2;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (!r && info) *info = i1;
+  return r;
+}
+
+int moons_pcg_residual(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, moons_sf* const* rout) {
+  if (!s || !x || !b || !rout) {
+    set_error("moons_pcg_residual: null pointer");
+    return MOONS_ERR_ARG;
+  }
+  DF X[3], B[3];
+  for (int c = 0; c < s->nc; c++) {
+    if (!x[c] || !b[c] || !rout[c] || x[c]->f.dl != s->x_dl[c] || b[c]->f.n() != x[c]->f.n() ||
+        rout[c]->f.n() != x[c]->f.n()) {
+      set_error("moons_pcg_residual: field does not match the solver");
+      return MOONS_ERR_SHAPE;
+    }
+    X[c] = x[c]->f;
+    B[c] = b[c]->f;
+  }
+  moons_mesh* m = s->m;
+  cudaSetDevice(m->device);
+  int r = modify_rhs(s, X, B);
+  for (int c = 0; c < s->nc && !r; c++) r = launch_pw(m, PW_COPY, rout[c]->f, &s->r[c], 0.0);
+  if (!r) MG_CUDA(cudaStreamSynchronize(m->stream));
+  return r;
+}
+
+int moons_pcg_set_unet(moons_pcg* s, moons_unet* u) {
+  if (!s || !u) {
+    set_error("moons_pcg_set_unet: null argument");
+    return MOONS_ERR_ARG;
+  }
+  if (!s->learned) {
+    set_error("moons_pcg_set_unet: the solver was not created with MOONS_PREC_UNET");
+    return MOONS_ERR_ARG;
+  }
+  if (unet_mesh(u) != s->m) {
+    set_error("moons_pcg_set_unet: the network lives on another mesh");
+    return MOONS_ERR_SHAPE;
+  }
+  int r = unet_prepare(u);
   if (r) return r;
-  MG_CUDA(e);
-  return mg_pcg_collect(s, info, ms);
+  s->unet = u;
+  drop_graphs(s);
+  return MOONS_OK;
 }
 
 }  // extern "C"
+
+namespace mg {
+MGHier* pcg_mg_hier(moons_pcg* s) { return s ? s->mgh : nullptr; }
+moons_mesh* pcg_mesh(moons_pcg* s) { return s ? s->m : nullptr; }
+}  // namespace mg

@@ -29,6 +29,15 @@
 
 using namespace un;
 
+struct MGHier;
+namespace mg {
+int mg_apply_fine_f32(MGHier* h, const float* in, float* out, cudaStream_t st);
+int mg_energy_fine_f64(MGHier* h, const float* y, double* partial, int nblocks, cudaStream_t st);
+bool mg_is_mixed(const MGHier* h);
+MGHier* pcg_mg_hier(moons_pcg* s);
+moons_mesh* pcg_mesh(moons_pcg* s);
+}  // namespace mg
+
 namespace {
 
 enum {
@@ -64,6 +73,18 @@ int allow_max_smem(K kernel, int device) {
   cudaFuncAttributes fa{};
   MG_CUDA(cudaFuncGetAttributes(&fa, kernel));
   MG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+  return MOONS_OK;
+}
+
+bool g_attr_done[64] = {};
+
+// raise the dynamic shared memory limit of the tcgen05 kernels (once per
+// device, outside any stream capture)
+int ensure_attrs(int device) {
+  if (g_attr_done[device & 63]) return MOONS_OK;
+  if (int e = allow_max_smem(k_conv3, device)) return e;
+  if (int e = allow_max_smem(k_wgrad, device)) return e;
+  g_attr_done[device & 63] = true;
   return MOONS_OK;
 }
 
@@ -106,6 +127,9 @@ struct moons_unet {
   int adam_t = 0;
   long long ncell = 0;
   bool packed = false;
+  int loss_kind = 1;          // 0 relative L2, 1 cosine, 2 energy-norm cosine
+  MGHier* op = nullptr;       // kind 2: the solver operator (FP32 finest multigrid level)
+  float* ay32 = nullptr;      // kind 2: A y, cell-centred layout
 };
 
 namespace {
@@ -138,11 +162,11 @@ struct ConvOut {
   bf16* outA; bf16* outB; int ocgA;
   const bf16* maskA; const bf16* maskB;
   const float* head_w; const float* head_b; float* y32; double* z64; const double* zscale;
+  const int* skip;
 };
 
 int launch_conv(moons_unet* u, int lvl, const bf16* inA, int cgA, const bf16* inB, int cgB, const bf16* wt,
                 const float* bias, int N, int mode, const ConvOut& o) {
-  static bool attr_set[64] = {};
   const Geo& g = u->geo[lvl];
   ConvArgs a{};
   a.g = g;
@@ -160,15 +184,13 @@ int launch_conv(moons_unet* u, int lvl, const bf16* inA, int cgA, const bf16* in
   a.maskA = o.maskA; a.maskB = o.maskB;
   a.head_w = o.head_w; a.head_b = o.head_b; a.y32 = o.y32; a.z64 = o.z64; a.zscale = o.zscale;
   a.err = u->err;
+  a.skip = o.skip;
   if (N % 16 || N < 16 || N > 256) {
     mg::set_error("U-Net convolution: output channels must be a multiple of 16 in [16, 256]");
     return MOONS_ERR_ARG;
   }
   const int smem = S * SB;
-  if (!attr_set[u->device & 63]) {
-    if (int e = allow_max_smem(k_conv3, u->device)) return e;
-    attr_set[u->device & 63] = true;
-  }
+  if (int e = ensure_attrs(u->device)) return e;
   dim3 grid(g.tiles_per_plane(), g.Z);
   k_conv3<<<grid, kConvThreads, smem, u->stream>>>(a);
   return launch_err("k_conv3");
@@ -176,7 +198,6 @@ int launch_conv(moons_unet* u, int lvl, const bf16* inA, int cgA, const bf16* in
 
 int launch_wgrad(moons_unet* u, int lvl, const bf16* inA, int cgA, const bf16* inB, int cgB, const bf16* dout, int N,
                  float* dW, int cin) {
-  static bool attr_set[64] = {};
   const Geo& g = u->geo[lvl];
   WgradArgs a{};
   a.g = g;
@@ -195,10 +216,7 @@ int launch_wgrad(moons_unet* u, int lvl, const bf16* inA, int cgA, const bf16* i
   a.S = std::max(2, std::min(4, (200 * 1024) / SB));
   a.dW = dW; a.cin = cin;
   a.err = u->err;
-  if (!attr_set[u->device & 63]) {
-    if (int e = allow_max_smem(k_wgrad, u->device)) return e;
-    attr_set[u->device & 63] = true;
-  }
+  if (int e = ensure_attrs(u->device)) return e;
   dim3 grid(nsg, nct, chunks);
   k_wgrad<<<grid, kConvThreads, a.S * SB, u->stream>>>(a);
   return launch_err("k_wgrad");
@@ -223,25 +241,26 @@ int pack_weights(moons_unet* u) {
 }
 
 // rms of r (FP64 cell-centred) -> u->scal
-int scale_of(moons_unet* u, const double* r) {
+int scale_of(moons_unet* u, const double* r, const int* skip) {
   const Geo& g = u->geo[0];
-  k_sumsq_cc<<<kURedBlocks, kURedThreads, 0, u->stream>>>(g, r, u->dpart);
+  k_sumsq_cc<<<kURedBlocks, kURedThreads, 0, u->stream>>>(g, r, u->dpart, skip);
   int e = launch_err("k_sumsq_cc");
   if (e) return e;
-  k_scale_fin<<<1, 32, 0, u->stream>>>(u->dpart, kURedBlocks, u->ncell, u->out_scale, u->scal);
+  k_scale_fin<<<1, 32, 0, u->stream>>>(u->dpart, kURedBlocks, u->ncell, u->out_scale, u->scal, skip);
   return launch_err("k_scale_fin");
 }
 
-// forward pass from r; z64 (optional) receives out_scale*rms(r)*y
-int forward(moons_unet* u, const double* r, double* z64) {
+// forward pass from r; z64 (optional) receives out_scale*rms(r)*y; every
+// kernel returns at once while *skip (optional device flag) is nonzero
+int forward(moons_unet* u, const double* r, double* z64, const int* skip = nullptr) {
   if (!u->packed) {
     int e = pack_weights(u);
     if (e) return e;
   }
-  int e = scale_of(u, r);
+  int e = scale_of(u, r, skip);
   if (e) return e;
   const Geo& g0 = u->geo[0];
-  k_pack_in<<<ew_grid(u->ncell, u->nsm), 256, 0, u->stream>>>(g0, r, u->feat, u->scal, u->t[T_IN]);
+  k_pack_in<<<ew_grid(u->ncell, u->nsm), 256, 0, u->stream>>>(g0, r, u->feat, u->scal, u->t[T_IN], skip);
   if ((e = launch_err("k_pack_in"))) return e;
   for (int l = 0; l < kNL; l++) {
     const LayerDef& D = kLayers[l];
@@ -252,7 +271,7 @@ int forward(moons_unet* u, const double* r, double* z64) {
       const int lf = kTLvl[src];
       const long long n = (long long)u->geo[lf + 1].X * u->geo[lf + 1].Y * u->geo[lf + 1].Z * (kTC[src] / 8);
       k_pool<<<ew_grid(n, u->nsm), 256, 0, u->stream>>>(u->geo[lf], u->geo[lf + 1], kTC[src] / 8, u->t[src],
-                                                         u->t[D.inA]);
+                                                         u->t[D.inA], skip);
       if ((e = launch_err("k_pool"))) return e;
     }
     if (D.inA == T_U2 || D.inA == T_U1 || D.inA == T_U0) {
@@ -260,12 +279,13 @@ int forward(moons_unet* u, const double* r, double* z64) {
       const int lc = kTLvl[src];
       const long long n = (long long)u->geo[lc - 1].X * u->geo[lc - 1].Y * u->geo[lc - 1].Z * (kTC[src] / 8);
       k_up<<<ew_grid(n, u->nsm), 256, 0, u->stream>>>(u->geo[lc], u->geo[lc - 1], kTC[src] / 8, u->t[src],
-                                                       u->t[D.inA]);
+                                                       u->t[D.inA], skip);
       if ((e = launch_err("k_up"))) return e;
     }
     ConvOut o{};
     o.outA = u->t[D.out];
     o.ocgA = kTC[D.out] / 8;
+    o.skip = skip;
     if (l == kNL - 1) {
       o.head_w = u->params + u->head_ofs;
       o.head_b = u->params + u->head_ofs + 16;
@@ -290,6 +310,10 @@ int bias_grad(moons_unet* u, int lvl, const bf16* dpre, int C, float* out) {
 
 // forward + backward for one (r, e) pair: grads (flat) and fred[0] = loss
 int forward_backward(moons_unet* u, const double* r, const double* ecorr) {
+  if (u->loss_kind == 2 && !u->op) {
+    mg::set_error("U-Net energy-norm loss: no operator (moons_unet_set_operator)");
+    return MOONS_ERR_STATE;
+  }
   int e = forward(u, r, nullptr);
   if (e) return e;
   const Geo& g0 = u->geo[0];
@@ -299,9 +323,30 @@ int forward_backward(moons_unet* u, const double* r, const double* ecorr) {
   k_sum_partials<<<1, 32, 0, u->stream>>>(u->fpart, kURedBlocks, 1, u->fred + 1);
   if ((e = launch_err("k_sum_partials"))) return e;
   MG_CUDA(cudaMemsetAsync(u->grads, 0, u->nparams * sizeof(float), u->stream));
+  // cosine losses: their global sums first (fred[20..22])
+  if (u->loss_kind == 1) {
+    k_yt<<<kURedBlocks, kURedThreads, 0, u->stream>>>(g0, u->y32, u->t32, u->fpart);
+    if ((e = launch_err("k_yt"))) return e;
+    k_sum_partials<<<1, 32, 0, u->stream>>>(u->fpart, kURedBlocks, 2, u->fred + 20);
+    if ((e = launch_err("k_sum_partials"))) return e;
+  } else if (u->loss_kind == 2) {
+    if ((e = mg::mg_apply_fine_f32(u->op, u->y32, u->ay32, u->stream))) return e;
+    if ((e = mg::mg_energy_fine_f64(u->op, u->y32, u->dpart + 2 * kURedBlocks, kURedBlocks, u->stream))) return e;
+    k_energy_sums<<<kURedBlocks, kURedThreads, 0, u->stream>>>(g0, u->y32, ecorr, r, u->scal, u->dpart);
+    if ((e = launch_err("k_energy_sums"))) return e;
+    k_energy_fin<<<1, 32, 0, u->stream>>>(u->dpart, u->dpart + 2 * kURedBlocks, kURedBlocks, u->fred + 20);
+    if ((e = launch_err("k_energy_fin"))) return e;
+  }
   // loss + head backward -> d[T_D0] (dPre of dec0b)
-  k_loss_head<<<kURedBlocks, kURedThreads, 0, u->stream>>>(g0, u->y32, u->t32, u->fred + 1, u->t[T_D0],
-                                                         u->params + u->head_ofs, u->d[T_D0], u->fpart);
+  LossArgs la{};
+  la.g = g0;
+  la.y = u->y32; la.t = u->t32; la.T2p = u->fred + 1;
+  la.kind = u->loss_kind;
+  la.sums = u->fred + 20;
+  la.ay = u->ay32; la.r = r; la.scal = u->scal;
+  la.h = u->t[T_D0]; la.head_w = u->params + u->head_ofs; la.dh = u->d[T_D0];
+  la.partial = u->fpart;
+  k_loss_head<<<kURedBlocks, kURedThreads, 0, u->stream>>>(la);
   if ((e = launch_err("k_loss_head"))) return e;
   k_sum_partials<<<1, 32, 0, u->stream>>>(u->fpart, kURedBlocks, 18, u->fred + 2);
   if ((e = launch_err("k_sum_partials"))) return e;
@@ -355,6 +400,25 @@ int forward_backward(moons_unet* u, const double* r, const double* ecorr) {
   return MOONS_OK;
 }
 
+// the loss of the last forward_backward (syncs)
+int read_loss(moons_unet* u, float* loss) {
+  float h[23];  // [1] |t|^2, [2] |y-t|^2, [20..22] the cosine sums
+  MG_CUDA(cudaMemcpyAsync(h, u->fred, 23 * sizeof(float), cudaMemcpyDeviceToHost, u->stream));
+  if (int e = check_err(u)) return e;
+  const float T2 = h[1] > 0.f ? h[1] : 1.f;
+  if (!loss) return MOONS_OK;
+  if (u->loss_kind == 1) {
+    const float yy = h[21] > 0.f ? h[21] : 1.f;
+    *loss = 1.f - h[20] / sqrtf(yy * T2);
+  } else if (u->loss_kind == 2) {
+    const float B = h[21] > 0.f ? h[21] : 1.f, E = h[22] > 0.f ? h[22] : 1.f;
+    *loss = 1.f - h[20] / sqrtf(B * E);
+  } else {
+    *loss = h[2] / T2;
+  }
+  return MOONS_OK;
+}
+
 int unet_fail_arg(const char* m) {
   mg::set_error(m);
   return MOONS_ERR_ARG;
@@ -368,10 +432,19 @@ bool cc_field_ok(const moons_unet* u, const moons_sf* f) {
 }  // namespace
 
 namespace mg {
-// the preconditioner apply for flexible CG: z = M(r) on the net's stream
-int unet_apply_dev(moons_unet* u, double* z, const double* r) { return forward(u, r, z); }
+// the preconditioner apply for flexible CG: z = M(r) on the mesh stream,
+// skipped while *skip is nonzero (graph-capturable once prepared)
+int unet_apply_dev(moons_unet* u, double* z, const double* r, const int* skip) { return forward(u, r, z, skip); }
+// pack the weights and set kernel attributes outside any stream capture
+int unet_prepare(moons_unet* u) {
+  int e = MOONS_OK;
+  if (!u->packed) e = pack_weights(u);
+  if (!e) e = ensure_attrs(u->device);
+  if (!e) e = check_err(u);
+  return e;
+}
 int unet_check(moons_unet* u) { return check_err(u); }
-cudaStream_t unet_stream(moons_unet* u) { return u->stream; }
+moons_mesh* unet_mesh(moons_unet* u) { return u->m; }
 }  // namespace mg
 
 extern "C" {
@@ -427,12 +500,13 @@ int moons_unet_create(moons_mesh* m, unsigned long long seed, moons_unet** out) 
   u->feat = dalloc<float>(u, ncc);
   u->y32 = dalloc<float>(u, ncc);
   u->t32 = dalloc<float>(u, ncc);
+  u->ay32 = dalloc<float>(u, ncc);
   u->scal = dalloc<double>(u, 4);
-  u->dpart = dalloc<double>(u, kURedBlocks);
+  u->dpart = dalloc<double>(u, 3 * kURedBlocks);
   u->fpart = dalloc<float>(u, (size_t)kURedBlocks * 256);
   u->fred = dalloc<float>(u, 64);
   u->err = dalloc<int>(u, 1);
-  okm = okm && u->params && u->grads && u->am && u->av && u->feat && u->y32 && u->t32 && u->scal && u->dpart &&
+  okm = okm && u->params && u->grads && u->am && u->av && u->feat && u->y32 && u->t32 && u->ay32 && u->scal && u->dpart &&
         u->fpart && u->fred && u->err;
   if (!okm) {
     for (void* p : u->allocs) cudaFree(p);
@@ -499,6 +573,22 @@ int moons_unet_set_params(moons_unet* u, const float* host, long long n) {
   return MOONS_OK;
 }
 
+int moons_unet_set_loss(moons_unet* u, int kind) {
+  if (!u || kind < 0 || kind > 2) return unet_fail_arg("moons_unet_set_loss: kind must be 0, 1 or 2");
+  u->loss_kind = kind;
+  return MOONS_OK;
+}
+
+int moons_unet_set_operator(moons_unet* u, moons_pcg* s) {
+  if (!u || !s) return unet_fail_arg("moons_unet_set_operator: null argument");
+  MGHier* h = mg::pcg_mg_hier(s);
+  if (!h || !mg::mg_is_mixed(h) || mg::pcg_mesh(s) != u->m)
+    return unet_fail_arg("moons_unet_set_operator: needs a MOONS_PREC_MG_MIXED or MOONS_PREC_UNET solver on the "
+                         "net's mesh");
+  u->op = h;
+  return MOONS_OK;
+}
+
 int moons_unet_set_out_scale(moons_unet* u, double c) {
   if (!u || !(c > 0.0)) return unet_fail_arg("moons_unet_set_out_scale: bad argument");
   u->out_scale = c;
@@ -520,6 +610,18 @@ int moons_unet_set_feature(moons_unet* u, const float* host, long long n) {
   return MOONS_OK;
 }
 
+int moons_unet_set_coeff(moons_unet* u, const moons_sf* kx, const moons_sf* ky, const moons_sf* kz) {
+  if (!u || !kx || !ky || !kz) return unet_fail_arg("moons_unet_set_coeff: null argument");
+  const Geo& g = u->geo[0];
+  if (kx->m != u->m || ky->m != u->m || kz->m != u->m || kx->f.dl != MOONS_FX || ky->f.dl != MOONS_FY ||
+      kz->f.dl != MOONS_FZ)
+    return unet_fail_arg("moons_unet_set_coeff: kx, ky, kz must be x, y, z face fields of the net's mesh");
+  k_feat_faces<<<ew_grid(u->ncell, u->nsm), 256, 0, u->stream>>>(g, kx->f.f, ky->f.f, kz->f.f, u->feat);
+  int e = launch_err("k_feat_faces");
+  if (e) return e;
+  return check_err(u);
+}
+
 int moons_unet_apply(moons_unet* u, moons_sf* z, const moons_sf* r) {
   if (!u || !cc_field_ok(u, z) || !cc_field_ok(u, r))
     return unet_fail_arg("moons_unet_apply: z and r must be cell-centred fields of the net's mesh");
@@ -536,13 +638,9 @@ int moons_unet_loss_grad(moons_unet* u, const moons_sf* r, const moons_sf* ecorr
   if (grads_host && n != u->nparams) return unet_fail_arg("moons_unet_loss_grad: gradient size mismatch");
   int e = forward_backward(u, r->f.f, ecorr->f.f);
   if (e) return e;
-  float h[2];
-  MG_CUDA(cudaMemcpyAsync(h, u->fred + 1, 2 * sizeof(float), cudaMemcpyDeviceToHost, u->stream));
   if (grads_host)
     MG_CUDA(cudaMemcpyAsync(grads_host, u->grads, n * sizeof(float), cudaMemcpyDeviceToHost, u->stream));
-  if ((e = check_err(u))) return e;
-  if (loss) *loss = h[1] / (h[0] > 0.f ? h[0] : 1.f);
-  return MOONS_OK;
+  return read_loss(u, loss);
 }
 
 int moons_unet_train_step(moons_unet* u, const moons_sf* r, const moons_sf* ecorr, float lr, float* loss) {
@@ -558,12 +656,7 @@ int moons_unet_train_step(moons_unet* u, const moons_sf* r, const moons_sf* ecor
                                                               b2, 1e-8f, c1, c2);
   if ((e = launch_err("k_adam"))) return e;
   if ((e = pack_weights(u))) return e;
-  if (loss) {
-    float h[2];
-    MG_CUDA(cudaMemcpyAsync(h, u->fred + 1, 2 * sizeof(float), cudaMemcpyDeviceToHost, u->stream));
-    if ((e = check_err(u))) return e;
-    *loss = h[1] / (h[0] > 0.f ? h[0] : 1.f);
-  }
+  if (loss) return read_loss(u, loss);
   return MOONS_OK;
 }
 

@@ -117,6 +117,7 @@ struct ConvArgs {
   const bf16* maskA; const bf16* maskB;   // kLinear: zero where mask <= 0
   const float* head_w; const float* head_b; float* y32; double* z64; const double* zscale;
   int* err;
+  const int* skip;       // nonzero *skip: return at once (the enclosing solve is done)
 };
 
 __host__ __device__ inline int conv_stage_bytes(int L, int N) {
@@ -131,6 +132,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(ConvArgs a) {
   __shared__ __align__(8) uint64_t bar_done;
   __shared__ uint32_t tmem_slot;
 
+  if (a.skip && *a.skip) return;
   const int tid = threadIdx.x, warp = tid >> 5;
   const Geo& g = a.g;
   const int z = blockIdx.y + 1;
@@ -474,7 +476,8 @@ __device__ __forceinline__ bool interior_of(const Geo& g, long long i, int& x, i
 
 // input tensor (one group): ch0 = r / rms(r), ch1 = feature, ch2..7 = 0;
 // r and feat in the (X+2)(Y+2)(Z+2) cell-centred layout
-__global__ void k_pack_in(Geo g, const double* r, const float* feat, const double* scal, bf16* in) {
+__global__ void k_pack_in(Geo g, const double* r, const float* feat, const double* scal, bf16* in, const int* skip) {
+  if (skip && *skip) return;
   const double sinv = scal[1];
   const long long n = (long long)g.X * g.Y * g.Z;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -486,8 +489,26 @@ __global__ void k_pack_in(Geo g, const double* r, const float* feat, const doubl
   }
 }
 
+// per-cell feature of a face-coefficient operator: log10(mean of the six
+// face values) / 3, cell-centred layout (kx, ky, kz face fields of the mesh)
+__global__ void k_feat_faces(Geo g, const double* kx, const double* ky, const double* kz, float* feat) {
+  const long long n = (long long)g.X * g.Y * g.Z;
+  const long long sx = g.X + 2, sy = g.Y + 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    interior_of(g, i, x, y, z);
+    // face arrays: Fx (sx+1, sy, sz), Fy (sx, sy+1, sz), Fz (sx, sy, sz+1)
+    const double a = kx[x + (sx + 1) * (y + sy * (long long)z)] + kx[x + 1 + (sx + 1) * (y + sy * (long long)z)];
+    const double b = ky[x + sx * (y + (sy + 1) * (long long)z)] + ky[x + sx * (y + 1 + (sy + 1) * (long long)z)];
+    const double c = kz[x + sx * (y + sy * (long long)z)] + kz[x + sx * (y + sy * (long long)(z + 1))];
+    const double mean = (a + b + c) / 6.0;
+    feat[x + sx * (y + sy * (long long)z)] = mean > 0.0 ? (float)(log10(mean) / 3.0) : 0.f;
+  }
+}
+
 // 2x2x2 average: out (coarse geometry gc) from in (fine geometry gf)
-__global__ void k_pool(Geo gf, Geo gc, int ncg, const bf16* in, bf16* out) {
+__global__ void k_pool(Geo gf, Geo gc, int ncg, const bf16* in, bf16* out, const int* skip) {
+  if (skip && *skip) return;
   const long long n = (long long)gc.X * gc.Y * gc.Z * ncg;
   const long long nv = (long long)gc.X * gc.Y * gc.Z;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -509,7 +530,8 @@ __global__ void k_pool(Geo gf, Geo gc, int ncg, const bf16* in, bf16* out) {
 }
 
 // nearest-neighbour x2: out (fine) from in (coarse)
-__global__ void k_up(Geo gc, Geo gf, int ncg, const bf16* in, bf16* out) {
+__global__ void k_up(Geo gc, Geo gf, int ncg, const bf16* in, bf16* out, const int* skip) {
+  if (skip && *skip) return;
   const long long nv = (long long)gf.X * gf.Y * gf.Z;
   const long long n = nv * ncg;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -588,7 +610,8 @@ __device__ __forceinline__ void block_sums(float (&v)[K], float* out /* K values
 }
 
 // sum of squares of r over the interior, in FP64: partial[b]
-__global__ void __launch_bounds__(kURedThreads) k_sumsq_cc(Geo g, const double* r, double* partial) {
+__global__ void __launch_bounds__(kURedThreads) k_sumsq_cc(Geo g, const double* r, double* partial, const int* skip) {
+  if (skip && *skip) return;
   const long long n = (long long)g.X * g.Y * g.Z;
   double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -609,8 +632,9 @@ __global__ void __launch_bounds__(kURedThreads) k_sumsq_cc(Geo g, const double* 
 }
 
 // scal[0] = rms(r), scal[1] = 1/rms, scal[2] = out_scale * rms  (0 when r == 0)
-__global__ void k_scale_fin(const double* partial, int nb, long long n, double out_scale, double* scal) {
-  if (threadIdx.x != 0) return;
+__global__ void k_scale_fin(const double* partial, int nb, long long n, double out_scale, double* scal,
+                            const int* skip) {
+  if (threadIdx.x != 0 || (skip && *skip)) return;
   double s = 0.0;
   for (int b = 0; b < nb; b++) s += partial[b];
   const double rms = sqrt(s / (double)n);
@@ -663,14 +687,110 @@ __global__ void __launch_bounds__(kURedThreads) k_target(Geo g, const double* e,
   block_sums<1>(acc, partial + blockIdx.x);
 }
 
-// loss L = sum (y - t)^2 / sum t^2 and the head backward:
-//   dy = 2 (y - t) / T2;  dh[c] = head_w[c] * dy * [h_c > 0]  (dPre of the last conv)
-//   partial sums per block: [0] (y-t)^2, [1] dy, [2..17] dy * h_c
-__global__ void __launch_bounds__(kURedThreads) k_loss_head(Geo g, const float* y, const float* t, const float* T2p,
-                                                           const bf16* h, const float* head_w, bf16* dh,
-                                                           float* partial) {
+// partial sums per block of y.t and y.y (cosine loss)
+__global__ void __launch_bounds__(kURedThreads) k_yt(Geo g, const float* y, const float* t, float* partial) {
   const long long n = (long long)g.X * g.Y * g.Z;
-  const float T2 = T2p[0] > 0.f ? T2p[0] : 1.f;
+  float acc[2] = {0.f, 0.f};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    int x, y_, z;
+    interior_of(g, i, x, y_, z);
+    const long long c = x + (long long)g.Xp * (y_ + (long long)g.Yp * z);
+    acc[0] += y[c] * t[c];
+    acc[1] += y[c] * y[c];
+  }
+  block_sums<2>(acc, partial + (long long)blockIdx.x * 2);
+}
+
+// FP64 partial sums per block for the energy-norm loss, with A the solver's
+// (negative definite, volume-weighted) operator, s = out_scale rms(r) the
+// scale of the target t = e / s (so A t = r / s):
+//   [0] a = -y.(A t) = -y.r / s,  [1] E = -t.(A t) = -e.r / s^2
+// (these sums cancel heavily where the coefficients are large: FP64)
+__global__ void __launch_bounds__(kURedThreads) k_energy_sums(Geo g, const float* y, const double* e,
+                                                             const double* r, const double* scal, double* partial) {
+  const long long n = (long long)g.X * g.Y * g.Z;
+  const double tinv = scal[2] > 0.0 ? 1.0 / scal[2] : 0.0;
+  double a0 = 0.0, a1 = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    int x, y_, z;
+    interior_of(g, i, x, y_, z);
+    const long long c = x + (long long)g.Xp * (y_ + (long long)g.Yp * z);
+    const double at = r[c] * tinv;
+    a0 -= (double)y[c] * at;
+    a1 -= e[c] * tinv * at;
+  }
+  __shared__ double sh[2][kURedThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = a0;
+    sh[1][threadIdx.x >> 5] = a1;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double s = 0.0;
+    for (int w = 0; w < kURedThreads / 32; w++) s += sh[threadIdx.x][w];
+    partial[(long long)blockIdx.x * 2 + threadIdx.x] = s;
+  }
+}
+
+// out = (a, B, E) as FP32 from the FP64 partials: pa[b][2] = (a, E) and
+// pb[b] = y.(A y) (B = -y.(A y))
+__global__ void k_energy_fin(const double* pa, const double* pb, int nb, float* out) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0, E = 0.0, yay = 0.0;
+  for (int b = 0; b < nb; b++) {
+    a += pa[2 * b];
+    E += pa[2 * b + 1];
+    yay += pb[b];
+  }
+  out[0] = (float)a;
+  out[1] = (float)(-yay);
+  out[2] = (float)E;
+}
+
+// the loss and the head backward.
+//  kind 0 (relative L2):  L = sum (y - t)^2 / T2,  dL/dy = 2 (y - t) / T2
+//  kind 1 (cosine, invariant to a positive scale of y: flexible CG is
+//    invariant to a rescaling of z at every iteration, so only the direction
+//    counts; the sign is kept):
+//    L = 1 - y.t / (|y| |t|),  dL/dy = -t / (|y| |t|) + (y.t) y / (|y|^3 |t|)
+//  kind 2 (cosine in the energy norm of -A, the norm CG minimises; A e = r,
+//    t = e / s, A t = r / s):
+//    L = 1 - a / sqrt(B E) with a = -y.(A t), B = -y.(A y), E = -t.(A t),
+//    dL/dy = (A t) / sqrt(B E) - a (A y) / (B^1.5 sqrt(E))
+// then dh[c] = head_w[c] * dL/dy * [h_c > 0] (dPre of the last conv);
+// partial sums per block: [0] (y-t)^2, [1] dL/dy, [2..17] dL/dy * h_c
+struct LossArgs {
+  Geo g;
+  const float* y; const float* t; const float* T2p;
+  int kind;
+  const float* sums;     // kind 1: y.t, y.y; kind 2: a, B, E
+  const float* ay;       // kind 2: A y
+  const double* r; const double* scal;   // kind 2: r and s (scal[2])
+  const bf16* h; const float* head_w; bf16* dh;
+  float* partial;
+};
+
+__global__ void __launch_bounds__(kURedThreads) k_loss_head(LossArgs a) {
+  const Geo& g = a.g;
+  const long long n = (long long)g.X * g.Y * g.Z;
+  const float T2 = a.T2p[0] > 0.f ? a.T2p[0] : 1.f;
+  float ca = 0.f, cb = 0.f;  // dL/dy = ca * (t or rh) + cb * (y or Ay)
+  if (a.kind == 1) {
+    const float yt = a.sums[0], yy = a.sums[1] > 0.f ? a.sums[1] : 1.f;
+    const float ny = sqrtf(yy), nt = sqrtf(T2);
+    ca = -1.f / (ny * nt);
+    cb = yt / (yy * ny * nt);
+  } else if (a.kind == 2) {
+    const float aa = a.sums[0], B = a.sums[1] > 0.f ? a.sums[1] : 1.f, E = a.sums[2] > 0.f ? a.sums[2] : 1.f;
+    const float sBE = sqrtf(B * E);
+    ca = 1.f / sBE;
+    cb = -aa / (B * sqrtf(B) * sqrtf(E));
+  }
+  const double tinv = (a.kind == 2 && a.scal[2] > 0.0) ? 1.0 / a.scal[2] : 0.0;
   float acc[18];
 #pragma unroll
   for (int k = 0; k < 18; k++) acc[k] = 0.f;
@@ -678,24 +798,27 @@ __global__ void __launch_bounds__(kURedThreads) k_loss_head(Geo g, const float* 
     int x, y_, z;
     interior_of(g, i, x, y_, z);
     const long long c = x + (long long)g.Xp * (y_ + (long long)g.Yp * z);
-    const float d = y[c] - t[c];
-    const float dy = 2.f * d / T2;
+    const float d = a.y[c] - a.t[c];
+    float dy;
+    if (a.kind == 1) dy = ca * a.t[c] + cb * a.y[c];
+    else if (a.kind == 2) dy = ca * (float)(a.r[c] * tinv) + cb * a.ay[c];
+    else dy = 2.f * d / T2;
     acc[0] += d * d;
     acc[1] += dy;
     const long long vo = g.vox(x, y_, z) * 8;
 #pragma unroll
     for (int cg = 0; cg < 2; cg++) {
       float hv[8], o[8];
-      unpack8(*reinterpret_cast<const uint4*>(h + cg * g.GS * 8 + vo), hv);
+      unpack8(*reinterpret_cast<const uint4*>(a.h + cg * g.GS * 8 + vo), hv);
 #pragma unroll
       for (int e = 0; e < 8; e++) {
         acc[2 + 8 * cg + e] += dy * hv[e];
-        o[e] = hv[e] > 0.f ? head_w[8 * cg + e] * dy : 0.f;
+        o[e] = hv[e] > 0.f ? a.head_w[8 * cg + e] * dy : 0.f;
       }
-      *reinterpret_cast<uint4*>(dh + cg * g.GS * 8 + vo) = pack8(o);
+      *reinterpret_cast<uint4*>(a.dh + cg * g.GS * 8 + vo) = pack8(o);
     }
   }
-  block_sums<18>(acc, partial + (long long)blockIdx.x * 18);
+  block_sums<18>(acc, a.partial + (long long)blockIdx.x * 18);
 }
 
 // Adam (decoupled from the layout: one flat FP32 parameter array)

@@ -76,7 +76,8 @@ def lib():
             "or_unet_nparams": (C.c_longlong, []),
             "or_unet_set_exact": (None, [C.c_int]),
             "or_unet_forward": (C.c_int, [C.c_int, C.c_int, C.c_int, _F, C.c_double, _D, _F, _D]),
-            "or_unet_loss_grad": (C.c_int, [C.c_int, C.c_int, C.c_int, _F, C.c_double, _D, _F, _D, _D, _F]),
+            "or_unet_loss_grad": (C.c_int, [C.c_int, C.c_int, C.c_int, _F, C.c_double, _D, _F, _D, C.c_int, _D, _D,
+                                            _D, C.c_double, _D, _F]),
         }
         for n, (rt, at) in sig.items():
             f = getattr(L, n)
@@ -329,12 +330,18 @@ def unet_forward(X, Y, Z, params, out_scale, r, feat=None):
     return z.reshape((X + 2, Y + 2, Z + 2), order="F")
 
 
-def unet_loss_grad(X, Y, Z, params, out_scale, r, e, feat=None):
+def unet_loss_grad(X, Y, Z, params, out_scale, r, e, feat=None, kind=1, k=None, h=1.0):
+    """Loss (kind 0 relative L2, 1 cosine, 2 energy-norm cosine with the
+    uniform-mesh all-Neumann operator of face coefficients k and spacing h)
+    and its gradient."""
     p = _f32(params)
     rr, ee = _cc(r), _cc(e)
     ff = None if feat is None else np.ascontiguousarray(np.asarray(feat, dtype=np.float32).ravel(order="F"))
     loss = np.zeros(1, dtype=np.float64)
     g = np.zeros(p.size, dtype=np.float32)
+    kf = [None] * 3 if k is None else [_cc(a) for a in k]
+    kk = [None if a is None else a.ctypes.data_as(_D) for a in kf]
     _check(lib().or_unet_loss_grad(X, Y, Z, _fptr(p), float(out_scale), rr.ctypes.data_as(_D), _fptr(ff),
-                                   ee.ctypes.data_as(_D), loss.ctypes.data_as(_D), _fptr(g)))
+                                   ee.ctypes.data_as(_D), int(kind), *kk, float(h), loss.ctypes.data_as(_D),
+                                   _fptr(g)))
     return float(loss[0]), g

@@ -316,7 +316,8 @@ int or_unet_forward(int X, int Y, int Z, const float* params, double out_scale, 
 // loss = sum (y - t)^2 / sum t^2 with t = e / (out_scale * rms(r)), and its
 // gradient with respect to every parameter (same flat order as the GPU)
 int or_unet_loss_grad(int X, int Y, int Z, const float* params, double out_scale, const double* r, const float* feat,
-                      const double* e, double* loss, float* grads) {
+                      const double* e, int kind, const double* kx, const double* ky, const double* kz, double hgrid,
+                      double* loss, float* grads) {
   Net N(params);
   const double rms = rms_interior(r, X, Y, Z);
   Acts a;
@@ -334,13 +335,57 @@ int or_unet_loss_grad(int X, int Y, int Z, const float* params, double out_scale
   const float T2f = T2 > 0 ? (float)T2 : 1.f;
   std::fill(grads, grads + N.n, 0.f);
   double L = 0.0, gb = 0.0;
+  // kind 1 (cosine): L = 1 - y.t / (|y| |t|), dL/dy = ca t + cb y
+  double yt = 0.0, yy = 0.0;
+  for (size_t i = 0; i < t.v.size(); i++) {
+    yt += (double)a.y.v[i] * t.v[i];
+    yy += (double)a.y.v[i] * a.y.v[i];
+  }
+  if (!(yy > 0)) yy = 1.0;
+  const double ny = std::sqrt(yy), nt = std::sqrt((double)T2f);
+  double ca = -1.0 / (ny * nt), cb = yt / (yy * ny * nt);
+  // kind 2: energy norm of the volume-weighted sigma-Laplacian on a uniform
+  // mesh (spacing hgrid) with homogeneous Neumann walls:
+  // (A y)_c = h * sum over the six faces of k_f (y_nb - y_c), no wall flux
+  T4 ay(1, X, Y, Z);
+  std::vector<double> rh((size_t)X * Y * Z);
+  double ea = 0.0, eB = 0.0, eE = 0.0;
+  if (kind == 2) {
+    const size_t sx = X + 2, sy = Y + 2;
+    for (int zz = 0; zz < Z; zz++)
+      for (int y = 0; y < Y; y++)
+        for (int x = 0; x < X; x++) {
+          const int xi = x + 1, yi = y + 1, zi = zz + 1;  // padded cell indices
+          const double yc = a.y.at(0, x, y, zz);
+          double v = 0.0;
+          if (x > 0) v += kx[xi + (sx + 1) * (yi + sy * zi)] * (a.y.at(0, x - 1, y, zz) - yc);
+          if (x < X - 1) v += kx[xi + 1 + (sx + 1) * (yi + sy * zi)] * (a.y.at(0, x + 1, y, zz) - yc);
+          if (y > 0) v += ky[xi + sx * (yi + (sy + 1) * zi)] * (a.y.at(0, x, y - 1, zz) - yc);
+          if (y < Y - 1) v += ky[xi + sx * (yi + 1 + (sy + 1) * zi)] * (a.y.at(0, x, y + 1, zz) - yc);
+          if (zz > 0) v += kz[xi + sx * (yi + sy * zi)] * (a.y.at(0, x, y, zz - 1) - yc);
+          if (zz < Z - 1) v += kz[xi + sx * (yi + sy * (zi + 1))] * (a.y.at(0, x, y, zz + 1) - yc);
+          ay.at(0, x, y, zz) = (float)(hgrid * v);
+          const double rv = r[xi + sx * (yi + sy * zi)] * inv;  // A t = r / s
+          rh[((size_t)zz * Y + y) * X + x] = rv;
+          ea -= yc * rv;
+          eB -= yc * ay.at(0, x, y, zz);
+          eE -= t.at(0, x, y, zz) * rv;
+        }
+    if (!(eB > 0)) eB = 1.0;
+    if (!(eE > 0)) eE = 1.0;
+    ca = 1.0 / std::sqrt(eB * eE);
+    cb = -ea / (eB * std::sqrt(eB) * std::sqrt(eE));
+  }
   std::vector<double> gw(16, 0.0);
   T4 dd0(16, X, Y, Z);
   for (int zz = 0; zz < Z; zz++)
     for (int y = 0; y < Y; y++)
       for (int x = 0; x < X; x++) {
         const float d = a.y.at(0, x, y, zz) - t.at(0, x, y, zz);
-        const float dy = 2.f * d / T2f;
+        float dy;
+        if (kind == 1) dy = (float)(ca * t.at(0, x, y, zz) + cb * a.y.at(0, x, y, zz));
+        else if (kind == 2) dy = (float)(ca * rh[((size_t)zz * Y + y) * X + x] + cb * ay.at(0, x, y, zz));
+        else dy = 2.f * d / T2f;
         L += (double)d * d;
         gb += dy;
         for (int c = 0; c < 16; c++) {
@@ -349,7 +394,7 @@ int or_unet_loss_grad(int X, int Y, int Z, const float* params, double out_scale
           dd0.at(c, x, y, zz) = h > 0.f ? bf16r(params[N.head + c] * dy) : 0.f;
         }
       }
-  *loss = L / T2f;
+  *loss = kind == 1 ? 1.0 - yt / (ny * nt) : (kind == 2 ? 1.0 - ea / std::sqrt(eB * eE) : L / T2f);
   for (int c = 0; c < 16; c++) grads[N.head + c] = (float)gw[c];
   grads[N.head + 16] = (float)gb;
 

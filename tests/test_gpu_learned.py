@@ -1,0 +1,88 @@
+"""Flexible CG with the learned preconditioner (MOONS_PREC_UNET) on the
+sigma-shell Poisson case, small grid: the network is trained on the GPU on
+pairs the solver generates, then solves held-out draws to 1e-10; the test
+states what the trained network gains over the method without it (the
+reference's Jacobi-PCG), and that a useless network hands over to the
+multigrid fallback."""
+import numpy as np
+import pytest
+
+from moons_b200 import capi as G
+from moons_b200 import learned as L
+
+pytestmark = pytest.mark.gpu
+
+N, SHELL = 32, 2
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """Train on 20 draws: Jacobi-PCG iterates first, then one round of the
+    learned solve's own iterates (the energy-norm cosine loss)."""
+    mesh = L.shell_mesh(N)
+    cases = [L.ShellCase.build(mesh, N, SHELL, s) for s in range(20)]
+    pairs = L.make_pairs(cases, iterates=(0, 2, 8, 32))
+    net = G.UNet(mesh, seed=0)
+    net.out_scale = L.output_scale(pairs)
+    hist = L.train(net, cases, pairs, epochs=20, lr=1e-3, lr_min=1e-4)
+    pairs += L.make_pairs_learned(cases, net, iterates=(1, 2, 4, 8, 16))
+    hist += L.train(net, cases, pairs, epochs=8, lr=5e-4, lr_min=5e-5, seed=1)
+    return mesh, net, hist
+
+
+def _solve(case, prec, net=None, tol=1e-10):
+    s = case.solver(prec)
+    if net is not None:
+        net.set_coeff(case.k)
+        s.set_unet(net)
+    case.phi.fill(0.0)
+    info = s.solve([case.phi], [case.rhs], G.isp(20000, tol, 1e-300))
+    x = case.phi.download()[1:-1, 1:-1, 1:-1]
+    s.close()
+    return info, x - x.mean()
+
+
+def test_training_lowers_the_loss(trained):
+    _, _, hist = trained
+    assert np.all(np.isfinite(hist))
+    assert hist[19] < 0.5 * hist[0], hist
+
+
+@pytest.mark.parametrize("seed", [100, 103])
+def test_learned_fcg_solves_held_out_draws(trained, seed):
+    mesh, net, _ = trained
+    case = L.ShellCase.build(mesh, N, SHELL, seed)
+    ij, xj = _solve(case, G.PREC_LAP)                  # the reference's Jacobi-PCG
+    im, xm = _solve(case, G.PREC_MG_MIXED)             # multigrid flexible CG
+    il, xl = _solve(case, G.PREC_UNET, net)            # learned (multigrid fallback)
+    assert ij["exit_reason"] == 1 and im["exit_reason"] == 1
+    assert il["exit_reason"] in (1, 11)
+    assert il["rel"] < 1e-10
+    scale = np.abs(xm).max()
+    assert np.abs(xl - xm).max() < 1e-7 * scale
+    assert np.abs(xj - xm).max() < 1e-7 * scale
+    # what the trained network gains over the method without it (the
+    # reference's Jacobi preconditioner in the same CG)
+    assert il["iterations"] < 0.5 * ij["iterations"], (il, ij)
+
+
+def test_useless_network_falls_back_to_multigrid(trained):
+    mesh, net, _ = trained
+    case = L.ShellCase.build(mesh, N, SHELL, 102)
+    zero = G.UNet(mesh, seed=1)
+    zero.set_params(np.zeros(zero.nparams, dtype=np.float32))   # z = 0: no descent direction
+    info, x = _solve(case, G.PREC_UNET, zero)
+    _, xm = _solve(case, G.PREC_MG_MIXED)
+    assert info["exit_reason"] == 11
+    assert info["rel"] < 1e-10
+    assert np.abs(x - xm).max() < 1e-7 * np.abs(xm).max()
+
+
+def test_unet_solver_needs_a_network():
+    mesh = L.shell_mesh(16)
+    case = L.ShellCase.build(mesh, 16, SHELL, 0)
+    s = case.solver(G.PREC_UNET)
+    case.phi.fill(0.0)
+    with pytest.raises(G.MoonsError):
+        s.solve([case.phi], [case.rhs], G.isp(100, 1e-10, 1e-300))
+    s.close()

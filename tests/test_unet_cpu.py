@@ -75,13 +75,39 @@ def _params(seed):
     return p
 
 
-def test_backward_matches_finite_differences():
+def _faces(X, Y, Z, seed):
+    rng = np.random.default_rng(seed)
+    return [rng.uniform(0.5, 2.0, (X + 2 + (d == 0), Y + 2 + (d == 1), Z + 2 + (d == 2))) for d in range(3)]
+
+
+def _apply_neumann(e, k, h):
+    """(A e) of the volume-weighted sigma-Laplacian, uniform spacing h,
+    homogeneous Neumann walls, on cell-centred arrays with ghosts."""
+    out = np.zeros_like(e)
+    c = e[1:-1, 1:-1, 1:-1]
+    v = np.zeros_like(c)
+    kx, ky, kz = k
+    v[1:, :, :] += kx[2:-2, 1:-1, 1:-1] * (c[:-1] - c[1:])
+    v[:-1, :, :] += kx[2:-2, 1:-1, 1:-1] * (c[1:] - c[:-1])
+    v[:, 1:, :] += ky[1:-1, 2:-2, 1:-1] * (c[:, :-1] - c[:, 1:])
+    v[:, :-1, :] += ky[1:-1, 2:-2, 1:-1] * (c[:, 1:] - c[:, :-1])
+    v[:, :, 1:] += kz[1:-1, 1:-1, 2:-2] * (c[:, :, :-1] - c[:, :, 1:])
+    v[:, :, :-1] += kz[1:-1, 1:-1, 2:-2] * (c[:, :, 1:] - c[:, :, :-1])
+    out[1:-1, 1:-1, 1:-1] = h * v
+    return out
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2], ids=["rel_l2", "cosine", "energy"])
+def test_backward_matches_finite_differences(kind):
     X, Y, Z = 8, 8, 8
     r, e, feat = _pair(X, Y, Z, 1)
     p = _params(2)
+    k = _faces(X, Y, Z, 9) if kind == 2 else None
+    if kind == 2:
+        r = _apply_neumann(e, k, 0.125)  # a consistent pair: A e = r
     O.unet_set_exact(True)
     try:
-        loss, g = O.unet_loss_grad(X, Y, Z, p, 0.7, r, e, feat)
+        loss, g = O.unet_loss_grad(X, Y, Z, p, 0.7, r, e, feat, kind, k, 0.125)
         assert np.isfinite(loss) and loss > 0
         rng = np.random.default_rng(5)
         # probe a few parameters of every layer (weights and biases) and the head
@@ -104,11 +130,13 @@ def test_backward_matches_finite_differences():
                 pp, pm = p.copy(), p.copy()
                 pp[i] += h
                 pm[i] -= h
-                lp, _ = O.unet_loss_grad(X, Y, Z, pp, 0.7, r, e, feat)
-                lm, _ = O.unet_loss_grad(X, Y, Z, pm, 0.7, r, e, feat)
+                lp, _ = O.unet_loss_grad(X, Y, Z, pp, 0.7, r, e, feat, kind, k, 0.125)
+                lm, _ = O.unet_loss_grad(X, Y, Z, pm, 0.7, r, e, feat, kind, k, 0.125)
                 fd = (lp - lm) / (float(pp[i]) - float(pm[i]))  # the step as stored in FP32
                 best = min(best, abs(fd - g[i]) / max(abs(g[i]), abs(fd), 1e-2 * np.abs(g).max()))
             worst = max(worst, best)
-        assert worst < 2e-2, worst
+        # the cosine loss sits near 1 at initialisation and moves by ~1e-7 per
+        # step, close to the FP32 noise of the forward values
+        assert worst < (2e-2 if kind == 0 else 5e-2), worst
     finally:
         O.unet_set_exact(False)
