@@ -42,9 +42,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="moons", choices=["moons", "reference"])
     ap.add_argument("--small", action="store_true", help="small mesh (debug only)")
-    ap.add_argument("--profile", choices=["step", "jacobi", "mg", "mixed"], default=None,
-                    help="profiling run for ncu launch lists: one duct step, or one duct pressure solve with the "
-                         "given preconditioner capped at --profile-iters iterations; prints what ran, no bench line")
+    ap.add_argument("--profile", choices=["step", "jacobi", "mg", "mixed", "unet", "unet_train"], default=None,
+                    help="profiling run for ncu launch lists: one duct step, one duct pressure solve with the "
+                         "given preconditioner capped at --profile-iters iterations, or --profile-iters U-Net "
+                         "forward applies / training steps on the 128^3 sigma-shell grid; prints what ran, no "
+                         "bench line")
     ap.add_argument("--profile-iters", type=int, default=40)
     return ap.parse_args()
 
@@ -56,6 +58,29 @@ def run_profile(args):
         sim = configs.make(G, configs.duct, seed=0, **kw)
         info = sim.step(1)
         print(json.dumps({"profile": "step", "workload": WORKLOAD, "info": info}), flush=True)
+        return
+    if args.profile in ("unet", "unet_train"):
+        # U-Net forward applies (or training steps) on the sigma-shell grid
+        from moons_b200 import learned as L
+        n = 32 if args.small else 128
+        mesh = L.shell_mesh(n)
+        case = L.ShellCase.build(mesh, n, 2 if args.small else 4, 0)
+        net = G.UNet(mesh, seed=0)
+        net.set_coeff(case.k)
+        r = mesh.field(G.CC)
+        case.phi.fill(0.0)
+        case.op.residual([case.phi], [case.rhs], [r])
+        z = mesh.field(G.CC)
+        if args.profile == "unet_train":
+            net.set_operator(case.op)
+            net.set_loss(2)
+        for _ in range(args.profile_iters):
+            if args.profile == "unet":
+                net.apply(z, r)
+            else:
+                net.train_step(r, r, 1e-4)
+        print(json.dumps({"profile": args.profile, "workload": f"U-Net {n}^3", "iters": args.profile_iters}),
+              flush=True)
         return
     prec = {"jacobi": G.PREC_LAP, "mg": G.PREC_MG, "mixed": G.PREC_MG_MIXED}[args.profile]
     mom, _, prm, _ = configs.duct(**kw)

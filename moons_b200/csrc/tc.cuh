@@ -43,6 +43,33 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint: the thread may sleep up to `ns`
+// nanoseconds in the barrier instead of spinning (waiting threads then take
+// no issue slots from the ones that work)
+__device__ __forceinline__ bool mbar_try_sleep(uint32_t bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+// the same bounded wait as mbar_wait, sleeping in the barrier between polls
+__device__ __forceinline__ bool mbar_wait_sleep(uint32_t bar, uint32_t parity, int* err, int code) {
+  if (mbar_try_sleep(bar, parity, 20000u)) return true;
+  const unsigned long long t0 = globaltimer();
+  while (true) {
+    if (mbar_try_sleep(bar, parity, 20000u)) return true;
+    if (globaltimer() - t0 > kWaitLimitNs) {
+      if (err) atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+}
+
 // Wait for the phase with the given parity to complete; false (and *err set
 // to `code`) when the wall-clock limit runs out first.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {

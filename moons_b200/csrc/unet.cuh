@@ -125,6 +125,61 @@ __host__ __device__ inline int conv_stage_bytes(int L, int N) {
   return (b + 127) & ~127;
 }
 
+// epilogue of one 128-position tile: thread m (warp m/32 reads TMEM lanes
+// 32*(m/32) ..) takes row m of the accumulator at TMEM column `tcol`:
+// bias + ReLU (kRelu) or mask (kLinear), BF16 stores to the interior voxels,
+// and the fused 1x1 head when requested.  Warp-collective (tcgen05.ld).
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& a, uint32_t tcol, int m, int z, int p0, bool done) {
+  const Geo& g = a.g;
+  const int N = a.N;
+  const int warp = m >> 5;
+  const int p = p0 + m;
+  const int yy = p / g.Xp, xx = p - yy * g.Xp;
+  const bool valid = done && xx >= 1 && xx <= g.X && yy >= 1 && yy <= g.Y;
+  const long long vo = kGuard + (long long)z * g.PS + p;   // voxel offset in a group
+  const long long gsE = g.GS * 8;
+  float hy = 0.f;
+  for (int c0 = 0; c0 < N; c0 += 16) {
+    float v[16];
+    tc::tmem_ld16(tcol + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+    if (!done) continue;
+    if (a.mode == kRelu) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + a.bias[c0 + i], 0.f);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int cg = c0 / 8 + h;
+      const bool inA = cg < a.ocgA;
+      const long long off = (inA ? cg : cg - a.ocgA) * gsE + vo * 8;
+      if (a.mode == kLinear) {
+        const bf16* mk = inA ? a.maskA : a.maskB;
+        if (mk && valid) {
+          float mv[8];
+          unpack8(*reinterpret_cast<const uint4*>(mk + off), mv);
+#pragma unroll
+          for (int i = 0; i < 8; i++) v[8 * h + i] = mv[i] > 0.f ? v[8 * h + i] : 0.f;
+        }
+      }
+      if (valid) {
+        bf16* dst = (inA ? a.outA : a.outB) + off;
+        *reinterpret_cast<uint4*>(dst) = pack8(v + 8 * h);
+      }
+    }
+    if (a.head_w) {
+      // the head sees the stored (BF16-rounded) activations
+#pragma unroll
+      for (int i = 0; i < 16; i++) hy += a.head_w[c0 + i] * __bfloat162float(__float2bfloat16_rn(v[i]));
+    }
+  }
+  if (a.head_w && valid) {
+    const float yv = hy + a.head_b[0];
+    const long long ci = (long long)xx + (long long)g.Xp * (yy + (long long)g.Yp * z);
+    if (a.y32) a.y32[ci] = yv;
+    if (a.z64) a.z64[ci] = a.zscale[0] * (double)yv;
+  }
+}
+
 __global__ void __launch_bounds__(kConvThreads) k_conv3(ConvArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar_full[8];
@@ -222,56 +277,10 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(ConvArgs a) {
   __syncwarp();
   // every thread waits for the accumulator (thread 0 committed it even when
   // it gave up early, so the phase completes once the issued MMAs retire)
-  const bool done = __syncthreads_and(tc::mbar_wait(tc::smem_u32(&bar_done), 0, a.err, kErrDone)) != 0;
+  const bool done = __syncthreads_and(tc::mbar_wait_sleep(tc::smem_u32(&bar_done), 0, a.err, kErrDone)) != 0;
   tc::tc_fence_after();
 
-  // ---- epilogue: row m = tid, TMEM lane m --------------------------------
-  const int m = tid;
-  const int p = p0 + m;
-  const int yy = p / g.Xp, xx = p - yy * g.Xp;
-  const bool valid = done && xx >= 1 && xx <= g.X && yy >= 1 && yy <= g.Y;
-  const long long vo = kGuard + (long long)z * g.PS + p;   // voxel offset in a group
-  const long long gsE = g.GS * 8;
-  float hy = 0.f;
-  for (int c0 = 0; c0 < N; c0 += 16) {
-    float v[16];
-    tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
-    if (!done) continue;
-    if (a.mode == kRelu) {
-#pragma unroll
-      for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + a.bias[c0 + i], 0.f);
-    }
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int cg = c0 / 8 + h;
-      const bool inA = cg < a.ocgA;
-      const long long off = (inA ? cg : cg - a.ocgA) * gsE + vo * 8;
-      if (a.mode == kLinear) {
-        const bf16* mk = inA ? a.maskA : a.maskB;
-        if (mk && valid) {
-          float mv[8];
-          unpack8(*reinterpret_cast<const uint4*>(mk + off), mv);
-#pragma unroll
-          for (int i = 0; i < 8; i++) v[8 * h + i] = mv[i] > 0.f ? v[8 * h + i] : 0.f;
-        }
-      }
-      if (valid) {
-        bf16* dst = (inA ? a.outA : a.outB) + off;
-        *reinterpret_cast<uint4*>(dst) = pack8(v + 8 * h);
-      }
-    }
-    if (a.head_w) {
-      // the head sees the stored (BF16-rounded) activations
-#pragma unroll
-      for (int i = 0; i < 16; i++) hy += a.head_w[c0 + i] * __bfloat162float(__float2bfloat16_rn(v[i]));
-    }
-  }
-  if (a.head_w && valid) {
-    const float yv = hy + a.head_b[0];
-    const long long ci = (long long)xx + (long long)g.Xp * (yy + (long long)g.Yp * z);
-    if (a.y32) a.y32[ci] = yv;
-    if (a.z64) a.z64[ci] = a.zscale[0] * (double)yv;
-  }
+  conv_epilogue(a, tmem, tid, z, p0, done);
   tc::tc_fence_before();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, ncols);
@@ -408,7 +417,7 @@ __global__ void __launch_bounds__(kConvThreads) k_wgrad(WgradArgs a) {
   }
   __syncwarp();
   bool done = true;
-  if (nit > 0) done = tc::mbar_wait(tc::smem_u32(&bar_done), 0, a.err, kErrDone);
+  if (nit > 0) done = tc::mbar_wait_sleep(tc::smem_u32(&bar_done), 0, a.err, kErrDone);
   done = __syncthreads_and(done) != 0 && nit > 0;
   tc::tc_fence_after();
 
