@@ -20,6 +20,7 @@ module moons_gpu_mod
   integer(c_int), parameter :: MOONS_OP_IND_DIFFUSION = 3, MOONS_OP_MOM_DIFFUSION = 4
   integer(c_int), parameter :: MOONS_PREC_IDENTITY = 0, MOONS_PREC_LAP = 1
   integer(c_int), parameter :: MOONS_PREC_MOM = 2, MOONS_PREC_IND = 3
+  integer(c_int), parameter :: MOONS_PREC_MG = 4, MOONS_PREC_MG_MIXED = 5, MOONS_PREC_UNET = 6
 
   type, bind(C) :: moons_bc_spec
     integer(c_int) :: type(6)
@@ -156,6 +157,48 @@ module moons_gpu_mod
     function moons_pcg_destroy(s) bind(C, name="moons_pcg_destroy") result(st)
       import :: c_ptr, c_int
       type(c_ptr), value :: s
+      integer(c_int) :: st
+    end function
+
+    ! learned preconditioner: a trained U-Net attached to a MOONS_PREC_UNET solver
+    function moons_unet_create(m, seed, u) bind(C, name="moons_unet_create") result(st)
+      import :: c_ptr, c_int, c_long_long
+      type(c_ptr), value :: m
+      integer(c_long_long), value :: seed
+      type(c_ptr), intent(out) :: u
+      integer(c_int) :: st
+    end function
+
+    function moons_unet_set_params(u, p, n) bind(C, name="moons_unet_set_params") result(st)
+      import :: c_ptr, c_int, c_float, c_long_long
+      type(c_ptr), value :: u
+      real(c_float), intent(in) :: p(*)
+      integer(c_long_long), value :: n
+      integer(c_int) :: st
+    end function
+
+    function moons_unet_set_out_scale(u, c) bind(C, name="moons_unet_set_out_scale") result(st)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: u
+      real(c_double), value :: c
+      integer(c_int) :: st
+    end function
+
+    function moons_unet_set_coeff(u, kx, ky, kz) bind(C, name="moons_unet_set_coeff") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: u, kx, ky, kz
+      integer(c_int) :: st
+    end function
+
+    function moons_pcg_set_unet(s, u) bind(C, name="moons_pcg_set_unet") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s, u
+      integer(c_int) :: st
+    end function
+
+    function moons_unet_destroy(u) bind(C, name="moons_unet_destroy") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: u
       integer(c_int) :: st
     end function
   end interface
