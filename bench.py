@@ -350,6 +350,39 @@ def learned_poisson(G, n=128, shell=4, ntrain=8, held=(1000, 1001, 1002), epochs
     }
 
 
+def at_scale_steps(G, small=False, steps=3):
+    """Configuration 5: the finite-Rem (constrained transport) MHD step on
+    256 x 128 x 128 cells, plain FP64 Jacobi-PCG Poisson solves vs FP32
+    V-cycle flexible CG; div(B) after every step, and the two runs' fields
+    against each other after the last step (same seed, same tolerances)."""
+    from moons_b200 import configs
+    kw = dict(nx=16, ny=16, nz=32) if small else {}
+    out, fields = {}, {}
+    for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED)):
+        sim = configs.make(G, configs.at_scale, seed=0, prec_poisson=prec, **kw)
+        sim.step(1)  # warm-up (graphs)
+        divb, ms, its = [], 0.0, {}
+        for _ in range(steps):
+            info = sim.step(1)
+            ms += info["ms"]
+            for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+                its[k] = its.get(k, 0) + info[k] / steps
+            divb.append(sim.divergence()[1])
+        fields[name] = [sim.download(G.MHD_U, c) for c in range(3)] + [sim.download(G.MHD_B, c) for c in range(3)]
+        out[name] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps, "iters_per_step": its,
+                     "div_B_l2sq_max": max(divb)}
+        del sim
+    rel = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+              for a, b in zip(fields["mixed_fp32_vcycle"], fields["plain_fp64"]))
+    out["mixed_vs_plain_fields_max_rel_l2"] = rel
+    out["speedup_mixed_vs_plain"] = out["plain_fp64"]["ms_per_step"] / out["mixed_fp32_vcycle"]["ms_per_step"]
+    n = kw.get("nx", 128), kw.get("ny", 128), kw.get("nz", 256)
+    out["workload"] = (f"finite-Rem MHD with constrained transport, {n[0]}x{n[1]}x{n[2]} cells (Roberts-stretched "
+                       f"cross-section), Re=1000, Ha=500, Rem=10, dt=2e-4; {steps} steps after 1 warm-up step "
+                       f"(the case's 200 steps shortened to keep the bench within minutes)")
+    return out
+
+
 def cpu_sample(kw, gpu_iters=None):
     """Bounded CPU sample: the oracle (single thread) on the full-size duct.
     It times init + one step with every PCG capped at a few iterations, and
@@ -488,6 +521,7 @@ def main():
     shell = sigma_shell_poisson(G, n=32 if args.small else 128, seeds_plain=1 if args.small else 4,
                                 seeds_mg=2 if args.small else 16)
     mxinfo, _ = poisson_ms(G, kw, G.PREC_MG_MIXED)
+    scale5 = at_scale_steps(G, small=args.small)
     learned = learned_poisson(G, n=32 if args.small else 128, shell=2 if args.small else 4,
                               ntrain=4 if args.small else 8, held=(1000,) if args.small else (1000, 1001, 1002))
     alg_bytes = 88.0 * ncc * pinfo["iterations"]  # 88 B per cell per FP64 PCG iteration (algorithmic)
@@ -536,6 +570,7 @@ def main():
                         "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"]},
             "poisson_sigma_shell": shell,
             "poisson_learned": learned,
+            "at_scale": scale5,
             "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (duct fluid mesh)",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -148,6 +148,17 @@ def duct(nx: int = 64, ny: int = 64, nz: int = 256, Re: float = 1000.0, Ha: floa
     return mom, ind, prm, init
 
 
+def at_scale(nx: int = 128, ny: int = 128, nz: int = 256, **kw):
+    """Full solver at scale: finite magnetic Reynolds number with constrained
+    transport (the B form), 256 x 128 x 128 cells (streamwise z uniform, the
+    cross-section Roberts-stretched), Re = 1000, Ha = 500, Rem = 10,
+    dt = 2e-4, seeded N(0, 1e-3) velocity, insulating walls (no wall layer).
+    The duct geometry and BCs of ``duct``."""
+    args = dict(Re=1000.0, Ha=500.0, Rem=10.0, dt=2e-4, noise=1e-3, n_wall=0)
+    args.update(kw)
+    return duct(nx=nx, ny=ny, nz=nz, **args)
+
+
 def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, **kw):
     """Create meshes + the MHD object on ``backend`` (moons_b200.capi or the
     oracle module) from a builder, upload the seeded initial state and init.

@@ -19,6 +19,8 @@ CASES = [
     ("ldc_bform", configs.ldc, dict(n=10, induction=G.IND_B, tol=1e-12)),
     ("duct_walls", configs.duct, dict(nx=10, ny=8, nz=12, n_wall=2, t_wall=0.5, tol=1e-12, noise=1e-2)),
     ("duct_nowall", configs.duct, dict(nx=8, ny=8, nz=12, n_wall=0, tol=1e-12, noise=1e-2)),
+    # configuration 5's physics (Ha = 500, Rem = 10, dt = 2e-4) on a small grid
+    ("at_scale_small", configs.at_scale, dict(nx=8, ny=8, nz=16, tol=1e-12)),
 ]
 
 
@@ -58,7 +60,7 @@ def test_mhd_steps_match_oracle(name, builder, kw):
 
 
 @pytest.mark.parametrize("prec", [G.PREC_MG, G.PREC_MG_MIXED], ids=["mg", "mixed"])
-@pytest.mark.parametrize("name,builder,kw", [CASES[0], CASES[2]], ids=[CASES[0][0], CASES[2][0]])
+@pytest.mark.parametrize("name,builder,kw", [CASES[0], CASES[2], CASES[4]], ids=[CASES[0][0], CASES[2][0], CASES[4][0]])
 def test_mhd_steps_multigrid_poisson(name, builder, kw, prec):
     """The step with multigrid-preconditioned pressure/potential solves reaches
     the same fields as the oracle's Jacobi-PCG step: the solves converge to the
