@@ -99,6 +99,30 @@ extern long long g_launch_count;
     ++mg::g_launch_count;                                 \
   } while (0)
 
+// the same, launched with programmatic stream serialisation (programmatic
+// dependent launch; the kernel must call griddepcontrol.wait before reading
+// what its predecessor wrote); returns from the caller on a launch error
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ++g_launch_count;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+#define MG_LAUNCH_PDL(K, GRID, BLOCK, STREAM, ...)                                             \
+  do {                                                                                         \
+    cudaError_t e_ = mg::launch_pdl(K, dim3(GRID), dim3(BLOCK), (STREAM), __VA_ARGS__);        \
+    if (e_ != cudaSuccess) return mg::cuda_fail(e_, #K);                                       \
+  } while (0)
+
 constexpr int kBlock = 256;
 inline unsigned nblocks(size_t n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }
 

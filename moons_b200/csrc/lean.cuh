@@ -24,6 +24,17 @@
 
 namespace mg {
 
+// Programmatic dependent launch: the solver loop's kernels are launched with
+// programmatic stream serialisation, so the next kernel's blocks are
+// scheduled while this one drains; each kernel lets its dependent launch at
+// once and waits for its predecessor's completion (and memory) before it
+// reads anything the predecessor wrote.  Both are no-ops in a plain launch.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+
 constexpr int kLB = 256;  // threads per block (points of one plane)
 constexpr int kKC = 4;    // planes per thread
 
@@ -251,6 +262,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kLB, 2) k_l_lap(FComp Ap, FComp P, DGrid g, FBC b0, FBC b1, FBC b2, DF kx, DF ky,
                                                    DF kz, double coeff, PcgScalars* S, double* partial,
                                                    unsigned* ticket) {
+  pdl_enter();
   if (S->done) return;
   double acc;
   if (blockIdx.z == 0) acc = lap_col<MODE>(Ap.f[0], P.f[0], b0, g, kx, ky, kz, coeff);
@@ -308,6 +320,7 @@ __device__ __forceinline__ void curl_sig_col(const DF& E, const DF& pa, const DF
 }
 __global__ void __launch_bounds__(kLB) k_l_curl_sig(DF E0, DF E1, DF E2, FComp P, DF s0, DF s1, DF s2, DGrid g,
                                                      PcgScalars* S) {
+  pdl_enter();
   if (S->done) return;
   if (blockIdx.z == 0) curl_sig_col<0>(E0, P.f[2], P.f[1], s0, g);
   else if (blockIdx.z == 1) curl_sig_col<1>(E1, P.f[0], P.f[2], s1, g);
@@ -375,6 +388,7 @@ __device__ __forceinline__ double curl_ap_col(const DF& A, const DF& p, const FB
 __global__ void __launch_bounds__(kLB) k_l_curl_ap(FComp Ap, FComp P, DF E0, DF E1, DF E2, DGrid g, FBC b0, FBC b1,
                                                     FBC b2, double coeff, PcgScalars* S, double* partial,
                                                     unsigned* ticket) {
+  pdl_enter();
   if (S->done) return;
   double acc;
   if (blockIdx.z == 0) acc = curl_ap_col<0>(Ap.f[0], P.f[0], b0, E2, E1, g, coeff);
@@ -426,6 +440,7 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
 template <int KC>
 __global__ void __launch_bounds__(kLB) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, FBC b0, FBC b1,
                                                    FBC b2, PcgScalars* S, double* partial, unsigned* ticket) {
+  pdl_enter();
   if (S->done) return;
   double arr = 0.0, azr = 0.0;
   const double alpha = S->alpha;
@@ -504,6 +519,7 @@ __device__ __forceinline__ void pupd_col(const DF& p, const DF& pn, const DF& r,
 }
 template <int KC>
 __global__ void __launch_bounds__(kLB) k_l_pupd(FComp P, FComp Pn, FComp R, FComp M, PcgScalars* S) {
+  pdl_enter();
   if (S->done) return;
   const double beta = S->beta;
   if (blockIdx.z == 0) pupd_col<KC>(P.f[0], Pn.f[0], R.f[0], M.f[0], beta);
@@ -619,6 +635,7 @@ __device__ __forceinline__ void bcfill_col(const DF& p, const FBC& b, unsigned n
   }
 }
 __global__ void __launch_bounds__(kLB) k_l_bcfill(FComp P, FBC b0, FBC b1, FBC b2, unsigned npbP, PcgScalars* S) {
+  pdl_enter();
   if (S->done) return;
   if (blockIdx.z == 0) bcfill_col(P.f[0], b0, npbP);
   else if (blockIdx.z == 1) bcfill_col(P.f[1], b1, npbP);

@@ -161,6 +161,7 @@ __global__ void k_prec(DF M, DGrid g, int mode, double coeff, int comp, DF sx, D
 
 
 __global__ void k_set_cond(cudaGraphConditionalHandle h, PcgScalars* S) {
+  pdl_enter();
   S->body_runs += 1;
   S->runs_total += 1;
   bool go = !S->done && S->body_runs < S->iter_max + 2;
@@ -387,28 +388,28 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
     DF* pn = half == 0 ? s->p2 : s->p;
     switch (s->op) {
       case MOONS_OP_LAP_UNIFORM:
-        MG_LAUNCH(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
+        MG_LAUNCH_PDL(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
                   0.0, s->S, s->partial, tA);
         break;
       case MOONS_OP_LAP_PROPS:
-        MG_LAUNCH(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], s->k[0],
+        MG_LAUNCH_PDL(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], s->k[0],
                   s->k[1], s->k[2], 0.0, s->S, s->partial, tA);
         break;
       case MOONS_OP_MOM_DIFFUSION:
-        MG_LAUNCH(k_l_lap<2>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
+        MG_LAUNCH_PDL(k_l_lap<2>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
                   s->coeff, s->S, s->partial, tA);
         break;
       case MOONS_OP_IND_DIFFUSION:
-        MG_LAUNCH(k_l_curl_sig, L.gE, kLB, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(pc, 3), s->k[0],
+        MG_LAUNCH_PDL(k_l_curl_sig, L.gE, kLB, m->stream, s->tempk[0], s->tempk[1], s->tempk[2], fc(pc, 3), s->k[0],
                   s->k[1], s->k[2], m->dg, s->S);
-        MG_LAUNCH(k_l_curl_ap, L.gA, kLB, m->stream, fc(s->Ax, 3), fc(pc, 3), s->tempk[0], s->tempk[1], s->tempk[2],
+        MG_LAUNCH_PDL(k_l_curl_ap, L.gA, kLB, m->stream, fc(s->Ax, 3), fc(pc, 3), s->tempk[0], s->tempk[1], s->tempk[2],
                   m->dg, b[0], b[1], b[2], s->coeff, s->S, s->partial, tA);
         break;
     }
-    MG_LAUNCH(k_l_update<kKCU>, L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc), fc(s->Ax, nc),
+    MG_LAUNCH_PDL(k_l_update<kKCU>, L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc), fc(s->Ax, nc),
               fc(s->Minv, nc), b[0], b[1], b[2], s->S, s->partial, tB);
-    MG_LAUNCH(k_l_pupd<kKCU>, L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc), fc(s->Minv, nc), s->S);
-    if (L.bc) MG_LAUNCH(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, nc), b[0], b[1], b[2], L.npbP, s->S);
+    MG_LAUNCH_PDL(k_l_pupd<kKCU>, L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc), fc(s->Minv, nc), s->S);
+    if (L.bc) MG_LAUNCH_PDL(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, nc), b[0], b[1], b[2], L.npbP, s->S);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
@@ -537,7 +538,10 @@ int build_graph(moons_pcg* s, DF* x) {
   MG_CUDA(cudaStreamBeginCaptureToGraph(m->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   long long before = g_launch_count;  // captured launches run later, once per body execution
   int r = enqueue_iteration(s, x);
-  MG_LAUNCH(k_set_cond, 1, 1, m->stream, h, s->S);
+  if (!r) {
+    cudaError_t e_ = launch_pdl(k_set_cond, dim3(1), dim3(1), m->stream, h, s->S);
+    if (e_ != cudaSuccess) r = cuda_fail(e_, "k_set_cond");
+  }
   s->body_launches = g_launch_count - before;
   g_launch_count = before;
   cudaGraph_t captured = nullptr;
