@@ -96,7 +96,8 @@ enum {
   MOONS_OP_LAP_UNIFORM = 1,   /* Lap_uniform_SF/VF      :35-90              */
   MOONS_OP_LAP_PROPS = 2,     /* Lap_nonuniform_props   :92-118  div(k grad) */
   MOONS_OP_IND_DIFFUSION = 3, /* ind_diffusion          :120-146             */
-  MOONS_OP_MOM_DIFFUSION = 4  /* mom_diffusion          :176-202             */
+  MOONS_OP_MOM_DIFFUSION = 4, /* mom_diffusion          :176-202             */
+  MOONS_OP_NRG_DIFFUSION = 5  /* nrg_diffusion          :148-174  I + c div(k grad) */
 };
 /* Diagonal preconditioners (preconditioners.f90). */
 enum {
@@ -255,6 +256,22 @@ typedef struct {
                                or MOONS_PREC_MG / MOONS_PREC_MG_MIXED (no
                                reference counterpart: same system, same exit
                                tests, far fewer iterations)                   */
+  /* energy equation (energy_extend.f90:236-262, add_all_energy_sources.f90:
+   * 21-67), solved on the induction mesh before the momentum step as
+   * solve_MOONS does (MOONS_solver.f90:81-85); fields MOONS_MHD_T, _KT,
+   * _GRAVITY */
+  int energy;               /* 1: solve for T                               */
+  int solve_method_T;       /* 2: Euler_time_no_diff_AB2_sources_SF (explicit),
+                               3: Euler_time_AB2_sources_SF (PCG_T, nrg_diffusion,
+                               prec_lap_SF) (time_marching_methods_SF.f90:71-160) */
+  double coeff_implicit_T;  /* SP%VS%T%MFP%coeff_implicit                    */
+  double scale_advection_T; /* SP%ET%advection%scale: F += s (-div(u T))     */
+  double scale_diffusion_T; /* SP%ET%diffusion%scale: F += s lap(T) (explicit) */
+  double scale_heating_T;   /* SP%ET%volumetric_heating%scale
+                               (add_volumetric_heating_Nuclear)              */
+  double scale_buoyancy;    /* SP%MT%Buoyancy%scale: F_U += s face(T g)      */
+  moons_isp isp_T;
+  moons_bc_spec bc_T;
 } moons_mhd_params;
 
 typedef struct {
@@ -262,6 +279,7 @@ typedef struct {
   int iters_U, iters_p, iters_B, iters_phi;  /* summed over the steps       */
   double res_p, res_phi;                     /* last relative residuals     */
   double ms;                                 /* device time of the steps    */
+  int iters_T;                               /* energy PCG (solve_method 3) */
 } moons_step_info;
 
 /* Field handles of an MHD object (for upload / download / probes). */
@@ -275,7 +293,10 @@ enum {
   MOONS_MHD_SIGMA_INV = 6,/* comp 0..2: edges (B form) / sigma on faces (potential) */
   MOONS_MHD_JXB = 7,      /* comp 0..2, faces on the induction mesh          */
   MOONS_MHD_DIVU = 8,     /* CC on the fluid mesh (probe)                    */
-  MOONS_MHD_DIVB = 9      /* CC on the induction mesh (probe)                */
+  MOONS_MHD_DIVB = 9,     /* CC on the induction mesh (probe)                */
+  MOONS_MHD_T = 10,       /* temperature, CC on the induction mesh           */
+  MOONS_MHD_KT = 11,      /* comp 0..2: thermal conductivity on the faces    */
+  MOONS_MHD_GRAVITY = 12  /* comp 0..2: gravity vector field, CC             */
 };
 
 /* mesh_ind may equal mesh_mom.  Fields start at 0; upload initial U, B, B0

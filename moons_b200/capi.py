@@ -23,7 +23,7 @@ from . import build as _build
 
 CC, FX, FY, FZ, EX, EY, EZ, NODE = range(8)
 DIRICHLET, NEUMANN, PERIODIC, ROBIN = 1, 2, 3, 4
-OP_LAP_UNIFORM, OP_LAP_PROPS, OP_IND_DIFFUSION, OP_MOM_DIFFUSION = 1, 2, 3, 4
+OP_LAP_UNIFORM, OP_LAP_PROPS, OP_IND_DIFFUSION, OP_MOM_DIFFUSION, OP_NRG_DIFFUSION = 1, 2, 3, 4, 5
 PREC_IDENTITY, PREC_LAP, PREC_MOM, PREC_IND = 0, 1, 2, 3
 PREC_MG, PREC_MG_MIXED = 4, 5  # multigrid V-cycle in CG (FP64) / in flexible CG (FP32 V-cycle)
 PREC_UNET = 6  # learned U-Net in flexible CG, FP32 V-cycle fallback (PCG.set_unet)
@@ -63,6 +63,7 @@ class SolveInfo(C.Structure):
         ("rel", C.c_double),
         ("exit_reason", C.c_int),
         ("ms", C.c_double),
+        ("iters_T", C.c_int),
     ]
 
     def as_dict(self):
@@ -70,7 +71,8 @@ class SolveInfo(C.Structure):
 
 
 IND_OFF, IND_B, IND_POTENTIAL = 0, 1, 2
-MHD_U, MHD_P, MHD_B, MHD_B0, MHD_PHI, MHD_J, MHD_SIGMA_INV, MHD_JXB, MHD_DIVU, MHD_DIVB = range(10)
+MHD_U, MHD_P, MHD_B, MHD_B0, MHD_PHI, MHD_J, MHD_SIGMA_INV, MHD_JXB, MHD_DIVU, MHD_DIVB, MHD_T, MHD_KT, MHD_GRAVITY = \
+    range(13)
 
 
 class MHDParams(C.Structure):
@@ -100,6 +102,15 @@ class MHDParams(C.Structure):
         ("prescribed_Ustar", C.c_int),
         ("prescribed_Bstar", C.c_int),
         ("prec_poisson", C.c_int),
+        ("energy", C.c_int),
+        ("solve_method_T", C.c_int),
+        ("coeff_implicit_T", C.c_double),
+        ("scale_advection_T", C.c_double),
+        ("scale_diffusion_T", C.c_double),
+        ("scale_heating_T", C.c_double),
+        ("scale_buoyancy", C.c_double),
+        ("isp_T", ISP),
+        ("bc_T", BCSpec),
     ]
 
 
@@ -113,6 +124,7 @@ class StepInfo(C.Structure):
         ("res_p", C.c_double),
         ("res_phi", C.c_double),
         ("ms", C.c_double),
+        ("iters_T", C.c_int),
     ]
 
     def as_dict(self):

@@ -159,6 +159,38 @@ def at_scale(nx: int = 128, ny: int = 128, nz: int = 256, **kw):
     return duct(nx=nx, ny=ny, nz=nz, **args)
 
 
+def ldc_energy(n: int = 16, Pe: float = 100.0, Gr_Re2: float = 10.0, heating: float = 0.5,
+               solve_method_T: int = 3, tol: float = 1e-10, **kw):
+    """The lid-driven cavity with the energy equation: T = 1 on the x-min
+    wall, 0 on x-max, insulated elsewhere; conductivity on the faces varying
+    by +-20% (seeded); gravity -y; advection scale 1 (S += -div(u T)),
+    diffusion by the implicit nrg_diffusion PCG (solve_method 3, coefficient
+    -1/Pe) or explicitly (solve_method 2, scale 1/Pe); volumetric heating
+    (add_volumetric_heating_Nuclear) and buoyancy Gr/Re^2 in momentum."""
+    mom, ind, prm, init0 = ldc(n=n, tol=tol, **kw)
+    prm.energy = 1
+    prm.solve_method_T = solve_method_T
+    prm.coeff_implicit_T = -1.0 / Pe
+    prm.scale_advection_T = 1.0
+    prm.scale_diffusion_T = 0.0 if solve_method_T == 3 else 1.0 / Pe
+    prm.scale_heating_T = heating
+    prm.scale_buoyancy = Gr_Re2
+    prm.isp_T = _isp(5000, tol)
+    D, Nn = G.DIRICHLET, G.NEUMANN
+    prm.bc_T = G.bc_spec([D, D, Nn, Nn, Nn, Nn], values=[1.0, 0.0, 0.0, 0.0, 0.0, 0.0], order=ORDER_LDC)
+
+    def init(sim, rng):
+        init0(sim, rng)
+        for c in range(3):
+            sim.upload(G.MHD_KT, c, 1.0 + 0.2 * rng.uniform(-1.0, 1.0, sim.shape(G.MHD_KT, c)))
+            g = np.zeros(sim.shape(G.MHD_GRAVITY, c))
+            if c == 1:
+                g[:] = -1.0
+            sim.upload(G.MHD_GRAVITY, c, g)
+
+    return mom, ind, prm, init
+
+
 def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, **kw):
     """Create meshes + the MHD object on ``backend`` (moons_b200.capi or the
     oracle module) from a builder, upload the seeded initial state and init.

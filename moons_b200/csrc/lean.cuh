@@ -160,7 +160,7 @@ __device__ __forceinline__ Ax6 axis_coef(const DCoord& c, bool N, int t) {
   return r;
 }
 
-// ---- K1: LAP_UNIFORM (MODE 0), LAP_PROPS (1), MOM_DIFFUSION (2) ---------------
+// ---- K1: LAP_UNIFORM (MODE 0), LAP_PROPS (1), MOM_DIFFUSION (2), NRG_DIFFUSION (3)
 // all k chunks of this block's columns (blockIdx.y strides over them)
 template <int MODE>
 __device__ __forceinline__ double lap_col(const DF& A, const DF& p, const FBC& b, const DGrid& g, const DF& kx,
@@ -211,7 +211,7 @@ __device__ __forceinline__ double lap_col(const DF& A, const DF& p, const FBC& b
     }
     // coefficient fields have their own (face) extents
     size_t ix = 0, iy = 0, iz = 0, szx = 0, szy = 0, szz = 0;
-    if (MODE == 1) {
+    if (MODE == 1 || MODE == 3) {
       ix = kx.at(i, j, k0);
       iy = ky.at(i, j, k0);
       iz = kz.at(i, j, k0);
@@ -231,17 +231,17 @@ __device__ __forceinline__ double lap_col(const DF& A, const DF& p, const FBC& b
       const double pm = pc[q], p0 = pc[q + 1], pp = pc[q + 2];
       const Ax6 Z = axis_coef(g.c[2], Nz, k);
       double gl = xm[q] * X.a1 + p0 * X.a2, gr = p0 * X.b1 + xp[q] * X.b2;
-      if (MODE == 1 && !Nx) { gl = gl * ld(kx.f + ix + q * szx); gr = gr * ld(kx.f + ix + q * szx + 1); }
+      if ((MODE == 1 || MODE == 3) && !Nx) { gl = gl * ld(kx.f + ix + q * szx); gr = gr * ld(kx.f + ix + q * szx + 1); }
       double v = gl * X.o1 + gr * X.o2;
       gl = ym[q] * Y.a1 + p0 * Y.a2;
       gr = p0 * Y.b1 + yp[q] * Y.b2;
-      if (MODE == 1 && !Ny) { gl = gl * ld(ky.f + iy + q * szy); gr = gr * ld(ky.f + iy + q * szy + ky.s0); }
+      if ((MODE == 1 || MODE == 3) && !Ny) { gl = gl * ld(ky.f + iy + q * szy); gr = gr * ld(ky.f + iy + q * szy + ky.s0); }
       v = v + (gl * Y.o1 + gr * Y.o2);
       gl = pm * Z.a1 + p0 * Z.a2;
       gr = p0 * Z.b1 + pp * Z.b2;
-      if (MODE == 1 && !Nz) { gl = gl * ld(kz.f + iz + q * szz); gr = gr * ld(kz.f + iz + (q + 1) * szz); }
+      if ((MODE == 1 || MODE == 3) && !Nz) { gl = gl * ld(kz.f + iz + q * szz); gr = gr * ld(kz.f + iz + (q + 1) * szz); }
       v = v + (gl * Z.o1 + gr * Z.o2);
-      if (MODE == 2) {
+      if (MODE == 2 || MODE == 3) {
         v = v * coeff;
         v = v + p0;
       }

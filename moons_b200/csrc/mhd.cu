@@ -65,6 +65,14 @@ __global__ void k_embed_extract(DF dst, DF src, int o0, int o1, int o2, int embe
   if (embed) dst(i + o0, j + o1, k + o2) = src(i, j, k);
   else dst(i, j, k) = src(i + o0, j + o1, k + o2);
 }
+// t(i,j,k) = prof[j-1] over the whole array (a profile along y)
+__global__ void k_fill_y(DF t, const double* prof) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= t.n()) return;
+  int i, j, k;
+  ijk_of(idx, t, i, j, k);
+  t.f[idx] = prof[j - 1];
+}
 // u += c everywhere (compute_add_MPG: add(U%x, scale*dt))
 __global__ void k_add_scalar(double* a, double c, size_t n) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -110,8 +118,13 @@ struct moons_mhd {
       *tCCi, *tFi1[3], *tFi2[3], *tE[3], *curlUxB[3], *divB, *Ui[3], *E[3];
   moons_sf *UEi[3][3], *BE[3][3], *TF1[3][3], *TF2[3][3];
   moons_pcg *pcgB = nullptr, *pcgPhi = nullptr;
-  double coefU = NAN, coefB = NAN;
-  int iters[4] = {0, 0, 0, 0};
+  // energy (on the induction mesh)
+  moons_sf *T = nullptr, *Tnm1 = nullptr, *FT = nullptr, *FnmT = nullptr, *LT = nullptr, *tCCT = nullptr,
+           *tCCT2 = nullptr, *tmpT = nullptr, *kT[3] = {}, *grav[3] = {}, *tFT[3] = {}, *UFT[3] = {};
+  moons_pcg* pcgT = nullptr;
+  double* heat_prof = nullptr;  // add_volumetric_heating_Nuclear profile per y index (device)
+  double coefU = NAN, coefB = NAN, coefT = NAN;
+  int iters[5] = {0, 0, 0, 0, 0};
   double res_p = 0, res_phi = 0;
   double* d_red = nullptr;
   cudaStream_t mi_stream_saved = nullptr;  // the induction mesh runs on the fluid mesh's stream
@@ -317,11 +330,82 @@ int advect_U_convection1(moons_mhd* s) {
   return r;
 }
 
+// ---- energy equation ---------------------------------------------------------
+// add_all_energy_sources (add_all_energy_sources.f90:21-67) with the
+// advection, diffusion and volumetric-heating terms (energy_sources.f90),
+// then solve_energy (energy_extend.f90:236-262), methods 2 and 3
+int energy_step(moons_mhd* s) {
+  moons_mesh* mi = s->mi;
+  const moons_mhd_params& P = s->P;
+  int r = copy(mi, s->FnmT, s->FT);
+  if (!r) r = launch_pw(mi, PW_FILL, D(s->FT), nullptr, 0.0);
+  if (!r && P.scale_advection_T != 0.0) {
+    // add_advection: S += scale * (-div(face(T) * U_F)), U_F = embedFace(U)
+    for (int c = 0; c < 3 && !r; c++) {
+      if (s->same) r = copy(mi, s->UFT[c], s->U[c]);
+      else r = embed_extract(mi, s->UFT[c], s->U[c], P.ind_offset, true);
+    }
+    for (int c = 0; c < 3 && !r; c++) {
+      r = launch_interp(mi, D(s->tFT[c]), D(s->T), c + 1);
+      if (!r) r = launch_pw(mi, PW_MUL, D(s->tFT[c]), &D(s->UFT[c]), 0.0);
+    }
+    if (!r) r = div3(mi, s->tCCT, s->tFT);
+    if (!r) r = launch_pw(mi, PW_SCALE, D(s->tCCT), nullptr, -1.0);
+    if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_advection_T);
+  }
+  if (!r && P.scale_diffusion_T != 0.0) {
+    // add_diffusion: S += scale * lap(T) (lapUniformCoeff_SF)
+    r = launch_del(mi, D(s->tCCT), D(s->T), 2, 1, 0, 1);
+    if (!r) r = launch_del(mi, D(s->tCCT), D(s->T), 2, 2, 0, 2);
+    if (!r) r = launch_del(mi, D(s->tCCT), D(s->T), 2, 3, 0, 2);
+    if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_diffusion_T);
+  }
+  if (!r && P.scale_heating_T != 0.0) {
+    // add_volumetric_heating_Nuclear: temp = scale*F0*exp(-m (y_c + 1)); S += scale * temp
+    MG_LAUNCH(k_fill_y, nblocks(D(s->tCCT).n()), kBlock, mi->stream, D(s->tCCT), s->heat_prof);
+    r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_heating_T);
+  }
+  if (r) return r;
+  // X* = X + dt AB2(F, Fnm1) (wall-Dirichlet points of the increment zeroed)
+  const int wb = dirichlet_wall_bits(s->T->bc.defined ? &s->T->bc : nullptr, D(s->T).dl);
+  MG_LAUNCH(k_ab2_rhs, nblocks(D(s->tmpT).n()), kBlock, mi->stream, D(s->tmpT), D(s->FT), D(s->FnmT), D(s->LT),
+            D(s->T), D(s->Tnm1), P.dt, wb);
+  MG_CUDA(cudaGetLastError());
+  if (P.solve_method_T == 2) return copy(mi, s->T, s->tmpT);  // X = X + dt AB2 (no diffusion solve)
+  const double c = P.dt * 1.0 * P.coeff_implicit_T;
+  if (!(c == s->coefT)) {
+    if ((r = moons_pcg_update_mfp(s->pcgT, c, 1))) return r;
+    s->coefT = c;
+  }
+  moons_sf* xt[1] = {s->T};
+  moons_sf* bt[1] = {s->tmpT};
+  return solve(s->pcgT, xt, bt, P.isp_T, &s->iters[4], nullptr);
+}
+
+// compute_add_buoyancy (momentum_sources.f90:133-150): F += scale extractFace(face(T g))
+int add_buoyancy(moons_mhd* s) {
+  moons_mesh *m = s->mm, *mi = s->mi;
+  int r = MOONS_OK;
+  for (int c = 0; c < 3 && !r; c++) {
+    r = copy(mi, s->tCCT2, s->T);
+    if (!r) r = launch_pw(mi, PW_MUL, D(s->tCCT2), &D(s->grav[c]), 0.0);
+    if (!r) r = launch_interp(mi, D(s->tFT[c]), D(s->tCCT2), c + 1);
+    if (!r) {
+      if (s->same) r = copy(m, s->tF1[c], s->tFT[c]);
+      else r = embed_extract(m, s->tF1[c], s->tFT[c], s->P.ind_offset, false);
+    }
+    if (!r) r = launch_pw(m, PW_ADD_PRODUCT, D(s->F[c]), &D(s->tF1[c]), s->P.scale_buoyancy);
+  }
+  return r;
+}
+
 int step_once(moons_mhd* s) {
   moons_mesh* m = s->mm;
   const moons_mhd_params& P = s->P;
   double dt = P.dt;
   int r = MOONS_OK;
+  // ---- energy (solve_MOONS: energy sources and solve before momentum)
+  if (P.energy && (r = energy_step(s))) return r;
   // ---- add_all_momentum_sources
   if (P.mpg_dir >= 1 && P.mpg_dir <= 3) {
     DF u = D(s->U[P.mpg_dir - 1]);
@@ -351,6 +435,7 @@ int step_once(moons_mhd* s) {
       if (!r) r = launch_pw(m, PW_ADD_PRODUCT, D(s->F[c]), &D(s->tF1[c]), 1.0);
     }
   }
+  if (!r && P.energy && P.scale_buoyancy != 0.0) r = add_buoyancy(s);
   if (r) return r;
   // ---- solve_momentum (method 6)
   r = euler_ab2(s, m, s->pcgU, s->pcgP, P.isp_U, P.isp_p, s->U, s->Ustar, s->Unm1, s->p, s->F, s->Fnm1, s->L, s->tF1,
@@ -418,6 +503,10 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
     set_error("moons_mhd_create: bad induction mode or dt");
     return MOONS_ERR_ARG;
   }
+  if (prm->energy && prm->solve_method_T != 2 && prm->solve_method_T != 3) {
+    set_error("moons_mhd_create: solve_method_T must be 2 or 3");
+    return MOONS_ERR_ARG;
+  }
   auto* s = new moons_mhd();
   s->mm = mm;
   s->mi = mi;
@@ -476,6 +565,29 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
   F(mi, MOONS_CC, &s->phi);
   F(mi, MOONS_CC, &s->tCCi);
   F(mi, MOONS_CC, &s->divB);
+  if (prm->energy) {
+    for (moons_sf** f : {&s->T, &s->Tnm1, &s->FT, &s->FnmT, &s->LT, &s->tCCT, &s->tCCT2, &s->tmpT}) F(mi, MOONS_CC, f);
+    for (int c = 0; c < 3; c++) {
+      F(mi, MOONS_FX + c, &s->kT[c]);
+      F(mi, MOONS_CC, &s->grav[c]);
+      F(mi, MOONS_FX + c, &s->tFT[c]);
+      F(mi, MOONS_FX + c, &s->UFT[c]);
+    }
+    if (!r) r = set_bcs_from(s->T, prm->bc_T);
+    if (!r && prm->scale_heating_T != 0.0) {
+      // add_volumetric_heating_Nuclear (energy_sources.f90:98-114): a = L = 1,
+      // m = a/L, F = scale 2m/(1-exp(-2m)), temp(j) = F exp(-m (hc(j)+1))
+      const std::vector<double>& hy = mi->hn[1];
+      const double a = 1.0, Lh = 1.0, mm_ = a / Lh;
+      const double Fh = prm->scale_heating_T * 2.0 * mm_ / (1.0 - std::exp(-2.0 * mm_));
+      std::vector<double> prof(hy.size() - 1);
+      for (size_t j = 0; j + 1 < hy.size(); j++) prof[j] = Fh * std::exp(-mm_ * (0.5 * (hy[j] + hy[j + 1]) + 1.0));
+      if (cudaMalloc((void**)&s->heat_prof, prof.size() * sizeof(double)) != cudaSuccess) r = MOONS_ERR_NOMEM;
+      else if (cudaMemcpy(s->heat_prof, prof.data(), prof.size() * sizeof(double), cudaMemcpyHostToDevice) !=
+               cudaSuccess)
+        r = MOONS_ERR_CUDA;
+    }
+  }
   // BCs
   for (int c = 0; c < 3 && !r; c++) {
     r = set_bcs_from(s->U[c], prm->bc_U[c]);
@@ -518,10 +630,11 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
 
 int moons_mhd_destroy(moons_mhd* s) {
   if (!s) return MOONS_OK;
-  for (moons_pcg* p : {s->pcgU, s->pcgP, s->pcgB, s->pcgPhi})
+  for (moons_pcg* p : {s->pcgU, s->pcgP, s->pcgB, s->pcgPhi, s->pcgT})
     if (p) moons_pcg_destroy(p);
   for (moons_sf* f : s->owned) moons_sf_destroy(f);
   if (s->d_red) cudaFree(s->d_red);
+  if (s->heat_prof) cudaFree(s->heat_prof);
   if (s->mi_stream_saved) s->mi->stream = s->mi_stream_saved;
   moons_mesh *mm = s->mm, *mi = s->mi;
   delete s;
@@ -547,6 +660,9 @@ int moons_mhd_field(moons_mhd* s, int which, int comp, moons_sf** out) {
     case MOONS_MHD_JXB: f = s->jxb[comp]; break;
     case MOONS_MHD_DIVU: f = s->divU; break;
     case MOONS_MHD_DIVB: f = s->divB; break;
+    case MOONS_MHD_T: f = s->T; break;
+    case MOONS_MHD_KT: f = s->kT[comp]; break;
+    case MOONS_MHD_GRAVITY: f = s->grav[comp]; break;
     default:
       set_error("moons_mhd_field: unknown field");
       return MOONS_ERR_ARG;
@@ -587,6 +703,16 @@ int moons_mhd_init(moons_mhd* s) {
       moons_sf* xf[1] = {s->phi};
       if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_PROPS, pp, 1, xf, xf, s->sig, &s->pcgPhi))) return r;
     }
+    if (s->P.energy && s->P.solve_method_T == 3) {
+      // init(nrg%PCG_T, nrg_diffusion, nrg_diffusion_explicit, prec_lap_SF, ...) (energy_extend.f90:129)
+      moons_sf* xt[1] = {s->T};
+      if ((r = moons_pcg_create(s->mi, MOONS_OP_NRG_DIFFUSION, MOONS_PREC_LAP, 1, xt, xt, s->kT, &s->pcgT))) return r;
+    }
+  }
+  if (s->P.energy) {  // init_energy tail (energy_extend.f90:119-120): apply_BCs(T); Tnm1 = T
+    r = launch_bcs(s->mi, D(s->T), s->T->bc, false);
+    if (!r) r = copy(s->mi, s->Tnm1, s->T);
+    if (r) return r;
   }
   moons_mesh* mi = s->mi;
   if (s->P.induction == MOONS_IND_B) {
@@ -624,8 +750,8 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
   }
   moons_mesh* m = s->mm;
   cudaSetDevice(m->device);
-  for (int k = 0; k < 4; k++) s->iters[k] = 0;
-  moons_pcg* solvers[4] = {s->pcgU, s->pcgP, s->pcgB, s->pcgPhi};
+  for (int k = 0; k < 5; k++) s->iters[k] = 0;
+  moons_pcg* solvers[5] = {s->pcgU, s->pcgP, s->pcgB, s->pcgPhi, s->pcgT};
   for (moons_pcg* p : solvers)
     if (p) mg_pcg_clear_totals(p);
   cudaEvent_t e0, e1;
@@ -645,7 +771,7 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
   if (r) return r;
   MG_CUDA(e);
   int nan = 0;
-  for (int k = 0; k < 4; k++) {
+  for (int k = 0; k < 5; k++) {
     if (!solvers[k]) continue;
     int it = 0, na = 0;
     double rel = 0;
@@ -665,6 +791,7 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
     info->iters_p = s->iters[1];
     info->iters_B = s->iters[2];
     info->iters_phi = s->iters[3];
+    info->iters_T = s->iters[4];
     info->res_p = s->res_p;
     info->res_phi = s->res_phi;
     info->ms = ms;

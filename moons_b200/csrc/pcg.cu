@@ -302,13 +302,16 @@ int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
         }
       }
       break;
-    case MOONS_OP_LAP_PROPS: {
+    case MOONS_OP_LAP_PROPS:
+    case MOONS_OP_NRG_DIFFUSION: {
       for (int d = 0; d < 3 && !r; d++) r = launch_del(m, s->tempk[d], x[0], 1, d + 1, 0, 1);
       for (int d = 0; d < 3 && !r; d++) r = launch_pw(m, PW_MUL, s->tempk[d], &s->k[d], 0.0);
       if (!r) r = launch_del(m, out[0], s->tempk[0], 1, 1, 0, 1);
       if (!r) r = launch_del(m, out[0], s->tempk[1], 1, 2, 0, 2);
       if (!r) r = launch_del(m, out[0], s->tempk[2], 1, 3, 0, 2);
       if (!r) r = mask_ghost_XPeriodic(m, out[0], nullptr);
+      // nrg_diffusion_explicit (matrix_free_operators.f90:148-162): Ax*coeff + x
+      if (!r && s->op == MOONS_OP_NRG_DIFFUSION) r = launch_pw(m, PW_PRODUCT_ADD, out[0], &x[0], s->coeff);
     } break;
     case MOONS_OP_IND_DIFFUSION: {
       DF* t = s->tempk;
@@ -395,6 +398,10 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
         MG_LAUNCH_PDL(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], s->k[0],
                   s->k[1], s->k[2], 0.0, s->S, s->partial, tA);
         break;
+      case MOONS_OP_NRG_DIFFUSION:
+        MG_LAUNCH_PDL(k_l_lap<3>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], s->k[0],
+                      s->k[1], s->k[2], s->coeff, s->S, s->partial, tA);
+        break;
       case MOONS_OP_MOM_DIFFUSION:
         MG_LAUNCH_PDL(k_l_lap<2>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
                   s->coeff, s->S, s->partial, tA);
@@ -471,6 +478,7 @@ void plan_lean(moons_pcg* s) {
   const void* ka = s->op == MOONS_OP_LAP_UNIFORM ? (const void*)k_l_lap<0>
                    : s->op == MOONS_OP_LAP_PROPS ? (const void*)k_l_lap<1>
                    : s->op == MOONS_OP_MOM_DIFFUSION ? (const void*)k_l_lap<2>
+                   : s->op == MOONS_OP_NRG_DIFFUSION ? (const void*)k_l_lap<3>
                                                     : (const void*)k_l_curl_ap;
   L.gA = lean_grid(s, ka, s->Ax, nc, kKC);
   L.gB = lean_grid(s, (const void*)k_l_update<kKCU>, s->Ax, nc, kKCU);
@@ -568,15 +576,15 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: ncomp must be 1 or 3");
     return MOONS_ERR_ARG;
   }
-  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_MOM_DIFFUSION || prec < 0 || prec > MOONS_PREC_UNET) {
+  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_NRG_DIFFUSION || prec < 0 || prec > MOONS_PREC_UNET) {
     set_error("moons_pcg_create: bad operator/preconditioner");
     return MOONS_ERR_ARG;
   }
-  if ((op == MOONS_OP_LAP_PROPS && nc != 1) || (op == MOONS_OP_IND_DIFFUSION && nc != 3)) {
+  if (((op == MOONS_OP_LAP_PROPS || op == MOONS_OP_NRG_DIFFUSION) && nc != 1) || (op == MOONS_OP_IND_DIFFUSION && nc != 3)) {
     set_error("moons_pcg_create: operator/component count mismatch");
     return MOONS_ERR_ARG;
   }
-  bool needk = (op == MOONS_OP_LAP_PROPS || op == MOONS_OP_IND_DIFFUSION);
+  bool needk = (op == MOONS_OP_LAP_PROPS || op == MOONS_OP_IND_DIFFUSION || op == MOONS_OP_NRG_DIFFUSION);
   if (needk && (!k || !k[0] || !k[1] || !k[2])) {
     set_error("moons_pcg_create: operator needs three coefficient fields");
     return MOONS_ERR_ARG;

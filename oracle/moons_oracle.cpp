@@ -829,7 +829,7 @@ void PCG::init(const Grid& g_, int op_, int prec_, int nc_, SF* const* x, SF* co
     z.push_back(like(*g, *x[c]));
     Minv.push_back(like(*g, *x[c]));
   }
-  int nk = (op == OP_LAP_PROPS || op == OP_IND_DIFFUSION) ? 3 : 0;
+  int nk = (op == OP_LAP_PROPS || op == OP_IND_DIFFUSION || op == OP_NRG_DIFFUSION) ? 3 : 0;
   for (int c = 0; c < nk; c++) {
     k.push_back(*kin[c]);
     SF t = like(*g, *kin[c]);
@@ -927,6 +927,13 @@ void PCG::apply_operator(std::vector<SF>& A, std::vector<SF>& x, bool explicit_o
       break;
     case OP_LAP_PROPS:
       lap_var(A[0], x[0], k[0], k[1], k[2], *g);
+      break;
+    case OP_NRG_DIFFUSION:
+      // nrg_diffusion_explicit (matrix_free_operators.f90:148-162):
+      // grad(tempk,x); multiply(tempk,k); div(Ax,tempk); multiply(Ax,coeff); add(Ax,x)
+      lap_var(A[0], x[0], k[0], k[1], k[2], *g);
+      multiply(A[0], coeff);
+      add(A[0], x[0]);
       break;
     case OP_MOM_DIFFUSION:
       for (int c = 0; c < nc; c++) {

@@ -138,7 +138,7 @@ void lap_var(SF& out, const SF& u, const SF& kx, const SF& ky, const SF& kz, con
 void interp(SF& out, const SF& in, const Grid& g, int dir);
 
 // ---- PCG
-enum { OP_LAP_UNIFORM = 1, OP_LAP_PROPS = 2, OP_IND_DIFFUSION = 3, OP_MOM_DIFFUSION = 4 };
+enum { OP_LAP_UNIFORM = 1, OP_LAP_PROPS = 2, OP_IND_DIFFUSION = 3, OP_MOM_DIFFUSION = 4, OP_NRG_DIFFUSION = 5 };
 enum { PREC_IDENTITY = 0, PREC_LAP = 1, PREC_MOM = 2, PREC_IND = 3 };
 
 struct ISP {

@@ -104,7 +104,12 @@ struct MHD {
   TF UEi, BE, TF1, TF2;
   PCG pcgB, pcgPhi;
   ISP ispB, ispPhi;
-  int iters[4] = {0, 0, 0, 0};
+  // energy (on the induction mesh)
+  SF T, Tnm1, FT, FnmT, LT, tCCT, tCCT2, tmpT, kT[3], grav[3], tFT[3], UFT[3];
+  PCG pcgT;
+  ISP ispT;
+  bool pcgT_made = false;
+  int iters[5] = {0, 0, 0, 0, 0};
   double res_p = 0, res_phi = 0;
 
   void create(const Grid& gmom, const Grid& gind, const moons_mhd_params& prm) {
@@ -165,7 +170,17 @@ struct MHD {
       }
       set_bcs_spec(phi, g, P.bc_phi);
     }
-    for (auto* I : {&ispU, &ispP, &ispB, &ispPhi}) *I = ISP();
+    if (P.energy) {
+      for (SF* f : {&T, &Tnm1, &FT, &FnmT, &LT, &tCCT, &tCCT2, &tmpT}) f->init(g, 0);
+      for (int c = 0; c < 3; c++) {
+        kT[c].init(g, dl_face(c));
+        grav[c].init(g, 0);
+        tFT[c].init(g, dl_face(c));
+        UFT[c].init(g, dl_face(c));
+      }
+      set_bcs_spec(T, g, P.bc_T);
+    }
+    for (auto* I : {&ispU, &ispP, &ispB, &ispPhi, &ispT}) *I = ISP();
     auto cp = [](ISP& d, const moons_isp& s) {
       d.iter_max = s.iter_max;
       d.tol_rel = s.tol_rel;
@@ -176,6 +191,7 @@ struct MHD {
     cp(ispP, P.isp_p);
     cp(ispB, P.isp_B);
     cp(ispPhi, P.isp_phi);
+    cp(ispT, P.isp_T);
   }
 
   void make_solvers() {
@@ -195,6 +211,77 @@ struct MHD {
       SF* xf[1] = {&phi};
       SF* ks[3] = {&sig[0], &sig[1], &sig[2]};
       pcgPhi.init(gi, OP_LAP_PROPS, PREC_LAP, 1, xf, xf, ks, 0.0);
+    }
+    if (P.energy && P.solve_method_T == 3) {
+      // init(nrg%PCG_T, nrg_diffusion, nrg_diffusion_explicit, prec_lap_SF, ...) (energy_extend.f90:129)
+      SF* xt[1] = {&T};
+      SF* ks[3] = {&kT[0], &kT[1], &kT[2]};
+      pcgT.init(gi, OP_NRG_DIFFUSION, PREC_LAP, 1, xt, xt, ks, P.coeff_implicit_T);
+      pcgT_made = true;
+    }
+  }
+
+  // ---- energy: add_all_energy_sources (add_all_energy_sources.f90:21-67),
+  // advection / diffusion / volumetric heating (energy_sources.f90), then
+  // solve_energy methods 2 and 3 (energy_extend.f90:236-262,
+  // time_marching_methods_SF.f90:71-160)
+  void energy_step() {
+    assign(FnmT, FT);
+    assign(FT, 0.0);
+    if (P.scale_advection_T != 0.0) {  // add_advection (energy_sources.f90:22-35)
+      for (int c = 0; c < 3; c++) {
+        if (same) assign(UFT[c], U[c]);
+        else embed_extract(UFT[c], U[c], off, true);
+      }
+      for (int c = 0; c < 3; c++) {
+        interp(tFT[c], T, gi, c + 1);  // cellCenter2Face
+        multiply(tFT[c], UFT[c]);
+      }
+      div(tCCT, tFT[0], tFT[1], tFT[2], gi);
+      multiply(tCCT, -1.0);
+      add_product(FT, tCCT, P.scale_advection_T);
+    }
+    if (P.scale_diffusion_T != 0.0) {  // add_diffusion: lap = lapUniformCoeff_SF
+      lap_uniform_coeff(tCCT, T, gi);
+      add_product(FT, tCCT, P.scale_diffusion_T);
+    }
+    if (P.scale_heating_T != 0.0) {  // add_volumetric_heating_Nuclear (energy_sources.f90:98-114)
+      const double a = 1.0, Lh = 1.0, m_ = a / Lh;
+      const double Fh = P.scale_heating_T * 2.0 * m_ / (1.0 - std::exp(-2.0 * m_));
+      const Coord& cy = gi.c[1];
+      for (int k = 1; k <= tCCT.s[3]; k++)
+        for (int j = 1; j <= tCCT.s[2]; j++)
+          for (int i = 1; i <= tCCT.s[1]; i++) tCCT(i, j, k) = Fh * std::exp(-m_ * (cy.hc(j) + 1.0));
+      add_product(FT, tCCT, P.scale_heating_T);
+    }
+    // AB2_SF: temp = Fn*1.5 ; temp += Fnm1*(-0.5) ; temp *= dt ; wall Dirichlet 0
+    for (size_t i = 0; i < tmpT.n(); i++) tmpT.f[i] = FT.f[i] * 1.5;
+    add_product(tmpT, FnmT, -0.5);
+    add(tmpT, LT);
+    multiply(tmpT, P.dt);
+    assign_wall_Dirichlet(tmpT, 0.0, &T);
+    if (P.solve_method_T == 2) {  // Euler_time_no_diff_AB2_sources_SF: X += X*
+      add(T, tmpT);
+      return;
+    }
+    add(tmpT, T);  // Euler_time_AB2_sources_SF
+    assign(Tnm1, T);
+    pcgT.update_MFP(P.dt * 1.0 * P.coeff_implicit_T, true);
+    SF* xt[1] = {&T};
+    SF* bt[1] = {&tmpT};
+    SolveInfo si = pcgT.solve(xt, bt, ispT);
+    iters[4] += si.iterations;
+  }
+
+  // compute_add_buoyancy (momentum_sources.f90:133-150)
+  void add_buoyancy() {
+    for (int c = 0; c < 3; c++) {
+      assign(tCCT2, T);
+      multiply(tCCT2, grav[c]);
+      interp(tFT[c], tCCT2, gi, c + 1);
+      if (same) assign(tF1[c], tFT[c]);
+      else embed_extract(tF1[c], tFT[c], off, false);
+      add_product(F[c], tF1[c], P.scale_buoyancy);
     }
   }
 
@@ -260,6 +347,10 @@ struct MHD {
   }
 
   void init() {
+    if (P.energy) {  // init_energy tail (energy_extend.f90:119-120)
+      apply_BCs(T);
+      assign(Tnm1, T);
+    }
     // init_mom tail (momentum_extend.f90:139-181)
     apply_BCs(p);
     for (int c = 0; c < 3; c++) {
@@ -329,6 +420,7 @@ struct MHD {
 
   void step() {
     double dt = P.dt;
+    if (P.energy) energy_step();
     // ---- add_all_momentum_sources
     if (P.mpg_dir >= 1 && P.mpg_dir <= 3) {  // compute_add_MPG (momentum_sources.f90:97-109)
       SF& u = U[P.mpg_dir - 1];
@@ -356,6 +448,7 @@ struct MHD {
         add_product(F[c], tF1[c], 1.0);
       }
     }
+    if (P.energy && P.scale_buoyancy != 0.0) add_buoyancy();
     // ---- solve_momentum (method 6)
     euler_ab2(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p);
     for (int c = 0; c < 3; c++) interp(UCC[c], U[c], gm, c + 1);
@@ -443,6 +536,9 @@ struct MHD {
       case MOONS_MHD_JXB: return &jxb[comp];
       case MOONS_MHD_DIVU: return &divU;
       case MOONS_MHD_DIVB: return &divB;
+      case MOONS_MHD_T: return &T;
+      case MOONS_MHD_KT: return &kT[comp];
+      case MOONS_MHD_GRAVITY: return &grav[comp];
     }
     return nullptr;
   }
@@ -498,7 +594,7 @@ int or_mhd_init(void* s) {
 }
 int or_mhd_step(void* s, int n, moons_step_info* info) {
   auto* m = (mo::MHD*)s;
-  for (int k = 0; k < 4; k++) m->iters[k] = 0;
+  for (int k = 0; k < 5; k++) m->iters[k] = 0;
   for (int i = 0; i < n; i++) m->step();
   if (info) {
     info->steps = n;
@@ -506,6 +602,7 @@ int or_mhd_step(void* s, int n, moons_step_info* info) {
     info->iters_p = m->iters[1];
     info->iters_B = m->iters[2];
     info->iters_phi = m->iters[3];
+    info->iters_T = m->iters[4];
     info->res_p = m->res_p;
     info->res_phi = m->res_phi;
     info->ms = 0;

@@ -21,6 +21,9 @@ CASES = [
     ("duct_nowall", configs.duct, dict(nx=8, ny=8, nz=12, n_wall=0, tol=1e-12, noise=1e-2)),
     # configuration 5's physics (Ha = 500, Rem = 10, dt = 2e-4) on a small grid
     ("at_scale_small", configs.at_scale, dict(nx=8, ny=8, nz=16, tol=1e-12)),
+    # the energy equation (implicit and explicit diffusion), buoyancy into momentum
+    ("ldc_energy_implicit", configs.ldc_energy, dict(n=10, tol=1e-12, solve_method_T=3)),
+    ("ldc_energy_explicit", configs.ldc_energy, dict(n=10, tol=1e-12, solve_method_T=2)),
 ]
 
 
@@ -38,7 +41,9 @@ def test_mhd_steps_match_oracle(name, builder, kw):
     ig = g.step(nsteps)
     io = o.step(nsteps)
     fields = [(G.MHD_U, c) for c in range(3)] + [(G.MHD_P, 0), (G.MHD_JXB, 0), (G.MHD_JXB, 1), (G.MHD_JXB, 2)]
-    ind = kw.get("induction", G.IND_B)
+    ind = kw.get("induction", G.IND_POTENTIAL if builder in (configs.ldc, configs.ldc_energy) else G.IND_B)
+    if builder is configs.ldc_energy:
+        fields += [(G.MHD_T, 0)]
     if ind != G.IND_OFF:
         fields += [(G.MHD_J, c) for c in range(3)]
     if ind == G.IND_POTENTIAL:
@@ -55,7 +60,7 @@ def test_mhd_steps_match_oracle(name, builder, kw):
     duo, dbo = o.divergence()
     assert dug <= max(10 * duo, 1e-24)
     assert dbg <= max(10 * dbo, 1e-24)
-    for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+    for k in ("iters_U", "iters_p", "iters_B", "iters_phi", "iters_T"):
         assert abs(ig[k] - io[k]) <= nsteps, (k, ig, io)
 
 

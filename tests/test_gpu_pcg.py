@@ -9,7 +9,8 @@ import pytest
 import oracle.oracle as O
 from moons_b200 import capi as G
 from moons_b200.capi import (CC, FX, FY, FZ, EX, EY, EZ, DIRICHLET, NEUMANN, PERIODIC, ROBIN, OP_LAP_UNIFORM,
-                             OP_LAP_PROPS, OP_MOM_DIFFUSION, OP_IND_DIFFUSION, PREC_LAP, PREC_MOM, PREC_IND,
+                             OP_LAP_PROPS, OP_MOM_DIFFUSION, OP_IND_DIFFUSION, OP_NRG_DIFFUSION, PREC_LAP, PREC_MOM,
+                             PREC_IND,
                              PREC_IDENTITY, isp)
 from tests.common import small_mesh_coords, rel_err, bc
 
@@ -99,6 +100,26 @@ def test_pcg_lap_props_sigma():
     assert abs(ig["iterations"] - io["iterations"]) <= max(1, 0.02 * io["iterations"]), (ig, io)
     assert ig["rel"] < 1e-10 and io["rel"] < 1e-10
     assert rel_err(phi[0].download(), phi[1].download()) < 1e-7
+
+
+@pytest.mark.parametrize("bctypes", [[DIRICHLET, DIRICHLET, NEUMANN, NEUMANN, DIRICHLET, NEUMANN],
+                                     [NEUMANN, NEUMANN, DIRICHLET, DIRICHLET, PERIODIC, PERIODIC]])
+def test_pcg_nrg_diffusion(bctypes):
+    """The energy equation's implicit operator I + c div(k grad) with the
+    reference's prec_lap_SF (energy_extend.f90:129), T at cell centres."""
+    ms = both(small_mesh_coords())
+    rng = np.random.default_rng(9)
+    s = shape(ms[1], CC)
+    (T,) = fields(ms, [CC], [rng.standard_normal(s) * 0.1])
+    spec = bc(bctypes, values=[1.0, 0.0, 0.0, 0.0, 0.5, 0.0])
+    T[0].set_bcs(spec)
+    T[1].set_bcs(spec)
+    ks = fields(ms, [FX, FY, FZ], [10.0 ** rng.uniform(-1, 1, shape(ms[1], d)) for d in (FX, FY, FZ)])
+    (b,) = fields(ms, [CC], [rng.standard_normal(s)])
+    ig, io = run_both(ms, OP_NRG_DIFFUSION, PREC_LAP, [T], [T], [b], isp(3000, 1e-10, 1e-15), ks=ks, coeff=-0.02)
+    assert ig["exit_reason"] == io["exit_reason"] == 1
+    assert abs(ig["iterations"] - io["iterations"]) <= 1, (ig, io)
+    assert rel_err(T[0].download(), T[1].download()) < 1e-9
 
 
 def test_pcg_mom_diffusion_vf():
