@@ -214,16 +214,23 @@ int launch_wgrad(moons_unet* u, int lvl, const bf16* inA, int cgA, const bf16* i
   const int nsg = 9 / a.nsh;
   const int nct = (cgT + a.ncg - 1) / a.ncg;
   a.items = g.Z * g.tiles_per_plane();
-  int chunks = std::max(1, std::min(a.items, (2 * u->nsm) / std::max(1, nsg * nct)));
+  const int NR = a.nsh * a.ncg;
+  const int SB = wgrad_stage_bytes(N, NR), tail = wgrad_tail_bytes(N, NR);
+  a.S = std::max(2, std::min(4, (160 * 1024 - tail) / SB));
+  const int smem = a.S * SB + tail;
+  if (int e = ensure_attrs(u->device)) return e;
+  // enough CTAs for every SM's resident slots (shared memory and TMEM)
+  int occ = 0;
+  MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wgrad, kConvThreads, smem));
+  const int cols = 3 * N <= 32 ? 32 : (3 * N <= 64 ? 64 : (3 * N <= 128 ? 128 : (3 * N <= 256 ? 256 : 512)));
+  occ = std::max(1, std::min(occ, 512 / cols));
+  int chunks = std::max(1, std::min(a.items, (2 * occ * u->nsm) / std::max(1, nsg * nct)));
   a.per_cta = (a.items + chunks - 1) / chunks;
   chunks = (a.items + a.per_cta - 1) / a.per_cta;
-  const int SB = wgrad_stage_bytes(N);
-  a.S = std::max(2, std::min(4, (200 * 1024) / SB));
   a.dW = dW; a.cin = cin;
   a.err = u->err;
-  if (int e = ensure_attrs(u->device)) return e;
   dim3 grid(nsg, nct, chunks);
-  k_wgrad<<<grid, kConvThreads, a.S * SB, u->stream>>>(a);
+  k_wgrad<<<grid, kConvThreads, smem, u->stream>>>(a);
   return launch_err("k_wgrad");
 }
 

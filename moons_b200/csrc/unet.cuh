@@ -315,7 +315,16 @@ struct WgradArgs {
   int* err;
 };
 
-__host__ __device__ inline int wgrad_stage_bytes(int N) { return 16 * kWRows * 16 + N * 256; }
+// one stage: the nreal staged input planes, then the dOut tile; the rows of
+// the 16 - nreal padded plane groups read past them (into the dOut tile or
+// the next stage), and past the last stage into wgrad_tail_bytes of padding
+__host__ __device__ inline int wgrad_stage_bytes(int N, int nreal) {
+  return (nreal * kWRows * 16 + N * 256 + 127) & ~127;
+}
+__host__ __device__ inline int wgrad_tail_bytes(int N, int nreal) {
+  const int t = 16 * kWRows * 16 - wgrad_stage_bytes(N, nreal);
+  return t > 0 ? ((t + 127) & ~127) : 0;
+}
 
 __global__ void __launch_bounds__(kConvThreads) k_wgrad(WgradArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -334,7 +343,8 @@ __global__ void __launch_bounds__(kConvThreads) k_wgrad(WgradArgs a) {
   const int cg0 = ct * a.ncg;
   const int cgT = a.cgA + a.cgB;
   const int ncg = min(a.ncg, cgT - cg0);
-  const int SB = wgrad_stage_bytes(N);
+  const int NR = a.nsh * a.ncg;                // staged planes per stage
+  const int SB = wgrad_stage_bytes(N, NR);
   const int APL = kWRows * 16;                 // bytes per staged input plane
   const uint32_t sbase = tc::smem_u32(smem);
   const int cols = 3 * N;
@@ -380,7 +390,7 @@ __global__ void __launch_bounds__(kConvThreads) k_wgrad(WgradArgs a) {
       }
       const long long vo = kGuard + (long long)z * g.PS + p0;
       for (int c = 0; c < N / 8; c++)
-        tc::bulk_g2s(st + 16 * APL + c * 2048, a.dout + c * gsE + vo * 8, 2048, bar);
+        tc::bulk_g2s(st + NR * APL + c * 2048, a.dout + c * gsE + vo * 8, 2048, bar);
     };
     const int pro = nit < S ? nit : S;
     for (int q = 0; q < pro; q++) issue(q);
@@ -393,7 +403,7 @@ __global__ void __launch_bounds__(kConvThreads) k_wgrad(WgradArgs a) {
       if (!ok) break;
       tc::tc_fence_after();
       const uint32_t st = sbase + s * SB;
-      const uint32_t sB = st + 16 * APL;
+      const uint32_t sB = st + NR * APL;
 #pragma unroll 1
       for (int dx = 0; dx < 3; dx++) {
 #pragma unroll 1
