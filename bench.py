@@ -383,6 +383,38 @@ def at_scale_steps(G, small=False, steps=3):
     return out
 
 
+def full_bc_steps(G, small=False, steps=5):
+    """The reference's full_BC case: lid-driven MHD cavity on the mesh bank's
+    full_BC_w_vacuum_3D meshes (fluid 80 x 85 x 80, induction mesh with
+    walls and vacuum 140 x 127 x 140), Re = 2000, Ha = 100, Rem = 2000,
+    dt = 2.5e-3, the case's PCG limits (U 5, p 20, B 20, phi 20 iterations,
+    tol_rel 1e-6), plain FP64 Jacobi-PCG and FP32 V-cycle Poisson solves."""
+    from moons_b200 import configs
+    kw = dict(N=12, N_w=3) if small else {}
+    out = {}
+    for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED)):
+        sim = configs.make(G, configs.full_bc, seed=0, prec_poisson=prec, **kw)
+        sim.step(1)  # warm-up (graphs)
+        ms, its, divb = 0.0, {}, []
+        for _ in range(steps):
+            info = sim.step(1)
+            ms += info["ms"]
+            for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+                its[k] = its.get(k, 0) + info[k] / steps
+            divb.append(sim.divergence()[1])
+        out[name] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps, "iters_per_step": its,
+                     "div_B_l2sq_max": max(divb)}
+        if name == "plain_fp64":
+            sm, si = sim.shape(G.MHD_U, 0), sim.shape(G.MHD_B, 0)
+        del sim
+    out["speedup_mixed_vs_plain"] = out["plain_fp64"]["ms_per_step"] / out["mixed_fp32_vcycle"]["ms_per_step"]
+    out["workload"] = (f"full_BC case (mesh bank full_BC_w_vacuum_3D): fluid {sm[0] - 3}x{sm[1] - 2}x{sm[2] - 2} "
+                       f"cells in an induction mesh of {si[0] - 3}x{si[1] - 2}x{si[2] - 2} (walls sigma=1, vacuum "
+                       f"sigma=1e-3), Re=2000, Ha=100, Rem=2000, dt=2.5e-3, PCG caps U5/p20/B20/phi20 at tol 1e-6; "
+                       f"{steps} steps after 1 warm-up step")
+    return out
+
+
 def cpu_sample(kw, gpu_iters=None):
     """Bounded CPU sample: the oracle (single thread) on the full-size duct.
     It times init + one step with every PCG capped at a few iterations, and
@@ -522,6 +554,7 @@ def main():
                                 seeds_mg=2 if args.small else 16)
     mxinfo, _ = poisson_ms(G, kw, G.PREC_MG_MIXED)
     scale5 = at_scale_steps(G, small=args.small)
+    fullbc = full_bc_steps(G, small=args.small)
     learned = learned_poisson(G, n=32 if args.small else 128, shell=2 if args.small else 4,
                               ntrain=4 if args.small else 8, held=(1000,) if args.small else (1000, 1001, 1002))
     alg_bytes = 88.0 * ncc * pinfo["iterations"]  # 88 B per cell per FP64 PCG iteration (algorithmic)
@@ -571,6 +604,7 @@ def main():
             "poisson_sigma_shell": shell,
             "poisson_learned": learned,
             "at_scale": scale5,
+            "full_bc_vacuum": fullbc,
             "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (duct fluid mesh)",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -13,12 +13,20 @@ the CPU oracle, so both see identical inputs.
   periodic streamwise, mean pressure gradient, finite Rem, solve_method 6),
   Roberts two-sided clustering (robertsBoth, beta=1.05) across, and a
   conducting wall layer in the induction mesh (MD_sigma/MD_fluid split).
+* ``full_bc`` -- the reference's full_BC case (sim_params_default_full_BC):
+  lid-driven MHD cavity on the mesh bank's full_BC_w_vacuum_3D meshes
+  (boundary-layer clustered fluid, thin conducting walls, vacuum out to
+  |x| = 7), finite Rem, B form, sigma = 1 in fluid and walls and
+  sig_local_over_sig_f outside them.
 """
 from __future__ import annotations
+
+import math
 
 import numpy as np
 
 from . import capi as G
+from . import mesh_bank as mb
 from . import mesh_gen as mg
 
 ORDER_LDC = (5, 6, 1, 2, 3, 4)   # get_apply_BC_order for periodic_dir = 0 (sim_params_aux.f90:41)
@@ -189,6 +197,75 @@ def ldc_energy(n: int = 16, Pe: float = 100.0, Gr_Re2: float = 10.0, heating: fl
             sim.upload(G.MHD_GRAVITY, c, g)
 
     return mom, ind, prm, init
+
+
+def sigma_inv_edges(ind, sigma, sig_local: float):
+    """1/sigma on the induction mesh's edges as set_sigma_inv_VF sets it
+    (solvers/induction/induction_aux.f90:178-194): 1/sig_local_over_sig_f
+    everywhere, then 1 embedded over the conductor mesh's physical overlap
+    (edge along c: the shared cells along c, the shared nodes, boundary nodes
+    included, along the other two directions)."""
+    rng = mg.sub_domain_ranges(sigma, ind)
+    out = []
+    for c in range(3):
+        shape = tuple(len(ind[d]) - 1 if d == c else len(ind[d]) for d in range(3))
+        si = np.full(shape, 1.0 / sig_local)
+        sl = tuple(slice(*rng[d][0]) if d == c else slice(*rng[d][1]) for d in range(3))
+        si[sl] = 1.0
+        out.append(si)
+    return out
+
+
+def full_bc(N: int = 80, N_w: int = 9, vacuum: bool = True, Re: float = 2000.0, N_stuart: float = 5.0,
+            Rem: float = 2000.0, dt: float = 2.5e-3, sig_local: float = 1e-3, tol: float = 1e-6,
+            tol_abs: float = 1e-13, iter_max=(5, 20, 20, 20), noise: float = 0.0, mqp=None):
+    """sim_params_default_full_BC: Re = 2000, N = 5 (Ha = sqrt(N Re) = 100),
+    Rem = 2000 with finite_Rem, dt = 2.5e-3, the lid-driven cavity
+    (U preset 1: LDC_at_ymax), B0 = 1 along z (uniform_B0_dir = 3), B = 0 on
+    the induction mesh's outer boundary (B preset 0: Dirichlet), Neumann
+    pressure, Dirichlet potential, prescribed BCs on U* and B*, solve
+    method 6, PCG limits U 5, p 20, B 20, phi 20 iterations at tol_rel 1e-6,
+    tol_abs 1e-13.  Meshes from the mesh bank (full_BC_w_vacuum_3D, or
+    full_BC_n_vacuum_3D with ``vacuum=False``) at N and N_w; the fluid sits
+    in the induction mesh at the offset the sub-domain overlap finds.
+    ``iter_max`` = (U, p, B, phi)."""
+    Ha = math.sqrt(N_stuart * Re)
+    ms = (mb.full_bc_w_vacuum_3d if vacuum else mb.full_bc_n_vacuum_3d)(N, N_w, mqp)
+    m = mb.generate(ms, Re, Ha)
+    off = mg.sub_domain_offset(m.mom, m.ind)
+    prm = G.MHDParams()
+    prm.dt = dt
+    prm.induction = G.IND_B
+    _coeffs(prm, Re, Ha, Rem, True)
+    prm.mpg_dir = 0
+    prm.mpg_scale = 0.0
+    for name, it in zip(("isp_U", "isp_p", "isp_B", "isp_phi"), iter_max):
+        setattr(prm, name, G.isp(it, tol, tol_abs, 1))
+    for c in range(3):
+        vals = [0.0] * 6
+        if c == 0:
+            vals[3] = 1.0  # LDC_at_ymax
+        prm.bc_U[c] = G.bc_spec([G.DIRICHLET] * 6, values=vals, order=ORDER_LDC)
+        prm.bc_B[c] = G.bc_spec([G.DIRICHLET] * 6, order=ORDER_LDC)
+    prm.bc_p = G.bc_spec([G.NEUMANN] * 6, order=ORDER_LDC, all_neumann=True)
+    prm.bc_phi = G.bc_spec([G.DIRICHLET] * 6, order=ORDER_LDC)
+    prm.prescribed_Ustar = 1
+    prm.prescribed_Bstar = 1
+    for d in range(3):
+        prm.ind_offset[d] = off[d]
+    si = sigma_inv_edges(m.ind, m.sigma, sig_local)
+
+    def init(sim, rng):
+        for c in range(3):
+            s = sim.shape(G.MHD_U, c)
+            sim.upload(G.MHD_U, c, rng.normal(0.0, noise, s) if noise > 0 else np.zeros(s))
+            b0 = np.zeros(sim.shape(G.MHD_B0, c))
+            if c == 2:
+                b0[:] = 1.0  # uniform_B_field dir = 3
+            sim.upload(G.MHD_B0, c, b0)
+            sim.upload(G.MHD_SIGMA_INV, c, si[c])
+
+    return m.mom, m.ind, prm, init
 
 
 def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, **kw):
