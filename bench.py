@@ -383,35 +383,41 @@ def at_scale_steps(G, small=False, steps=3):
     return out
 
 
-def full_bc_steps(G, small=False, steps=5):
+def full_bc_steps(G, small=False, steps=5, steps_tol=2):
     """The reference's full_BC case: lid-driven MHD cavity on the mesh bank's
     full_BC_w_vacuum_3D meshes (fluid 80 x 85 x 80, induction mesh with
     walls and vacuum 140 x 127 x 140), Re = 2000, Ha = 100, Rem = 2000,
-    dt = 2.5e-3, the case's PCG limits (U 5, p 20, B 20, phi 20 iterations,
-    tol_rel 1e-6), plain FP64 Jacobi-PCG and FP32 V-cycle Poisson solves."""
+    dt = 2.5e-3.  Two settings: the case's own PCG limits (U 5, p 20, B 20,
+    phi 20 iterations at tol_rel 1e-6), and the same tolerance without the
+    iteration caps; each with plain FP64 Jacobi-PCG and with FP32 V-cycle
+    Poisson solves."""
     from moons_b200 import configs
     kw = dict(N=12, N_w=3) if small else {}
     out = {}
-    for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED)):
-        sim = configs.make(G, configs.full_bc, seed=0, prec_poisson=prec, **kw)
-        sim.step(1)  # warm-up (graphs)
-        ms, its, divb = 0.0, {}, []
-        for _ in range(steps):
-            info = sim.step(1)
-            ms += info["ms"]
-            for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
-                its[k] = its.get(k, 0) + info[k] / steps
-            divb.append(sim.divergence()[1])
-        out[name] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps, "iters_per_step": its,
-                     "div_B_l2sq_max": max(divb)}
-        if name == "plain_fp64":
+    for setting, extra, nst in (("case_caps", {}, steps), ("to_tol_1e-6", dict(iter_max=(20000,) * 4), steps_tol)):
+        res = {}
+        for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED)):
+            sim = configs.make(G, configs.full_bc, seed=0, prec_poisson=prec, **kw, **extra)
+            sim.step(1)  # warm-up (graphs)
+            ms, its, divb = 0.0, {}, []
+            for _ in range(nst):
+                info = sim.step(1)
+                ms += info["ms"]
+                for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+                    its[k] = its.get(k, 0) + info[k] / nst
+                divb.append(sim.divergence()[1])
+            res[name] = {"steps_per_s": nst / (ms / 1e3), "ms_per_step": ms / nst, "iters_per_step": its,
+                         "res_p_last": info["res_p"], "res_phi_last": info["res_phi"], "div_B_l2sq_max": max(divb)}
             sm, si = sim.shape(G.MHD_U, 0), sim.shape(G.MHD_B, 0)
-        del sim
-    out["speedup_mixed_vs_plain"] = out["plain_fp64"]["ms_per_step"] / out["mixed_fp32_vcycle"]["ms_per_step"]
+            del sim
+        res["speedup_mixed_vs_plain"] = res["plain_fp64"]["ms_per_step"] / res["mixed_fp32_vcycle"]["ms_per_step"]
+        res["steps"] = nst
+        out[setting] = res
     out["workload"] = (f"full_BC case (mesh bank full_BC_w_vacuum_3D): fluid {sm[0] - 3}x{sm[1] - 2}x{sm[2] - 2} "
                        f"cells in an induction mesh of {si[0] - 3}x{si[1] - 2}x{si[2] - 2} (walls sigma=1, vacuum "
-                       f"sigma=1e-3), Re=2000, Ha=100, Rem=2000, dt=2.5e-3, PCG caps U5/p20/B20/phi20 at tol 1e-6; "
-                       f"{steps} steps after 1 warm-up step")
+                       f"sigma=1e-3), Re=2000, Ha=100, Rem=2000, dt=2.5e-3; case_caps: the case's PCG limits "
+                       f"U5/p20/B20/phi20 at tol 1e-6; to_tol_1e-6: the same tolerance without caps; timed steps "
+                       f"after 1 warm-up step")
     return out
 
 

@@ -9,8 +9,12 @@
 // the FP32 rounding inside the V-cycle cannot stall the recurrence.
 // Supported: one CC unknown (pressure, potential) with LAP_UNIFORM or
 // LAP_PROPS and Dirichlet / Neumann / periodic BCs.  Each level halves every
-// axis whose interior cell count is even and >= 4 and keeps the others
-// (semi-coarsening), until no axis can be halved.
+// axis with at least 4 interior cells (periodic axes: an even count) and
+// keeps the others (semi-coarsening), until no axis can be halved: fine
+// cells are merged in pairs from the low end; an odd count leaves its last
+// fine cell as a coarse cell of its own.  An odd count on a periodic axis of
+// the finest mesh works but weakens the smoother (same-colour neighbours
+// across the seam).
 #include <array>
 
 #include "mgrid.cuh"
@@ -39,8 +43,7 @@ struct MGHier {
   double* rprev = nullptr;  // flexible CG: previous residual
   // coarsest level: dense inverse (direct solve) when small enough
   int ncoarse = 0;
-  double* cinv_d = nullptr;
-  float* cinv_f = nullptr;
+  double* cinv_d = nullptr;  // coarsest-level inverse (FP64 for both variants)
   std::vector<void*> allocs;
   ~MGHier() {
     for (void* p : allocs) cudaFree(p);
@@ -71,15 +74,26 @@ std::vector<T> conv(const std::vector<double>& v) {
 }
 
 // coarse node coordinates (with ghost nodes) keeping every other fine node
-std::vector<double> coarsen_nodes(const std::vector<double>& hn) {
+// from the first physical one, and the last physical node (an odd cell
+// count leaves its last fine cell unpaired).  Ghost cells mirror the end
+// cells, or on a periodic axis take the size of the periodic partner (the
+// cell at the other end), so that both sides of the seam see the same
+// centre distance and the coarse operator stays symmetric.
+std::vector<double> coarsen_nodes(const std::vector<double>& hn, bool periodic) {
   const int sn = (int)hn.size();
   std::vector<double> c;
   c.push_back(0.0);
-  for (int i = 1; i <= sn - 2; i += 2) c.push_back(hn[i]);
+  int last = 0;
+  for (int i = 1; i <= sn - 2; i += 2) {
+    c.push_back(hn[i]);
+    last = i;
+  }
+  if (last != sn - 2) c.push_back(hn[sn - 2]);
   c.push_back(0.0);
   const int m = (int)c.size();
-  c[0] = c[1] - (c[2] - c[1]);
-  c[m - 1] = c[m - 2] + (c[m - 2] - c[m - 3]);
+  const double h_first = c[2] - c[1], h_last = c[m - 2] - c[m - 3];
+  c[0] = c[1] - (periodic ? h_last : h_first);
+  c[m - 1] = c[m - 2] + (periodic ? h_first : h_last);
   return c;
 }
 
@@ -122,8 +136,15 @@ Axis1D build_axis(const host::HostCoord& cc, int scf, int tlo, int thi, bool coa
     a.w0[f] = 1.0;
     cols[f].push_back({f, 1.0});
   }
+  const bool odd = ((scf - 2) & 1) != 0;
   for (int f = 2; f <= scf - 1 && coarsened; f++) {
     const int I = (f + 2) / 2;
+    if (odd && f == scf - 1) {  // unpaired last cell: same centre as its coarse cell
+      a.i0[f] = a.i1[f] = I;
+      a.w0[f] = 1.0;
+      cols[I].push_back({f, 1.0});
+      continue;
+    }
     int nb;
     double wp, wn;
     if ((f & 1) == 0) {  // left child: face I-1|I
@@ -189,12 +210,14 @@ std::vector<double> coarsen_faces(const std::vector<double>& kf, int d, const st
         }
         if (!inner) continue;
         int F[3];
-        F[d] = cz[d] ? 2 * C[d] - 2 : C[d];  // coincident fine node
+        // coincident fine node (the last physical node closes an unpaired cell)
+        F[d] = cz[d] ? std::min(2 * C[d] - 2, ef[d] - 1) : C[d];
         double num = 0.0, den = 0.0;
         for (int u = 0; u < (cz[a] ? 2 : 1); u++)
           for (int v = 0; v < (cz[b] ? 2 : 1); v++) {
             F[a] = cz[a] ? 2 * C[a] - 2 + u : C[a];
             F[b] = cz[b] ? 2 * C[b] - 2 + v : C[b];
+            if (F[a] > sf[a] - 1 || F[b] > sf[b] - 1) continue;  // no second child
             const double w = cf[a].dhn[F[a]] * cf[b].dhn[F[b]];
             num += w * kf[fid(F[0], F[1], F[2])];
             den += w;
@@ -302,8 +325,15 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
   std::array<int, 3> s0 = {m->sn[0] - 1, m->sn[1] - 1, m->sn[2] - 1};
   for (int d = 0; d < 3; d++) C[d].push_back(host::build_coord(m->hn[d].data(), m->sn[d]));
   h->s.push_back(s0);
-  // each level halves every axis whose interior count is even and >= 4 (the
-  // others are kept), until no axis can be halved
+  int bt[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int f = 1; f <= 6; f++) bt[f] = bc.defined ? bc.type[f] : MOONS_BC_NEUMANN;
+  // each level halves every axis with at least 4 interior cells (the others
+  // are kept), until no axis can be halved.  A periodic axis is halved only
+  // while its count is even: on an odd periodic ring the red-black colouring
+  // gives the two seam cells the same colour, so the sweeps would update
+  // neighbours together there
+  bool per[3];
+  for (int d = 0; d < 3; d++) per[d] = bt[2 * d + 1] == MOONS_BC_PERIODIC || bt[2 * d + 2] == MOONS_BC_PERIODIC;
   std::vector<std::array<bool, 3>> coarsened(1, std::array<bool, 3>{false, false, false});
   for (;;) {
     const auto& sl = h->s.back();
@@ -311,7 +341,7 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
     bool any = false;
     for (int d = 0; d < 3; d++) {
       const int N = sl[d] - 2;
-      cz[d] = N >= 4 && (N & 1) == 0;
+      cz[d] = N >= 4 && (!per[d] || (N & 1) == 0);
       any = any || cz[d];
     }
     // small enough for the dense direct solve: stop
@@ -321,7 +351,7 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
     for (int d = 0; d < 3; d++) {
       const std::vector<double>& hf = C[d].back().hn;  // 1-based
       std::vector<double> h0(hf.begin() + 1, hf.end());
-      std::vector<double> hc = cz[d] ? coarsen_nodes(h0) : h0;
+      std::vector<double> hc = cz[d] ? coarsen_nodes(h0, per[d]) : h0;
       C[d].push_back(host::build_coord(hc.data(), (int)hc.size()));
       sc[d] = (int)hc.size() - 1;
     }
@@ -329,8 +359,6 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
     coarsened.push_back(cz);
   }
   h->nl = (int)h->s.size();
-  int bt[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int f = 1; f <= 6; f++) bt[f] = bc.defined ? bc.type[f] : MOONS_BC_NEUMANN;
   // face coefficients per level (LAP_PROPS)
   std::vector<std::array<std::vector<double>, 3>> K(h->nl);
   if (kf) {
@@ -425,8 +453,12 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
       std::vector<double> inv;
       if (invert(A, n, inv)) {
         h->ncoarse = n;
-        if (!h->mixed) h->cinv_d = dev_copy(h.get(), inv, st);
-        else h->cinv_f = dev_copy(h.get(), conv<float>(inv), st);
+        // stored transposed (column c contiguous over rows) so the direct-solve
+        // kernel's threads read consecutive entries
+        std::vector<double> invT((size_t)n * n);
+        for (int r = 0; r < n; r++)
+          for (int c = 0; c < n; c++) invT[(size_t)c * n + r] = inv[(size_t)r * n + c];
+        h->cinv_d = dev_copy(h.get(), invT, st);
       }
     }
   }
@@ -542,17 +574,14 @@ bool mg_is_mixed(const MGHier* h) { return h && h->mixed; }
 double* mg_rprev(MGHier* h) { return h->rprev; }
 
 namespace {
+// coarsest levels up to this many cells are swept by one block
+constexpr size_t kCoarseOneBlock = 8192;
+
 // grid-stride kernels: at most one resident wave
 unsigned vgrid(size_t n, int occ = 8, int nsm = 148) {
   return (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)occ * nsm));
 }
 
-template <typename T>
-const T* coarse_inv(const MGHier* h);
-template <>
-const double* coarse_inv<double>(const MGHier* h) { return h->cinv_d; }
-template <>
-const float* coarse_inv<float>(const MGHier* h) { return h->cinv_f; }
 
 template <typename T>
 int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::array<MGProl<T>, 3>>& P,
@@ -570,11 +599,22 @@ int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::a
     MG_LAUNCH(k_mg_restrict<T>, vgrid(npts(l + 1), h->occ[2], h->nsm), 256, st, L[l], L[l + 1], R[l + 1][0],
               R[l + 1][1], R[l + 1][2], S);
   }
-  if (h->ncoarse > 0)
-    MG_LAUNCH(k_mg_direct<T>, (unsigned)((h->ncoarse + 255) / 256), 256, st, L[nl - 1], coarse_inv<T>(h), h->ncoarse,
-              S);
-  else
+  if (h->ncoarse > 0) {
+    MG_LAUNCH(k_mg_direct<T>, (unsigned)((h->ncoarse + 255) / 256), 256, st, L[nl - 1], (const double*)h->cinv_d,
+              h->ncoarse, S);
+  } else if (npts(nl - 1) <= kCoarseOneBlock) {
     MG_LAUNCH(k_mg_coarse<T>, 1, 256, st, L[nl - 1], h->sweeps_coarse, S);
+  } else {  // large coarsest level (the level cap): the same sweeps, grid-wide
+    const unsigned g = vgrid(npts(nl - 1) / 2 + 1, h->occ[0], h->nsm);
+    for (int q = 0; q < h->sweeps_coarse; q++) {
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 0, q == 0 ? 1 : 0, (T)1, S);
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 1, 0, (T)1, S);
+    }
+    for (int q = 0; q < h->sweeps_coarse; q++) {
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 1, 0, (T)1, S);
+      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 0, 0, (T)1, S);
+    }
+  }
   for (int l = nl - 2; l >= 0; l--) {  // up: prolong + correct, post-smooth (reverse colours)
     const unsigned g = vgrid(npts(l) / 2 + 1, h->occ[0], h->nsm);
     MG_LAUNCH(k_mg_prolong<T>, vgrid(npts(l), h->occ[3], h->nsm), 256, st, L[l], L[l + 1], P[l + 1][0], P[l + 1][1],

@@ -334,19 +334,22 @@ __global__ void __launch_bounds__(256) k_mg_coarse(MGLev<T> L, int sweeps, const
 
 // coarsest level solved directly: e = Minv r over the n interior cells
 // (Minv: the inverse of the level's operator, regularised on the constant
-// mode when no face is Dirichlet; built on the host)
+// mode when no face is Dirichlet; built on the host and stored transposed,
+// Minv[c * n + row] = inverse(row, c)).  Minv and the sum are
+// FP64 on every level type: a stretched, high-contrast coarsest operator can
+// have a condition number at which an FP32 inverse is no solve at all.
 template <typename T>
-__global__ void __launch_bounds__(256) k_mg_direct(MGLev<T> L, const T* Minv, int n, const PcgScalars* S) {
+__global__ void __launch_bounds__(256) k_mg_direct(MGLev<T> L, const double* Minv, int n, const PcgScalars* S) {
   if (S && S->done) return;
   const int nx = L.s0 - 2, ny = L.s1 - 2;
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    T acc = T(0);
+    double acc = 0.0;
     for (int c = 0; c < n; c++) {
       const int i = c % nx + 2, q = c / nx, j = q % ny + 2, k = q / ny + 2;
-      acc = acc + Minv[(size_t)c * n + row] * L.r[lidx(L, i, j, k)];  // symmetric: coalesced over rows
+      acc += Minv[(size_t)c * n + row] * (double)L.r[lidx(L, i, j, k)];  // Minv stored transposed
     }
     const int i = row % nx + 2, q = row / nx, j = q % ny + 2, k = q / ny + 2;
-    L.e[lidx(L, i, j, k)] = acc;
+    L.e[lidx(L, i, j, k)] = (T)acc;
   }
 }
 

@@ -66,6 +66,11 @@ CASES = [
     ((16, 8, 32), [NEUMANN, NEUMANN, NEUMANN, NEUMANN, PERIODIC, PERIODIC], True),
     ((16, 16, 8), [DIRICHLET, DIRICHLET, NEUMANN, NEUMANN, NEUMANN, DIRICHLET], False),
     ((8, 16, 16), [PERIODIC, PERIODIC, DIRICHLET, NEUMANN, PERIODIC, PERIODIC], False),
+    # odd cell counts: pairs plus one unpaired cell per coarsening
+    ((15, 9, 13), [NEUMANN] * 6, True),
+    ((13, 8, 21), [NEUMANN, NEUMANN, NEUMANN, NEUMANN, PERIODIC, PERIODIC], True),
+    ((9, 17, 7), [DIRICHLET, DIRICHLET, NEUMANN, NEUMANN, NEUMANN, DIRICHLET], False),
+    ((12, 17, 10), [PERIODIC, PERIODIC, DIRICHLET, NEUMANN, PERIODIC, PERIODIC], False),
 ]
 
 
