@@ -353,12 +353,13 @@ def learned_poisson(G, n=128, shell=4, ntrain=8, held=(1000, 1001, 1002), epochs
 def at_scale_steps(G, small=False, steps=3):
     """Configuration 5: the finite-Rem (constrained transport) MHD step on
     256 x 128 x 128 cells, plain FP64 Jacobi-PCG Poisson solves vs FP32
-    V-cycle flexible CG; div(B) after every step, and the two runs' fields
-    against each other after the last step (same seed, same tolerances)."""
+    V-cycle flexible CG vs the direct fast-diagonalization solve in CG;
+    div(B) after every step, and the runs' fields against the plain one's
+    after the last step (same seed, same tolerances)."""
     from moons_b200 import configs
     kw = dict(nx=16, ny=16, nz=32) if small else {}
     out, fields = {}, {}
-    for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED)):
+    for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED), ("fd_direct", G.PREC_FD)):
         sim = configs.make(G, configs.at_scale, seed=0, prec_poisson=prec, **kw)
         sim.step(1)  # warm-up (graphs)
         divb, ms, its = [], 0.0, {}
@@ -376,6 +377,9 @@ def at_scale_steps(G, small=False, steps=3):
               for a, b in zip(fields["mixed_fp32_vcycle"], fields["plain_fp64"]))
     out["mixed_vs_plain_fields_max_rel_l2"] = rel
     out["speedup_mixed_vs_plain"] = out["plain_fp64"]["ms_per_step"] / out["mixed_fp32_vcycle"]["ms_per_step"]
+    out["speedup_fd_vs_plain"] = out["plain_fp64"]["ms_per_step"] / out["fd_direct"]["ms_per_step"]
+    out["fd_vs_plain_fields_max_rel_l2"] = max(
+        float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)) for a, b in zip(fields["fd_direct"], fields["plain_fp64"]))
     n = kw.get("nx", 128), kw.get("ny", 128), kw.get("nz", 256)
     out["workload"] = (f"finite-Rem MHD with constrained transport, {n[0]}x{n[1]}x{n[2]} cells (Roberts-stretched "
                        f"cross-section), Re=1000, Ha=500, Rem=10, dt=2e-4; {steps} steps after 1 warm-up step "
@@ -389,14 +393,14 @@ def full_bc_steps(G, small=False, steps=5, steps_tol=2):
     walls and vacuum 140 x 127 x 140), Re = 2000, Ha = 100, Rem = 2000,
     dt = 2.5e-3.  Two settings: the case's own PCG limits (U 5, p 20, B 20,
     phi 20 iterations at tol_rel 1e-6), and the same tolerance without the
-    iteration caps; each with plain FP64 Jacobi-PCG and with FP32 V-cycle
-    Poisson solves."""
+    iteration caps; each with plain FP64 Jacobi-PCG, with FP32 V-cycle and
+    with direct fast-diagonalization Poisson solves."""
     from moons_b200 import configs
     kw = dict(N=12, N_w=3) if small else {}
     out = {}
     for setting, extra, nst in (("case_caps", {}, steps), ("to_tol_1e-6", dict(iter_max=(20000,) * 4), steps_tol)):
         res = {}
-        for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED)):
+        for name, prec in (("plain_fp64", 0), ("mixed_fp32_vcycle", G.PREC_MG_MIXED), ("fd_direct", G.PREC_FD)):
             sim = configs.make(G, configs.full_bc, seed=0, prec_poisson=prec, **kw, **extra)
             sim.step(1)  # warm-up (graphs)
             ms, its, divb = 0.0, {}, []
@@ -411,6 +415,7 @@ def full_bc_steps(G, small=False, steps=5, steps_tol=2):
             sm, si = sim.shape(G.MHD_U, 0), sim.shape(G.MHD_B, 0)
             del sim
         res["speedup_mixed_vs_plain"] = res["plain_fp64"]["ms_per_step"] / res["mixed_fp32_vcycle"]["ms_per_step"]
+        res["speedup_fd_vs_plain"] = res["plain_fp64"]["ms_per_step"] / res["fd_direct"]["ms_per_step"]
         res["steps"] = nst
         out[setting] = res
     out["workload"] = (f"full_BC case (mesh bank full_BC_w_vacuum_3D): fluid {sm[0] - 3}x{sm[1] - 2}x{sm[2] - 2} "
@@ -552,6 +557,13 @@ def main():
     msx = max_over_ranks(infox["ms"], dist)
     value_mixed = replica_rate(world, args.steps, msx)
     del simx
+    # ... and with the direct (fast-diagonalization) pressure / potential solves
+    simf = configs.make(G, configs.duct, seed=rank, prec_poisson=G.PREC_FD, **kw)
+    simf.step(args.warmup)
+    infof = simf.step(args.steps)
+    msf = max_over_ranks(infof["ms"], dist)
+    value_fd = replica_rate(world, args.steps, msf)
+    del simf
 
     # ---- Poisson ms to 1e-10 + roofline of the pressure PCG iteration
     pinfo, ncc = poisson_ms(G, kw)
@@ -559,6 +571,7 @@ def main():
     shell = sigma_shell_poisson(G, n=32 if args.small else 128, seeds_plain=1 if args.small else 4,
                                 seeds_mg=2 if args.small else 16)
     mxinfo, _ = poisson_ms(G, kw, G.PREC_MG_MIXED)
+    fdinfo, _ = poisson_ms(G, kw, G.PREC_FD)
     scale5 = at_scale_steps(G, small=args.small)
     fullbc = full_bc_steps(G, small=args.small)
     learned = learned_poisson(G, n=32 if args.small else 128, shell=2 if args.small else 4,
@@ -600,13 +613,20 @@ def main():
             "steps_per_s_mixed_poisson": {"value": value_mixed, "per_step": {k: infox[k] / max(args.steps, 1) for k in (
                 "iters_U", "iters_p", "iters_B", "iters_phi")}, "note": "pressure and potential solves by FP64 "
                 "flexible CG + FP32 multigrid (MOONS_PREC_MG_MIXED); everything else as in value"},
+            "steps_per_s_fd_poisson": {"value": value_fd, "per_step": {k: infof[k] / max(args.steps, 1) for k in (
+                "iters_U", "iters_p", "iters_B", "iters_phi")}, "note": "pressure and cleaning-potential solves "
+                "by CG with the direct fast-diagonalization solve of the separable operator (MOONS_PREC_FD); "
+                "everything else as in value"},
             "poisson": {"ms_to_1e-10": pinfo["ms"], "iterations": pinfo["iterations"], "rel": pinfo["rel"],
                         "cells": ncc, "solver": "FP64 Jacobi-PCG (reference algorithm)",
                         "mg_fp64": {"ms_to_1e-10": mginfo["ms"], "iterations": mginfo["iterations"],
                                     "rel": mginfo["rel"], "solver": "CG + FP64 multigrid V(2,2), red-black SOR 1.15"},
                         "mixed": {"ms_to_1e-10": mxinfo["ms"], "iterations": mxinfo["iterations"],
                                   "rel": mxinfo["rel"], "solver": "FP64 flexible CG + FP32 multigrid V(2,2), red-black SOR 1.15"},
-                        "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"]},
+                        "fd": {"ms_to_1e-10": fdinfo["ms"], "iterations": fdinfo["iterations"],
+                               "rel": fdinfo["rel"], "solver": "FP64 CG + direct fast-diagonalization solve"},
+                        "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"],
+                        "speedup_fd_vs_plain": pinfo["ms"] / fdinfo["ms"]},
             "poisson_sigma_shell": shell,
             "poisson_learned": learned,
             "at_scale": scale5,

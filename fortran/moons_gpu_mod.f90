@@ -21,6 +21,7 @@ module moons_gpu_mod
   integer(c_int), parameter :: MOONS_PREC_IDENTITY = 0, MOONS_PREC_LAP = 1
   integer(c_int), parameter :: MOONS_PREC_MOM = 2, MOONS_PREC_IND = 3
   integer(c_int), parameter :: MOONS_PREC_MG = 4, MOONS_PREC_MG_MIXED = 5, MOONS_PREC_UNET = 6
+  integer(c_int), parameter :: MOONS_PREC_FD = 7
 
   type, bind(C) :: moons_bc_spec
     integer(c_int) :: type(6)

@@ -111,9 +111,14 @@ enum {
    * compiled V-cycle (code_not_compiled/9.6.2017/MG/MG.f90:241-396). */
   MOONS_PREC_MG = 4,          /* FP64 V-cycle inside CG                      */
   MOONS_PREC_MG_MIXED = 5,    /* FP32 V-cycle inside FP64 flexible CG         */
-  MOONS_PREC_UNET = 6         /* learned: the U-Net (moons_pcg_set_unet) inside
+  MOONS_PREC_UNET = 6,        /* learned: the U-Net (moons_pcg_set_unet) inside
                                  FP64 flexible CG, FP32 V-cycle as the fallback
                                  when 10 iterations fail to halve the residual */
+  /* Direct solve of the separable operator by fast diagonalization (one CC
+   * unknown, LAP_UNIFORM, Dirichlet/Neumann/periodic BCs): the B200 form of
+   * the reference's FFT Poisson (FFT_poisson.f90:107-189, solve_method 9),
+   * exact for stretched meshes too; CG converges in one or two iterations. */
+  MOONS_PREC_FD = 7
 };
 
 typedef struct moons_mesh moons_mesh;
@@ -255,7 +260,10 @@ typedef struct {
                                solves: 0 (default) = the reference's prec_Lap,
                                or MOONS_PREC_MG / MOONS_PREC_MG_MIXED (no
                                reference counterpart: same system, same exit
-                               tests, far fewer iterations)                   */
+                               tests, far fewer iterations), or MOONS_PREC_FD
+                               (direct solve of the separable pressure and
+                               cleaning potential; the sigma-weighted potential
+                               of the low-Rem form takes MG_MIXED)            */
   /* energy equation (energy_extend.f90:236-262, add_all_energy_sources.f90:
    * 21-67), solved on the induction mesh before the momentum step as
    * solve_MOONS does (MOONS_solver.f90:81-85); fields MOONS_MHD_T, _KT,

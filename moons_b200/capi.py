@@ -26,6 +26,7 @@ DIRICHLET, NEUMANN, PERIODIC, ROBIN = 1, 2, 3, 4
 OP_LAP_UNIFORM, OP_LAP_PROPS, OP_IND_DIFFUSION, OP_MOM_DIFFUSION, OP_NRG_DIFFUSION = 1, 2, 3, 4, 5
 PREC_IDENTITY, PREC_LAP, PREC_MOM, PREC_IND = 0, 1, 2, 3
 PREC_MG, PREC_MG_MIXED = 4, 5  # multigrid V-cycle in CG (FP64) / in flexible CG (FP32 V-cycle)
+PREC_FD = 7  # direct solve of the separable Poisson operator (fast diagonalization) in CG
 PREC_UNET = 6  # learned U-Net in flexible CG, FP32 V-cycle fallback (PCG.set_unet)
 
 

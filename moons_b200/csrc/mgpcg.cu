@@ -44,6 +44,16 @@ struct MGHier {
   // coarsest level: dense inverse (direct solve) when small enough
   int ncoarse = 0;
   double* cinv_d = nullptr;  // coarsest-level inverse (FP64 for both variants)
+  // MOONS_PREC_FD: fast diagonalization of the separable operator instead of
+  // a V-cycle (interior extents, per-axis transforms and eigenvalues, two
+  // interior-sized work arrays)
+  bool fd = false;
+  int fn[3] = {0, 0, 0};
+  double *fwd[3] = {nullptr, nullptr, nullptr}, *bwd[3] = {nullptr, nullptr, nullptr};
+  double *fwdT0 = nullptr, *bwdT0 = nullptr;
+  double* lam[3] = {nullptr, nullptr, nullptr};
+  double lam_tol = 0.0;
+  double *w0 = nullptr, *w1 = nullptr;
   std::vector<void*> allocs;
   ~MGHier() {
     for (void* p : allocs) cudaFree(p);
@@ -629,14 +639,338 @@ int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::a
 }
 }  // namespace
 
+int fd_apply(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S);
+
 // z = V(r) on the PCG's fine level (z, r: FP64 PCG arrays)
 int mg_vcycle(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
+  if (h->fd) return fd_apply(h, z, r, st, S);
   if (!h->mixed) return vcycle_t<double>(h, h->Ld, h->Pd, h->Rd, st, S);
   const size_t n = r.n();
   MG_LAUNCH((k_mg_cast<float, double>), vgrid(n), 256, st, h->Lf[0].r, (const double*)r.f, n, S);
   int rc = vcycle_t<float>(h, h->Lf, h->Pf, h->Rf, st, S);
   if (rc) return rc;
   MG_LAUNCH((k_mg_cast<double, float>), vgrid(n), 256, st, z.f, (const float*)h->Lf[0].e, n, S);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MOONS_PREC_FD: direct solve of the separable constant-coefficient operator
+// by fast diagonalization (Lynch, Rice & Thomas, Numer. Math. 6, 1964).
+//
+// The PCG's LAP_UNIFORM operator on a CC field is A = V (Lx (+) Ly (+) Lz):
+// V = vx (x) vy (x) vz the cell volumes, L_d the 1-D two-gradient second
+// difference of axis d with its homogeneous BC folded in (Neumann: ghost =
+// first cell, Dirichlet: minus it, periodic: the opposite cell).  v_d L_d is
+// symmetric, so M_d = v_d^{1/2} L_d v_d^{-1/2} = W_d Lam_d W_d^T with W_d
+// orthogonal, and
+//   A^{-1} b = (B_x (x) B_y (x) B_z) diag(1 / (lx_a + ly_b + lz_c)) (F_x (x) F_y (x) F_z) b,
+//   F_d = W_d^T v_d^{-1/2},  B_d = v_d^{-1/2} W_d,
+// with the zero mode of an all-Neumann/periodic problem set to zero.  The
+// eigen-decomposition (implicit QL on the tridiagonal M_d; cyclic Jacobi
+// rotations, Golub & Van Loan 8.4, on a periodic axis) runs once on the host
+// at create time; each application is six dense 1-D
+// transforms (mode products) and one diagonal scaling on the device.  As
+// the preconditioner of the reference's CG recurrence it makes the solve
+// converge in one or two iterations, to the same tolerance and solution.
+// ---------------------------------------------------------------------------
+namespace {
+
+// symmetric eigen-decomposition by cyclic Jacobi: A (n x n, row-major) ->
+// eigenvalues w and eigenvectors as the columns of V (row-major)
+void jacobi_eigen(std::vector<double> A, int n, std::vector<double>& w, std::vector<double>& V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+  double tot = 0.0;
+  for (double v : A) tot += v * v;
+  for (int sweep = 0; sweep < 60; sweep++) {
+    double off = 0.0;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) off += A[(size_t)p * n + q] * A[(size_t)p * n + q];
+    if (off <= 1e-32 * tot) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double apq = A[(size_t)p * n + q];
+        if (apq == 0.0) continue;
+        const double tau = (A[(size_t)q * n + q] - A[(size_t)p * n + p]) / (2.0 * apq);
+        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+        const double c = 1.0 / std::sqrt(1.0 + t * t), sn = t * c;
+        for (int k = 0; k < n; k++) {  // A <- A J
+          const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+          A[(size_t)k * n + p] = c * akp - sn * akq;
+          A[(size_t)k * n + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < n; k++) {  // A <- J^T A
+          const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+          A[(size_t)p * n + k] = c * apk - sn * aqk;
+          A[(size_t)q * n + k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < n; k++) {  // V <- V J
+          const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+          V[(size_t)k * n + p] = c * vkp - sn * vkq;
+          V[(size_t)k * n + q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+  w.resize(n);
+  for (int i = 0; i < n; i++) w[i] = A[(size_t)i * n + i];
+}
+
+// symmetric tridiagonal eigen-decomposition by the implicit QL iteration
+// with Wilkinson shifts (Bowdler, Martin, Reinsch & Wilkinson, Numer. Math.
+// 11, 1968): diagonal d, off-diagonal e (e[i] couples i and i+1) ->
+// eigenvalues in d, eigenvectors as the columns of V (row-major); false
+// when an eigenvalue needs more than 60 sweeps
+bool tridiag_ql(std::vector<double> d, std::vector<double> e, int n, std::vector<double>& w, std::vector<double>& V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+  e.resize(n, 0.0);
+  e[n - 1] = 0.0;
+  for (int l = 0; l < n; l++) {
+    for (int iter = 0;; iter++) {
+      int m = l;
+      for (; m < n - 1; m++) {
+        const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= 1e-16 * dd) break;
+      }
+      if (m == l) break;
+      if (iter >= 60) return false;
+      // shift from the leading 2x2 block's eigenvalue closer to d[l]
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = std::hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+      double sn = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      bool split = false;
+      for (; i >= l; i--) {  // chase the bulge from the bottom of the block up
+        const double f = sn * e[i], b = c * e[i];
+        r = std::hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {  // the block splits: deflate and restart
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          split = true;
+          break;
+        }
+        sn = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * sn + 2.0 * c * b;
+        p = sn * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
+        for (int k = 0; k < n; k++) {  // accumulate the rotation in the vectors
+          const double vi = V[(size_t)k * n + i], vi1 = V[(size_t)k * n + i + 1];
+          V[(size_t)k * n + i + 1] = sn * vi + c * vi1;
+          V[(size_t)k * n + i] = c * vi - sn * vi1;
+        }
+      }
+      if (split) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  w = d;
+  return true;
+}
+
+// the 1-D operator L of one CC axis over its interior cells (row a = cell
+// a + 2), homogeneous BCs folded in; vol = the cells' widths
+bool axis_operator(const host::HostCoord& c, int s, int tlo, int thi, std::vector<double>& L, std::vector<double>& vol) {
+  const int n = s - 2;
+  L.assign((size_t)n * n, 0.0);
+  vol.assign(n, 0.0);
+  for (int t = 2; t <= s - 1; t++) {
+    const int a = t - 2;
+    vol[a] = c.dhn[t];
+    const double cm = c.cc2nD[t - 1] * c.n2ccD[t];
+    const double c0 = c.cc2nU[t - 1] * c.n2ccD[t] + c.cc2nD[t] * c.n2ccU[t];
+    const double cp = c.cc2nU[t] * c.n2ccU[t];
+    L[(size_t)a * n + a] += c0;
+    for (int side = 0; side < 2; side++) {
+      int nb = side == 0 ? t - 1 : t + 1;
+      double w = side == 0 ? cm : cp;
+      if (nb == 1 || nb == s) {
+        const int ty = nb == 1 ? tlo : thi;
+        if (ty == MOONS_BC_PERIODIC) nb = nb == 1 ? s - 1 : 2;
+        else if (ty == MOONS_BC_NEUMANN) nb = t;
+        else if (ty == MOONS_BC_DIRICHLET) { nb = t; w = -w; }
+        else return false;
+      }
+      L[(size_t)a * n + (nb - 2)] += w;
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(256) k_fd_gather(const double* __restrict__ r, int s0, int s1, double* __restrict__ T,
+                                                   int nx, int ny, int nz, const PcgScalars* S) {
+  if (S && S->done) return;
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx);
+    const size_t q = t / nx;
+    const int j = (int)(q % ny), k = (int)(q / ny);
+    T[t] = r[(size_t)(i + 1) + (size_t)s0 * ((size_t)(j + 1) + (size_t)s1 * (size_t)(k + 1))];
+  }
+}
+__global__ void __launch_bounds__(256) k_fd_scatter(double* __restrict__ z, int s0, int s1, const double* __restrict__ T,
+                                                    int nx, int ny, int nz, const PcgScalars* S) {
+  if (S && S->done) return;
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx);
+    const size_t q = t / nx;
+    const int j = (int)(q % ny), k = (int)(q / ny);
+    z[(size_t)(i + 1) + (size_t)s0 * ((size_t)(j + 1) + (size_t)s1 * (size_t)(k + 1))] = T[t];
+  }
+}
+// out = F applied along one axis of the interior tensor (x fastest).  Axis 0
+// reads F transposed (FT[m * nx + a]) so that a warp's consecutive outputs
+// read consecutive entries; axes 1 and 2 read F[a * n + m], one row per warp.
+__global__ void __launch_bounds__(256) k_fd_mode(const double* __restrict__ in, double* __restrict__ out,
+                                                 const double* __restrict__ F, int nx, int ny, int nz, int axis,
+                                                 const PcgScalars* S) {
+  if (S && S->done) return;
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx);
+    const size_t q = t / nx;
+    const int j = (int)(q % ny), k = (int)(q / ny);
+    double acc = 0.0;
+    if (axis == 0) {
+      const double* col = in + (size_t)nx * q;
+      for (int m = 0; m < nx; m++) acc += F[(size_t)m * nx + i] * col[m];
+    } else if (axis == 1) {
+      const double* row = F + (size_t)j * ny;
+      const double* base = in + i + (size_t)nx * ny * k;
+      for (int m = 0; m < ny; m++) acc += row[m] * base[(size_t)nx * m];
+    } else {
+      const double* row = F + (size_t)k * nz;
+      const double* base = in + i + (size_t)nx * j;
+      const size_t st = (size_t)nx * ny;
+      for (int m = 0; m < nz; m++) acc += row[m] * base[st * m];
+    }
+    out[t] = acc;
+  }
+}
+__global__ void __launch_bounds__(256) k_fd_scale(double* __restrict__ T, const double* __restrict__ lx,
+                                                  const double* __restrict__ ly, const double* __restrict__ lz, int nx,
+                                                  int ny, int nz, double tol, const PcgScalars* S) {
+  if (S && S->done) return;
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx);
+    const size_t q = t / nx;
+    const int j = (int)(q % ny), k = (int)(q / ny);
+    const double l = lx[i] + ly[j] + lz[k];
+    T[t] = std::fabs(l) <= tol ? 0.0 : T[t] / l;
+  }
+}
+
+}  // namespace
+
+int fd_build(moons_pcg* s, moons_mesh* m, const DBC& bc, MGHier** out) {
+  (void)s;
+  *out = nullptr;
+  auto h = std::make_unique<MGHier>();
+  h->fd = true;
+  cudaStream_t st = m->stream;
+  int bt[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int f = 1; f <= 6; f++) bt[f] = bc.defined ? bc.type[f] : MOONS_BC_NEUMANN;
+  double lmax = 0.0;
+  for (int d = 0; d < 3; d++) {
+    const host::HostCoord c = host::build_coord(m->hn[d].data(), m->sn[d]);
+    const int sc = m->sn[d] - 1, n = sc - 2;
+    h->fn[d] = n;
+    std::vector<double> L, vol;
+    if (n < 1 || !axis_operator(c, sc, bt[2 * d + 1], bt[2 * d + 2], L, vol)) {
+      set_error("fast diagonalization: each axis needs interior cells and Dirichlet/Neumann/periodic BCs");
+      return MOONS_ERR_ARG;
+    }
+    // symmetric form M = v^{1/2} L v^{-1/2}; the operator must be symmetric
+    // in the volume-weighted sense (true for any node distribution, and for
+    // periodic axes whose two end cells have the same width)
+    std::vector<double> M((size_t)n * n);
+    double mmax = 0.0, asym = 0.0;
+    for (int a = 0; a < n; a++)
+      for (int b = 0; b < n; b++) {
+        M[(size_t)a * n + b] = std::sqrt(vol[a]) * L[(size_t)a * n + b] / std::sqrt(vol[b]);
+        mmax = std::max(mmax, std::fabs(M[(size_t)a * n + b]));
+      }
+    for (int a = 0; a < n; a++)
+      for (int b = a + 1; b < n; b++) {
+        const double x = M[(size_t)a * n + b], y = M[(size_t)b * n + a];
+        asym = std::max(asym, std::fabs(x - y));
+        M[(size_t)a * n + b] = M[(size_t)b * n + a] = 0.5 * (x + y);
+      }
+    if (asym > 1e-10 * mmax) {
+      set_error("fast diagonalization: the axis operator is not symmetric (periodic axis with unequal end cells)");
+      return MOONS_ERR_ARG;
+    }
+    std::vector<double> w, W;
+    if (bt[2 * d + 1] == MOONS_BC_PERIODIC || bt[2 * d + 2] == MOONS_BC_PERIODIC) {
+      jacobi_eigen(M, n, w, W);  // cyclic: corner entries
+    } else {
+      std::vector<double> dg(n), od(n, 0.0);
+      for (int a = 0; a < n; a++) dg[a] = M[(size_t)a * n + a];
+      for (int a = 0; a + 1 < n; a++) od[a] = M[(size_t)a * n + a + 1];
+      if (!tridiag_ql(dg, od, n, w, W)) {
+        set_error("fast diagonalization: the tridiagonal eigen-iteration did not converge");
+        return MOONS_ERR_ARG;
+      }
+    }
+    std::vector<double> F((size_t)n * n), B((size_t)n * n), FT((size_t)n * n), BT((size_t)n * n);
+    for (int a = 0; a < n; a++)
+      for (int b = 0; b < n; b++) {
+        F[(size_t)a * n + b] = W[(size_t)b * n + a] / std::sqrt(vol[b]);  // W^T v^{-1/2}
+        B[(size_t)a * n + b] = W[(size_t)a * n + b] / std::sqrt(vol[a]);  // v^{-1/2} W
+      }
+    for (int a = 0; a < n; a++)
+      for (int b = 0; b < n; b++) {
+        FT[(size_t)b * n + a] = F[(size_t)a * n + b];
+        BT[(size_t)b * n + a] = B[(size_t)a * n + b];
+      }
+    for (double v : w) lmax = std::max(lmax, std::fabs(v));
+    h->lam[d] = dev_copy(h.get(), w, st);
+    if (d == 0) {
+      h->fwdT0 = dev_copy(h.get(), FT, st);
+      h->bwdT0 = dev_copy(h.get(), BT, st);
+    } else {
+      h->fwd[d] = dev_copy(h.get(), F, st);
+      h->bwd[d] = dev_copy(h.get(), B, st);
+    }
+    if (!h->lam[d] || (d == 0 ? !h->fwdT0 || !h->bwdT0 : !h->fwd[d] || !h->bwd[d])) return MOONS_ERR_NOMEM;
+  }
+  h->lam_tol = 1e-12 * lmax;
+  const size_t nint = (size_t)h->fn[0] * h->fn[1] * h->fn[2];
+  h->w0 = dev_zeros<double>(h.get(), nint, st);
+  h->w1 = dev_zeros<double>(h.get(), nint, st);
+  if (!h->w0 || !h->w1) return MOONS_ERR_NOMEM;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+  h->nsm = std::max(nsm, 1);
+  MG_CUDA(cudaStreamSynchronize(st));
+  *out = h.release();
+  return MOONS_OK;
+}
+
+int fd_apply(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
+  const int nx = h->fn[0], ny = h->fn[1], nz = h->fn[2];
+  const size_t n = (size_t)nx * ny * nz;
+  const unsigned g = vgrid(n, 8, h->nsm);
+  double *a = h->w0, *b = h->w1;
+  MG_LAUNCH(k_fd_gather, g, 256, st, (const double*)r.f, r.s0, r.s1, a, nx, ny, nz, S);
+  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)a, b, (const double*)h->fwdT0, nx, ny, nz, 0, S);
+  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)b, a, (const double*)h->fwd[1], nx, ny, nz, 1, S);
+  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)a, b, (const double*)h->fwd[2], nx, ny, nz, 2, S);
+  MG_LAUNCH(k_fd_scale, g, 256, st, b, (const double*)h->lam[0], (const double*)h->lam[1], (const double*)h->lam[2], nx,
+            ny, nz, h->lam_tol, S);
+  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)b, a, (const double*)h->bwdT0, nx, ny, nz, 0, S);
+  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)a, b, (const double*)h->bwd[1], nx, ny, nz, 1, S);
+  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)b, a, (const double*)h->bwd[2], nx, ny, nz, 2, S);
+  MG_LAUNCH(k_fd_scatter, g, 256, st, z.f, z.s0, z.s1, (const double*)a, nx, ny, nz, S);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }

@@ -691,8 +691,10 @@ int moons_mhd_init(moons_mhd* s) {
     moons_sf* xbu[3] = {s->U[0], s->U[1], s->U[2]};
     if ((r = moons_pcg_create(m, MOONS_OP_MOM_DIFFUSION, MOONS_PREC_MOM, 3, s->Ustar, xbu, nullptr, &s->pcgU))) return r;
     moons_sf* xp[1] = {s->p};
-    const int pp = s->P.prec_poisson == MOONS_PREC_MG || s->P.prec_poisson == MOONS_PREC_MG_MIXED ? s->P.prec_poisson
-                                                                                                : MOONS_PREC_LAP;
+    const int pq = s->P.prec_poisson;
+    const int pp = pq == MOONS_PREC_MG || pq == MOONS_PREC_MG_MIXED || pq == MOONS_PREC_FD ? pq : MOONS_PREC_LAP;
+    // the sigma-weighted potential solve is not separable: multigrid under FD
+    const int pv = pp == MOONS_PREC_FD ? MOONS_PREC_MG_MIXED : pp;
     if ((r = moons_pcg_create(m, MOONS_OP_LAP_UNIFORM, pp, 1, xp, xp, nullptr, &s->pcgP))) return r;
     if (s->P.induction == MOONS_IND_B) {
       if ((r = moons_pcg_create(s->mi, MOONS_OP_IND_DIFFUSION, MOONS_PREC_IND, 3, s->Bstar, s->B, s->sig, &s->pcgB)))
@@ -701,7 +703,7 @@ int moons_mhd_init(moons_mhd* s) {
       if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_UNIFORM, pp, 1, xf, xf, nullptr, &s->pcgPhi))) return r;
     } else if (s->P.induction == MOONS_IND_POTENTIAL) {
       moons_sf* xf[1] = {s->phi};
-      if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_PROPS, pp, 1, xf, xf, s->sig, &s->pcgPhi))) return r;
+      if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_PROPS, pv, 1, xf, xf, s->sig, &s->pcgPhi))) return r;
     }
     if (s->P.energy && s->P.solve_method_T == 3) {
       // init(nrg%PCG_T, nrg_diffusion, nrg_diffusion_explicit, prec_lap_SF, ...) (energy_extend.f90:129)

@@ -193,6 +193,7 @@ int unet_prepare(moons_unet* u);
 moons_mesh* unet_mesh(moons_unet* u);
 }  // namespace mg
 int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const mg::DBC& bc, const mg::DF* kf, MGHier** out);
+int fd_build(moons_pcg* s, moons_mesh* m, const mg::DBC& bc, MGHier** out);
 void mg_free(MGHier* h);
 int mg_vcycle(MGHier* h, mg::DF z, mg::DF r, cudaStream_t st, const mg::PcgScalars* S);
 double* mg_rprev(MGHier* h);
@@ -340,7 +341,7 @@ int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
 int compute_prec(moons_pcg* s) {
   moons_mesh* m = s->m;
   int mode = s->prec;
-  if (mode == MOONS_PREC_MG || mode == MOONS_PREC_MG_MIXED || mode == MOONS_PREC_UNET)
+  if (mode == MOONS_PREC_MG || mode == MOONS_PREC_MG_MIXED || mode == MOONS_PREC_UNET || mode == MOONS_PREC_FD)
     mode = MOONS_PREC_IDENTITY;  // Minv unused
   DF dummy{};
   if (mode == MOONS_PREC_IND && s->op != MOONS_OP_IND_DIFFUSION) {
@@ -576,7 +577,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: ncomp must be 1 or 3");
     return MOONS_ERR_ARG;
   }
-  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_NRG_DIFFUSION || prec < 0 || prec > MOONS_PREC_UNET) {
+  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_NRG_DIFFUSION || prec < 0 || prec > MOONS_PREC_FD) {
     set_error("moons_pcg_create: bad operator/preconditioner");
     return MOONS_ERR_ARG;
   }
@@ -589,9 +590,10 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: operator needs three coefficient fields");
     return MOONS_ERR_ARG;
   }
-  const bool use_mg = prec == MOONS_PREC_MG || prec == MOONS_PREC_MG_MIXED || prec == MOONS_PREC_UNET;
+  const bool use_mg =
+      prec == MOONS_PREC_MG || prec == MOONS_PREC_MG_MIXED || prec == MOONS_PREC_UNET || prec == MOONS_PREC_FD;
   if (use_mg) {
-    bool ok = nc == 1 && (op == MOONS_OP_LAP_UNIFORM || op == MOONS_OP_LAP_PROPS) && x[0] &&
+    bool ok = nc == 1 && (op == MOONS_OP_LAP_UNIFORM || (op == MOONS_OP_LAP_PROPS && prec != MOONS_PREC_FD)) && x[0] &&
               x[0]->f.dl == MOONS_CC;
     if (ok && x[0]->bc.defined)
       for (int f = 1; f <= 6; f++) {
@@ -599,8 +601,11 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
         if (t != MOONS_BC_DIRICHLET && t != MOONS_BC_NEUMANN && t != MOONS_BC_PERIODIC) ok = false;
       }
     if (!ok) {
-      set_error("moons_pcg_create: multigrid needs one CC unknown, LAP_UNIFORM or LAP_PROPS, and "
-                "Dirichlet/Neumann/periodic BCs");
+      set_error(prec == MOONS_PREC_FD
+                    ? "moons_pcg_create: fast diagonalization needs one CC unknown, LAP_UNIFORM, and "
+                      "Dirichlet/Neumann/periodic BCs"
+                    : "moons_pcg_create: multigrid needs one CC unknown, LAP_UNIFORM or LAP_PROPS, and "
+                      "Dirichlet/Neumann/periodic BCs");
       return MOONS_ERR_ARG;
     }
   }
@@ -697,7 +702,9 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     }
   }
   if (!r && use_mg) {
-    r = mg_build(s, m, prec != MOONS_PREC_MG, s->x_bc[0], op == MOONS_OP_LAP_PROPS ? s->k : nullptr, &s->mgh);
+    r = prec == MOONS_PREC_FD
+            ? fd_build(s, m, s->x_bc[0], &s->mgh)
+            : mg_build(s, m, prec != MOONS_PREC_MG, s->x_bc[0], op == MOONS_OP_LAP_PROPS ? s->k : nullptr, &s->mgh);
     s->learned = prec == MOONS_PREC_UNET;
     if (r == MOONS_ERR_NOMEM) set_error("moons_pcg_create: device allocation failed (multigrid levels)");
   }

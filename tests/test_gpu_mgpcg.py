@@ -90,3 +90,25 @@ def test_mgpcg_matches_jacobi_pcg(n, bctypes, alln, prec, props):
         b = b - b.mean()
     err = np.abs(a - b).max() / np.abs(b).max()
     assert err < 1e-7, err
+
+
+@pytest.mark.parametrize("n,bctypes,alln", CASES)
+def test_fast_diagonalization_is_a_direct_solve(n, bctypes, alln):
+    """MOONS_PREC_FD: the separable operator's exact inverse as the
+    preconditioner; CG stops after one or two iterations at the tolerance
+    with the Jacobi-PCG solution."""
+    ig, io, xg, xo, alln = solve_pair(n, bctypes, alln, G.PREC_FD)
+    assert ig["exit_reason"] == 1 and io["exit_reason"] == 1, (ig, io)
+    assert ig["rel"] < 1e-10
+    assert abs(ig["res0"] - io["res0"]) <= 1e-12 * io["res0"]
+    assert ig["iterations"] <= 3, ig
+    a, b = interior(xg), interior(xo)
+    if alln:
+        a = a - a.mean()
+        b = b - b.mean()
+    assert np.abs(a - b).max() / np.abs(b).max() < 1e-7
+
+
+def test_fast_diagonalization_needs_a_separable_operator():
+    with pytest.raises(G.MoonsError):
+        solve_pair((8, 8, 8), [NEUMANN] * 6, True, G.PREC_FD, props=True)

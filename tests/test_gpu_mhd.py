@@ -67,7 +67,7 @@ def test_mhd_steps_match_oracle(name, builder, kw):
         assert abs(ig[k] - io[k]) <= nsteps, (k, ig, io)
 
 
-@pytest.mark.parametrize("prec", [G.PREC_MG, G.PREC_MG_MIXED], ids=["mg", "mixed"])
+@pytest.mark.parametrize("prec", [G.PREC_MG, G.PREC_MG_MIXED, G.PREC_FD], ids=["mg", "mixed", "fd"])
 @pytest.mark.parametrize("name,builder,kw", [CASES[0], CASES[2], CASES[4]], ids=[CASES[0][0], CASES[2][0], CASES[4][0]])
 def test_mhd_steps_multigrid_poisson(name, builder, kw, prec):
     """The step with multigrid-preconditioned pressure/potential solves reaches
