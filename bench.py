@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="moons", choices=["moons", "reference"])
     ap.add_argument("--small", action="store_true", help="small mesh (debug only)")
-    ap.add_argument("--profile", choices=["step", "jacobi", "mg", "mixed", "unet", "unet_train"], default=None,
+    ap.add_argument("--profile", choices=["step", "jacobi", "mg", "mixed", "fd", "unet", "unet_train"], default=None,
                     help="profiling run for ncu launch lists: one duct step, one duct pressure solve with the "
                          "given preconditioner capped at --profile-iters iterations, or --profile-iters U-Net "
                          "forward applies / training steps on the 128^3 sigma-shell grid; prints what ran, no "
@@ -82,7 +82,7 @@ def run_profile(args):
         print(json.dumps({"profile": args.profile, "workload": f"U-Net {n}^3", "iters": args.profile_iters}),
               flush=True)
         return
-    prec = {"jacobi": G.PREC_LAP, "mg": G.PREC_MG, "mixed": G.PREC_MG_MIXED}[args.profile]
+    prec = {"jacobi": G.PREC_LAP, "mg": G.PREC_MG, "mixed": G.PREC_MG_MIXED, "fd": G.PREC_FD}[args.profile]
     mom, _, prm, _ = configs.duct(**kw)
     m = G.Mesh(*mom)
     p = m.field(G.CC)

@@ -50,7 +50,6 @@ struct MGHier {
   bool fd = false;
   int fn[3] = {0, 0, 0};
   double *fwd[3] = {nullptr, nullptr, nullptr}, *bwd[3] = {nullptr, nullptr, nullptr};
-  double *fwdT0 = nullptr, *bwdT0 = nullptr;
   double* lam[3] = {nullptr, nullptr, nullptr};
   double lam_tol = 0.0;
   double *w0 = nullptr, *w1 = nullptr;
@@ -826,34 +825,67 @@ __global__ void __launch_bounds__(256) k_fd_scatter(double* __restrict__ z, int 
     z[(size_t)(i + 1) + (size_t)s0 * ((size_t)(j + 1) + (size_t)s1 * (size_t)(k + 1))] = T[t];
   }
 }
-// out = F applied along one axis of the interior tensor (x fastest).  Axis 0
-// reads F transposed (FT[m * nx + a]) so that a warp's consecutive outputs
-// read consecutive entries; axes 1 and 2 read F[a * n + m], one row per warp.
-__global__ void __launch_bounds__(256) k_fd_mode(const double* __restrict__ in, double* __restrict__ out,
-                                                 const double* __restrict__ F, int nx, int ny, int nz, int axis,
-                                                 const PcgScalars* S) {
+// One axis transform of the interior tensor (x fastest) as a tiled FP64 GEMM,
+// C (R x Cn, column-major) = X (R x K) Y (K x Cn), 64 x 64 outputs per block,
+// 4 x 4 per thread, K in steps of 16 through shared memory:
+//  LEFT  (axis 0):    X = F (row-major K x K), Y = the tensor as K x (ny nz)
+//  RIGHT (axes 1, 2): X = the tensor slice as R x K (leading dim R, batch
+//                     blockIdx.z at stride R K), Y = F^T (F row-major)
+constexpr int kFT = 64, kFK = 16;
+template <bool LEFT>
+__global__ void __launch_bounds__(256) k_fd_gemm(const double* __restrict__ T, const double* __restrict__ F,
+                                                 double* __restrict__ C, int R, int Cn, int K, const PcgScalars* S) {
   if (S && S->done) return;
-  const size_t n = (size_t)nx * ny * nz;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % nx);
-    const size_t q = t / nx;
-    const int j = (int)(q % ny), k = (int)(q / ny);
-    double acc = 0.0;
-    if (axis == 0) {
-      const double* col = in + (size_t)nx * q;
-      for (int m = 0; m < nx; m++) acc += F[(size_t)m * nx + i] * col[m];
-    } else if (axis == 1) {
-      const double* row = F + (size_t)j * ny;
-      const double* base = in + i + (size_t)nx * ny * k;
-      for (int m = 0; m < ny; m++) acc += row[m] * base[(size_t)nx * m];
-    } else {
-      const double* row = F + (size_t)k * nz;
-      const double* base = in + i + (size_t)nx * j;
-      const size_t st = (size_t)nx * ny;
-      for (int m = 0; m < nz; m++) acc += row[m] * base[st * m];
+  __shared__ double Xs[kFK][kFT + 1];
+  __shared__ double Ys[kFK][kFT + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int r0 = blockIdx.x * kFT, c0 = blockIdx.y * kFT;
+  const size_t boff = (size_t)blockIdx.z * (size_t)R * (size_t)K;  // RIGHT: batch of slices
+  double acc[4][4] = {};
+  for (int m0 = 0; m0 < K; m0 += kFK) {
+    for (int e = threadIdx.x; e < kFK * kFT; e += 256) {
+      // X tile: element (kk, r)
+      if (LEFT) {  // F row-major: kk fastest across threads
+        const int kk = e % kFK, r = e / kFK;
+        const int gr = r0 + r, gk = m0 + kk;
+        Xs[kk][r] = (gr < R && gk < K) ? F[(size_t)gr * K + gk] : 0.0;
+      } else {  // tensor slice, column-major: r fastest
+        const int r = e % kFT, kk = e / kFT;
+        const int gr = r0 + r, gk = m0 + kk;
+        Xs[kk][r] = (gr < R && gk < K) ? T[boff + (size_t)gr + (size_t)R * gk] : 0.0;
+      }
+      // Y tile: element (kk, c)
+      {
+        const int kk = e % kFK, c = e / kFK;
+        const int gc = c0 + c, gk = m0 + kk;
+        double v = 0.0;
+        if (gc < Cn && gk < K) v = LEFT ? T[(size_t)gk + (size_t)K * gc] : F[(size_t)gc * K + gk];
+        Ys[kk][c] = v;
+      }
     }
-    out[t] = acc;
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kFK; kk++) {
+      double xv[4], yv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) xv[u] = Xs[kk][tx + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 4; v++) yv[v] = Ys[kk][ty + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[u][v] += xv[u] * yv[v];
+    }
+    __syncthreads();
   }
+  const size_t coff = LEFT ? 0 : boff / (size_t)K * (size_t)Cn;  // RIGHT: batch of R x Cn slices
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const int gr = r0 + tx + 16 * u, gc = c0 + ty + 16 * v;
+      if (gr < R && gc < Cn) C[coff + (size_t)gr + (size_t)R * gc] = acc[u][v];
+    }
 }
 __global__ void __launch_bounds__(256) k_fd_scale(double* __restrict__ T, const double* __restrict__ lx,
                                                   const double* __restrict__ ly, const double* __restrict__ lz, int nx,
@@ -921,27 +953,17 @@ int fd_build(moons_pcg* s, moons_mesh* m, const DBC& bc, MGHier** out) {
         return MOONS_ERR_ARG;
       }
     }
-    std::vector<double> F((size_t)n * n), B((size_t)n * n), FT((size_t)n * n), BT((size_t)n * n);
+    std::vector<double> F((size_t)n * n), B((size_t)n * n);
     for (int a = 0; a < n; a++)
       for (int b = 0; b < n; b++) {
         F[(size_t)a * n + b] = W[(size_t)b * n + a] / std::sqrt(vol[b]);  // W^T v^{-1/2}
         B[(size_t)a * n + b] = W[(size_t)a * n + b] / std::sqrt(vol[a]);  // v^{-1/2} W
       }
-    for (int a = 0; a < n; a++)
-      for (int b = 0; b < n; b++) {
-        FT[(size_t)b * n + a] = F[(size_t)a * n + b];
-        BT[(size_t)b * n + a] = B[(size_t)a * n + b];
-      }
     for (double v : w) lmax = std::max(lmax, std::fabs(v));
     h->lam[d] = dev_copy(h.get(), w, st);
-    if (d == 0) {
-      h->fwdT0 = dev_copy(h.get(), FT, st);
-      h->bwdT0 = dev_copy(h.get(), BT, st);
-    } else {
-      h->fwd[d] = dev_copy(h.get(), F, st);
-      h->bwd[d] = dev_copy(h.get(), B, st);
-    }
-    if (!h->lam[d] || (d == 0 ? !h->fwdT0 || !h->bwdT0 : !h->fwd[d] || !h->bwd[d])) return MOONS_ERR_NOMEM;
+    h->fwd[d] = dev_copy(h.get(), F, st);
+    h->bwd[d] = dev_copy(h.get(), B, st);
+    if (!h->lam[d] || !h->fwd[d] || !h->bwd[d]) return MOONS_ERR_NOMEM;
   }
   h->lam_tol = 1e-12 * lmax;
   const size_t nint = (size_t)h->fn[0] * h->fn[1] * h->fn[2];
@@ -961,15 +983,23 @@ int fd_apply(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
   const size_t n = (size_t)nx * ny * nz;
   const unsigned g = vgrid(n, 8, h->nsm);
   double *a = h->w0, *b = h->w1;
+  const unsigned tiles = (unsigned)kFT;
+  // axis 0: (nx x nx) F times the tensor as nx x (ny nz)
+  const dim3 g0((nx + tiles - 1) / tiles, (unsigned)(((size_t)ny * nz + tiles - 1) / tiles), 1);
+  // axis 1: each z slice (nx x ny) times F^T
+  const dim3 g1((nx + tiles - 1) / tiles, (ny + tiles - 1) / tiles, (unsigned)nz);
+  // axis 2: the tensor as (nx ny) x nz times F^T
+  const dim3 g2((unsigned)(((size_t)nx * ny + tiles - 1) / tiles), (nz + tiles - 1) / tiles, 1);
+  const int nxy = nx * ny;
   MG_LAUNCH(k_fd_gather, g, 256, st, (const double*)r.f, r.s0, r.s1, a, nx, ny, nz, S);
-  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)a, b, (const double*)h->fwdT0, nx, ny, nz, 0, S);
-  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)b, a, (const double*)h->fwd[1], nx, ny, nz, 1, S);
-  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)a, b, (const double*)h->fwd[2], nx, ny, nz, 2, S);
+  MG_LAUNCH(k_fd_gemm<true>, g0, 256, st, (const double*)a, (const double*)h->fwd[0], b, nx, ny * nz, nx, S);
+  MG_LAUNCH(k_fd_gemm<false>, g1, 256, st, (const double*)b, (const double*)h->fwd[1], a, nx, ny, ny, S);
+  MG_LAUNCH(k_fd_gemm<false>, g2, 256, st, (const double*)a, (const double*)h->fwd[2], b, nxy, nz, nz, S);
   MG_LAUNCH(k_fd_scale, g, 256, st, b, (const double*)h->lam[0], (const double*)h->lam[1], (const double*)h->lam[2], nx,
             ny, nz, h->lam_tol, S);
-  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)b, a, (const double*)h->bwdT0, nx, ny, nz, 0, S);
-  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)a, b, (const double*)h->bwd[1], nx, ny, nz, 1, S);
-  MG_LAUNCH(k_fd_mode, g, 256, st, (const double*)b, a, (const double*)h->bwd[2], nx, ny, nz, 2, S);
+  MG_LAUNCH(k_fd_gemm<true>, g0, 256, st, (const double*)b, (const double*)h->bwd[0], a, nx, ny * nz, nx, S);
+  MG_LAUNCH(k_fd_gemm<false>, g1, 256, st, (const double*)a, (const double*)h->bwd[1], b, nx, ny, ny, S);
+  MG_LAUNCH(k_fd_gemm<false>, g2, 256, st, (const double*)b, (const double*)h->bwd[2], a, nxy, nz, nz, S);
   MG_LAUNCH(k_fd_scatter, g, 256, st, z.f, z.s0, z.s1, (const double*)a, nx, ny, nz, S);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
