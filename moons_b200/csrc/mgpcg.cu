@@ -51,7 +51,7 @@ struct MGHier {
   int fn[3] = {0, 0, 0};
   double *fwd[3] = {nullptr, nullptr, nullptr}, *bwd[3] = {nullptr, nullptr, nullptr};
   double* lam[3] = {nullptr, nullptr, nullptr};
-  double lam_tol = 0.0;
+  int zmode[3] = {-1, -1, -1};  // the constant mode's index per axis, all -1 if the operator is regular
   double *w0 = nullptr, *w1 = nullptr;
   std::vector<void*> allocs;
   ~MGHier() {
@@ -665,10 +665,11 @@ int mg_vcycle(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
 // orthogonal, and
 //   A^{-1} b = (B_x (x) B_y (x) B_z) diag(1 / (lx_a + ly_b + lz_c)) (F_x (x) F_y (x) F_z) b,
 //   F_d = W_d^T v_d^{-1/2},  B_d = v_d^{-1/2} W_d,
-// with the zero mode of an all-Neumann/periodic problem set to zero.  The
-// eigen-decomposition (implicit QL on the tridiagonal M_d; cyclic Jacobi
-// rotations, Golub & Van Loan 8.4, on a periodic axis) runs once on the host
-// at create time; each application is six dense 1-D
+// with the constant (zero) mode of an operator without a Dirichlet face
+// dropped.  The
+// eigen-decomposition (implicit QL on the tridiagonal M_d; on a periodic
+// axis, whose M_d has corner entries, after a Householder reduction to
+// tridiagonal form) runs once on the host at create time; each application is six dense 1-D
 // transforms (mode products) and one diagonal scaling on the device.  As
 // the preconditioner of the reference's CG recurrence it makes the solve
 // converge in one or two iterations, to the same tolerance and solution.
@@ -772,6 +773,82 @@ bool tridiag_ql(std::vector<double> d, std::vector<double> e, int n, std::vector
   }
   w = d;
   return true;
+}
+
+// Householder reduction of a symmetric matrix to tridiagonal form, A =
+// Q T Q^T (Golub & Van Loan, Alg. 8.3.1): diagonal d and off-diagonal e of
+// T, Q row-major.  Reflector k zeroes column k below the subdiagonal, applied
+// to the trailing block as the symmetric rank-2 update A -= v w^T + w v^T.
+void householder_tridiag(std::vector<double> A, int n, std::vector<double>& d, std::vector<double>& e,
+                         std::vector<double>& Q) {
+  Q.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) Q[(size_t)i * n + i] = 1.0;
+  std::vector<double> v(n), p(n), w(n);
+  for (int k = 0; k + 2 < n; k++) {
+    const int m = n - k - 1;  // length of the column part below the diagonal
+    double nrm = 0.0;
+    for (int i = 0; i < m; i++) nrm += A[(size_t)(k + 1 + i) * n + k] * A[(size_t)(k + 1 + i) * n + k];
+    nrm = std::sqrt(nrm);
+    if (nrm == 0.0) continue;
+    const double x0 = A[(size_t)(k + 1) * n + k];
+    const double alpha = x0 >= 0.0 ? -nrm : nrm;
+    for (int i = 0; i < m; i++) v[i] = A[(size_t)(k + 1 + i) * n + k];
+    v[0] -= alpha;
+    double vn = 0.0;
+    for (int i = 0; i < m; i++) vn += v[i] * v[i];
+    vn = std::sqrt(vn);
+    if (vn == 0.0) continue;
+    for (int i = 0; i < m; i++) v[i] /= vn;
+    // p = 2 A22 v, w = p - (v.p) v
+    double vp = 0.0;
+    for (int i = 0; i < m; i++) {
+      double acc = 0.0;
+      const double* row = &A[(size_t)(k + 1 + i) * n + (k + 1)];
+      for (int j = 0; j < m; j++) acc += row[j] * v[j];
+      p[i] = 2.0 * acc;
+      vp += v[i] * p[i];
+    }
+    for (int i = 0; i < m; i++) w[i] = p[i] - vp * v[i];
+    for (int i = 0; i < m; i++) {
+      double* row = &A[(size_t)(k + 1 + i) * n + (k + 1)];
+      for (int j = 0; j < m; j++) row[j] -= v[i] * w[j] + w[i] * v[j];
+    }
+    A[(size_t)(k + 1) * n + k] = A[(size_t)k * n + k + 1] = alpha;
+    for (int i = 1; i < m; i++) A[(size_t)(k + 1 + i) * n + k] = A[(size_t)k * n + k + 1 + i] = 0.0;
+    // Q <- Q H: Q[:, k+1:] -= 2 (Q[:, k+1:] v) v^T
+    for (int r = 0; r < n; r++) {
+      double* row = &Q[(size_t)r * n + (k + 1)];
+      double acc = 0.0;
+      for (int j = 0; j < m; j++) acc += row[j] * v[j];
+      acc *= 2.0;
+      for (int j = 0; j < m; j++) row[j] -= acc * v[j];
+    }
+  }
+  d.assign(n, 0.0);
+  e.assign(n, 0.0);
+  for (int i = 0; i < n; i++) d[i] = A[(size_t)i * n + i];
+  for (int i = 0; i + 1 < n; i++) e[i] = A[(size_t)i * n + i + 1];
+}
+
+// symmetric eigen-decomposition of a full matrix: Householder reduction,
+// then the QL iteration on T, eigenvectors Q V_T; cyclic Jacobi if the QL
+// iteration does not converge
+void symmetric_eigen(const std::vector<double>& A, int n, std::vector<double>& w, std::vector<double>& V) {
+  std::vector<double> d, e, Q, VT;
+  householder_tridiag(A, n, d, e, Q);
+  if (!tridiag_ql(d, e, n, w, VT)) {
+    jacobi_eigen(A, n, w, V);
+    return;
+  }
+  V.assign((size_t)n * n, 0.0);
+  for (int r = 0; r < n; r++)
+    for (int k = 0; k < n; k++) {
+      const double q = Q[(size_t)r * n + k];
+      if (q == 0.0) continue;
+      const double* vt = &VT[(size_t)k * n];
+      double* out = &V[(size_t)r * n];
+      for (int c = 0; c < n; c++) out[c] += q * vt[c];
+    }
 }
 
 // the 1-D operator L of one CC axis over its interior cells (row a = cell
@@ -887,17 +964,18 @@ __global__ void __launch_bounds__(256) k_fd_gemm(const double* __restrict__ T, c
       if (gr < R && gc < Cn) C[coff + (size_t)gr + (size_t)R * gc] = acc[u][v];
     }
 }
+// divide by the 3-D eigenvalue; (zi, zj, zk): the constant mode of an
+// operator without a Dirichlet face (dropped), or -1
 __global__ void __launch_bounds__(256) k_fd_scale(double* __restrict__ T, const double* __restrict__ lx,
                                                   const double* __restrict__ ly, const double* __restrict__ lz, int nx,
-                                                  int ny, int nz, double tol, const PcgScalars* S) {
+                                                  int ny, int nz, int zi, int zj, int zk, const PcgScalars* S) {
   if (S && S->done) return;
   const size_t n = (size_t)nx * ny * nz;
   for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(t % nx);
     const size_t q = t / nx;
     const int j = (int)(q % ny), k = (int)(q / ny);
-    const double l = lx[i] + ly[j] + lz[k];
-    T[t] = std::fabs(l) <= tol ? 0.0 : T[t] / l;
+    T[t] = (i == zi && j == zj && k == zk) ? 0.0 : T[t] / (lx[i] + ly[j] + lz[k]);
   }
 }
 
@@ -911,7 +989,6 @@ int fd_build(moons_pcg* s, moons_mesh* m, const DBC& bc, MGHier** out) {
   cudaStream_t st = m->stream;
   int bt[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int f = 1; f <= 6; f++) bt[f] = bc.defined ? bc.type[f] : MOONS_BC_NEUMANN;
-  double lmax = 0.0;
   for (int d = 0; d < 3; d++) {
     const host::HostCoord c = host::build_coord(m->hn[d].data(), m->sn[d]);
     const int sc = m->sn[d] - 1, n = sc - 2;
@@ -943,7 +1020,7 @@ int fd_build(moons_pcg* s, moons_mesh* m, const DBC& bc, MGHier** out) {
     }
     std::vector<double> w, W;
     if (bt[2 * d + 1] == MOONS_BC_PERIODIC || bt[2 * d + 2] == MOONS_BC_PERIODIC) {
-      jacobi_eigen(M, n, w, W);  // cyclic: corner entries
+      symmetric_eigen(M, n, w, W);  // cyclic: corner entries
     } else {
       std::vector<double> dg(n), od(n, 0.0);
       for (int a = 0; a < n; a++) dg[a] = M[(size_t)a * n + a];
@@ -959,13 +1036,20 @@ int fd_build(moons_pcg* s, moons_mesh* m, const DBC& bc, MGHier** out) {
         F[(size_t)a * n + b] = W[(size_t)b * n + a] / std::sqrt(vol[b]);  // W^T v^{-1/2}
         B[(size_t)a * n + b] = W[(size_t)a * n + b] / std::sqrt(vol[a]);  // v^{-1/2} W
       }
-    for (double v : w) lmax = std::max(lmax, std::fabs(v));
+    // an axis without a Dirichlet face has the constant as its zero mode:
+    // the eigenvalue of smallest magnitude
+    if (bt[2 * d + 1] != MOONS_BC_DIRICHLET && bt[2 * d + 2] != MOONS_BC_DIRICHLET) {
+      int z = 0;
+      for (int a = 1; a < n; a++)
+        if (std::fabs(w[a]) < std::fabs(w[z])) z = a;
+      h->zmode[d] = z;
+    }
     h->lam[d] = dev_copy(h.get(), w, st);
     h->fwd[d] = dev_copy(h.get(), F, st);
     h->bwd[d] = dev_copy(h.get(), B, st);
     if (!h->lam[d] || !h->fwd[d] || !h->bwd[d]) return MOONS_ERR_NOMEM;
   }
-  h->lam_tol = 1e-12 * lmax;
+  if (h->zmode[0] < 0 || h->zmode[1] < 0 || h->zmode[2] < 0) h->zmode[0] = h->zmode[1] = h->zmode[2] = -1;
   const size_t nint = (size_t)h->fn[0] * h->fn[1] * h->fn[2];
   h->w0 = dev_zeros<double>(h.get(), nint, st);
   h->w1 = dev_zeros<double>(h.get(), nint, st);
@@ -996,7 +1080,7 @@ int fd_apply(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
   MG_LAUNCH(k_fd_gemm<false>, g1, 256, st, (const double*)b, (const double*)h->fwd[1], a, nx, ny, ny, S);
   MG_LAUNCH(k_fd_gemm<false>, g2, 256, st, (const double*)a, (const double*)h->fwd[2], b, nxy, nz, nz, S);
   MG_LAUNCH(k_fd_scale, g, 256, st, b, (const double*)h->lam[0], (const double*)h->lam[1], (const double*)h->lam[2], nx,
-            ny, nz, h->lam_tol, S);
+            ny, nz, h->zmode[0], h->zmode[1], h->zmode[2], S);
   MG_LAUNCH(k_fd_gemm<true>, g0, 256, st, (const double*)b, (const double*)h->bwd[0], a, nx, ny * nz, nx, S);
   MG_LAUNCH(k_fd_gemm<false>, g1, 256, st, (const double*)a, (const double*)h->bwd[1], b, nx, ny, ny, S);
   MG_LAUNCH(k_fd_gemm<false>, g2, 256, st, (const double*)b, (const double*)h->bwd[2], a, nxy, nz, nz, S);
