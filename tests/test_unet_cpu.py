@@ -121,11 +121,16 @@ def test_backward_matches_finite_differences(kind):
             idx.append(o + nw + int(np.argmax(np.abs(g[o + nw:o + nw + cout]))))
             o += nw + cout
         idx += [o + 3, o + 16]
-        # ReLU kinks make single steps unreliable: take the best of three
+        # ReLU kinks make single steps unreliable: take the best of three (a
+        # step that already meets the bound ends the search; the bound on the
+        # worst parameter is unchanged by it)
+        thr = 2e-2 if kind == 0 else 5e-2
         worst = 0.0
         for i in idx:
             best = np.inf
             for hh in (3e-3, 1e-3, 3e-4):
+                if best < thr:
+                    break
                 h = hh * max(1.0, abs(float(p[i])))
                 pp, pm = p.copy(), p.copy()
                 pp[i] += h
@@ -137,6 +142,6 @@ def test_backward_matches_finite_differences(kind):
             worst = max(worst, best)
         # the cosine loss sits near 1 at initialisation and moves by ~1e-7 per
         # step, close to the FP32 noise of the forward values
-        assert worst < (2e-2 if kind == 0 else 5e-2), worst
+        assert worst < thr, worst
     finally:
         O.unet_set_exact(False)
