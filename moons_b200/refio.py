@@ -16,6 +16,13 @@ restart dumps and write files that MOONS and its post-processing read.
   header, then per block a ZONE record and one record per point (x, y, z and
   the components), i fastest, the coordinates of the field's data location
   (nodes or cell centres along each axis), ``pad`` points dropped per side.
+* ``export_tecplot_2d`` / ``export_tecplot_1d`` -- a plane or a line of a
+  field (``exp_2D_*C`` / ``exp_1D_*C``, base_export.f90:45-70, 95-144,
+  161-182; GF_export.f90:116-364, comment records :391-432; headers
+  exp_Tecplot_Header.f90; zones exp_Tecplot_Zone.f90:36-55).
+* ``export_tecplot_0d`` -- a history (step, value) as the reference writes
+  its probes (``exp_Header_0D_1C``, ``exp_Zone_0I``).
+* ``import_tecplot`` -- reads any of these (comment records skipped).
 
 Reading follows Fortran list-directed input: every READ starts at a new
 record, takes values across as many records as it needs and discards the
@@ -228,6 +235,202 @@ def import_tecplot_3d(src: PathOrFile) -> List[Tuple[Tuple[int, int, int], np.nd
             d = np.asarray(vals, dtype=np.float64).reshape(K, J, I, nvar).transpose(2, 1, 0, 3)
             zones.append(((I, J, K), d))
     return zones
+
+
+_XYZ = ("x", "y", "z")
+
+
+def _adj(d: int) -> Tuple[int, int]:
+    """adj_dir_given_dir: the two other directions (1-based), ascending."""
+    return {1: (2, 3), 2: (1, 3), 3: (1, 2)}[d]
+
+
+def _cp2str(v: float) -> str:
+    """cp2str: F40.20, blanks trimmed."""
+    return f"{float(v):.20f}"
+
+
+def _check_dir(dir: int):
+    if dir not in (1, 2, 3):
+        raise ValueError("dir must be 1, 2 or 3")
+
+
+def i_midplane(n_cells_with_ghosts: int) -> int:
+    """coordinates%i_midplane = sc/2 + 1 (1-based)."""
+    return n_cells_with_ghosts // 2 + 1
+
+
+def export_tecplot_2d(dst: PathOrFile, coords: Sequence[np.ndarray], comps: Sequence[np.ndarray], name: str,
+                      dir: int, plane: int, pad: int = 0, zone: int = 1, header: bool = True):
+    """One block of exp_2D_1C/2C/3C: the plane of 1-based index ``plane``
+    normal to direction ``dir`` (1..3).  ``coords`` are the field's data
+    location coordinates (location_coords); with two components they are
+    the ones other than ``dir``, as in the reference.  Records: the two
+    in-plane coordinates and the components, the first in-plane direction
+    fastest."""
+    _check_dir(dir)
+    comps = [np.asarray(c, dtype=np.float64) for c in comps]
+    s = comps[0].shape
+    if any(c.shape != s for c in comps) or [len(c) for c in coords] != list(s):
+        raise ValueError("components and coordinates must share the field's shape")
+    if not 1 <= plane <= s[dir - 1]:
+        raise ValueError(f"plane {plane} outside 1..{s[dir - 1]}")
+    d1, d2 = _adj(dir)
+    nc = len(comps)
+    w, own = _open_w(dst)
+    try:
+        if header:
+            if nc == 1:
+                w.write(' TITLE = "2D Scalar Field"\n')
+                # the reference names the scalar with the normal's suffix
+                w.write(f' VARIABLES = "{_XYZ[d1 - 1]}","{_XYZ[d2 - 1]}","{name}_{_XYZ[dir - 1]}"\n')
+            else:
+                w.write(' TITLE = "2D Vector Field"\n')
+                kept = (0, 1, 2) if nc == 3 else (d1 - 1, d2 - 1)
+                if nc not in (2, 3):
+                    raise ValueError("one, two or three components")
+                names = ",".join(f'"{name}_{_XYZ[i]}"' for i in kept)
+                w.write(f' VARIABLES = "{_XYZ[d1 - 1]}","{_XYZ[d2 - 1]}",{names}\n')
+        w.write(f' ZONE , T ="{zone}", I ={s[d1 - 1] - 2 * pad}, J ={s[d2 - 1] - 2 * pad} DATAPACKING = POINT\n')
+        c = _XYZ[dir - 1]
+        w.write(f"# Plane direction = {dir}\n")
+        w.write(f"# Plane index({c})  = {plane}\n")
+        w.write(f"# Plane location({c})  = {_cp2str(coords[dir - 1][plane - 1])}\n")
+        for j in range(pad, s[d2 - 1] - pad):
+            for i in range(pad, s[d1 - 1] - pad):
+                idx = [0, 0, 0]
+                idx[dir - 1] = plane - 1
+                idx[d1 - 1] = i
+                idx[d2 - 1] = j
+                row = [coords[d1 - 1][i], coords[d2 - 1][j]] + [a[tuple(idx)] for a in comps]
+                w.write("   " + "   ".join(_fmt(v) for v in row) + "\n")
+    finally:
+        if own:
+            w.close()
+
+
+def export_tecplot_1d(dst: PathOrFile, coords: Sequence[np.ndarray], comps: Sequence[np.ndarray], name: str,
+                      dir: int, line: Sequence[int], pad: int = 0, zone: int = 1, header: bool = True):
+    """One block of exp_1D_1C/2C/3C: the line along direction ``dir`` through
+    the 1-based indices ``line`` of the two other directions (ascending).
+    With two components they are the ones other than ``dir``."""
+    _check_dir(dir)
+    comps = [np.asarray(c, dtype=np.float64) for c in comps]
+    s = comps[0].shape
+    if any(c.shape != s for c in comps) or [len(c) for c in coords] != list(s):
+        raise ValueError("components and coordinates must share the field's shape")
+    d1, d2 = _adj(dir)
+    if not (1 <= line[0] <= s[d1 - 1] and 1 <= line[1] <= s[d2 - 1]):
+        raise ValueError("line indices outside the field")
+    nc = len(comps)
+    w, own = _open_w(dst)
+    try:
+        if header:
+            if nc == 1:
+                w.write(' TITLE = "1D Scalar Field"\n')
+                w.write(f' VARIABLES = "{_XYZ[dir - 1]}","{name}"\n')
+            else:
+                if nc not in (2, 3):
+                    raise ValueError("one, two or three components")
+                w.write(' TITLE = "1D Vector Field"\n')
+                kept = (0, 1, 2) if nc == 3 else (d1 - 1, d2 - 1)
+                names = ",".join(f'"{name}_{_XYZ[i]}"' for i in kept)
+                w.write(f' VARIABLES = "{_XYZ[dir - 1]}",{names}\n')
+        w.write(f' ZONE , T ="{zone}", I ={s[dir - 1] - 2 * pad} DATAPACKING = POINT\n')
+        c1, c2 = _XYZ[d1 - 1], _XYZ[d2 - 1]
+        w.write(f"# Line direction = {dir}\n")
+        w.write(f"# Line index({c1})  = {line[0]}\n")
+        w.write(f"# Line index({c2})  = {line[1]}\n")
+        w.write(f"# Line location({c1})  = {_cp2str(coords[d1 - 1][line[0] - 1])}\n")
+        w.write(f"# Line location({c2})  = {_cp2str(coords[d2 - 1][line[1] - 1])}\n")
+        for i in range(pad, s[dir - 1] - pad):
+            idx = [0, 0, 0]
+            idx[dir - 1] = i
+            idx[d1 - 1] = line[0] - 1
+            idx[d2 - 1] = line[1] - 1
+            row = [coords[dir - 1][i]] + [a[tuple(idx)] for a in comps]
+            w.write("   " + "   ".join(_fmt(v) for v in row) + "\n")
+    finally:
+        if own:
+            w.close()
+
+
+def export_tecplot_0d(dst: PathOrFile, n: Sequence[float], values: Sequence[float], name: str):
+    """A probe history as the reference writes it: exp_Header_0D_1C
+    (TITLE "0D Scalar Field", VARIABLES "N" and the name), the zone record
+    of exp_Zone_0I, then one (N, value) record per entry."""
+    n = list(n)
+    values = list(values)
+    if len(n) != len(values):
+        raise ValueError("one value per entry")
+    w, own = _open_w(dst)
+    try:
+        w.write(' TITLE = "0D Scalar Field"\n')
+        w.write(f' VARIABLES = "N","{name}"\n')
+        w.write(" ZONE DATAPACKING = POINT\n")
+        for a, b in zip(n, values):
+            w.write("   " + _fmt(a) + "   " + _fmt(b) + "\n")
+    finally:
+        if own:
+            w.close()
+
+
+def import_tecplot(src: PathOrFile):
+    """Read a POINT file of any dimension written by the reference or by the
+    exporters here.  Returns (variables, zones): the variable names and a list
+    of (extents, data) with data[..., v] over the variables, the first extent
+    fastest; a zone without I/J/K (the 0-D history) holds every remaining
+    record.  Comment records ("#") are skipped."""
+    lines = _text(src).splitlines()
+    names: List[str] = []
+    zones = []
+    p = 0
+    while p < len(lines):
+        ln = lines[p].strip()
+        p += 1
+        if not ln or ln.startswith("#"):
+            continue
+        up = ln.upper()
+        if up.startswith("TITLE"):
+            continue
+        if up.startswith("VARIABLES"):
+            body = ln.split("=", 1)[1]
+            names = [t.strip().strip('"') for t in body.replace(",", " ").split()]
+            continue
+        if up.startswith("ZONE"):
+            if not names:
+                raise ValueError("ZONE before VARIABLES")
+            toks = ln.replace(",", " ").replace("=", " = ").split()
+            ext = {}
+            for t_i, t in enumerate(toks):
+                if t.upper() in ("I", "J", "K") and t_i + 2 < len(toks) and toks[t_i + 1] == "=":
+                    ext[t.upper()] = int(toks[t_i + 2])
+            shape = tuple(ext[k] for k in ("I", "J", "K") if k in ext)
+            body = [l for l in lines[p:] if l.strip() and not l.strip().startswith("#")
+                    and not l.strip().upper().startswith("ZONE")]
+            nv = len(names)
+            if shape:
+                cnt = int(np.prod(shape)) * nv
+                r = _Records("\n".join(l for l in lines[p:] if not l.strip().startswith("#")))
+                vals = r.read(cnt, float)
+                # advance past the records consumed (comment lines do not count)
+                used, k = 0, p
+                while used < r.pos and k < len(lines):
+                    if not lines[k].strip().startswith("#"):
+                        used += 1
+                    k += 1
+                p = k
+                data = np.asarray(vals, dtype=np.float64).reshape(tuple(reversed(shape)) + (nv,))
+                data = data.transpose(tuple(reversed(range(len(shape)))) + (len(shape),))
+            else:
+                rows = []
+                for l in body:
+                    rows.append([float(t.replace("D", "E").replace("d", "e")) for t in l.replace(",", " ").split()])
+                p = len(lines)
+                data = np.asarray(rows, dtype=np.float64).reshape(-1, nv)
+                shape = (data.shape[0],)
+            zones.append((shape, data))
+    return names, zones
 
 
 # ---- fields of the library ---------------------------------------------------
