@@ -8,21 +8,22 @@ sub-domain index ranges the GPU path embeds and extracts with.
 
 Coordinate distributions (code/handwritten/grid/coordinate_distribution_funcs.f90):
 
-* ``uniform`` / ``linspace``        -- uniform_func / linspace_func (:34-70)
-* ``uniform_left`` / ``uniform_right`` -- uniformDirection_func (:72-110)
-* ``roberts_left``   -- transformation1, clustered at hmin (:112-150, :306-312)
-* ``roberts_right``  -- transformation2 with alpha = 0, clustered at hmax (:192-248, :316-322)
+* ``uniform`` / ``linspace``        -- uniform_func / linspace_func (:34-81)
+* ``uniform_left`` / ``uniform_right`` -- uniformDirection_func (:83-143)
+* ``roberts_left``   -- transformation1, clustered at hmin (:145-190, :309-315)
+* ``roberts_right``  -- transformation2 with alpha = 0, clustered at hmax (:192-248, :317-323)
 * ``roberts_both``   -- transformation2 with alpha = 0.5 (:325-331)
-* ``cluster``        -- transformation3, clustered about yc (:250-302, :334-340)
+* ``cluster``        -- transformation3, clustered about yc (:250-307, :333-339)
 
 Iterated forms that add points until the neighbour spacing ratio is at most
-``max_mesh_stretch_ratio`` (coordinate_distribution_funcs_iterate.f90:86-172),
-boundary-layer stretching parameters (coordinate_stretch_parameters.f90:17-135),
+``max_mesh_stretch_ratio`` (coordinate_distribution_funcs_iterate.f90:64-152),
+boundary-layer stretching parameters (coordinate_stretch_parameters.f90:16-135),
 the Newton match of a Roberts parameter to a given end spacing
-(coordinate_stretch_param_match.f90:37-265), grid construction and extension
-(grid/grid_init.f90:22-79, grid/grid_continue.f90:1-317), the segment list of
+(coordinate_stretch_param_match.f90:37-265, newtonT2 :181-234), grid
+construction and extension (grid/grid_init.f90:22-79,
+grid/grid_continue.f90:1-317), the segment list of
 a mesh (mesh_params/segment_extend.f90, mesh_params_extend.f90) and its
-generator (mesh/generate_mesh_generic.f90:19-97), and the index overlap of
+generator (mesh/generate_mesh_generic.f90:20-97), and the index overlap of
 two meshes (sub_domain/overlap_extend.f90:204-290, 364-380).
 
 The reference stops the program on bad input; these functions raise
