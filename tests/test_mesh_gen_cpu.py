@@ -319,3 +319,20 @@ def test_sigma_inv_of_the_vacuum_case():
         assert len(ones) == n_in
     mom, ind, prm, _ = configs.full_bc(N=8, N_w=3)
     assert tuple(prm.ind_offset) == mg.sub_domain_offset(mom, ind)
+
+
+def test_full_bc_case_steps_in_the_oracle():
+    """The full_BC preset (mesh-bank meshes, walls, vacuum) wired into the
+    oracle's step: two steps solved to 1e-12 keep div U and div B at
+    round-off level and every field finite."""
+    import oracle.oracle as O
+    from moons_b200 import capi as G
+    o = configs.make(O, configs.full_bc, seed=2, N=6, N_w=2, mqp=mg.MeshQuality(), tol=1e-12,
+                     iter_max=(20000,) * 4, noise=1e-2)
+    info = o.step(2)
+    du, db = o.divergence()
+    assert du < 1e-16 and db < 1e-22, (du, db)
+    assert info["res_p"] < 1e-11
+    for which in (G.MHD_U, G.MHD_B, G.MHD_J):
+        for c in range(3):
+            assert np.isfinite(o.download(which, c)).all()
