@@ -6,9 +6,9 @@
 // code it cites.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
 // baseline may load it; the product never links or calls it.
 //
-// Parity status: the reference is Fortran and no Fortran compiler exists in
-// this build environment, so this restatement cannot be run side by side with
-// the reference.  It is pinned by the reference's own verification routines
+// Parity status: the reference is Fortran and no Fortran compiler is
+// installed next to this code, so this restatement cannot be run side by side
+// with the reference.  It is pinned by the reference's own verification routines
 // restated as tests (operator identities, Poisson residual drop, SPD
 // symmetry, analytic profiles); per-field parity with a Fortran build is
 // therefore "unpinned" beyond those pins.
