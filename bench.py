@@ -48,6 +48,9 @@ def parse():
                          "forward applies / training steps on the 128^3 sigma-shell grid; prints what ran, no "
                          "bench line")
     ap.add_argument("--profile-iters", type=int, default=40)
+    ap.add_argument("--profile-mesh", choices=["duct", "at_scale"], default="duct",
+                    help="mesh of the --profile Poisson solve: the duct fluid mesh (64x64x256) or the "
+                         "configuration-5 mesh (128x128x256, working set above the L2)")
     return ap.parse_args()
 
 
@@ -83,7 +86,8 @@ def run_profile(args):
               flush=True)
         return
     prec = {"jacobi": G.PREC_LAP, "mg": G.PREC_MG, "mixed": G.PREC_MG_MIXED, "fd": G.PREC_FD}[args.profile]
-    mom, _, prm, _ = configs.duct(**kw)
+    mom, _, prm, _ = (configs.at_scale(**at_scale_kw(args.small)) if args.profile_mesh == "at_scale"
+                      else configs.duct(**kw))
     m = G.Mesh(*mom)
     p = m.field(G.CC)
     p.set_bcs(prm.bc_p)
@@ -99,6 +103,11 @@ def duct_kw(small):
     if small:
         return dict(nx=16, ny=16, nz=32)
     return dict(nx=64, ny=64, nz=256)
+
+
+def at_scale_kw(small):
+    """Configuration 5's mesh: 256 streamwise (z) x 128 x 128 cells."""
+    return dict(nx=16, ny=16, nz=32) if small else {}
 
 
 class Clocks:
@@ -182,12 +191,12 @@ def replica_rate(world, steps, ms_max):
     return world * steps / (ms_max / 1e3)
 
 
-def poisson_ms(G, kw, prec=None):
-    """Pressure-Poisson time to 1e-10 on the duct fluid mesh (random RHS),
-    best of 3 solves from x = 0, with the given preconditioner (default the
-    reference's Jacobi prec_Lap)."""
+def poisson_ms(G, kw, prec=None, builder=None):
+    """Pressure-Poisson time to 1e-10 on the duct fluid mesh, or the mesh of
+    ``builder`` (random RHS), best of 3 solves from x = 0, with the given
+    preconditioner (default the reference's Jacobi prec_Lap)."""
     from moons_b200 import configs
-    mom, _, prm, _ = configs.duct(**kw)
+    mom, _, prm, _ = (builder or configs.duct)(**kw)
     m = G.Mesh(*mom)
     p = m.field(G.CC)
     p.set_bcs(prm.bc_p)
@@ -426,50 +435,29 @@ def full_bc_steps(G, small=False, steps=5, steps_tol=2):
     return out
 
 
-def cpu_sample(kw, gpu_iters=None):
-    """Bounded CPU sample: the oracle (single thread) on the full-size duct.
-    It times init + one step with every PCG capped at a few iterations, and
-    one capped pressure solve, then scales to a full step with the
-    iteration counts of the full step (from the GPU run, which runs the same
-    algorithm).  Returns (steps_per_s, description)."""
+def cpu_sample(kw, steps=1, warmup=0):
+    """The oracle (the C++ restatement of the reference's algorithm, on all
+    host threads) stepping the full-size duct: `warmup` untimed steps, then
+    `steps` full time steps timed one by one, every PCG solved to the case's
+    1e-10 exactly as on the GPU path (no caps, no extrapolation).  Returns
+    (steps_per_s, description, per-step iteration counts)."""
     import oracle.oracle as O
-    from moons_b200 import configs, capi as G
-    cap = 3
-    mom, ind, prm, init = configs.duct(**kw)
-    for name in ("isp_U", "isp_p", "isp_B", "isp_phi"):
-        setattr(prm, name, G.isp(cap, 0.0, 0.0))
-    mm = O.Mesh(*mom)
-    mi = O.Mesh(*ind)
-    sim = O.MHD(mm, mi, prm)
-    init(sim, np.random.default_rng(0))
-    sim.init()
-    t0 = time.perf_counter()
-    info = sim.step(1)
-    t_capped = time.perf_counter() - t0
-    # per-iteration cost of each solve family on the full mesh
-    p = mm.field(G.CC)
-    p.set_bcs(prm.bc_p)
-    b = mm.field(G.CC)
-    b.upload(np.random.default_rng(1).standard_normal(b.shape))
-    s = O.PCG(mm, G.OP_LAP_UNIFORM, G.PREC_LAP, [p], [p])
-    t0 = time.perf_counter()
-    s.solve([p], [b], G.isp(2, 0.0, 0.0))
-    t2 = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    s.solve([p], [b], G.isp(6, 0.0, 0.0))
-    t6 = time.perf_counter() - t0
-    t_iter_cc = max((t6 - t2) / 4.0, 1e-9)
-    # without a GPU run beside it: the per-step iteration counts that the same
-    # algorithm takes on this workload (measured on the GPU path, 5-step mean)
-    iters = gpu_iters or {"iters_U": 5.0, "iters_p": 939.2, "iters_B": 391.6, "iters_phi": 231.4}
-    # VF solves cost ~3x a CC iteration per component set; the B curl-curl ~2x more
-    extra = ((iters["iters_p"] - cap) + (iters["iters_phi"] - cap)) * t_iter_cc + \
-        (iters["iters_U"] - cap) * 3 * t_iter_cc + (iters["iters_B"] - cap) * 6 * t_iter_cc
-    t_step = t_capped + max(extra, 0.0)
-    desc = (f"oracle (C++ restatement, {O.threads()} host threads) on the full duct mesh: 1 step with PCG capped at {cap} iterations "
-            f"({t_capped:.2f} s) + {t_iter_cc * 1e3:.1f} ms per CC PCG iteration x the full step's iteration counts "
-            f"{iters}")
-    return 1.0 / t_step, desc
+    from moons_b200 import configs
+    sim = configs.make(O, configs.duct, seed=0, **kw)
+    if warmup:
+        sim.step(warmup)
+    secs, its = [], {}
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        info = sim.step(1)
+        secs.append(time.perf_counter() - t0)
+        for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+            its[k] = its.get(k, 0) + info[k] / steps
+    t = float(np.sum(secs))
+    desc = (f"oracle (C++ restatement of the reference algorithm, {O.threads()} host threads), full-size duct, "
+            f"seed 0: {steps} full time step(s) after {warmup} untimed step(s), every PCG to 1e-10 "
+            f"({t:.1f} s; per step {[round(x, 2) for x in secs]} s)")
+    return steps / t, desc, its
 
 
 def run_reference(args):
@@ -479,21 +467,46 @@ def run_reference(args):
     kw = duct_kw(args.small)
     import oracle.oracle as O
     cores = O.threads()
-    vals = []
-    desc = ""
-    for _ in range(max(1, min(args.steps, 2))):
-        v, desc = cpu_sample(kw)
-        vals.append(v)
-    value = float(np.median(vals))
+    value, desc, its = cpu_sample(kw, steps=args.steps, warmup=args.warmup)
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1e-4) velocity)",
-        "config": {"workload": WORKLOAD}, "impl": "reference",
+        "config": {"workload": WORKLOAD, "mesh_fluid": [kw["nx"], kw["ny"], kw["nz"]], "pcg_tol_rel": 1e-10},
+        "impl": "reference", "per_step": its,
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def ldc32_config1(G, steps=1000):
+    """Configuration 1 at its stated size: the MHD lid-driven cavity, uniform
+    32^3, Re = 400, Ha = 10, potential form, dt = 1e-3, PCG to 1e-10, 1000
+    steps from the seeded state; steps/s and the fields' relative L2 against
+    the oracle's 1000-step fixture."""
+    fx = os.path.join(ROOT, "tests", "golden", "ldc32_step1000.npz")
+    from tests.golden import make_ldc32 as mk
+    sim = mk.build_case(G)
+    ms, tot = 0.0, {"iters_U": 0, "iters_p": 0, "iters_phi": 0}
+    for _ in range(steps // 100):
+        info = sim.step(100)
+        ms += info["ms"]
+        for k in tot:
+            tot[k] += info[k]
+    out = {"workload": "MHD lid-driven cavity 32^3 uniform, Re=400, Ha=10, low-Rem potential form, dt=1e-3, "
+                       "PCG to 1e-10, 1000 steps from U0 = N(0,1e-6)",
+           "steps": steps, "steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
+           "iters_per_step": {k: v / steps for k, v in tot.items()}}
+    if os.path.exists(fx) and steps == 1000:
+        z = np.load(fx)
+        errs = {}
+        for name, which, c in mk.FIELDS_LONG:
+            a, b = sim.download(which, c), z[name]
+            errs[name] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        out["rel_l2_vs_oracle_fixture"] = errs
+        out["rel_l2_max"] = max(errs.values())
+    return out
 
 
 def main():
@@ -525,29 +538,38 @@ def main():
     ms = max_over_ranks(info["ms"], dist)
     value = replica_rate(world, args.steps, ms)
     du, db = sim.divergence()
+    its_v = {k: info[k] / max(args.steps, 1) for k in ("iters_U", "iters_p", "iters_B", "iters_phi")}
 
     # ---- end to end through the C-ABI with pinned host buffers, as a host
-    # code driving the time loop: each step uploads the state (U, B) from the
-    # host, advances it, and downloads it back into the same host buffers,
-    # so the steps follow the simulation's own trajectory.
-    state = [sim.field(G.MHD_U, c) for c in range(3)] + [sim.field(G.MHD_B, c) for c in range(3)]
+    # code driving the time loop: a second simulation from the same seed
+    # takes the same warm-up steps on the device, then each of the same K
+    # steps uploads the state (U, B) from the host, advances it, and
+    # downloads it back into the same host buffers -- the same trajectory
+    # and solver work as `value`, plus the copies.
+    del sim
+    sim_e = configs.make(G, configs.duct, seed=rank, **kw)
+    sim_e.step(args.warmup)
+    state = [sim_e.field(G.MHD_U, c) for c in range(3)] + [sim_e.field(G.MHD_B, c) for c in range(3)]
     host = [torch.from_numpy(f.download().ravel(order="F").copy()).pin_memory() for f in state]
     h2d = sum(f.n * 8 for f in state)
     d2h = h2d
-    ke = max(2, args.steps)
+    its_e = {}
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(ke):
+    for _ in range(args.steps):
         for f, h in zip(state, host):
             f.upload_ptr(h.data_ptr())
-        sim.step(1)
+        ie = sim_e.step(1)
         for f, h in zip(state, host):
             f.download_ptr(h.data_ptr())
+        for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+            its_e[k] = its_e.get(k, 0) + ie[k] / args.steps
     t_e2e = time.perf_counter() - t0
     t_e2e = max_over_ranks(t_e2e, dist)
-    e2e = world * ke / t_e2e
+    e2e = world * args.steps / t_e2e
+    del sim_e
 
     # ---- the same step with multigrid (FP32 V-cycle) pressure / potential
     # solves: same systems and exit tests, far fewer iterations
@@ -576,8 +598,12 @@ def main():
     fullbc = full_bc_steps(G, small=args.small)
     learned = learned_poisson(G, n=32 if args.small else 128, shell=2 if args.small else 4,
                               ntrain=4 if args.small else 8, held=(1000,) if args.small else (1000, 1001, 1002))
-    alg_bytes = 88.0 * ncc * pinfo["iterations"]  # 88 B per cell per FP64 PCG iteration (algorithmic)
-    achieved = alg_bytes / (pinfo["ms"] / 1e3) / 1e9
+    # roofline: the pressure Jacobi-PCG on configuration 5's mesh (4.36 M
+    # cells, 35 MB per array: the iteration's working set is above the L2)
+    rinfo, ncc_r = poisson_ms(G, at_scale_kw(args.small), builder=configs.at_scale)
+    alg_bytes = 88.0 * ncc_r * rinfo["iterations"]  # 88 B per cell per FP64 PCG iteration (algorithmic)
+    achieved = alg_bytes / (rinfo["ms"] / 1e3) / 1e9
+    ldc = ldc32_config1(G, steps=100 if args.small else 1000)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -586,29 +612,29 @@ def main():
     except Exception:
         peak = 6650.0
         peak_src = "fallback"
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "pcg_traffic.json")
+    traffic, traffic_src = None, None
+    tf = os.path.join(ROOT, "profiles", "pcg_traffic_at_scale.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("bytes_per_cell_iter")
-            if traffic is not None:
-                traffic = traffic * ncc  # per PCG iteration, like alg_bytes_per_launch
+            tj = json.load(open(tf))
+            traffic = tj["bytes_per_cell_iter"] * ncc_r  # per PCG iteration, like alg_bytes_per_launch
+            traffic_src = tj.get("source")
         except Exception:
             traffic = None
 
     if rank == 0:
         import oracle.oracle as O
         cpu_cores = O.threads()
-        cpu_v, cpu_desc = cpu_sample(kw, {k: info[k] / max(args.steps, 1) for k in
-                                          ("iters_U", "iters_p", "iters_B", "iters_phi")})
+        cpu_v, cpu_desc, cpu_its = cpu_sample(kw, steps=1, warmup=0)
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1e-4) velocity, uniform B0)",
             "config": {"workload": WORKLOAD, "mesh_fluid": [kw["nx"], kw["ny"], kw["nz"]],
                        "pcg_tol_rel": 1e-10, "parallelism": f"replicas x{world}",
-                       "l2": "working set (~60 FP64 arrays x 10.7 MB) exceeds the 126 MB L2; no flush"},
-            "per_step": {k: info[k] / max(args.steps, 1) for k in ("iters_U", "iters_p", "iters_B", "iters_phi")},
+                       "l2": "working set (~60 FP64 arrays x 10.7 MB) exceeds the 126 MB L2; no flush; the "
+                             "roofline solve's iteration working set (5 arrays x 35 MB) exceeds it too"},
+            "per_step": its_v,
             "div_U_l2sq": du, "div_B_l2sq": db,
             "steps_per_s_mixed_poisson": {"value": value_mixed, "per_step": {k: infox[k] / max(args.steps, 1) for k in (
                 "iters_U", "iters_p", "iters_B", "iters_phi")}, "note": "pressure and potential solves by FP64 "
@@ -631,13 +657,19 @@ def main():
             "poisson_learned": learned,
             "at_scale": scale5,
             "full_bc_vacuum": fullbc,
-            "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (duct fluid mesh)",
+            "config1_ldc32": ldc,
+            "roofline": {"bound": "hbm", "kernel": "pressure Jacobi-PCG iteration (k_l_lap + k_l_update + k_l_pupd "
+                                                  "+ k_l_bcfill) on configuration 5's mesh, 128x128x256 cells",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "alg_bytes_per_launch": 88.0 * ncc},
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
+                         "alg_bytes_per_launch": 88.0 * ncc_r, "cells": ncc_r,
+                         "iterations": rinfo["iterations"], "ms_to_1e-10": rinfo["ms"],
+                         "us_per_iteration": rinfo["ms"] * 1e3 / max(rinfo["iterations"], 1)},
             "cpu_baseline": {"value": cpu_v, "unit": "steps/s", "cores": cpu_cores, "kind": "port",
-                             "sample": cpu_desc},
-            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                             "sample": cpu_desc, "per_step": cpu_its},
+            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "per_step": its_e, "note": "the same K steps as value (after the same warm-up), driven from "
+                                              "the host with U and B copied up and down each step"},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }

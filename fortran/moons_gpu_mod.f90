@@ -22,6 +22,8 @@ module moons_gpu_mod
   integer(c_int), parameter :: MOONS_PREC_MOM = 2, MOONS_PREC_IND = 3
   integer(c_int), parameter :: MOONS_PREC_MG = 4, MOONS_PREC_MG_MIXED = 5, MOONS_PREC_UNET = 6
   integer(c_int), parameter :: MOONS_PREC_FD = 7
+  ! largest face temporary (points) that moons_lap_var_noalloc accepts
+  integer(c_long_long), parameter :: MOONS_LAP_VAR_NOALLOC_MAX_POINTS = 131072_c_long_long
 
   type, bind(C) :: moons_bc_spec
     integer(c_int) :: type(6)
@@ -125,6 +127,21 @@ module moons_gpu_mod
     function moons_curl(ox, oy, oz, ux, uy, uz) bind(C, name="moons_curl") result(st)
       import :: c_ptr, c_int
       type(c_ptr), value :: ox, oy, oz, ux, uy, uz
+      integer(c_int) :: st
+    end function
+
+    function moons_lap_var(out, u, kx, ky, kz) bind(C, name="moons_lap_var") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: out, u, kx, ky, kz
+      integer(c_int) :: st
+    end function
+
+    ! the same operator without device allocation (temporaries in the
+    ! library's built-in device array; fields beyond the limit above are
+    ! rejected with MOONS_ERR_LIMIT)
+    function moons_lap_var_noalloc(out, u, kx, ky, kz) bind(C, name="moons_lap_var_noalloc") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: out, u, kx, ky, kz
       integer(c_int) :: st
     end function
 

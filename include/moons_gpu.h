@@ -192,9 +192,10 @@ int moons_interp(moons_sf* out, const moons_sf* in, int dir);
  * array instead of the allocator.
  *  - each temporary holds at most MOONS_LAP_VAR_NOALLOC_MAX_POINTS doubles;
  *    larger fields are rejected with MOONS_ERR_LIMIT (use moons_lap_var);
- *  - the first call on a device looks up the array on that device and does
- *    nothing else on later calls: make the first call before any stream
- *    capture;
+ *  - the first call on a device looks up the array's address on that
+ *    device (the caller's current device is left as it was) and later calls
+ *    reuse it: make the first call before any stream capture;
+ *  - every call synchronizes the mesh's stream before it returns;
  *  - the array needs no initial contents (every element read is written
  *    earlier in the same call);
  *  - the array is shared per device: calls that overlap in time race. */

@@ -16,8 +16,10 @@
 //  * each temporary holds at most kNoallocMaxPoints doubles; a field whose
 //    face temporaries would be larger is rejected with MOONS_ERR_LIMIT;
 //  * the first call on a device looks up the array's address on that device
-//    (cudaGetSymbolAddress, with the device made current) and keeps it; make
-//    that first call before any stream capture;
+//    (cudaGetSymbolAddress, with that device made current for the lookup and
+//    the caller's current device restored after it) and keeps it; make that
+//    first call before any stream capture;
+//  * every call synchronizes the mesh's stream before it returns;
 //  * nothing in the array needs an initial value: the gradient pass writes
 //    every element that the divergence pass reads;
 //  * the array is shared by all callers on a device, so calls that overlap in
@@ -47,11 +49,16 @@ int noalloc_scratch(int dev, double** out) {
   }
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (!g_noalloc_base[dev]) {
-    cudaError_t e = cudaSetDevice(dev);
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return mg::cuda_fail(e, "cudaGetDevice");
+    e = cudaSetDevice(dev);
     if (e != cudaSuccess) return mg::cuda_fail(e, "cudaSetDevice");
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_lap_var_scratch);
+    const cudaError_t e2 = cudaSetDevice(prev);  // the caller's current device stays current
     if (e != cudaSuccess) return mg::cuda_fail(e, "cudaGetSymbolAddress(g_lap_var_scratch)");
+    if (e2 != cudaSuccess) return mg::cuda_fail(e2, "cudaSetDevice (restore)");
     g_noalloc_base[dev] = static_cast<double*>(p);
   }
   *out = g_noalloc_base[dev];

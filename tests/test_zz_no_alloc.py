@@ -49,6 +49,24 @@ def test_noalloc_matches_lap_var_twice_in_a_row():
     assert np.abs(out.download() - ref.download()).max() <= 1e-13 * np.abs(ref.download()).max()
 
 
+def test_noalloc_takes_no_device_memory():
+    """Free device memory is the same before and after calls of the no-alloc
+    entry point (the library module, and with it the built-in array, is
+    loaded by the fields' first kernels, before the first reading)."""
+    import torch
+    m = _mesh(20)
+    u, ks = _case(m, 13)
+    out = m.field(G.CC)
+    G.lap_var_noalloc(out, u, ks)  # first call: the one-time address lookup
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        G.lap_var_noalloc(out, u, ks)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_noalloc_rejects_fields_beyond_the_scratch():
     # 52^3 cells: face temporaries of 55*54*54 = 160380 > 131072 points
     m = _mesh(52)
