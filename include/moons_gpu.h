@@ -133,6 +133,14 @@ const char* moons_last_error(void);
  * run in this process, host launches plus the launches a solver's
  * device-side loop executed. */
 long long moons_kernel_launches(void);
+/* Diagnostic (no reference counterpart): runs one bounded in-kernel wait on
+ * an mbarrier that nothing completes, with the given limit (0 < limit_ns <=
+ * 1e9); returns MOONS_ERR_CUDA with "bounded wait ran out (site 900)" in
+ * moons_last_error once the limit has passed.  It exercises, without any
+ * fault, the path every bounded wait of the library takes when it runs out:
+ * the kernel records the site and returns, and the CUDA context stays
+ * usable.  Synchronizes the device. */
+int moons_debug_bounded_wait(unsigned long long limit_ns);
 
 /* ---- mesh: single block (coordinates_extend.f90:78-173 init_c,
  *      :506-523 init_stencils_c).  hn_* are the node coordinates including

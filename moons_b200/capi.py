@@ -214,6 +214,7 @@ def lib() -> C.CDLL:
             "moons_mhd_step": (C.c_int, [_P, C.c_int, C.POINTER(StepInfo)]),
             "moons_mhd_divergence": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             "moons_kernel_launches": (C.c_longlong, []),
+            "moons_debug_bounded_wait": (C.c_int, [C.c_ulonglong]),
             "moons_unet_create": (C.c_int, [_P, C.c_ulonglong, C.POINTER(_P)]),
             "moons_unet_destroy": (C.c_int, [_P]),
             "moons_unet_nparams": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
@@ -490,6 +491,12 @@ class PCG:
             self.close()
         except Exception:
             pass
+
+
+def debug_bounded_wait(limit_ns: int):
+    """Run one bounded in-kernel wait that nothing completes (raises
+    MoonsError MOONS_ERR_CUDA naming the site once the limit has passed)."""
+    _check(lib().moons_debug_bounded_wait(int(limit_ns)))
 
 
 def kernel_launches() -> int:

@@ -6,3 +6,4 @@
 #include "mhd.cu"
 #include "noalloc.cu"
 #include "unet.cu"
+#include "diag.cu"

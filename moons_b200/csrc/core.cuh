@@ -122,6 +122,28 @@ inline cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, cudaSt
     cudaError_t e_ = mg::launch_pdl(K, dim3(GRID), dim3(BLOCK), (STREAM), __VA_ARGS__);        \
     if (e_ != cudaSuccess) return mg::cuda_fail(e_, #K);                                       \
   } while (0)
+// the same with dynamic shared memory
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl_smem(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                   Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ++g_launch_count;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+#define MG_LAUNCH_PDL_SMEM(K, GRID, BLOCK, SMEM, STREAM, ...)                                  \
+  do {                                                                                         \
+    cudaError_t e_ = mg::launch_pdl_smem(K, dim3(GRID), dim3(BLOCK), (SMEM), (STREAM), __VA_ARGS__); \
+    if (e_ != cudaSuccess) return mg::cuda_fail(e_, #K);                                       \
+  } while (0)
 
 constexpr int kBlock = 256;
 inline unsigned nblocks(size_t n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }

@@ -37,6 +37,8 @@ struct PcgScalars {
   // below stag_factor times its value stag_window iterations before
   int stag_window;
   double stag_factor, stag_ref;
+  // nonzero: a bounded wait in a loop kernel ran out (the code names the site)
+  int wait_err;
 };
 
 // implicit BCs + masks of one unknown component, as the fused kernels see them

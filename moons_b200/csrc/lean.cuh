@@ -18,7 +18,9 @@
 //    writes these points, and only from one interior point each; edge and
 //    corner ghosts, which no interior stencil reads, are composed in a fixed
 //    order);
-//  * Minv is read, as the reference stores it (prec_* fill PCG%Minv once).
+//  * Minv of prec_Lap / prec_mom is formed per point from the per-axis tables
+//    (the same expression k_prec stores, so bit-identical); prec_ind and the
+//    identity read the stored PCG%Minv.
 #pragma once
 #include "fused.cuh"
 
@@ -398,15 +400,45 @@ __global__ void __launch_bounds__(kLB) k_l_curl_ap(FComp Ap, FComp P, DF E0, DF 
 }
 
 // ---- K2: x += alpha p ; r -= alpha Ap ; z = Minv r ; r.r, z.r ; exit test ; beta ----
-template <int KC>
+// Minv at a point, MM = 0: stored (PCG%Minv); 1: prec_Lap, 2: prec_mom
+// (coeff), formed from the per-axis tables exactly as k_prec stores it
+// (minv_at): 1/(((dx + dy) + dz) * ((hx*hy)*hz)).  The x,y parts are formed
+// once per column (dxy, vxy).
+struct MinvCol {
+  double dxy, vxy;
+};
+template <int MM>
+__device__ __forceinline__ MinvCol minv_col(const DGrid& g, int dl, int i, int j) {
+  MinvCol c{0.0, 0.0};
+  if (MM != 0) {
+    const bool Nx = n_along(dl, 1), Ny = n_along(dl, 2);
+    c.dxy = (Nx ? g.c[0].diagN[i] : g.c[0].diagC[i]) + (Ny ? g.c[1].diagN[j] : g.c[1].diagC[j]);
+    c.vxy = vol_axis(g.c[0], Nx, i) * vol_axis(g.c[1], Ny, j);
+  }
+  return c;
+}
+template <int MM>
+__device__ __forceinline__ double minv_k(const MinvCol& c, const DGrid& g, int dl, int k, double coeff) {
+  const bool Nz = n_along(dl, 3);
+  double d = c.dxy + (Nz ? g.c[2].diagN[k] : g.c[2].diagC[k]);
+  if (MM == 2) {
+    d = d * coeff;
+    d = d + 1.0;
+  }
+  return 1.0 / (d * (c.vxy * vol_axis(g.c[2], Nz, k)));
+}
+
+template <int KC, int MM>
 __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r, const DF& Ap, const DF& M,
-                                           const FBC& b, double alpha, double& arr, double& azr) {
+                                           const FBC& b, const DGrid& g, double coeff, double alpha, double& arr,
+                                           double& azr) {
   const Col cl = col_of(x, blockIdx.x);
   if (!cl.ok) return;
   const int i = cl.i, j = cl.j;
   const bool inxy = !cl.gij && dot_xy(x, b, i, j);
   const size_t sz = (size_t)x.s0 * x.s1;
   const int nkc = (x.s2 + KC - 1) / KC;
+  const MinvCol mc = minv_col<MM>(g, x.dl, i, j);
   for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
     const int k0 = kc * KC + 1, k1 = min(k0 + KC - 1, x.s2);
     const size_t idx0 = x.at(i, j, k0);
@@ -419,7 +451,7 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
       pv[q] = in ? ld(p.f + idx) : 0.0;
       rv[q] = in ? r.f[idx] : 0.0;
       av[q] = in ? ld(Ap.f + idx) : 0.0;
-      mv[q] = in ? ld(M.f + idx) : 0.0;
+      mv[q] = (MM == 0 && in) ? ld(M.f + idx) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < KC; q++) {
@@ -430,23 +462,25 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
       const double rn = rv[q] + av[q] * (-alpha);
       r.f[idx] = rn;
       if (inxy && k != 1 && k != x.s2 && dot_z(x, b, k)) {
-        const double zv = mv[q] * rn;
+        const double m = MM == 0 ? mv[q] : minv_k<MM>(mc, g, x.dl, k, coeff);
+        const double zv = m * rn;
         arr += rn * rn;
         azr += zv * rn;
       }
     }
   }
 }
-template <int KC>
-__global__ void __launch_bounds__(kLB) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, FBC b0, FBC b1,
-                                                   FBC b2, PcgScalars* S, double* partial, unsigned* ticket) {
+template <int KC, int MM>
+__global__ void __launch_bounds__(kLB, 5) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, FBC b0, FBC b1,
+                                                   FBC b2, DGrid g, double coeff, PcgScalars* S, double* partial,
+                                                   unsigned* ticket) {
   pdl_enter();
   if (S->done) return;
   double arr = 0.0, azr = 0.0;
   const double alpha = S->alpha;
-  if (blockIdx.z == 0) update_col<KC>(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, alpha, arr, azr);
-  else if (blockIdx.z == 1) update_col<KC>(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, alpha, arr, azr);
-  else update_col<KC>(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, alpha, arr, azr);
+  if (blockIdx.z == 0) update_col<KC, MM>(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, g, coeff, alpha, arr, azr);
+  else if (blockIdx.z == 1) update_col<KC, MM>(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, g, coeff, alpha, arr, azr);
+  else update_col<KC, MM>(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, g, coeff, alpha, arr, azr);
   const double s_rr = block_sum(arr);
   const double s_zr = block_sum(azr);
   const unsigned fb = flat_block(), nb = n_blocks();
@@ -494,12 +528,14 @@ __global__ void __launch_bounds__(kLB) k_l_update(FComp X, FComp P, FComp R, FCo
 }
 
 // ---- K3: p' = p*beta + Minv r at every point (BC points: k_l_bcfill) -------------
-template <int KC>
-__device__ __forceinline__ void pupd_col(const DF& p, const DF& pn, const DF& r, const DF& M, double beta) {
+template <int KC, int MM>
+__device__ __forceinline__ void pupd_col(const DF& p, const DF& pn, const DF& r, const DF& M, const DGrid& g,
+                                         double coeff, double beta) {
   const Col cl = col_of(p, blockIdx.x);
   if (!cl.ok) return;
   const size_t sz = (size_t)p.s0 * p.s1;
   const int nkc = (p.s2 + KC - 1) / KC;
+  const MinvCol mc = minv_col<MM>(g, p.dl, cl.i, cl.j);
   for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
     const int k0 = kc * KC + 1, k1 = min(k0 + KC - 1, p.s2);
     const size_t idx0 = p.at(cl.i, cl.j, k0);
@@ -510,21 +546,27 @@ __device__ __forceinline__ void pupd_col(const DF& p, const DF& pn, const DF& r,
       const size_t idx = idx0 + (size_t)q * sz;
       pv[q] = in ? ld(p.f + idx) : 0.0;
       rv[q] = in ? ld(r.f + idx) : 0.0;
-      mv[q] = in ? ld(M.f + idx) : 0.0;
+      mv[q] = (MM == 0 && in) ? ld(M.f + idx) : 0.0;
     }
 #pragma unroll
-    for (int q = 0; q < KC; q++)
-      if (k0 + q <= k1) pn.f[idx0 + (size_t)q * sz] = pv[q] * beta + mv[q] * rv[q];
+    for (int q = 0; q < KC; q++) {
+      const int k = k0 + q;
+      if (k > k1) break;
+      // Minv is 0 on the ghost points (k_prec)
+      const double m = MM == 0 ? mv[q] : ((cl.gij || k == 1 || k == p.s2) ? 0.0 : minv_k<MM>(mc, g, p.dl, k, coeff));
+      pn.f[idx0 + (size_t)q * sz] = pv[q] * beta + m * rv[q];
+    }
   }
 }
-template <int KC>
-__global__ void __launch_bounds__(kLB) k_l_pupd(FComp P, FComp Pn, FComp R, FComp M, PcgScalars* S) {
+template <int KC, int MM>
+__global__ void __launch_bounds__(kLB, 6) k_l_pupd(FComp P, FComp Pn, FComp R, FComp M, DGrid g, double coeff,
+                                                 PcgScalars* S) {
   pdl_enter();
   if (S->done) return;
   const double beta = S->beta;
-  if (blockIdx.z == 0) pupd_col<KC>(P.f[0], Pn.f[0], R.f[0], M.f[0], beta);
-  else if (blockIdx.z == 1) pupd_col<KC>(P.f[1], Pn.f[1], R.f[1], M.f[1], beta);
-  else pupd_col<KC>(P.f[2], Pn.f[2], R.f[2], M.f[2], beta);
+  if (blockIdx.z == 0) pupd_col<KC, MM>(P.f[0], Pn.f[0], R.f[0], M.f[0], g, coeff, beta);
+  else if (blockIdx.z == 1) pupd_col<KC, MM>(P.f[1], Pn.f[1], R.f[1], M.f[1], g, coeff, beta);
+  else pupd_col<KC, MM>(P.f[2], Pn.f[2], R.f[2], M.f[2], g, coeff, beta);
 }
 
 // ---- p's implicit BC values (apply_BCs_implicit, PCG_solver_algorithm.f90:70) ----

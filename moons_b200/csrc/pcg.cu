@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "lean_cc.cuh"
 #include "mgrid.cuh"
 #include "runtime.cuh"
 
@@ -173,6 +174,15 @@ struct LeanGrids {
   dim3 gA, gB, gC, gD, gE;  // K1 (op), K2 (update), K3 (p update), BC fill, curl-curl edge pass
   unsigned npbP;            // perimeter plane blocks (BC fill)
   bool bc;
+  // one CC unknown under LAP_UNIFORM / LAP_PROPS / NRG_DIFFUSION: K1 is the
+  // shared-memory staged k_cc_lap (ghost values formed from the interior, no
+  // BC fill of p); grid gF, klen planes per block
+  bool cc;
+  dim3 gF;
+  int klen;
+  bool tm;             // the staged operator loads p through tensor maps (even s0)
+  CUtensorMap tmap[2];  // of p and p2
+  int mm;  // Minv of K2/K3: 0 stored, 1 prec_Lap, 2 prec_mom (formed per point)
 };
 
 }  // namespace mg
@@ -237,13 +247,17 @@ struct moons_pcg {
 };
 
 namespace {
+// internal fields carry 64 doubles of padding past their last point: a bulk
+// row copy of k_cc_lap (a fixed 36 doubles from an even element) may end up
+// to 33 doubles past the field
+constexpr size_t kFieldPad = 64;
 int alloc_df(moons_pcg* s, DF& f, int dl) {
   f = make_df(s->m, dl, nullptr);
-  if (cudaMalloc(&f.f, f.n() * sizeof(double)) != cudaSuccess) {
+  if (cudaMalloc(&f.f, (f.n() + kFieldPad) * sizeof(double)) != cudaSuccess) {
     set_error("moons_pcg: device allocation failed");
     return MOONS_ERR_NOMEM;
   }
-  cudaMemsetAsync(f.f, 0, f.n() * sizeof(double), s->m->stream);
+  cudaMemsetAsync(f.f, 0, (f.n() + kFieldPad) * sizeof(double), s->m->stream);
   s->allocs.push_back(f.f);
   return MOONS_OK;
 }
@@ -360,7 +374,10 @@ int compute_prec(moons_pcg* s) {
 
 
 // one PCG iteration (PCG_solver_algorithm.f90:69-96), enqueued on the mesh stream
-constexpr int kKCU = 2;  // planes per thread of the pointwise kernels (measured best)
+#ifndef MOONS_KCU
+#define MOONS_KCU 2
+#endif
+constexpr int kKCU = MOONS_KCU;  // planes per thread of the pointwise kernels
 
 // grid of a grid-stride kernel: every block resident, at most one per item
 unsigned resident_grid(const moons_pcg* s, const void* kern, size_t items) {
@@ -390,7 +407,31 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
   for (int half = 0; half < 2; half++) {
     DF* pc = half == 0 ? s->p : s->p2;
     DF* pn = half == 0 ? s->p2 : s->p;
-    switch (s->op) {
+    if (L.cc) {
+      const bool ev = (s->Ax[0].s0 & 1) == 0;
+      const CUtensorMap& tm = L.tmap[half];
+#define MG_CC_LAP(MD, EV, T, KX, KY, KZ, CF)                                                                  \
+  MG_LAUNCH_PDL_SMEM((k_cc_lap<MD, EV, T>), L.gF, kCThreads, cc_smem(L.klen), m->stream, tm, s->Ax[0], pc[0], m->dg, \
+                     b[0], KX, KY, KZ, CF, L.klen, s->S, s->partial, tA)
+      switch (s->op) {
+        case MOONS_OP_LAP_UNIFORM:
+          if (L.tm) MG_CC_LAP(0, true, true, z0, z0, z0, 0.0);
+          else if (ev) MG_CC_LAP(0, true, false, z0, z0, z0, 0.0);
+          else MG_CC_LAP(0, false, false, z0, z0, z0, 0.0);
+          break;
+        case MOONS_OP_LAP_PROPS:
+          if (L.tm) MG_CC_LAP(1, true, true, s->k[0], s->k[1], s->k[2], 0.0);
+          else if (ev) MG_CC_LAP(1, true, false, s->k[0], s->k[1], s->k[2], 0.0);
+          else MG_CC_LAP(1, false, false, s->k[0], s->k[1], s->k[2], 0.0);
+          break;
+        default:
+          if (L.tm) MG_CC_LAP(3, true, true, s->k[0], s->k[1], s->k[2], s->coeff);
+          else if (ev) MG_CC_LAP(3, true, false, s->k[0], s->k[1], s->k[2], s->coeff);
+          else MG_CC_LAP(3, false, false, s->k[0], s->k[1], s->k[2], s->coeff);
+          break;
+      }
+#undef MG_CC_LAP
+    } else switch (s->op) {
       case MOONS_OP_LAP_UNIFORM:
         MG_LAUNCH_PDL(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
                   0.0, s->S, s->partial, tA);
@@ -414,10 +455,23 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
                   m->dg, b[0], b[1], b[2], s->coeff, s->S, s->partial, tA);
         break;
     }
-    MG_LAUNCH_PDL(k_l_update<kKCU>, L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc), fc(s->Ax, nc),
-              fc(s->Minv, nc), b[0], b[1], b[2], s->S, s->partial, tB);
-    MG_LAUNCH_PDL(k_l_pupd<kKCU>, L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc), fc(s->Minv, nc), s->S);
-    if (L.bc) MG_LAUNCH_PDL(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, nc), b[0], b[1], b[2], L.npbP, s->S);
+    if (L.mm == 1) {
+      MG_LAUNCH_PDL((k_l_update<kKCU, 1>), L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc),
+                    fc(s->Ax, nc), fc(s->Minv, nc), b[0], b[1], b[2], m->dg, s->coeff, s->S, s->partial, tB);
+      MG_LAUNCH_PDL((k_l_pupd<kKCU, 1>), L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc),
+                    fc(s->Minv, nc), m->dg, s->coeff, s->S);
+    } else if (L.mm == 2) {
+      MG_LAUNCH_PDL((k_l_update<kKCU, 2>), L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc),
+                    fc(s->Ax, nc), fc(s->Minv, nc), b[0], b[1], b[2], m->dg, s->coeff, s->S, s->partial, tB);
+      MG_LAUNCH_PDL((k_l_pupd<kKCU, 2>), L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc),
+                    fc(s->Minv, nc), m->dg, s->coeff, s->S);
+    } else {
+      MG_LAUNCH_PDL((k_l_update<kKCU, 0>), L.gB, kLB, m->stream, fc(x, nc), fc(pc, nc), fc(s->r, nc),
+                    fc(s->Ax, nc), fc(s->Minv, nc), b[0], b[1], b[2], m->dg, s->coeff, s->S, s->partial, tB);
+      MG_LAUNCH_PDL((k_l_pupd<kKCU, 0>), L.gC, kLB, m->stream, fc(pc, nc), fc(pn, nc), fc(s->r, nc),
+                    fc(s->Minv, nc), m->dg, s->coeff, s->S);
+    }
+    if (L.bc && !L.cc) MG_LAUNCH_PDL(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, nc), b[0], b[1], b[2], L.npbP, s->S);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
@@ -482,8 +536,33 @@ void plan_lean(moons_pcg* s) {
                    : s->op == MOONS_OP_NRG_DIFFUSION ? (const void*)k_l_lap<3>
                                                     : (const void*)k_l_curl_ap;
   L.gA = lean_grid(s, ka, s->Ax, nc, kKC);
-  L.gB = lean_grid(s, (const void*)k_l_update<kKCU>, s->Ax, nc, kKCU);
-  L.gC = lean_grid(s, (const void*)k_l_pupd<kKCU>, s->Ax, nc, kKCU);
+  L.mm = (s->prec == MOONS_PREC_LAP) ? 1 : (s->prec == MOONS_PREC_MOM ? 2 : 0);
+  // grids sized with the variant that runs (its occupancy sets the wave)
+  const void* kB = L.mm == 1 ? (const void*)k_l_update<kKCU, 1>
+                   : L.mm == 2 ? (const void*)k_l_update<kKCU, 2> : (const void*)k_l_update<kKCU, 0>;
+  const void* kC = L.mm == 1 ? (const void*)k_l_pupd<kKCU, 1>
+                   : L.mm == 2 ? (const void*)k_l_pupd<kKCU, 2> : (const void*)k_l_pupd<kKCU, 0>;
+  L.gB = lean_grid(s, kB, s->Ax, nc, kKCU);
+  L.gC = lean_grid(s, kC, s->Ax, nc, kKCU);
+  L.cc = nc == 1 && s->x_dl[0] == MOONS_CC && s->Ax[0].s0 >= 3 && s->Ax[0].s1 >= 3 && s->Ax[0].s2 >= 3 &&
+         (s->op == MOONS_OP_LAP_UNIFORM || s->op == MOONS_OP_LAP_PROPS || s->op == MOONS_OP_NRG_DIFFUSION);
+  L.gF = dim3(1, 1, 1);
+  L.klen = 1;
+  if (L.cc) {
+    const bool ev = (s->Ax[0].s0 & 1) == 0;
+    std::memset(L.tmap, 0, sizeof(L.tmap));
+    L.tm = ev && cc_tensor_map(&L.tmap[0], s->p[0]) && cc_tensor_map(&L.tmap[1], s->p2[0]);
+    const int md = s->op == MOONS_OP_LAP_UNIFORM ? 0 : (s->op == MOONS_OP_LAP_PROPS ? 1 : 3);
+    const void* kf = nullptr;
+#define MG_CC_PICK(MD)                                                                                   \
+  kf = L.tm ? (const void*)k_cc_lap<MD, true, true>                                                      \
+            : (ev ? (const void*)k_cc_lap<MD, true, false> : (const void*)k_cc_lap<MD, false, false>)
+    if (md == 0) MG_CC_PICK(0);
+    else if (md == 1) MG_CC_PICK(1);
+    else MG_CC_PICK(3);
+#undef MG_CC_PICK
+    L.gF = cc_lap_grid(s->Ax[0], s->nsm, kf, L.klen);
+  }
   L.gE = dim3(1, 1, 1);
   if (s->op == MOONS_OP_IND_DIFFUSION) L.gE = lean_grid(s, (const void*)k_l_curl_sig, s->tempk, 3, kKC);
   // BC fill: perimeter blocks over every plane, then inner blocks (ghost planes)
@@ -656,7 +735,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     const LeanGrids& L = s->lg;
     dim3 G2 = fgrid(s->Ax, nc);
     size_t nb = (size_t)G2.x * G2.y * G2.z;
-    for (const dim3& g : {L.gA, L.gB, L.gC, L.gD, L.gE}) nb = std::max(nb, (size_t)g.x * g.y * g.z);
+    for (const dim3& g : {L.gA, L.gB, L.gC, L.gD, L.gE, L.gF}) nb = std::max(nb, (size_t)g.x * g.y * g.z);
     nb = std::max<size_t>(nb, kRedBlocks);
     s->max_blocks = nb;
     void* p;
@@ -869,6 +948,8 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
   MG_LAUNCH(k_reduce, red_grid(s->r, nc), kBlock, m->stream, c3(s->r, nc), c3(s->z, nc), 0, dw[0], dw[1], dw[2],
             &s->S->rhok, m->d_partial, m->d_ticket);
   MG_LAUNCH(k_pcg_start, 1, 1, m->stream, s->S);
+  // k_cc_lap writes Ap on interior points only: its ghost points stay 0
+  if (s->lg.cc && !s->mgh) MG_CUDA(cudaMemsetAsync(s->Ax[0].f, 0, s->Ax[0].n() * sizeof(double), m->stream));
   MG_CUDA(cudaGetLastError());
   // ---- the loop.  MOONS_PCG_HOSTLOOP=1 launches the iteration as separate
   // kernels from the host in chunks of 32 iterations (kernels skip
@@ -917,6 +998,12 @@ int mg_pcg_collect(moons_pcg* s, moons_solve_info* info, float ms) {
     info->rel = (H.res0 == 0.0) ? H.res : H.res / H.res0;
     info->exit_reason = H.exit_reason;
     info->ms = ms;
+  }
+  if (H.wait_err) {
+    const int code = H.wait_err;
+    cudaMemsetAsync(&s->S->wait_err, 0, sizeof(int), m->stream);
+    set_error("moons_pcg_solve: a bounded shared-memory stage wait ran out (site " + std::to_string(code) + ")");
+    return MOONS_ERR_CUDA;
   }
   if (H.nan || std::isnan(H.res0) || std::isnan(H.res)) {
     set_error("moons_pcg_solve: NaN in residual norms");

@@ -75,6 +75,7 @@ def lib():
                                         _F, _F, _F, _F, C.c_int, _F]),
             "or_unet_nparams": (C.c_longlong, []),
             "or_unet_set_exact": (None, [C.c_int]),
+            "or_unet_adam": (None, [_F, _F, _F, _F, C.c_longlong, C.c_float, C.c_int]),
             "or_unet_forward": (C.c_int, [C.c_int, C.c_int, C.c_int, _F, C.c_double, _D, _F, _D]),
             "or_unet_loss_grad": (C.c_int, [C.c_int, C.c_int, C.c_int, _F, C.c_double, _D, _F, _D, C.c_int, _D, _D,
                                             _D, C.c_double, _D, _F]),
@@ -308,6 +309,14 @@ def unet_layer(op, X, Y, Z, cinA, cinB, cout, inp=None, dout=None, W=None, bias=
 def unet_set_exact(on: bool):
     """Exact arithmetic (no BF16 rounding) in the U-Net restatement."""
     lib().or_unet_set_exact(int(bool(on)))
+
+
+def unet_adam(w, g, m, v, lr: float, t: int):
+    """One Adam step on FP32 arrays (w, m, v updated in place), the CPU
+    statement of the library's training-step update."""
+    for a in (w, g, m, v):
+        assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    lib().or_unet_adam(_fptr(w), _fptr(g), _fptr(m), _fptr(v), C.c_longlong(w.size), C.c_float(lr), int(t))
 
 
 def unet_nparams() -> int:

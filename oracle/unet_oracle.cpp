@@ -476,4 +476,22 @@ int or_unet_loss_grad(int X, int Y, int Z, const float* params, double out_scale
   return 0;
 }
 
+// One Adam step (Kingma & Ba 2015, Algorithm 1) on a flat FP32 parameter
+// vector, in the form the library's training step applies it: m = b1 m +
+// (1-b1) g, v = b2 v + (1-b2) g^2, w -= lr (m c1) / (sqrt(v c2) + eps) with
+// the bias corrections c1 = 1/(1-b1^t), c2 = 1/(1-b2^t); FP32 throughout.
+void or_unet_adam(float* w, const float* g, float* m, float* v, long long n, float lr, int t) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float c1 = 1.f / (1.f - std::pow(b1, (float)t));
+  const float c2 = 1.f / (1.f - std::pow(b2, (float)t));
+  for (long long i = 0; i < n; i++) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi * c1) / (std::sqrt(vi * c2) + eps);
+  }
+}
+
 }  // extern "C"

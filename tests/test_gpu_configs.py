@@ -29,12 +29,28 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TOL = 1e-10
+# The pressure is the projection's Lagrange multiplier, solved to a 1e-10
+# relative residual: two CG runs whose dot products add in different orders
+# stop one iteration apart at that tolerance, which moves p by a few 1e-10
+# (relative) while the projected velocity agrees to ~1e-13.  Its bound is the
+# solver's stopping error, one decade above the other fields'.
+TOL_P = 1e-9
 
 
 def rel_l2(a, b):
     d = np.linalg.norm((a - b).ravel())
     n = np.linalg.norm(b.ravel())
     return d / n if n > 0 else d
+
+
+def rel_l2_mean_free(a, b):
+    """Relative L2 of interior values with each field's interior mean removed:
+    the pressure of an all-Neumann (or periodic) problem is defined up to a
+    constant, which the CG iterates leave at round-off-dependent values (the
+    velocity, formed from its gradient, is compared as is)."""
+    I = (slice(1, -1),) * 3
+    a, b = a[I] - a[I].mean(), b[I] - b[I].mean()
+    return rel_l2(a, b)
 
 
 def test_config1_ldc32_1000_steps_match_oracle_fixture():
@@ -48,9 +64,9 @@ def test_config1_ldc32_1000_steps_match_oracle_fixture():
             tot[k] += info[k]
     worst = {}
     for name, which, c in mk.FIELDS_LONG:
-        e = rel_l2(sim.download(which, c), z[name])
-        worst[name] = e
-    assert max(worst.values()) <= TOL, worst
+        f = rel_l2_mean_free if which == G.MHD_P else rel_l2
+        worst[name] = f(sim.download(which, c), z[name])
+    assert all(e <= (TOL_P if n == "p" else TOL) for n, e in worst.items()), worst
     du, db = sim.divergence()
     assert du <= max(10.0 * float(z["div_u"]), 1e-24), (du, float(z["div_u"]))
     assert db <= max(10.0 * float(z["div_b"]), 1e-24), (db, float(z["div_b"]))
@@ -67,8 +83,9 @@ def test_config2_duct_full_size_two_steps_match_oracle():
              [(G.MHD_J, c) for c in range(3)] + [(G.MHD_JXB, c) for c in range(3)]
     worst = {}
     for which, c in fields:
-        worst[(which, c)] = rel_l2(g.download(which, c), o.download(which, c))
-    assert max(worst.values()) <= TOL, worst
+        f = rel_l2_mean_free if which == G.MHD_P else rel_l2
+        worst[(which, c)] = f(g.download(which, c), o.download(which, c))
+    assert all(e <= (TOL_P if w == G.MHD_P else TOL) for (w, _), e in worst.items()), worst
     dug, dbg = g.divergence()
     duo, dbo = o.divergence()
     assert dug <= max(10 * duo, 1e-24) and dbg <= max(10 * dbo, 1e-24), (dug, duo, dbg, dbo)

@@ -63,8 +63,11 @@ def test_mhd_steps_match_oracle(name, builder, kw):
     duo, dbo = o.divergence()
     assert dug <= max(10 * duo, 1e-24)
     assert dbg <= max(10 * dbo, 1e-24)
+    # iteration counts: within one per solve, or 0.5% for solves of
+    # hundreds of iterations (whose last iteration moves with the order of
+    # the floating-point sums)
     for k in ("iters_U", "iters_p", "iters_B", "iters_phi", "iters_T"):
-        assert abs(ig[k] - io[k]) <= nsteps, (k, ig, io)
+        assert abs(ig[k] - io[k]) <= max(nsteps, 0.005 * io[k]), (k, ig, io)
 
 
 @pytest.mark.parametrize("prec", [G.PREC_MG, G.PREC_MG_MIXED, G.PREC_FD], ids=["mg", "mixed", "fd"])

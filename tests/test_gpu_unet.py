@@ -190,3 +190,34 @@ def test_adam_steps_lower_the_loss():
     for _ in range(40):
         last = net.train_step(fr, fe, 1e-3)
     assert np.isfinite(last) and last < 0.5 * first
+
+
+def test_adam_matches_oracle():
+    """Three training steps: the parameters after each step against a CPU Adam
+    (oracle, FP32) fed the same gradients (moons_unet_loss_grad at the
+    current parameters) and the same moments.  The training step recomputes
+    the gradient itself, whose FP32 atomic weight-gradient sums may differ
+    from the fetched one in the last bits, so the step (w_new - w_old) must
+    agree to 1e-4 relative (Adam's first steps move each weight by about lr)."""
+    X, Y, Z = 16, 16, 16
+    m, fr, fe, r, e, feat = _problem(X, Y, Z, 6)
+    net = G.UNet(m, seed=2)
+    net.set_loss(1)
+    net.set_feature(feat)
+    w = net.get_params().astype(np.float32)
+    mo = np.zeros_like(w)
+    vo = np.zeros_like(w)
+    lr = 1e-3
+    for t in range(1, 4):
+        _, g = net.loss_grad(fr, fe)
+        g = np.ascontiguousarray(g, dtype=np.float32)
+        w_cpu = w.copy()
+        O.unet_adam(w_cpu, g, mo, vo, lr, t)
+        net.train_step(fr, fe, lr)
+        w_gpu = net.get_params().astype(np.float32)
+        dg, dc = w_gpu - w, w_cpu - w
+        big = np.abs(g) > 1e-6  # away from eps = 1e-8 and from sign flips of ~0 gradients
+        assert big.sum() > 100000
+        rel = np.abs(dg[big] - dc[big]).max() / np.abs(dc[big]).max()
+        assert rel < 1e-4, (t, rel)
+        w = w_gpu
