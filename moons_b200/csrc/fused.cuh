@@ -39,6 +39,11 @@ struct PcgScalars {
   double stag_factor, stag_ref;
   // nonzero: a bounded wait in a loop kernel ran out (the code names the site)
   int wait_err;
+  // fused CC iteration: the x update x += alpha p of an iteration is applied
+  // by the next iteration's operator kernel; last_half names the p buffer of
+  // the iteration that ended the loop (0: p2, 1: p; -1: none ran), whose
+  // update a kernel after the loop applies
+  int last_half;
 };
 
 // implicit BCs + masks of one unknown component, as the fused kernels see them

@@ -428,10 +428,12 @@ __device__ __forceinline__ double minv_k(const MinvCol& c, const DGrid& g, int d
   return 1.0 / (d * (c.vxy * vol_axis(g.c[2], Nz, k)));
 }
 
-template <int KC, int MM>
+// SZ: also store z = Minv r at every non-ghost point (the fused CC iteration
+// forms the next p from it in its operator kernel)
+template <int KC, int MM, bool SZ = false>
 __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r, const DF& Ap, const DF& M,
                                            const FBC& b, const DGrid& g, double coeff, double alpha, double& arr,
-                                           double& azr) {
+                                           double& azr, const DF& zo = DF{}) {
   const Col cl = col_of(x, blockIdx.x);
   if (!cl.ok) return;
   const int i = cl.i, j = cl.j;
@@ -447,8 +449,8 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
     for (int q = 0; q < KC; q++) {
       const bool in = k0 + q <= k1;
       const size_t idx = idx0 + (size_t)q * sz;
-      xv[q] = in ? x.f[idx] : 0.0;
-      pv[q] = in ? ld(p.f + idx) : 0.0;
+      xv[q] = (!SZ && in) ? x.f[idx] : 0.0;
+      pv[q] = (!SZ && in) ? ld(p.f + idx) : 0.0;
       rv[q] = in ? r.f[idx] : 0.0;
       av[q] = in ? ld(Ap.f + idx) : 0.0;
       mv[q] = (MM == 0 && in) ? ld(M.f + idx) : 0.0;
@@ -458,10 +460,20 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
       const int k = k0 + q;
       if (k > k1) break;
       const size_t idx = idx0 + (size_t)q * sz;
-      x.f[idx] = xv[q] + pv[q] * alpha;
+      if (!SZ) x.f[idx] = xv[q] + pv[q] * alpha;  // SZ: x is updated by the next operator kernel
       const double rn = rv[q] + av[q] * (-alpha);
       r.f[idx] = rn;
-      if (inxy && k != 1 && k != x.s2 && dot_z(x, b, k)) {
+      if (SZ) {
+        if (!cl.gij && k != 1 && k != x.s2) {
+          const double m = MM == 0 ? mv[q] : minv_k<MM>(mc, g, x.dl, k, coeff);
+          const double zv = m * rn;
+          zo.f[idx] = zv;
+          if (inxy && dot_z(x, b, k)) {
+            arr += rn * rn;
+            azr += zv * rn;
+          }
+        }
+      } else if (inxy && k != 1 && k != x.s2 && dot_z(x, b, k)) {
         const double m = MM == 0 ? mv[q] : minv_k<MM>(mc, g, x.dl, k, coeff);
         const double zv = m * rn;
         arr += rn * rn;
@@ -470,17 +482,19 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
     }
   }
 }
-template <int KC, int MM>
+template <int KC, int MM, bool SZ = false>
 __global__ void __launch_bounds__(kLB, 5) k_l_update(FComp X, FComp P, FComp R, FComp Ap, FComp M, FBC b0, FBC b1,
                                                    FBC b2, DGrid g, double coeff, PcgScalars* S, double* partial,
-                                                   unsigned* ticket) {
+                                                   unsigned* ticket, DF zo, int half) {
   pdl_enter();
   if (S->done) return;
   double arr = 0.0, azr = 0.0;
   const double alpha = S->alpha;
-  if (blockIdx.z == 0) update_col<KC, MM>(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, g, coeff, alpha, arr, azr);
-  else if (blockIdx.z == 1) update_col<KC, MM>(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, g, coeff, alpha, arr, azr);
-  else update_col<KC, MM>(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, g, coeff, alpha, arr, azr);
+  if (blockIdx.z == 0)
+    update_col<KC, MM, SZ>(X.f[0], P.f[0], R.f[0], Ap.f[0], M.f[0], b0, g, coeff, alpha, arr, azr, zo);
+  else if (blockIdx.z == 1)
+    update_col<KC, MM, SZ>(X.f[1], P.f[1], R.f[1], Ap.f[1], M.f[1], b1, g, coeff, alpha, arr, azr, zo);
+  else update_col<KC, MM, SZ>(X.f[2], P.f[2], R.f[2], Ap.f[2], M.f[2], b2, g, coeff, alpha, arr, azr, zo);
   const double s_rr = block_sum(arr);
   const double s_zr = block_sum(azr);
   const unsigned fb = flat_block(), nb = n_blocks();
@@ -523,7 +537,24 @@ __global__ void __launch_bounds__(kLB, 5) k_l_update(FComp X, FComp P, FComp R, 
         }
       }
       S->done = stop ? 1 : 0;
+      if (SZ && stop) S->last_half = half;
     }
+  }
+}
+
+// fused CC iteration, after the loop: the update x += alpha p of the
+// iteration that ended it (interior points; apply_BCs of x follows)
+__global__ void k_cc_xfinal(DF x, DF p, DF p2, const PcgScalars* S) {
+  const int h = S->last_half;
+  if (h < 0) return;
+  const DF& pl = h == 0 ? p2 : p;
+  const double alpha = S->alpha;
+  const size_t n = x.n();
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    ijk_of(idx, x, i, j, k);
+    if (i == 1 || i == x.s0 || j == 1 || j == x.s1 || k == 1 || k == x.s2) continue;
+    x.f[idx] = x.f[idx] + pl.f[idx] * alpha;
   }
 }
 

@@ -40,12 +40,16 @@ constexpr int kCTY = kCW * kCRW;         // tile rows along y
 constexpr int kCRows = kCTY + 2;         // staged rows per plane
 constexpr int kCRS = kCTX + 4;           // row stride (doubles): 34 values + alignment shift, 16-byte multiple
 constexpr int kCStages = 8;              // planes in the ring
+constexpr int kCStagesF = 6;             // planes in the ring when p and z are staged
 constexpr int kCStage = ((kCRows * kCRS + 15) / 16) * 16;  // doubles per stage (128-byte multiple)
 constexpr int kCWaitCode = 101;          // wait_err code of a stage wait that ran out
 constexpr int kCThreads = (kCW + 1) * 32;  // compute warps and one producer warp
 // dynamic shared memory: 128 bytes of alignment slack, the ring, then 8
 // doubles of z coefficients per plane of the block's chunk
-inline size_t cc_smem(int klen) { return 128 + ((size_t)kCStages * kCStage + 8 * (size_t)klen) * sizeof(double); }
+inline size_t cc_smem(int klen, bool fz) {
+  const size_t ring = fz ? (size_t)kCStagesF * 2 * kCStage : (size_t)kCStages * kCStage;
+  return 128 + (ring + 8 * (size_t)klen) * sizeof(double);
+}
 
 // ghost rule at one face of a CC axis: kind 0 stored value, 1 fac * adjacent
 // interior cell, 2 the interior cell at the far end (periodic)
@@ -79,35 +83,39 @@ MG_HD int cc_tiles(const DF& a) { return cc_tiles_x(a) * ((a.s1 - 2 + kCTY - 1) 
 // stages are filled by one tiled tensor load (TMA) per plane through `tmap`
 // (a 3-D map of p with a 36 x 18 x 1 box; needs EVEN) instead of one bulk
 // copy per row.
-template <int MODE, bool EVEN, bool TM>
-__global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const __grid_constant__ CUtensorMap tmap,
-                                                         DF A, DF p, DGrid g, FBC b, DF kx, DF ky, DF kz,
-                                                         double coeff, int klen, PcgScalars* S, double* partial,
-                                                         unsigned* ticket) {
+// FZ (fused iteration): the operator acts on p' = beta p + z, formed here
+// from the staged p and z (z = Minv r, stored by the update kernel), and p'
+// is written to pn -- the p update of the previous iteration folded into
+// this kernel (PCG_solver_algorithm.f90:93-96, then :70-76); the previous
+// iteration's x += alpha p (:78-79), with the staged p, is applied here too.
+template <int MODE, bool EVEN, bool TM, bool FZ>
+__global__ void __launch_bounds__(kCThreads, (MODE == 0 && !FZ) ? 3 : 2)
+    k_cc_lap(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmapz, DF A, DF p, DF z,
+             DF pn, DF x, DGrid g, FBC b, DF kx, DF ky, DF kz, double coeff, int klen, PcgScalars* S, double* partial,
+             unsigned* ticket) {
+  constexpr int NST = FZ ? kCStagesF : kCStages;  // stages in the ring
+  constexpr int SST = (FZ ? 2 : 1) * kCStage;     // doubles per stage (p, then z)
   extern __shared__ __align__(16) double smem_raw[];
-  // kCStages stages of kCRows x kCRS doubles, 128-byte aligned (tensor loads)
+  // NST stages of kCRows x kCRS doubles per staged array, 128-byte aligned (tensor loads)
   double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
   __shared__ __align__(8) unsigned long long full[kCStages], empty[kCStages];
-  pdl_enter();
-  if (S->done) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int ntx = cc_tiles_x(A);
   const int i0 = 2 + (int)(blockIdx.x % (unsigned)ntx) * kCTX, j0 = 2 + (int)(blockIdx.x / (unsigned)ntx) * kCTY;
   const int kb = 2 + (int)blockIdx.y * klen, ke = min(A.s2 - 1, kb + klen - 1);
-  double acc = 0.0;
-  if (kb <= ke) {  // uniform per block
-    const unsigned s0 = (unsigned)A.s0, sxy = (unsigned)A.s0 * (unsigned)A.s1;
-    const int nq = ke - kb + 3;                       // staged planes kb-1 .. ke+1
-    const int nrows = min(kCRows, A.s1 - j0 + 2);     // staged rows j0-1 .. min(j0+kCTY, s1)
+  const bool work = kb <= ke;  // uniform per block
+  double* zt = ring + NST * SST;
+  // ---- set-up that reads nothing the preceding kernel writes: it runs
+  // while that kernel drains (programmatic dependent launch)
+  if (work) {
     if (threadIdx.x == 0) {
-      for (int s = 0; s < kCStages; s++) {
+      for (int s = 0; s < NST; s++) {
         tc::mbar_init(tc::smem_u32(&full[s]), 1);
         tc::mbar_init(tc::smem_u32(&empty[s]), kCW);  // one arrival per compute warp
       }
       tc::fence_mbar_init();
     }
     // the z coefficients of the block's planes, once: a1 a2 b1 b2 o1 o2 dhn
-    double* zt = ring + kCStages * kCStage;
     for (int t = threadIdx.x; t < (ke - kb + 1) * 8; t += blockDim.x) {
       const int k = kb + t / 8, f = t % 8;
       const DCoord& c = g.c[2];
@@ -119,7 +127,15 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
                 : f == 4 ? c.n2ccD[k] : f == 5 ? c.n2ccU[k] : f == 6 ? c.dhn[k] : 0.0;
       }
     }
-    __syncthreads();
+  }
+  __syncthreads();
+  pdl_enter();
+  if (S->done) return;
+  double acc = 0.0;
+  if (work) {
+    const unsigned s0 = (unsigned)A.s0, sxy = (unsigned)A.s0 * (unsigned)A.s1;
+    const int nq = ke - kb + 3;                       // staged planes kb-1 .. ke+1
+    const int nrows = min(kCRows, A.s1 - j0 + 2);     // staged rows j0-1 .. min(j0+kCTY, s1)
     if (w == kCW) {
       // ---- producer warp: row r of plane kb-1+q -> stage q % kCStages.  A
       // row copy is kCRS doubles from the even element at or below (i0-1, jr,
@@ -128,26 +144,28 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
       bool live = true;
       int issued = 0;
       for (int q = 0; q < nq; q++) {
-        const int st = q % kCStages;
-        if (q >= kCStages && live)
-          live = tc::mbar_wait_sleep(tc::smem_u32(&empty[st]), (uint32_t)(((q / kCStages) - 1) & 1), &S->wait_err,
-                               kCWaitCode);
+        const int st = q % NST;
+        if (q >= NST && live)
+          live = tc::mbar_wait_sleep(tc::smem_u32(&empty[st]), (uint32_t)(((q / NST) - 1) & 1), &S->wait_err,
+                                     kCWaitCode);
         if (!live) break;
         const int k = kb - 1 + q;
         const uint32_t bar = tc::smem_u32(&full[st]);
         if (TM) {
-          // one box: columns i0-1 .. i0+34, rows j0-1 .. j0+16 of plane k
-          // (0-based x = i0-2, even), zero fill past the field
+          // one box per staged array: columns i0-1 .. i0+34, rows j0-1 ..
+          // j0+16 of plane k (0-based x = i0-2, even), zero fill past the field
           if (lane == 0) {
-            tc::mbar_expect_tx(bar, (uint32_t)(kCRows * kCRS * 8));
-            tc::tma_load_3d(tc::smem_u32(ring + st * kCStage), &tmap, i0 - 2, j0 - 2, k - 1, bar);
+            tc::mbar_expect_tx(bar, (uint32_t)((FZ ? 2 : 1) * kCRows * kCRS * 8));
+            tc::tma_load_3d(tc::smem_u32(ring + st * SST), &tmap, i0 - 2, j0 - 2, k - 1, bar);
+            if (FZ) tc::tma_load_3d(tc::smem_u32(ring + st * SST + kCStage), &tmapz, i0 - 2, j0 - 2, k - 1, bar);
           }
         } else {
-          if (lane == 0) tc::mbar_expect_tx(bar, (uint32_t)nrows * (uint32_t)(kCRS * 8));
+          if (lane == 0) tc::mbar_expect_tx(bar, (uint32_t)((FZ ? 2 : 1) * nrows) * (uint32_t)(kCRS * 8));
           __syncwarp();
           for (int r = lane; r < nrows; r += 32) {
             const unsigned e0 = (unsigned)(k - 1) * sxy + (unsigned)(j0 - 2 + r) * s0 + (unsigned)(i0 - 2);
-            tc::bulk_g2s(tc::smem_u32(ring + st * kCStage + r * kCRS), p.f + (e0 & ~1u), kCRS * 8, bar);
+            tc::bulk_g2s(tc::smem_u32(ring + st * SST + r * kCRS), p.f + (e0 & ~1u), kCRS * 8, bar);
+            if (FZ) tc::bulk_g2s(tc::smem_u32(ring + st * SST + kCStage + r * kCRS), z.f + (e0 & ~1u), kCRS * 8, bar);
           }
         }
         issued = q + 1;
@@ -155,9 +173,8 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
       // no copy may land in this block's shared memory after it exits: wait
       // (bounded) for the last copy issued into each stage
       if (lane == 0)
-        for (int q = max(0, issued - kCStages); q < issued; q++)
-          tc::mbar_wait(tc::smem_u32(&full[q % kCStages]), (uint32_t)((q / kCStages) & 1), &S->wait_err,
-                        kCWaitCode);
+        for (int q = max(0, issued - NST); q < issued; q++)
+          tc::mbar_wait(tc::smem_u32(&full[q % NST]), (uint32_t)((q / NST) & 1), &S->wait_err, kCWaitCode);
     } else {
       // ---- compute warps: warp w owns tile rows jw .. jw+kCRW-1, lane the column
       const int i = i0 + lane, jw = j0 + w * kCRW;
@@ -197,12 +214,24 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
       bool ok = true;
       auto wait_q = [&](int q) {
         if (ok)
-          ok = tc::mbar_wait_sleep(tc::smem_u32(&full[q % kCStages]), (uint32_t)((q / kCStages) & 1), &S->wait_err,
-                             kCWaitCode);
+          ok = tc::mbar_wait_sleep(tc::smem_u32(&full[q % NST]), (uint32_t)((q / NST) & 1), &S->wait_err,
+                                   kCWaitCode);
       };
       auto release = [&](int q) {
         __syncwarp();
-        if (lane == 0) tc::mbar_arrive(tc::smem_u32(&empty[q % kCStages]));
+        if (lane == 0) tc::mbar_arrive(tc::smem_u32(&empty[q % NST]));
+      };
+      // the operand at a staged offset: p, or (FZ) p' = beta p + z
+      const double beta = FZ ? S->beta : 0.0;
+      const double alpha_prev = FZ ? S->alpha : 0.0;  // the previous iteration's alpha (x update)
+      auto sv = [&](int off) -> double {
+        if (FZ) return ring[off] * beta + ring[off + kCStage];
+        return ring[off];
+      };
+      // the operand at an interior point read from global memory (periodic ghost sources)
+      auto gv = [&](int ii, int jj, int kk) -> double {
+        if (FZ) return p(ii, jj, kk) * beta + z(ii, jj, kk);
+        return p(ii, jj, kk);
       };
       // planes kb-1 (pm) and kb (p0)
       wait_q(0);
@@ -210,41 +239,54 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
       double pm[kCRW], p0[kCRW];
       {
         const unsigned a0 = ((unsigned)(kb - 2) & 1u) & oddxy, a1 = ((unsigned)(kb - 1) & 1u) & oddxy;
-        const int s1b = (1 % kCStages) * kCStage;
+        const int s1b = (1 % NST) * SST;
 #pragma unroll
         for (int r = 0; r < kCRW; r++) {
-          p0[r] = ring[s1b + roff(jw + r, a1)];
-          pm[r] = ring[roff(jw + r, a0)];
+          p0[r] = sv(s1b + roff(jw + r, a1));
+          pm[r] = sv(roff(jw + r, a0));
           if (kb - 1 == 1) {  // plane 1 is the ghost plane
             const CGhost gzm = cghost(b, 5);
             if (gzm.kind == 1) pm[r] = gzm.fac * p0[r];
-            else if (gzm.kind == 2 && act[r]) pm[r] = p(i, jw + r, A.s2 - 1);
+            else if (gzm.kind == 2 && act[r]) pm[r] = gv(i, jw + r, A.s2 - 1);
           }
         }
       }
       release(0);
-      double* out = coli ? A.f + A.at(i, min(jw, A.s1), kb) : A.f;  // (i, jw, k): + r*s0 per row, + sxy per plane
+      const size_t o0 = coli ? A.at(i, min(jw, A.s1), kb) : 0;  // (i, jw, kb): + r*s0 per row, + sxy per plane
+      double* out = A.f + o0;
+      double* outp = FZ ? pn.f + o0 : nullptr;
+      double* xo = FZ ? x.f + o0 : nullptr;
+      double xv[kCRW];  // x of this plane, loaded one plane ahead
+      if (FZ) {
+#pragma unroll
+        for (int r = 0; r < kCRW; r++) xv[r] = act[r] ? xo[r * (int)s0] : 0.0;
+      }
 #pragma unroll 2
-      for (int k = kb; k <= ke; k++, out += sxy) {
+      for (int k = kb; k <= ke; k++, out += sxy, outp += FZ ? sxy : 0, xo += FZ ? sxy : 0) {
         const int qk = k - kb + 1;
+        double xn[kCRW];
+        if (FZ) {
+#pragma unroll
+          for (int r = 0; r < kCRW; r++) xn[r] = (act[r] && k < ke) ? xo[sxy + r * (int)s0] : 0.0;
+        }
         wait_q(qk + 1);
-        const int sk = (qk % kCStages) * kCStage, sn = ((qk + 1) % kCStages) * kCStage;
+        const int sk = (qk % NST) * SST, sn = ((qk + 1) % NST) * SST;
         const unsigned ak = ((unsigned)(k - 1) & 1u) & oddxy, an = ((unsigned)k & 1u) & oddxy;
         double pp[kCRW], xm[kCRW], xp[kCRW];
 #pragma unroll
         for (int r = 0; r < kCRW; r++) {
-          pp[r] = ring[sn + roff(jw + r, an)];
+          pp[r] = sv(sn + roff(jw + r, an));
           const int c0 = sk + roff(jw + r, ak);
-          xm[r] = ring[c0 - 1];
-          xp[r] = ring[c0 + 1];
+          xm[r] = sv(c0 - 1);
+          xp[r] = sv(c0 + 1);
         }
-        const double ylo = ring[sk + roff(jw - 1, ak)], yhi = ring[sk + roff(jw + kCRW, ak)];
+        const double ylo = sv(sk + roff(jw - 1, ak)), yhi = sv(sk + roff(jw + kCRW, ak));
         if (k + 1 == A.s2) {  // plane s2 is the ghost plane
           const CGhost gzp = cghost(b, 6);
 #pragma unroll
           for (int r = 0; r < kCRW; r++)
             if (gzp.kind == 1) pp[r] = gzp.fac * p0[r];
-            else if (gzp.kind == 2 && act[r]) pp[r] = p(i, jw + r, 2);
+            else if (gzp.kind == 2 && act[r]) pp[r] = gv(i, jw + r, 2);
         }
         const double* zk = zt + (k - kb) * 8;
         Ax6 Z{};
@@ -267,19 +309,19 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
           if (edge && act[r]) {
             if (i == 2) {
               const CGhost gh = cghost(b, 1);
-              if (gh.kind) xmr = gh.kind == 1 ? gh.fac * p0[r] : p(A.s0 - 1, j, k);
+              if (gh.kind) xmr = gh.kind == 1 ? gh.fac * p0[r] : gv(A.s0 - 1, j, k);
             }
             if (i == A.s0 - 1) {
               const CGhost gh = cghost(b, 2);
-              if (gh.kind) xpr = gh.kind == 1 ? gh.fac * p0[r] : p(2, j, k);
+              if (gh.kind) xpr = gh.kind == 1 ? gh.fac * p0[r] : gv(2, j, k);
             }
             if (j == 2) {
               const CGhost gh = cghost(b, 3);
-              if (gh.kind) ym = gh.kind == 1 ? gh.fac * p0[r] : p(i, A.s1 - 1, k);
+              if (gh.kind) ym = gh.kind == 1 ? gh.fac * p0[r] : gv(i, A.s1 - 1, k);
             }
             if (j == A.s1 - 1) {
               const CGhost gh = cghost(b, 4);
-              if (gh.kind) yp = gh.kind == 1 ? gh.fac * p0[r] : p(i, 2, k);
+              if (gh.kind) yp = gh.kind == 1 ? gh.fac * p0[r] : gv(i, 2, k);
             }
           }
           const double c = p0[r];
@@ -315,6 +357,10 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
           v = v * (vxy[r] * vz);
           if (act[r]) {
             out[r * (int)s0] = v;
+            if (FZ) {
+              outp[r * (int)s0] = c;
+              xo[r * (int)s0] = xv[r] + ring[sk + roff(j, ak)] * alpha_prev;  // x += alpha p (staged p)
+            }
             acc += c * v;
           }
         }
@@ -322,6 +368,7 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
         for (int r = 0; r < kCRW; r++) {
           pm[r] = p0[r];
           p0[r] = pp[r];
+          if (FZ) xv[r] = xn[r];
         }
         release(qk);  // this warp is done with plane k's stage
       }
@@ -332,13 +379,13 @@ __global__ void __launch_bounds__(kCThreads, MODE == 0 ? 3 : 2) k_cc_lap(const _
 
 // the CC operator kernel's grid: tiles x plane chunks, one resident wave;
 // klen = planes per chunk
-inline dim3 cc_lap_grid(const DF& a, int nsm, const void* kern, int& klen) {
+inline dim3 cc_lap_grid(const DF& a, int nsm, const void* kern, bool fz, int& klen) {
   // occupancy with the largest z table (one chunk), then the chunking
   const int tiles = cc_tiles(a);
   const int nk = a.s2 - 2;
   int occ = 0;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cc_smem(nk));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kCThreads, cc_smem(nk));
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cc_smem(nk, fz));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kCThreads, cc_smem(nk, fz));
   int chunks = std::max(1, std::min(nk, (std::max(occ, 1) * std::max(nsm, 1)) / std::max(tiles, 1)));
   klen = (nk + chunks - 1) / chunks;
   chunks = (nk + klen - 1) / klen;
