@@ -330,6 +330,23 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info);
  * divU/divB probes export) */
 int moons_mhd_divergence(moons_mhd* s, double* l2_divU, double* l2_divB);
 
+/* Diagnostics (no reference counterpart): the building blocks of an
+ * MOONS_PREC_MG solver's FP64 multigrid hierarchy, one at a time, on host
+ * arrays, so each can be checked against a CPU restatement of the
+ * reference's prolongate_C (grid_field/GF_MG/GF_prolongate.f90:22-56), its
+ * transpose, and the point update of redBlack (solvers/SOR/SOR.f90:234-268).
+ * Level 0 is the solver's mesh; moons_mg_level_shape gives a level's
+ * cell-centred extents (ghosts included) and the level count.  Arrays are
+ * Fortran-ordered level arrays with ghosts (ghost entries are implied by the
+ * homogeneous BCs: not read, returned as zeros).
+ *  op 0: out(level) = P a, a on level+1 (prolongation of a correction)
+ *  op 1: out(level+1) = P^T a, a on level (restriction of a residual)
+ *  op 2: out(level) = e after one red (i+j+k even) and one black SOR sweep
+ *        from e = a, right-hand side b (the V-cycle's omega)
+ *  op 3: out(level) = b - A a with A the level's volume-weighted operator */
+int moons_mg_level_shape(moons_pcg* s, int level, int* shape3, int* nlevels);
+int moons_mg_debug(moons_pcg* s, int op, int level, const double* a, const double* b, double* out);
+
 /* ---- learned preconditioner: 3-D U-Net -------------------------------------
  * No reference counterpart (the reference's preconditioners are the Jacobi
  * family of code/handwritten/solvers/preconditioners/preconditioners.f90:

@@ -215,6 +215,8 @@ def lib() -> C.CDLL:
             "moons_mhd_divergence": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             "moons_kernel_launches": (C.c_longlong, []),
             "moons_debug_bounded_wait": (C.c_int, [C.c_ulonglong]),
+            "moons_mg_level_shape": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "moons_mg_debug": (C.c_int, [_P, C.c_int, C.c_int, _D, _D, _D]),
             "moons_unet_create": (C.c_int, [_P, C.c_ulonglong, C.POINTER(_P)]),
             "moons_unet_destroy": (C.c_int, [_P]),
             "moons_unet_nparams": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
@@ -466,6 +468,27 @@ class PCG:
 
     def update_mfp(self, coeff: float, update_prec: bool = True):
         _check(lib().moons_pcg_update_mfp(self.h, float(coeff), 1 if update_prec else 0))
+
+    def mg_level_shape(self, level: int):
+        """(extents of the level's cell-centred arrays, number of levels) of an
+        MOONS_PREC_MG solver's hierarchy."""
+        s = (C.c_int * 3)()
+        nl = C.c_int()
+        _check(lib().moons_mg_level_shape(self.h, int(level), s, C.byref(nl)))
+        return (s[0], s[1], s[2]), nl.value
+
+    def mg_debug(self, op: int, level: int, a, b=None):
+        """One multigrid building block on host arrays (moons_mg_debug): op 0
+        prolongation (a on level+1), 1 restriction (result on level+1), 2 a
+        red and a black SOR sweep, 3 the residual b - A a."""
+        out_level = level + 1 if op == 1 else level
+        shp, _ = self.mg_level_shape(out_level)
+        aa = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+        bb = None if b is None else np.ascontiguousarray(np.asarray(b, dtype=np.float64).ravel(order="F"))
+        out = np.zeros(shp[0] * shp[1] * shp[2])
+        _check(lib().moons_mg_debug(self.h, int(op), int(level), aa.ctypes.data_as(_D),
+                                    None if bb is None else bb.ctypes.data_as(_D), out.ctypes.data_as(_D)))
+        return out.reshape(shp, order="F")
 
     def residual(self, x: Sequence[Field], b: Sequence[Field], out: Sequence[Field]):
         """The solver's internal residual vol*(b - A x) for the iterate x."""

@@ -914,3 +914,94 @@ int fd_apply(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Diagnostics (no reference counterpart): the multigrid building blocks of an
+// MOONS_PREC_MG solver's FP64 hierarchy, one launch each, on host arrays, so
+// that each can be checked against a CPU restatement of the reference's
+// prolongate_C (GF_prolongate.f90:22-56), its transpose and the point update
+// of redBlack (SOR.f90:234-268).  Level arrays are the level's cell-centred
+// arrays with ghosts, Fortran order; the level's ghost entries are not read
+// (homogeneous BCs imply them) and are returned as zeros.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int moons_mg_level_shape(moons_pcg* s, int level, int* shape3, int* nlevels) {
+  if (!s || !shape3) {
+    set_error("moons_mg_level_shape: null pointer");
+    return MOONS_ERR_ARG;
+  }
+  MGHier* h = s->mgh;
+  if (!h || h->fd || h->mixed) {
+    set_error("moons_mg_level_shape: the solver has no FP64 multigrid hierarchy (MOONS_PREC_MG)");
+    return MOONS_ERR_STATE;
+  }
+  if (nlevels) *nlevels = h->nl;
+  if (level < 0 || level >= h->nl) {
+    set_error("moons_mg_level_shape: level out of range");
+    return MOONS_ERR_ARG;
+  }
+  for (int d = 0; d < 3; d++) shape3[d] = h->s[level][d];
+  return MOONS_OK;
+}
+
+/* op 0: out (level) = P a, a the coarse correction on level+1;
+ * op 1: out (level+1) = R a = P^T a, a the residual on level;
+ * op 2: out (level) = e after one red and one black SOR sweep (omega of the
+ *       V-cycle) from e = a with right-hand side b;
+ * op 3: out (level) = b - A a (the level's volume-weighted operator). */
+int moons_mg_debug(moons_pcg* s, int op, int level, const double* a, const double* b, double* out) {
+  int sh[3], nl = 0;
+  int r = moons_mg_level_shape(s, level, sh, &nl);
+  if (r) return r;
+  if (!a || !out || ((op == 2 || op == 3) && !b) || op < 0 || op > 3 || ((op == 0 || op == 1) && level + 1 >= nl)) {
+    set_error("moons_mg_debug: bad op, level or array");
+    return MOONS_ERR_ARG;
+  }
+  MGHier* h = s->mgh;
+  cudaStream_t st = s->m->stream;
+  cudaSetDevice(s->m->device);
+  const MGLev<double>& L = h->Ld[level];
+  auto bytes = [&](int l) { return (size_t)h->s[l][0] * h->s[l][1] * h->s[l][2] * sizeof(double); };
+  auto npts = [&](int l) { return (size_t)(h->s[l][0] - 2) * (h->s[l][1] - 2) * (h->s[l][2] - 2); };
+  if (op == 0) {
+    const MGLev<double>& C = h->Ld[level + 1];
+    MG_CUDA(cudaMemcpyAsync(C.e, a, bytes(level + 1), cudaMemcpyHostToDevice, st));
+    MG_CUDA(cudaMemsetAsync(L.e, 0, bytes(level), st));
+    MG_LAUNCH(k_mg_prolong<double>, vgrid(npts(level), h->occ[3], h->nsm), 256, st, L, C, h->Pd[level + 1][0],
+              h->Pd[level + 1][1], h->Pd[level + 1][2], (const PcgScalars*)nullptr);
+    MG_CUDA(cudaMemcpyAsync(out, L.e, bytes(level), cudaMemcpyDeviceToHost, st));
+  } else if (op == 1) {
+    const MGLev<double>& C = h->Ld[level + 1];
+    MG_CUDA(cudaMemcpyAsync(L.t, a, bytes(level), cudaMemcpyHostToDevice, st));
+    MG_CUDA(cudaMemsetAsync(C.r, 0, bytes(level + 1), st));
+    MG_LAUNCH(k_mg_restrict<double>, vgrid(npts(level + 1), h->occ[2], h->nsm), 256, st, L, C, h->Rd[level + 1][0],
+              h->Rd[level + 1][1], h->Rd[level + 1][2], (const PcgScalars*)nullptr);
+    MG_CUDA(cudaMemcpyAsync(out, C.r, bytes(level + 1), cudaMemcpyDeviceToHost, st));
+  } else {
+    MG_CUDA(cudaMemcpyAsync(L.e, a, bytes(level), cudaMemcpyHostToDevice, st));
+    MG_CUDA(cudaMemcpyAsync(L.r, b, bytes(level), cudaMemcpyHostToDevice, st));
+    if (op == 2) {
+      const unsigned g = vgrid(npts(level) / 2 + 1, h->occ[0], h->nsm);
+      MG_LAUNCH(k_mg_smooth<double>, g, 256, st, L, 0, 0, h->omega, (const PcgScalars*)nullptr);
+      MG_LAUNCH(k_mg_smooth<double>, g, 256, st, L, 1, 0, h->omega, (const PcgScalars*)nullptr);
+      MG_CUDA(cudaMemcpyAsync(out, L.e, bytes(level), cudaMemcpyDeviceToHost, st));
+    } else {
+      MG_CUDA(cudaMemsetAsync(L.t, 0, bytes(level), st));
+      MG_LAUNCH(k_mg_resid<double>, vgrid(npts(level), h->occ[1], h->nsm), 256, st, L, (const PcgScalars*)nullptr);
+      MG_CUDA(cudaMemcpyAsync(out, L.t, bytes(level), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  MG_CUDA(cudaStreamSynchronize(st));
+  // ghost entries of the result: zero (the host arrays may carry any ghosts)
+  const int l = op == 1 ? level + 1 : level;
+  const int s0 = h->s[l][0], s1 = h->s[l][1], s2 = h->s[l][2];
+  for (int k = 1; k <= s2; k++)
+    for (int j = 1; j <= s1; j++)
+      for (int i = 1; i <= s0; i++)
+        if (i == 1 || i == s0 || j == 1 || j == s1 || k == 1 || k == s2)
+          out[(size_t)(i - 1) + (size_t)s0 * ((size_t)(j - 1) + (size_t)s1 * (size_t)(k - 1))] = 0.0;
+  return MOONS_OK;
+}
+
+}  // extern "C"
