@@ -289,6 +289,13 @@ typedef struct {
   double scale_buoyancy;    /* SP%MT%Buoyancy%scale: F_U += s face(T g)      */
   moons_isp isp_T;
   moons_bc_spec bc_T;
+  /* further energy sources (energy_sources.f90:51-94), with U_CC the cell-centre
+   * velocity embedded in the induction mesh (embedCC of face2CellCenter(U),
+   * add_all_energy_sources.f90:30-32): */
+  double scale_KE_diffusion_T;        /* SP%ET%KE_diffusion%scale: F += s lap(sum_c U_CC,c^2) */
+  double scale_viscous_dissipation_T; /* SP%ET%viscous_dissipation%scale: F += s sum_cd (d_d U_CC,c)^2 */
+  double scale_joule_heating_T;       /* SP%ET%joule_heating%scale: F += s (sum_c J_CC,c^2) sigmaInv_CC,
+                                         J_CC = edge2CellCenter(J) (faces in the potential form) */
 } moons_mhd_params;
 
 typedef struct {
@@ -313,7 +320,13 @@ enum {
   MOONS_MHD_DIVB = 9,     /* CC on the induction mesh (probe)                */
   MOONS_MHD_T = 10,       /* temperature, CC on the induction mesh           */
   MOONS_MHD_KT = 11,      /* comp 0..2: thermal conductivity on the faces    */
-  MOONS_MHD_GRAVITY = 12  /* comp 0..2: gravity vector field, CC             */
+  MOONS_MHD_GRAVITY = 12, /* comp 0..2: gravity vector field, CC             */
+  MOONS_MHD_SIGMA_INV_CC = 13, /* sigma^-1 at cell centres on the induction mesh,
+                               the factor of the Joule heating; 0 until uploaded
+                               (the reference's ind%sigmaInv_CC starts at 0 and
+                               its step never sets it)                       */
+  MOONS_MHD_U_CC = 14     /* comp 0..2: the energy equation's cell-centre
+                             velocity on the induction mesh (probe)           */
 };
 
 /* mesh_ind may equal mesh_mom.  Fields start at 0; upload initial U, B, B0

@@ -72,6 +72,7 @@ class SolveInfo(C.Structure):
 
 
 IND_OFF, IND_B, IND_POTENTIAL = 0, 1, 2
+MHD_SIGMA_INV_CC, MHD_U_CC = 13, 14
 MHD_U, MHD_P, MHD_B, MHD_B0, MHD_PHI, MHD_J, MHD_SIGMA_INV, MHD_JXB, MHD_DIVU, MHD_DIVB, MHD_T, MHD_KT, MHD_GRAVITY = \
     range(13)
 
@@ -112,6 +113,9 @@ class MHDParams(C.Structure):
         ("scale_buoyancy", C.c_double),
         ("isp_T", ISP),
         ("bc_T", BCSpec),
+        ("scale_KE_diffusion_T", C.c_double),
+        ("scale_viscous_dissipation_T", C.c_double),
+        ("scale_joule_heating_T", C.c_double),
     ]
 
 

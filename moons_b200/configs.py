@@ -168,13 +168,18 @@ def at_scale(nx: int = 128, ny: int = 128, nz: int = 256, **kw):
 
 
 def ldc_energy(n: int = 16, Pe: float = 100.0, Gr_Re2: float = 10.0, heating: float = 0.5,
-               solve_method_T: int = 3, tol: float = 1e-10, **kw):
+               solve_method_T: int = 3, tol: float = 1e-10, KE_diffusion: float = 0.0,
+               viscous_dissipation: float = 0.0, joule_heating: float = 0.0, **kw):
     """The lid-driven cavity with the energy equation: T = 1 on the x-min
     wall, 0 on x-max, insulated elsewhere; conductivity on the faces varying
     by +-20% (seeded); gravity -y; advection scale 1 (S += -div(u T)),
     diffusion by the implicit nrg_diffusion PCG (solve_method 3, coefficient
     -1/Pe) or explicitly (solve_method 2, scale 1/Pe); volumetric heating
-    (add_volumetric_heating_Nuclear) and buoyancy Gr/Re^2 in momentum."""
+    (add_volumetric_heating_Nuclear) and buoyancy Gr/Re^2 in momentum;
+    optionally the KE-diffusion, viscous-dissipation and Joule-heating
+    sources with the given scales (sigma^-1 at cell centres then 1 + 0.5 x,
+    so the Joule term does not vanish as it would with the reference's
+    never-set ind%sigmaInv_CC)."""
     mom, ind, prm, init0 = ldc(n=n, tol=tol, **kw)
     prm.energy = 1
     prm.solve_method_T = solve_method_T
@@ -184,6 +189,9 @@ def ldc_energy(n: int = 16, Pe: float = 100.0, Gr_Re2: float = 10.0, heating: fl
     prm.scale_heating_T = heating
     prm.scale_buoyancy = Gr_Re2
     prm.isp_T = _isp(5000, tol)
+    prm.scale_KE_diffusion_T = KE_diffusion
+    prm.scale_viscous_dissipation_T = viscous_dissipation
+    prm.scale_joule_heating_T = joule_heating
     D, Nn = G.DIRICHLET, G.NEUMANN
     prm.bc_T = G.bc_spec([D, D, Nn, Nn, Nn, Nn], values=[1.0, 0.0, 0.0, 0.0, 0.0, 0.0], order=ORDER_LDC)
 
@@ -195,6 +203,11 @@ def ldc_energy(n: int = 16, Pe: float = 100.0, Gr_Re2: float = 10.0, heating: fl
             if c == 1:
                 g[:] = -1.0
             sim.upload(G.MHD_GRAVITY, c, g)
+        if joule_heating != 0.0:
+            hx = ind[0]
+            xc = 0.5 * (hx[1:] + hx[:-1])
+            sic = np.ones(sim.shape(G.MHD_SIGMA_INV_CC)) * (1.0 + 0.5 * xc)[:, None, None]
+            sim.upload(G.MHD_SIGMA_INV_CC, 0, sic)
 
     return mom, ind, prm, init
 

@@ -121,6 +121,9 @@ struct moons_mhd {
   // energy (on the induction mesh)
   moons_sf *T = nullptr, *Tnm1 = nullptr, *FT = nullptr, *FnmT = nullptr, *LT = nullptr, *tCCT = nullptr,
            *tCCT2 = nullptr, *tmpT = nullptr, *kT[3] = {}, *grav[3] = {}, *tFT[3] = {}, *UFT[3] = {};
+  // nrg%U_CC, ind%sigmaInv_CC, nrg%temp_CC2, nrg%temp_CC1_VF (KE diffusion,
+  // viscous dissipation, Joule heating)
+  moons_sf *UCCn[3] = {}, *sigInvCC = nullptr, *tCCT3 = nullptr, *tVFT[3] = {};
   moons_pcg* pcgT = nullptr;
   double* heat_prof = nullptr;  // add_volumetric_heating_Nuclear profile per y index (device)
   double coefU = NAN, coefB = NAN, coefT = NAN;
@@ -331,6 +334,78 @@ int advect_U_convection1(moons_mhd* s) {
 }
 
 // ---- energy equation ---------------------------------------------------------
+// add_KE_diffusion, add_viscous_dissipation, add_joule_heating
+// (energy_sources.f90:51-94) as add_all_energy_sources calls them
+// (add_all_energy_sources.f90:30-32, 51-62).  Each assigns its scratch
+// (add(f,g,h,...) is f = g + h + ... in GF_add.f90:41-86,137-160), so no
+// term carries state from an earlier one.
+int energy_sources_KE_visc_joule(moons_mhd* s) {
+  moons_mesh* mi = s->mi;
+  const moons_mhd_params& P = s->P;
+  int r = MOONS_OK;
+  if (P.scale_KE_diffusion_T != 0.0 || P.scale_viscous_dissipation_T != 0.0) {
+    // embedCC(nrg%U_CC, mom%U_CC, nrg%MD)
+    for (int c = 0; c < 3 && !r; c++) {
+      if (s->same) r = copy(mi, s->UCCn[c], s->UCC[c]);
+      else r = embed_extract(mi, s->UCCn[c], s->UCC[c], P.ind_offset, true);
+    }
+  }
+  // temp = (a0 + a1) + a2 over three CC fields (add_GF_GF_GF_GF)
+  auto sum3 = [&](moons_sf* out, moons_sf* const* a) -> int {
+    int q = copy(mi, out, a[0]);
+    if (!q) q = launch_pw(mi, PW_ADD, D(out), &D(a[1]), 0.0);
+    if (!q) q = launch_pw(mi, PW_ADD, D(out), &D(a[2]), 0.0);
+    return q;
+  };
+  if (!r && P.scale_KE_diffusion_T != 0.0) {
+    // temp_CC1_VF = U_CC ; square ; temp_CC1 = x + y + z ; temp_CC2 = lap(temp_CC1) ; F += s temp_CC2
+    for (int c = 0; c < 3 && !r; c++) {
+      r = copy(mi, s->tVFT[c], s->UCCn[c]);
+      if (!r) r = launch_pw(mi, PW_MUL, D(s->tVFT[c]), &D(s->tVFT[c]), 0.0);
+    }
+    if (!r) r = sum3(s->tCCT, s->tVFT);
+    if (!r) r = launch_del(mi, D(s->tCCT3), D(s->tCCT), 2, 1, 0, 1);  // lapUniformCoeff_SF
+    if (!r) r = launch_del(mi, D(s->tCCT3), D(s->tCCT), 2, 2, 0, 2);
+    if (!r) r = launch_del(mi, D(s->tCCT3), D(s->tCCT), 2, 3, 0, 2);
+    if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT3), P.scale_KE_diffusion_T);
+  }
+  if (!r && P.scale_viscous_dissipation_T != 0.0) {
+    // temp_CC_TF = grad(U_CC) (collocated first derivatives, CC -> CC) ;
+    // square ; temp_CC1 = g%x%x + g%y%x + g%z%x + g%x%y + ... + g%z%z
+    // (add_SF_TF, TF_extend.f90:248-255) ; F += s temp_CC1
+    bool first = true;
+    for (int d = 0; d < 3 && !r; d++)
+      for (int c = 0; c < 3 && !r; c++) {
+        r = launch_del(mi, D(s->tCCT2), D(s->UCCn[c]), 1, d + 1, 0, 1);
+        if (!r) r = launch_pw(mi, PW_MUL, D(s->tCCT2), &D(s->tCCT2), 0.0);
+        if (!r) r = first ? copy(mi, s->tCCT, s->tCCT2) : launch_pw(mi, PW_ADD, D(s->tCCT), &D(s->tCCT2), 0.0);
+        first = false;
+      }
+    if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_viscous_dissipation_T);
+  }
+  if (!r && P.scale_joule_heating_T != 0.0) {
+    // temp_CC1_VF = edge2CellCenter(J) (edge -> face along the face direction
+    // (x: y, y: z, z: x), then face -> CC; ops_interp.f90:415-431, 688-696);
+    // the potential form keeps J on faces: face -> CC
+    const bool pot = P.induction == MOONS_IND_POTENTIAL;
+    for (int c = 0; c < 3 && !r; c++) {
+      if (pot) {
+        r = launch_interp(mi, D(s->tVFT[c]), D(s->J[c]), c + 1);
+      } else {
+        const int edir = c + 1, fdir = edir == 1 ? 2 : (edir == 2 ? 3 : 1);
+        moons_sf* tf = s->tFT[fdir - 1];
+        r = launch_interp(mi, D(tf), D(s->J[c]), 6 - edir - fdir);
+        if (!r) r = launch_interp(mi, D(s->tVFT[c]), D(tf), fdir);
+      }
+      if (!r) r = launch_pw(mi, PW_MUL, D(s->tVFT[c]), &D(s->tVFT[c]), 0.0);
+    }
+    if (!r) r = sum3(s->tCCT, s->tVFT);
+    if (!r) r = launch_pw(mi, PW_MUL, D(s->tCCT), &D(s->sigInvCC), 0.0);
+    if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_joule_heating_T);
+  }
+  return r;
+}
+
 // add_all_energy_sources (add_all_energy_sources.f90:21-67) with the
 // advection, diffusion and volumetric-heating terms (energy_sources.f90),
 // then solve_energy (energy_extend.f90:236-262), methods 2 and 3
@@ -360,6 +435,7 @@ int energy_step(moons_mhd* s) {
     if (!r) r = launch_del(mi, D(s->tCCT), D(s->T), 2, 3, 0, 2);
     if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_diffusion_T);
   }
+  if (!r) r = energy_sources_KE_visc_joule(s);
   if (!r && P.scale_heating_T != 0.0) {
     // add_volumetric_heating_Nuclear: temp = scale*F0*exp(-m (y_c + 1)); S += scale * temp
     MG_LAUNCH(k_fill_y, nblocks(D(s->tCCT).n()), kBlock, mi->stream, D(s->tCCT), s->heat_prof);
@@ -566,12 +642,16 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
   F(mi, MOONS_CC, &s->tCCi);
   F(mi, MOONS_CC, &s->divB);
   if (prm->energy) {
-    for (moons_sf** f : {&s->T, &s->Tnm1, &s->FT, &s->FnmT, &s->LT, &s->tCCT, &s->tCCT2, &s->tmpT}) F(mi, MOONS_CC, f);
+    for (moons_sf** f : {&s->T, &s->Tnm1, &s->FT, &s->FnmT, &s->LT, &s->tCCT, &s->tCCT2, &s->tmpT, &s->sigInvCC,
+                         &s->tCCT3})
+      F(mi, MOONS_CC, f);
     for (int c = 0; c < 3; c++) {
       F(mi, MOONS_FX + c, &s->kT[c]);
       F(mi, MOONS_CC, &s->grav[c]);
       F(mi, MOONS_FX + c, &s->tFT[c]);
       F(mi, MOONS_FX + c, &s->UFT[c]);
+      F(mi, MOONS_CC, &s->UCCn[c]);
+      F(mi, MOONS_CC, &s->tVFT[c]);
     }
     if (!r) r = set_bcs_from(s->T, prm->bc_T);
     if (!r && prm->scale_heating_T != 0.0) {
@@ -663,6 +743,8 @@ int moons_mhd_field(moons_mhd* s, int which, int comp, moons_sf** out) {
     case MOONS_MHD_T: f = s->T; break;
     case MOONS_MHD_KT: f = s->kT[comp]; break;
     case MOONS_MHD_GRAVITY: f = s->grav[comp]; break;
+    case MOONS_MHD_SIGMA_INV_CC: f = s->sigInvCC; break;
+    case MOONS_MHD_U_CC: f = s->UCCn[comp]; break;
     default:
       set_error("moons_mhd_field: unknown field");
       return MOONS_ERR_ARG;

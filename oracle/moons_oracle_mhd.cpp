@@ -106,6 +106,8 @@ struct MHD {
   ISP ispB, ispPhi;
   // energy (on the induction mesh)
   SF T, Tnm1, FT, FnmT, LT, tCCT, tCCT2, tmpT, kT[3], grav[3], tFT[3], UFT[3];
+  // nrg%U_CC, ind%sigmaInv_CC, nrg%temp_CC2, nrg%temp_CC1_VF
+  SF UCCn[3], sigInvCC, tCCT3, tVFT[3];
   PCG pcgT;
   ISP ispT;
   bool pcgT_made = false;
@@ -171,7 +173,11 @@ struct MHD {
       set_bcs_spec(phi, g, P.bc_phi);
     }
     if (P.energy) {
-      for (SF* f : {&T, &Tnm1, &FT, &FnmT, &LT, &tCCT, &tCCT2, &tmpT}) f->init(g, 0);
+      for (SF* f : {&T, &Tnm1, &FT, &FnmT, &LT, &tCCT, &tCCT2, &tmpT, &sigInvCC, &tCCT3}) f->init(g, 0);
+      for (int c = 0; c < 3; c++) {
+        UCCn[c].init(g, 0);
+        tVFT[c].init(g, 0);
+      }
       for (int c = 0; c < 3; c++) {
         kT[c].init(g, dl_face(c));
         grav[c].init(g, 0);
@@ -244,6 +250,55 @@ struct MHD {
     if (P.scale_diffusion_T != 0.0) {  // add_diffusion: lap = lapUniformCoeff_SF
       lap_uniform_coeff(tCCT, T, gi);
       add_product(FT, tCCT, P.scale_diffusion_T);
+    }
+    if (P.scale_KE_diffusion_T != 0.0 || P.scale_viscous_dissipation_T != 0.0) {
+      // embedCC(nrg%U_CC, mom%U_CC, nrg%MD) (add_all_energy_sources.f90:30-32)
+      for (int c = 0; c < 3; c++) {
+        if (same) assign(UCCn[c], UCC[c]);
+        else embed_extract(UCCn[c], UCC[c], off, true);
+      }
+    }
+    if (P.scale_KE_diffusion_T != 0.0) {  // add_KE_diffusion (energy_sources.f90:51-64)
+      for (int c = 0; c < 3; c++) {
+        assign(tVFT[c], UCCn[c]);
+        multiply(tVFT[c], tVFT[c]);  // square
+      }
+      // add(temp_CC1, temp_CC_VF): temp_CC1 = x + y + z (GF_add.f90:63-86)
+      for (size_t i = 0; i < tCCT.n(); i++) tCCT.f[i] = tVFT[0].f[i] + tVFT[1].f[i] + tVFT[2].f[i];
+      lap_uniform_coeff(tCCT3, tCCT, gi);  // lap = lapUniformCoeff_SF
+      add_product(FT, tCCT3, P.scale_KE_diffusion_T);
+    }
+    if (P.scale_viscous_dissipation_T != 0.0) {  // add_viscous_dissipation (energy_sources.f90:66-78)
+      // grad_TF (ops_discrete.f90:313-321): g%c%d = d U_CC,c / d x_d, CC -> CC
+      SF g[3][3];
+      for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) {
+          g[c][d].init(gi, 0);
+          del(g[c][d], UCCn[c], gi, 1, d + 1, 0, 1);
+          multiply(g[c][d], g[c][d]);  // square_TF
+        }
+      // add_SF_TF (TF_extend.f90:248-255): x%x + y%x + z%x + x%y + ... + z%z
+      for (size_t i = 0; i < tCCT.n(); i++)
+        tCCT.f[i] = g[0][0].f[i] + g[1][0].f[i] + g[2][0].f[i] + g[0][1].f[i] + g[1][1].f[i] + g[2][1].f[i] +
+                    g[0][2].f[i] + g[1][2].f[i] + g[2][2].f[i];
+      add_product(FT, tCCT, P.scale_viscous_dissipation_T);
+    }
+    if (P.scale_joule_heating_T != 0.0) {  // add_joule_heating (energy_sources.f90:80-94)
+      // edge2CellCenter_VF (ops_interp.f90:415-431, 688-696); faces in the potential form
+      const bool pot = P.induction == MOONS_IND_POTENTIAL;
+      for (int c = 0; c < 3; c++) {
+        if (pot) {
+          interp(tVFT[c], J[c], gi, c + 1);
+        } else {
+          const int edir = c + 1, fdir = edir == 1 ? 2 : (edir == 2 ? 3 : 1);
+          interp(tFT[fdir - 1], J[c], gi, 6 - edir - fdir);  // edge2Face
+          interp(tVFT[c], tFT[fdir - 1], gi, fdir);          // face2CellCenter
+        }
+        multiply(tVFT[c], tVFT[c]);
+      }
+      for (size_t i = 0; i < tCCT.n(); i++) tCCT.f[i] = tVFT[0].f[i] + tVFT[1].f[i] + tVFT[2].f[i];
+      multiply(tCCT, sigInvCC);
+      add_product(FT, tCCT, P.scale_joule_heating_T);
     }
     if (P.scale_heating_T != 0.0) {  // add_volumetric_heating_Nuclear (energy_sources.f90:98-114)
       const double a = 1.0, Lh = 1.0, m_ = a / Lh;
@@ -539,6 +594,8 @@ struct MHD {
       case MOONS_MHD_T: return &T;
       case MOONS_MHD_KT: return &kT[comp];
       case MOONS_MHD_GRAVITY: return &grav[comp];
+      case MOONS_MHD_SIGMA_INV_CC: return &sigInvCC;
+      case MOONS_MHD_U_CC: return &UCCn[comp];
     }
     return nullptr;
   }

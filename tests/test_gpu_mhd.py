@@ -24,6 +24,12 @@ CASES = [
     # the energy equation (implicit and explicit diffusion), buoyancy into momentum
     ("ldc_energy_implicit", configs.ldc_energy, dict(n=10, tol=1e-12, solve_method_T=3)),
     ("ldc_energy_explicit", configs.ldc_energy, dict(n=10, tol=1e-12, solve_method_T=2)),
+    # the KE-diffusion, viscous-dissipation and Joule-heating sources
+    # (energy_sources.f90:51-94), B form (J on edges) and potential form
+    ("ldc_energy_sources_bform", configs.ldc_energy, dict(n=10, tol=1e-12, induction=G.IND_B, KE_diffusion=0.3,
+                                                          viscous_dissipation=0.2, joule_heating=0.4)),
+    ("ldc_energy_sources_potential", configs.ldc_energy, dict(n=10, tol=1e-12, KE_diffusion=0.3,
+                                                              viscous_dissipation=0.2, joule_heating=0.4)),
     # the full_BC case on mesh-bank meshes: clustered fluid embedded in an
     # induction mesh with thin walls and a vacuum region (sigma = 1e-3)
     ("full_bc_vacuum", configs.full_bc, dict(N=8, N_w=3, tol=1e-12, iter_max=(20000,) * 4, noise=1e-2)),
