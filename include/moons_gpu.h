@@ -118,7 +118,12 @@ enum {
    * unknown, LAP_UNIFORM, Dirichlet/Neumann/periodic BCs): the B200 form of
    * the reference's FFT Poisson (FFT_poisson.f90:107-189, solve_method 9),
    * exact for stretched meshes too; CG converges in one or two iterations. */
-  MOONS_PREC_FD = 7
+  MOONS_PREC_FD = 7,
+  /* learned + mixed (no reference counterpart): z = V(r) + N(r - A V(r)),
+   * the FP32 V-cycle followed by the U-Net (moons_pcg_set_unet) on what the
+   * V-cycle leaves, inside FP64 flexible CG; the same stagnation fallback to
+   * the V-cycle alone as MOONS_PREC_UNET */
+  MOONS_PREC_UNET_MG = 8
 };
 
 typedef struct moons_mesh moons_mesh;
@@ -408,9 +413,15 @@ int moons_unet_set_coeff(moons_unet* u, const moons_sf* kx, const moons_sf* ky, 
  * residual of PCG_solver_algorithm.f90:55-66): r = vol*(b - A x_BC - A x),
  * mean removed for all-Neumann problems; what a preconditioner is applied to */
 int moons_pcg_residual(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, moons_sf* const* r);
-/* attach a network to a solver created with MOONS_PREC_UNET (same mesh; the
- * solver does not own it and reads its current weights at every solve) */
+/* attach a network to a solver created with MOONS_PREC_UNET or
+ * MOONS_PREC_UNET_MG (same mesh; the solver does not own it and reads its
+ * current weights at every solve) */
 int moons_pcg_set_unet(moons_pcg* s, moons_unet* u);
+/* z = M(r) with the solver's preconditioner (no reference counterpart): the
+ * Jacobi Minv r, or one multigrid V-cycle (MOONS_PREC_MG / _MG_MIXED /
+ * _UNET / _UNET_MG: the V-cycle alone), or the direct solve (MOONS_PREC_FD);
+ * used to form the training targets of the two-stage learned form */
+int moons_pcg_apply_prec(moons_pcg* s, moons_sf* const* z, moons_sf* const* r);
 /* kernel self-check of one layer on host data ([C][Z][Y][X] FP32, interior,
  * rounded to BF16 on upload): op 0 out = conv(in) (+bias, ReLU if relu);
  * op 1 out = transposed conv of dout (gradient w.r.t. the input); op 2 out =

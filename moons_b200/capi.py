@@ -27,6 +27,7 @@ OP_LAP_UNIFORM, OP_LAP_PROPS, OP_IND_DIFFUSION, OP_MOM_DIFFUSION, OP_NRG_DIFFUSI
 PREC_IDENTITY, PREC_LAP, PREC_MOM, PREC_IND = 0, 1, 2, 3
 PREC_MG, PREC_MG_MIXED = 4, 5  # multigrid V-cycle in CG (FP64) / in flexible CG (FP32 V-cycle)
 PREC_FD = 7  # direct solve of the separable Poisson operator (fast diagonalization) in CG
+PREC_UNET_MG = 8  # learned + mixed: z = V(r) + N(r - A V(r)) in flexible CG (V the FP32 V-cycle)
 PREC_UNET = 6  # learned U-Net in flexible CG, FP32 V-cycle fallback (PCG.set_unet)
 
 
@@ -235,6 +236,7 @@ def lib() -> C.CDLL:
             "moons_unet_set_operator": (C.c_int, [_P, _P]),
             "moons_pcg_set_unet": (C.c_int, [_P, _P]),
             "moons_pcg_residual": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+            "moons_pcg_apply_prec": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
             "moons_unet_loss_grad": (C.c_int, [_P, _P, _P, _F, _F, C.c_longlong]),
             "moons_unet_train_step": (C.c_int, [_P, _P, _P, C.c_float, _F]),
             "moons_unet_layer_check": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -498,8 +500,14 @@ class PCG:
         """The solver's internal residual vol*(b - A x) for the iterate x."""
         _check(lib().moons_pcg_residual(self.h, _ptrs(x), _ptrs(b), _ptrs(out)))
 
+    def apply_prec(self, z: Sequence[Field], r: Sequence[Field]):
+        """z = M(r) with the solver's preconditioner (a multigrid-family
+        solver applies one V-cycle alone)."""
+        _check(lib().moons_pcg_apply_prec(self.h, _ptrs(z), _ptrs(r)))
+
     def set_unet(self, net: "UNet"):
-        """Attach the network of a PREC_UNET solver (kept alive by the solver)."""
+        """Attach the network of a PREC_UNET / PREC_UNET_MG solver (kept alive
+        by the solver)."""
         _check(lib().moons_pcg_set_unet(self.h, net.h))
         self.net = net
 

@@ -42,6 +42,8 @@ struct MGHier {
   std::vector<std::array<MGRest<double>, 3>> Rd;
   std::vector<std::array<MGRest<float>, 3>> Rf;
   double* rprev = nullptr;  // flexible CG: previous residual
+  double* ts_part = nullptr;   // two-stage scaling: block partials of N.t, N.A N
+  double* ts_gamma = nullptr;  // and the resulting multiple of N
   // coarsest level: dense inverse (direct solve) when small enough
   int ncoarse = 0;
   double* cinv_d = nullptr;  // coarsest-level inverse (FP64 for both variants)
@@ -443,13 +445,15 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
   }
   if (h->mixed) {
     h->rprev = dev_zeros<double>(h.get(), (size_t)s0[0] * s0[1] * s0[2], st);
-    if (!h->rprev) return MOONS_ERR_NOMEM;
+    h->ts_part = dev_zeros<double>(h.get(), 2 * kTsBlocks, st);
+    h->ts_gamma = dev_zeros<double>(h.get(), 1, st);
+    if (!h->rprev || !h->ts_part || !h->ts_gamma) return MOONS_ERR_NOMEM;
   }
   {  // coarsest level: dense inverse, regularised on the constants when singular
     const int l = h->nl - 1;
     const auto& sc = h->s[l];
     const int n = (sc[0] - 2) * (sc[1] - 2) * (sc[2] - 2);
-    if (n <= 1024) {
+    if (n <= kDirectMax) {
       const host::HostCoord cc[3] = {C[0][l], C[1][l], C[2][l]};
       std::vector<double> A = dense_operator(cc, sc, bt, kf ? &K[l] : nullptr);
       bool dir = false;
@@ -463,12 +467,8 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
       std::vector<double> inv;
       if (invert(A, n, inv)) {
         h->ncoarse = n;
-        // stored transposed (column c contiguous over rows) so the direct-solve
-        // kernel's threads read consecutive entries
-        std::vector<double> invT((size_t)n * n);
-        for (int r = 0; r < n; r++)
-          for (int c = 0; c < n; c++) invT[(size_t)c * n + r] = inv[(size_t)r * n + c];
-        h->cinv_d = dev_copy(h.get(), invT, st);
+        // row-major: a warp of the direct-solve kernel reads one row
+        h->cinv_d = dev_copy(h.get(), inv, st);
       }
     }
   }
@@ -602,36 +602,36 @@ int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::a
   for (int l = 0; l < nl - 1; l++) {  // down: pre-smooth, residual, restrict
     const unsigned g = vgrid(npts(l) / 2 + 1, h->occ[0], h->nsm);
     for (int q = 0; q < h->nu; q++) {
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, q == 0 ? 1 : 0, om, S);
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, om, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[l], 0, q == 0 ? 1 : 0, om, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, om, S);
     }
-    MG_LAUNCH(k_mg_resid<T>, vgrid(npts(l), h->occ[1], h->nsm), 256, st, L[l], S);
-    MG_LAUNCH(k_mg_restrict<T>, vgrid(npts(l + 1), h->occ[2], h->nsm), 256, st, L[l], L[l + 1], R[l + 1][0],
+    MG_LAUNCH_PDL(k_mg_resid<T>, vgrid(npts(l), h->occ[1], h->nsm), 256, st, L[l], S);
+    MG_LAUNCH_PDL(k_mg_restrict<T>, vgrid(npts(l + 1), h->occ[2], h->nsm), 256, st, L[l], L[l + 1], R[l + 1][0],
               R[l + 1][1], R[l + 1][2], S);
   }
   if (h->ncoarse > 0) {
-    MG_LAUNCH(k_mg_direct<T>, (unsigned)((h->ncoarse + 255) / 256), 256, st, L[nl - 1], (const double*)h->cinv_d,
-              h->ncoarse, S);
+    MG_LAUNCH_PDL(k_mg_direct<T>, (unsigned)((h->ncoarse + kDirectRowsPerBlock - 1) / kDirectRowsPerBlock), 256, st,
+              L[nl - 1], (const double*)h->cinv_d, h->ncoarse, S);
   } else if (npts(nl - 1) <= kCoarseOneBlock) {
-    MG_LAUNCH(k_mg_coarse<T>, 1, 256, st, L[nl - 1], h->sweeps_coarse, S);
+    MG_LAUNCH_PDL(k_mg_coarse<T>, 1, 256, st, L[nl - 1], h->sweeps_coarse, S);
   } else {  // large coarsest level (the level cap): the same sweeps, grid-wide
     const unsigned g = vgrid(npts(nl - 1) / 2 + 1, h->occ[0], h->nsm);
     for (int q = 0; q < h->sweeps_coarse; q++) {
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 0, q == 0 ? 1 : 0, (T)1, S);
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 1, 0, (T)1, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[nl - 1], 0, q == 0 ? 1 : 0, (T)1, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[nl - 1], 1, 0, (T)1, S);
     }
     for (int q = 0; q < h->sweeps_coarse; q++) {
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 1, 0, (T)1, S);
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[nl - 1], 0, 0, (T)1, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[nl - 1], 1, 0, (T)1, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[nl - 1], 0, 0, (T)1, S);
     }
   }
   for (int l = nl - 2; l >= 0; l--) {  // up: prolong + correct, post-smooth (reverse colours)
     const unsigned g = vgrid(npts(l) / 2 + 1, h->occ[0], h->nsm);
-    MG_LAUNCH(k_mg_prolong<T>, vgrid(npts(l), h->occ[3], h->nsm), 256, st, L[l], L[l + 1], P[l + 1][0], P[l + 1][1],
+    MG_LAUNCH_PDL(k_mg_prolong<T>, vgrid(npts(l), h->occ[3], h->nsm), 256, st, L[l], L[l + 1], P[l + 1][0], P[l + 1][1],
               P[l + 1][2], S);
     for (int q = 0; q < h->nu; q++) {
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, om, S);
-      MG_LAUNCH(k_mg_smooth<T>, g, 256, st, L[l], 0, 0, om, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, om, S);
+      MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[l], 0, 0, om, S);
     }
   }
   MG_CUDA(cudaGetLastError());
@@ -646,10 +646,43 @@ int mg_vcycle(MGHier* h, DF z, DF r, cudaStream_t st, const PcgScalars* S) {
   if (h->fd) return fd_apply(h, z, r, st, S);
   if (!h->mixed) return vcycle_t<double>(h, h->Ld, h->Pd, h->Rd, st, S);
   const size_t n = r.n();
-  MG_LAUNCH((k_mg_cast<float, double>), vgrid(n), 256, st, h->Lf[0].r, (const double*)r.f, n, S);
+  MG_LAUNCH_PDL((k_mg_cast<float, double>), vgrid(n), 256, st, h->Lf[0].r, (const double*)r.f, n, S);
   int rc = vcycle_t<float>(h, h->Lf, h->Pf, h->Rf, st, S);
   if (rc) return rc;
-  MG_LAUNCH((k_mg_cast<double, float>), vgrid(n), 256, st, z.f, (const float*)h->Lf[0].e, n, S);
+  MG_LAUNCH_PDL((k_mg_cast<double, float>), vgrid(n), 256, st, z.f, (const float*)h->Lf[0].e, n, S);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+// after a mixed (FP32) V-cycle: t = r - A e on its finest level, in FP64
+int mg_vcycle_resid_f64(MGHier* h, DF t, cudaStream_t st, const PcgScalars* S) {
+  if (!h->mixed || h->fd) {
+    set_error("two-stage preconditioner: needs the FP32 V-cycle");
+    return MOONS_ERR_STATE;
+  }
+  const MGLev<float>& L = h->Lf[0];
+  const size_t npts = (size_t)(L.s0 - 2) * (L.s1 - 2) * (L.s2 - 2);
+  MG_LAUNCH_PDL(k_mg_resid<float>, vgrid(npts, h->occ[1], h->nsm), 256, st, L, S);
+  const size_t n = t.n();
+  MG_LAUNCH_PDL((k_mg_cast<double, float>), vgrid(n), 256, st, t.f, (const float*)L.t, n, S);
+  MG_CUDA(cudaGetLastError());
+  return MOONS_OK;
+}
+
+// z += gamma N, gamma = (N.t) / (N.A N) on the FP32 finest level (N, t: FP64
+// arrays of the PCG's layout; N's copy overwrites the level's e, which the
+// next V-cycle's first sweep rewrites)
+int mg_two_stage_combine(MGHier* h, DF z, const double* N, const double* t, cudaStream_t st, const PcgScalars* S) {
+  if (!h->mixed || h->fd || !h->ts_part) {
+    set_error("two-stage preconditioner: needs the FP32 V-cycle");
+    return MOONS_ERR_STATE;
+  }
+  const MGLev<float>& L = h->Lf[0];
+  const size_t n = z.n();
+  MG_LAUNCH_PDL((k_mg_cast<float, double>), vgrid(n), 256, st, L.e, N, n, S);
+  MG_LAUNCH_PDL(k_ts_dots<float>, kTsBlocks, 256, st, L, t, h->ts_part, S);
+  MG_LAUNCH_PDL(k_ts_gamma, 1, 32, st, (const double*)h->ts_part, kTsBlocks, h->ts_gamma, S);
+  MG_LAUNCH_PDL(k_ts_axpy, vgrid(n), 256, st, z.f, N, (const double*)h->ts_gamma, n, S);
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
 }

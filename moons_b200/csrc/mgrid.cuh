@@ -204,6 +204,7 @@ __device__ __forceinline__ T diag_A(const MGLev<T>& L, int i, int j, int k) {
 // first != 0: e starts at zero (both colours are written).
 template <typename T>
 __global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int first, T omega, const PcgScalars* S) {
+  pdl_enter();
   if (S && S->done) return;
   const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
   const int nxh = (nx + 1) / 2;
@@ -235,6 +236,7 @@ __global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int fi
 // t = r - A e at interior points
 template <typename T>
 __global__ void __launch_bounds__(256) k_mg_resid(MGLev<T> L, const PcgScalars* S) {
+  pdl_enter();
   if (S && S->done) return;
   const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
   const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
@@ -254,6 +256,7 @@ __global__ void __launch_bounds__(256) k_mg_resid(MGLev<T> L, const PcgScalars* 
 template <typename T>
 __global__ void __launch_bounds__(256) k_mg_restrict(MGLev<T> F, MGLev<T> C, MGRest<T> Rx, MGRest<T> Ry,
                                                      MGRest<T> Rz, const PcgScalars* S) {
+  pdl_enter();
   if (S && S->done) return;
   const int nx = C.s0 - 2, ny = C.s1 - 2, nz = C.s2 - 2;
   const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
@@ -282,6 +285,7 @@ __global__ void __launch_bounds__(256) k_mg_restrict(MGLev<T> F, MGLev<T> C, MGR
 template <typename T>
 __global__ void __launch_bounds__(256) k_mg_prolong(MGLev<T> F, MGLev<T> C, MGProl<T> Px, MGProl<T> Py,
                                                     MGProl<T> Pz, const PcgScalars* S) {
+  pdl_enter();
   if (S && S->done) return;
   const int nx = F.s0 - 2, ny = F.s1 - 2, nz = F.s2 - 2;
   const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
@@ -309,6 +313,7 @@ __global__ void __launch_bounds__(256) k_mg_prolong(MGLev<T> F, MGLev<T> C, MGPr
 // backward ones (symmetric), all inside one block
 template <typename T>
 __global__ void __launch_bounds__(256) k_mg_coarse(MGLev<T> L, int sweeps, const PcgScalars* S) {
+  pdl_enter();
   if (S && S->done) return;
   const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
   const int n = nx * ny * nz;
@@ -334,28 +339,118 @@ __global__ void __launch_bounds__(256) k_mg_coarse(MGLev<T> L, int sweeps, const
 
 // coarsest level solved directly: e = Minv r over the n interior cells
 // (Minv: the inverse of the level's operator, regularised on the constant
-// mode when no face is Dirichlet; built on the host and stored transposed,
-// Minv[c * n + row] = inverse(row, c)).  Minv and the sum are
+// mode when no face is Dirichlet; built on the host, row-major).  One warp
+// forms one row's dot product from the block's gathered copy of r.  Minv and
+// the sum are
 // FP64 on every level type: a stretched, high-contrast coarsest operator can
 // have a condition number at which an FP32 inverse is no solve at all.
+constexpr int kDirectMax = 1024;        // largest coarsest level solved by the dense inverse
+constexpr int kDirectRowsPerBlock = 8;  // one warp per row of the inverse
 template <typename T>
 __global__ void __launch_bounds__(256) k_mg_direct(MGLev<T> L, const double* Minv, int n, const PcgScalars* S) {
+  pdl_enter();
   if (S && S->done) return;
+  __shared__ double rs[kDirectMax];
   const int nx = L.s0 - 2, ny = L.s1 - 2;
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    double acc = 0.0;
-    for (int c = 0; c < n; c++) {
-      const int i = c % nx + 2, q = c / nx, j = q % ny + 2, k = q / ny + 2;
-      acc += Minv[(size_t)c * n + row] * (double)L.r[lidx(L, i, j, k)];  // Minv stored transposed
-    }
+  // the level's right-hand side, gathered once per block in the inverse's order
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    const int i = c % nx + 2, q = c / nx, j = q % ny + 2, k = q / ny + 2;
+    rs[c] = (double)L.r[lidx(L, i, j, k)];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * kDirectRowsPerBlock + (threadIdx.x >> 5);
+  if (row >= n) return;
+  const double* mr = Minv + (size_t)row * n;  // row-major
+  double acc = 0.0;
+  for (int c = lane; c < n; c += 32) acc += mr[c] * rs[c];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) {
     const int i = row % nx + 2, q = row / nx, j = q % ny + 2, k = q / ny + 2;
     L.e[lidx(L, i, j, k)] = (T)acc;
   }
 }
 
+// ---- the learned + mixed (two-stage) preconditioner's scaling -------------
+// z = V(r) + gamma N(t), t = r - A V(r): gamma = (N.t) / (N.A N) minimises the
+// energy norm of the remaining error e - V(r) - gamma N along N (A e = r, so
+// A (e - V(r)) = t).  N is in the finest level's e array; t and the sums are
+// FP64; fixed block partition and summation order.
+constexpr int kTsBlocks = 296;
+template <typename T>
+__global__ void __launch_bounds__(256) k_ts_dots(MGLev<T> L, const double* t, double* part, const PcgScalars* S) {
+  pdl_enter();
+  if (S && S->done) return;
+  const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
+  const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
+  double a = 0.0, b = 0.0;
+  for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < n; q0 += gridDim.x * blockDim.x) {
+    const unsigned q = q0 / (unsigned)nx;
+    const int i = (int)(q0 - q * (unsigned)nx) + 2;
+    const unsigned kk = q / (unsigned)ny;
+    const int j = (int)(q - kk * (unsigned)ny) + 2, k = (int)kk + 2;
+    T D;
+    const T An = apply_A<T>(L, L.e, i, j, k, D);
+    const size_t id = lidx(L, i, j, k);
+    const double nv = (double)L.e[id];
+    a += nv * t[id];
+    b += nv * (double)An;
+  }
+  __shared__ double sa[8], sb[8];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sa[threadIdx.x >> 5] = a;
+    sb[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      ta += sa[w];
+      tb += sb[w];
+    }
+    part[2 * blockIdx.x] = ta;
+    part[2 * blockIdx.x + 1] = tb;
+  }
+}
+
+__global__ void k_ts_gamma(const double* part, int nb, double* gamma, const PcgScalars* S) {
+  pdl_enter();
+  if (S && S->done) return;
+  const int lane = threadIdx.x & 31;
+  double a = 0.0, b = 0.0;
+  for (int q = lane; q < nb; q += 32) {
+    a += part[2 * q];
+    b += part[2 * q + 1];
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) {
+    const double g = a / b;
+    *gamma = (b != 0.0 && isfinite(g)) ? g : 0.0;  // A may be negative definite; no usable direction: z = V(r)
+  }
+}
+
+__global__ void k_ts_axpy(double* z, const double* N, const double* gamma, size_t n, const PcgScalars* S) {
+  pdl_enter();
+  if (S && S->done) return;
+  const double g = *gamma;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    z[i] = z[i] + g * N[i];
+}
+
 // dst = (Tdst) src over n entries
 template <typename Td, typename Ts>
 __global__ void k_mg_cast(Td* dst, const Ts* src, size_t n, const PcgScalars* S) {
+  pdl_enter();
   if (S && S->done) return;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     dst[i] = (Td)src[i];
@@ -367,6 +462,7 @@ __global__ void k_mg_cast(Td* dst, const Ts* src, size_t n, const PcgScalars* S)
 // interior; the last block runs update_exit_loop
 __global__ void __launch_bounds__(kLB) k_m_update(DF x, DF p, DF r, DF Ap, double* rprev, PcgScalars* S,
                                                   double* partial, unsigned* ticket) {
+  pdl_enter();
   if (S->done) return;
   const double alpha = S->alpha;
   if (S->stag_window > 0 && !(isfinite(alpha) && alpha > 0.0)) {
@@ -440,6 +536,7 @@ __global__ void __launch_bounds__(kLB) k_m_update(DF x, DF p, DF r, DF Ap, doubl
 // rho' = z.r (interior), flexible: minus z.r_prev; beta = that / rho
 __global__ void __launch_bounds__(kLB) k_m_beta(DF z, DF r, const double* rprev, PcgScalars* S, double* partial,
                                                 unsigned* ticket) {
+  pdl_enter();
   if (S->done) return;
   double azr = 0.0, azp = 0.0;
   const unsigned n = (unsigned)z.n();
@@ -472,6 +569,7 @@ __global__ void __launch_bounds__(kLB) k_m_beta(DF z, DF r, const double* rprev,
 
 // p' = z + beta p (every point; BC points are rewritten by k_l_bcfill)
 __global__ void __launch_bounds__(kLB) k_m_pupd(DF pn, DF p, DF z, const PcgScalars* S) {
+  pdl_enter();
   if (S->done) return;
   const double beta = S->beta;
   const unsigned n = (unsigned)p.n();

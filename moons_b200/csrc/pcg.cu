@@ -213,6 +213,9 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const mg::DBC& bc, const mg
 int fd_build(moons_pcg* s, moons_mesh* m, const mg::DBC& bc, MGHier** out);
 void mg_free(MGHier* h);
 int mg_vcycle(MGHier* h, mg::DF z, mg::DF r, cudaStream_t st, const mg::PcgScalars* S);
+int mg_vcycle_resid_f64(MGHier* h, mg::DF t, cudaStream_t st, const mg::PcgScalars* S);
+int mg_two_stage_combine(MGHier* h, mg::DF z, const double* N, const double* t, cudaStream_t st,
+                         const mg::PcgScalars* S);
 double* mg_rprev(MGHier* h);
 
 // ---------------------------------------------------------------------------
@@ -245,6 +248,7 @@ struct moons_pcg {
   // MOONS_PREC_UNET: the network (not owned) and the multigrid fallback mode
   moons_unet* unet = nullptr;
   bool learned = false;
+  bool two_stage = false;       // MOONS_PREC_UNET_MG: z = V(r) + N(r - A V(r))
   bool fb = false;              // true while the fallback (FP32 V-cycle) runs
   // the other mode's loop graph (swapped in and out with the fields above)
   cudaGraph_t graph_alt = nullptr;
@@ -362,7 +366,8 @@ int apply_op_explicit(moons_pcg* s, DF* out, DF* x) {
 int compute_prec(moons_pcg* s) {
   moons_mesh* m = s->m;
   int mode = s->prec;
-  if (mode == MOONS_PREC_MG || mode == MOONS_PREC_MG_MIXED || mode == MOONS_PREC_UNET || mode == MOONS_PREC_FD)
+  if (mode == MOONS_PREC_MG || mode == MOONS_PREC_MG_MIXED || mode == MOONS_PREC_UNET || mode == MOONS_PREC_FD ||
+      mode == MOONS_PREC_UNET_MG)
     mode = MOONS_PREC_IDENTITY;  // Minv unused
   DF dummy{};
   if (mode == MOONS_PREC_IND && s->op != MOONS_OP_IND_DIFFUSION) {
@@ -507,6 +512,23 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
   return MOONS_OK;
 }
 
+// z = M(r) of a multigrid-family solver: the V-cycle, the U-Net, or (two-
+// stage) the V-cycle then the U-Net on what it leaves:
+// z = V(r) + gamma N(r - A V(r)), with r - A V(r) the FP32 finest level's
+// residual and gamma the energy-optimal multiple of the network's output
+// (work arrays: tempx, xbc)
+int apply_prec_dev(moons_pcg* s, const int* skip, const PcgScalars* S) {
+  moons_mesh* m = s->m;
+  if (s->learned && !s->fb && !s->two_stage) return unet_apply_dev(s->unet, s->z[0].f, s->r[0].f, skip);
+  int r = mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, S);
+  if (r || !(s->learned && s->two_stage && !s->fb)) return r;
+  if ((r = mg_vcycle_resid_f64(s->mgh, s->tempx[0], m->stream, S))) return r;
+  // the network writes interior cells only: its output buffer's ghosts are 0
+  MG_CUDA(cudaMemsetAsync(s->xbc[0].f, 0, s->xbc[0].n() * sizeof(double), m->stream));
+  if ((r = unet_apply_dev(s->unet, s->xbc[0].f, s->tempx[0].f, skip))) return r;
+  return mg_two_stage_combine(s->mgh, s->z[0], s->xbc[0].f, s->tempx[0].f, m->stream, S);
+}
+
 // one multigrid-preconditioned CG iteration, twice (p -> p2 -> p)
 int enqueue_mg_iteration(moons_pcg* s, DF* x) {
   moons_mesh* m = s->m;
@@ -522,18 +544,17 @@ int enqueue_mg_iteration(moons_pcg* s, DF* x) {
     DF* pc = half == 0 ? s->p : s->p2;
     DF* pn = half == 0 ? s->p2 : s->p;
     if (s->op == MOONS_OP_LAP_PROPS)
-      MG_LAUNCH(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], s->k[0], s->k[1],
+      MG_LAUNCH_PDL(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], s->k[0], s->k[1],
                 s->k[2], 0.0, s->S, s->partial, tA);
     else
-      MG_LAUNCH(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], z0, z0, z0, 0.0,
+      MG_LAUNCH_PDL(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], z0, z0, z0, 0.0,
                 s->S, s->partial, tA);
-    MG_LAUNCH(k_m_update, gF, kLB, m->stream, x[0], pc[0], s->r[0], s->Ax[0], rprev, s->S, s->partial, tB);
-    int r = (s->learned && !s->fb) ? unet_apply_dev(s->unet, s->z[0].f, s->r[0].f, &s->S->done)
-                                   : mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, s->S);
+    MG_LAUNCH_PDL(k_m_update, gF, kLB, m->stream, x[0], pc[0], s->r[0], s->Ax[0], rprev, s->S, s->partial, tB);
+    int r = apply_prec_dev(s, &s->S->done, s->S);
     if (r) return r;
-    MG_LAUNCH(k_m_beta, gF, kLB, m->stream, s->z[0], s->r[0], rprev, s->S, s->partial, tA);
-    MG_LAUNCH(k_m_pupd, gF, kLB, m->stream, pn[0], pc[0], s->z[0], s->S);
-    if (L.bc) MG_LAUNCH(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, 1), b[0], b[1], b[2], L.npbP, s->S);
+    MG_LAUNCH_PDL(k_m_beta, gF, kLB, m->stream, s->z[0], s->r[0], rprev, s->S, s->partial, tA);
+    MG_LAUNCH_PDL(k_m_pupd, gF, kLB, m->stream, pn[0], pc[0], s->z[0], s->S);
+    if (L.bc) MG_LAUNCH_PDL(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, 1), b[0], b[1], b[2], L.npbP, s->S);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
@@ -702,7 +723,7 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: ncomp must be 1 or 3");
     return MOONS_ERR_ARG;
   }
-  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_NRG_DIFFUSION || prec < 0 || prec > MOONS_PREC_FD) {
+  if (op < MOONS_OP_LAP_UNIFORM || op > MOONS_OP_NRG_DIFFUSION || prec < 0 || prec > MOONS_PREC_UNET_MG) {
     set_error("moons_pcg_create: bad operator/preconditioner");
     return MOONS_ERR_ARG;
   }
@@ -715,8 +736,8 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     set_error("moons_pcg_create: operator needs three coefficient fields");
     return MOONS_ERR_ARG;
   }
-  const bool use_mg =
-      prec == MOONS_PREC_MG || prec == MOONS_PREC_MG_MIXED || prec == MOONS_PREC_UNET || prec == MOONS_PREC_FD;
+  const bool use_mg = prec == MOONS_PREC_MG || prec == MOONS_PREC_MG_MIXED || prec == MOONS_PREC_UNET ||
+                      prec == MOONS_PREC_FD || prec == MOONS_PREC_UNET_MG;
   if (use_mg) {
     bool ok = nc == 1 && (op == MOONS_OP_LAP_UNIFORM || (op == MOONS_OP_LAP_PROPS && prec != MOONS_PREC_FD)) && x[0] &&
               x[0]->f.dl == MOONS_CC;
@@ -830,7 +851,8 @@ int moons_pcg_create(moons_mesh* m, int op, int prec, int nc, moons_sf* const* x
     r = prec == MOONS_PREC_FD
             ? fd_build(s, m, s->x_bc[0], &s->mgh)
             : mg_build(s, m, prec != MOONS_PREC_MG, s->x_bc[0], op == MOONS_OP_LAP_PROPS ? s->k : nullptr, &s->mgh);
-    s->learned = prec == MOONS_PREC_UNET;
+    s->learned = prec == MOONS_PREC_UNET || prec == MOONS_PREC_UNET_MG;
+    s->two_stage = prec == MOONS_PREC_UNET_MG;
     if (r == MOONS_ERR_NOMEM) set_error("moons_pcg_create: device allocation failed (multigrid levels)");
   }
   if (!r && cudaStreamSynchronize(m->stream) != cudaSuccess) r = cuda_fail(cudaGetLastError(), "pcg create");
@@ -980,10 +1002,10 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
   // z = Minv r ; p = z ; rhok = dot(r,z)
   if (learned) {
     if (!s->unet) {
-      set_error("moons_pcg_solve: MOONS_PREC_UNET needs a network (moons_pcg_set_unet)");
+      set_error("moons_pcg_solve: MOONS_PREC_UNET / MOONS_PREC_UNET_MG needs a network (moons_pcg_set_unet)");
       return MOONS_ERR_STATE;
     }
-    r = unet_apply_dev(s->unet, s->z[0].f, s->r[0].f, nullptr);
+    r = apply_prec_dev(s, nullptr, nullptr);
     if (r) return r;
   } else if (s->mgh) {
     r = mg_vcycle(s->mgh, s->z[0], s->r[0], m->stream, nullptr);
@@ -1158,13 +1180,39 @@ int moons_pcg_residual(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, moo
   return r;
 }
 
+int moons_pcg_apply_prec(moons_pcg* s, moons_sf* const* z, moons_sf* const* r) {
+  if (!s || !z || !r) {
+    set_error("moons_pcg_apply_prec: null argument");
+    return MOONS_ERR_ARG;
+  }
+  moons_mesh* m = s->m;
+  cudaSetDevice(m->device);
+  for (int c = 0; c < s->nc; c++)
+    if (!z[c] || !r[c] || z[c]->f.n() != s->r[c].n() || r[c]->f.n() != s->r[c].n()) {
+      set_error("moons_pcg_apply_prec: field does not match the solver");
+      return MOONS_ERR_SHAPE;
+    }
+  int rc = MOONS_OK;
+  if (s->mgh) {
+    rc = mg_vcycle(s->mgh, z[0]->f, r[0]->f, m->stream, nullptr);
+  } else {
+    for (int c = 0; c < s->nc && !rc; c++) {
+      rc = launch_pw(m, PW_COPY, z[c]->f, &s->Minv[c], 0.0);
+      if (!rc) rc = launch_pw(m, PW_MUL, z[c]->f, &r[c]->f, 0.0);
+    }
+  }
+  if (rc) return rc;
+  MG_CUDA(cudaStreamSynchronize(m->stream));
+  return MOONS_OK;
+}
+
 int moons_pcg_set_unet(moons_pcg* s, moons_unet* u) {
   if (!s || !u) {
     set_error("moons_pcg_set_unet: null argument");
     return MOONS_ERR_ARG;
   }
   if (!s->learned) {
-    set_error("moons_pcg_set_unet: the solver was not created with MOONS_PREC_UNET");
+    set_error("moons_pcg_set_unet: the solver was not created with MOONS_PREC_UNET or MOONS_PREC_UNET_MG");
     return MOONS_ERR_ARG;
   }
   if (unet_mesh(u) != s->m) {

@@ -12,10 +12,19 @@ library's CUDA kernels (``capi.UNet``); this module only drives them:
   solver's own residual at x_k (what a preconditioner is applied to) and
   e = x* - x_k (mean removed: the all-Neumann operator ignores constants);
   ``make_pairs_learned`` adds the iterates of the learned solve itself;
+* ``make_pairs_two_stage`` -- pairs of the learned + mixed form
+  (MOONS_PREC_UNET_MG, z = V(r) + N(r - A V(r))): at each iterate x_k the
+  network's input is what one FP32 V-cycle leaves, t = r(x_k + V(r_k)), and
+  its target the remaining error e = x* - x_k - V(r_k); the iterates come
+  from the reference's Jacobi-PCG and from multigrid flexible CG (the
+  residuals the two-stage solve itself meets);
 * ``train`` -- Adam epochs over the pairs, shuffled by PyTorch (the only
   PyTorch use: the data order), cosine learning-rate schedule; the default
   loss is the cosine in the energy norm of each case's own operator (the
   norm CG minimises), so the network is trained for what FCG needs;
+  ``blocked=True`` shuffles the draws and the pairs within each draw and
+  builds a draw's operator only while its pairs run (for pair sets of
+  hundreds of draws, whose operators would not all stay resident);
 * ``save`` / ``load`` -- the flat parameter array and the output scale.
 """
 from __future__ import annotations
@@ -69,6 +78,22 @@ class ShellCase:
 
     def solver(self, prec: int) -> G.PCG:
         return G.PCG(self.mesh, G.OP_LAP_PROPS, prec, [self.phi], [self.phi], self.k)
+
+    def release(self, rhs: bool = True):
+        """Free the operator's solver (rebuilt on demand by operator()) and,
+        with `rhs`, the right-hand side, keeping what training reads (the
+        coefficient fields and phi, whose BCs define the operator)."""
+        if self.op is not None:
+            self.op.close()
+            self.op = None
+        if rhs and self.rhs is not None:
+            self.rhs.close()
+            self.rhs = None
+
+    def operator(self) -> G.PCG:
+        if self.op is None:
+            self.op = self.solver(G.PREC_MG_MIXED)
+        return self.op
 
 
 @dataclass
@@ -140,6 +165,62 @@ def make_pairs_learned(cases: Sequence[ShellCase], net: G.UNet, iterates=(1, 2, 
     return pairs
 
 
+def _zero_ghosts(a):
+    a[0, :, :] = a[-1, :, :] = 0.0
+    a[:, 0, :] = a[:, -1, :] = 0.0
+    a[:, :, 0] = a[:, :, -1] = 0.0
+    return a
+
+
+def make_pairs_two_stage(cases: Sequence[ShellCase], jacobi=(0, 8, 64), fcg=(1, 2, 3, 4, 5),
+                         tol_ref: float = 1e-12, release: bool = False) -> List[Pair]:
+    """(t, e) pairs of the learned + mixed form (see the module text): for
+    each iterate x_k -- of the reference's Jacobi-PCG capped at k iterations
+    (`jacobi`) and of multigrid flexible CG capped at k (`fcg`) -- the
+    residual r_k, one FP32 V-cycle v = V(r_k) (moons_pcg_apply_prec), the
+    network's input t = r(x_k + v) and its target e = x* - x_k - v (mean
+    removed).  `release` frees each draw's solver and right-hand side once
+    its pairs are made."""
+    pairs: List[Pair] = []
+    for ci, c in enumerate(cases):
+        op = c.operator()
+        c.phi.fill(0.0)
+        op.solve([c.phi], [c.rhs], G.isp(1000, tol_ref, 1e-300))
+        xstar = c.phi.download()
+        iterates = []
+        jac = c.solver(G.PREC_LAP)
+        for k in jacobi:
+            c.phi.fill(0.0)
+            if k > 0:
+                jac.solve([c.phi], [c.rhs], G.isp(k, 1e-300, 1e-300))
+            iterates.append((k, c.phi.download()))
+        jac.close()
+        for k in fcg:
+            c.phi.fill(0.0)
+            op.solve([c.phi], [c.rhs], G.isp(k, 1e-300, 1e-300))
+            iterates.append((1000 + k, c.phi.download()))
+        r = c.mesh.field(G.CC)
+        v = c.mesh.field(G.CC)
+        for k, xk in iterates:
+            c.phi.upload(xk)
+            op.residual([c.phi], [c.rhs], [r])
+            op.apply_prec([v], [r])
+            x1 = xk + _zero_ghosts(v.download())
+            c.phi.upload(x1)
+            t = c.mesh.field(G.CC)
+            op.residual([c.phi], [c.rhs], [t])
+            e = xstar - x1
+            e[1:-1, 1:-1, 1:-1] -= _interior(e).mean()
+            fe = c.mesh.field(G.CC)
+            fe.upload(_zero_ghosts(e))
+            pairs.append(Pair(t, fe, ci, k))
+        r.close()
+        v.close()
+        if release:
+            c.release()
+    return pairs
+
+
 def output_scale(pairs: Sequence[Pair]) -> float:
     """Median of rms(e) / rms(r) over the pairs: the network's output scale."""
     q = []
@@ -152,8 +233,22 @@ def output_scale(pairs: Sequence[Pair]) -> float:
     return float(np.median(q)) if q else 1.0
 
 
+def _blocked_order(pairs: Sequence[Pair], gen) -> List[int]:
+    import torch
+
+    by_case = {}
+    for i, p in enumerate(pairs):
+        by_case.setdefault(p.case, []).append(i)
+    keys = sorted(by_case)
+    order = []
+    for kc in torch.randperm(len(keys), generator=gen).tolist():
+        idx = by_case[keys[kc]]
+        order += [idx[j] for j in torch.randperm(len(idx), generator=gen).tolist()]
+    return order
+
+
 def train(net: G.UNet, cases: Sequence[ShellCase], pairs: Sequence[Pair], epochs: int = 4, lr: float = 1e-3,
-          lr_min: float = 5e-5, seed: int = 0, loss: int = 2, log=None) -> List[float]:
+          lr_min: float = 5e-5, seed: int = 0, loss: int = 2, log=None, blocked: bool = False) -> List[float]:
     """Adam over the pairs for `epochs` passes; returns the mean loss of each
     epoch.  The data order is drawn by PyTorch (torch.randperm)."""
     import torch
@@ -165,29 +260,85 @@ def train(net: G.UNet, cases: Sequence[ShellCase], pairs: Sequence[Pair], epochs
     hist = []
     cur_case = -1
     for ep in range(epochs):
-        order = torch.randperm(len(pairs), generator=gen).tolist()
+        order = _blocked_order(pairs, gen) if blocked else torch.randperm(len(pairs), generator=gen).tolist()
         acc = 0.0
         for i in order:
             p = pairs[i]
             if p.case != cur_case:
+                if blocked and cur_case >= 0:
+                    cases[cur_case].release(rhs=False)
                 net.set_coeff(cases[p.case].k)
                 if loss == 2:
-                    net.set_operator(cases[p.case].op)
+                    net.set_operator(cases[p.case].operator())
                 cur_case = p.case
             a = lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * t / max(1, steps)))
             acc += net.train_step(p.r, p.e, a)
             t += 1
         hist.append(acc / len(pairs))
+        if blocked and cur_case >= 0:
+            cases[cur_case].release(rhs=False)
+            cur_case = -1
         if log:
             log(f"epoch {ep}: mean loss {hist[-1]:.4f}")
     return hist
 
 
-def save(net: G.UNet, path: str):
-    np.savez_compressed(path, params=net.get_params(), out_scale=np.float64(net.out_scale))
+def save(net: G.UNet, path: str, meta: dict | None = None):
+    import json
+    np.savez_compressed(path, params=net.get_params(), out_scale=np.float64(net.out_scale),
+                        meta=np.array(json.dumps(meta or {})))
 
 
-def load(net: G.UNet, path: str):
+def load(net: G.UNet, path: str) -> dict:
+    import json
     d = np.load(path)
     net.set_params(d["params"])
     net.out_scale = float(d["out_scale"])
+    return json.loads(str(d["meta"])) if "meta" in d else {}
+
+
+def train_two_stage(n: int = 128, shell: int = 4, draws: int = 250, epochs: int = 8, lr: float = 1e-3,
+                    lr_min: float = 5e-5, seed: int = 0, log=None):
+    """The learned + mixed network of the sigma-shell case: `draws` seeded
+    draws (seeds 0 .. draws-1; held-out evaluation uses seeds from 1000), 8
+    pairs each (Jacobi-PCG iterates 0, 8, 64 and multigrid-FCG iterates 1-5),
+    Adam with the energy-norm cosine loss in blocked order.  Returns the
+    network, its mesh and a summary."""
+    import time
+    mesh = shell_mesh(n)
+    t0 = time.perf_counter()
+    cases, pairs = [], []
+    for s in range(draws):
+        c = ShellCase.build(mesh, n, shell, s)
+        ps = make_pairs_two_stage([c], release=True)   # keeps the coefficient fields and phi only
+        for p in ps:
+            p.case = s
+        cases.append(c)
+        pairs += ps
+        if log and (s + 1) % 25 == 0:
+            log(f"pairs: {s + 1} draws, {len(pairs)} pairs, {time.perf_counter() - t0:.0f} s")
+    t1 = time.perf_counter()
+    net = G.UNet(mesh, seed=seed)
+    net.out_scale = output_scale(pairs)
+    hist = train(net, cases, pairs, epochs=epochs, lr=lr, lr_min=lr_min, seed=seed, blocked=True, log=log)
+    t2 = time.perf_counter()
+    meta = {"n": n, "shell": shell, "draws": draws, "pairs": len(pairs), "epochs": epochs,
+            "adam_steps": epochs * len(pairs), "loss": "energy-norm cosine (kind 2)",
+            "loss_first_last": [hist[0], hist[-1]], "data_seconds": t1 - t0, "train_seconds": t2 - t1,
+            "out_scale": net.out_scale}
+    return net, mesh, meta
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="train the learned + mixed (two-stage) network on the "
+                                             "sigma-shell case and save its weights")
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--shell", type=int, default=4)
+    ap.add_argument("--draws", type=int, default=250)
+    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--out", required=True)
+    a = ap.parse_args()
+    net_, _, meta_ = train_two_stage(a.n, a.shell, a.draws, a.epochs, log=lambda s: print(s, flush=True))
+    save(net_, a.out, meta_)
+    print(meta_, flush=True)

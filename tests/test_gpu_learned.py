@@ -81,6 +81,41 @@ def test_useless_network_falls_back_to_multigrid(trained):
     assert np.abs(x - xm).max() < 1e-7 * np.abs(xm).max()
 
 
+def test_two_stage_with_zero_network_is_the_vcycle_fcg():
+    """MOONS_PREC_UNET_MG with N = 0 is z = V(r): flexible CG with the FP32
+    V-cycle, the same iterates to the last bit."""
+    mesh = L.shell_mesh(N)
+    case = L.ShellCase.build(mesh, N, SHELL, 104)
+    zero = G.UNet(mesh, seed=1)
+    zero.set_params(np.zeros(zero.nparams, dtype=np.float32))
+    i2, x2 = _solve(case, G.PREC_UNET_MG, zero)
+    im, xm = _solve(case, G.PREC_MG_MIXED)
+    assert i2["exit_reason"] == im["exit_reason"] == 1
+    assert i2["iterations"] == im["iterations"]
+    assert np.abs(x2 - xm).max() <= 1e-14 * np.abs(xm).max()
+
+
+def test_apply_prec_is_one_vcycle():
+    """moons_pcg_apply_prec of a multigrid solver is the V-cycle its CG uses:
+    one preconditioned step from x = 0 (z = V(r0), alpha = (r0.z)/(z.Az))
+    lands on alpha * V(r0)."""
+    mesh = L.shell_mesh(16)
+    case = L.ShellCase.build(mesh, 16, SHELL, 5)
+    op = case.operator()
+    r, z = mesh.field(G.CC), mesh.field(G.CC)
+    case.phi.fill(0.0)
+    op.residual([case.phi], [case.rhs], [r])
+    op.apply_prec([z], [r])
+    case.phi.fill(0.0)
+    op.solve([case.phi], [case.rhs], G.isp(1, 1e-300, 1e-300))
+    x1 = case.phi.download()[1:-1, 1:-1, 1:-1]
+    v = z.download()[1:-1, 1:-1, 1:-1]
+    x1, v = x1 - x1.mean(), v - v.mean()
+    a = float((x1 * v).sum() / (v * v).sum())
+    assert a > 0
+    assert np.abs(x1 - a * v).max() <= 1e-12 * np.abs(x1).max()
+
+
 def test_unet_solver_needs_a_network():
     mesh = L.shell_mesh(16)
     case = L.ShellCase.build(mesh, 16, SHELL, 0)
