@@ -22,6 +22,7 @@ module moons_gpu_mod
   integer(c_int), parameter :: MOONS_PREC_MOM = 2, MOONS_PREC_IND = 3
   integer(c_int), parameter :: MOONS_PREC_MG = 4, MOONS_PREC_MG_MIXED = 5, MOONS_PREC_UNET = 6
   integer(c_int), parameter :: MOONS_PREC_FD = 7
+  integer(c_int), parameter :: MOONS_PREC_UNET_MG = 8
   ! largest face temporary (points) that moons_lap_var_noalloc accepts
   integer(c_long_long), parameter :: MOONS_LAP_VAR_NOALLOC_MAX_POINTS = 131072_c_long_long
 
@@ -211,6 +212,13 @@ module moons_gpu_mod
     function moons_pcg_set_unet(s, u) bind(C, name="moons_pcg_set_unet") result(st)
       import :: c_ptr, c_int
       type(c_ptr), value :: s, u
+      integer(c_int) :: st
+    end function
+
+    function moons_pcg_apply_prec(s, z, r) bind(C, name="moons_pcg_apply_prec") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s
+      type(c_ptr), intent(in) :: z(*), r(*)
       integer(c_int) :: st
     end function
 

@@ -200,6 +200,34 @@ MGAxis<T> axis_tables(MGHier* h, const host::HostCoord& c, cudaStream_t st) {
   return a;
 }
 
+// face weights of axis d on a level (face array, x fastest): the volume-
+// weighted operator's coupling across the face, W = vol * cc2nD[t-1] * k *
+// n2ccD[t] for the low face of cell t, and vol * cc2nU[t] * k * n2ccU[t] of
+// the last cell for the top boundary face; (A e)(c) = sum_f W_f (e_nb - e_c)
+std::vector<double> face_weights(const host::HostCoord* c, const std::array<int, 3>& s, int d,
+                                 const std::vector<double>* K) {
+  std::array<int, 3> e = s;
+  e[d] += 1;
+  std::vector<double> w((size_t)e[0] * e[1] * e[2], 0.0);
+  auto fid = [&](int a, int b, int cc) { return (size_t)(a - 1) + (size_t)e[0] * ((b - 1) + (size_t)e[1] * (cc - 1)); };
+  for (int k = 2; k <= s[2] - 1; k++)
+    for (int j = 2; j <= s[1] - 1; j++)
+      for (int i = 2; i <= s[0] - 1; i++) {
+        const int ii[3] = {i, j, k};
+        const int t = ii[d];
+        const double vol = (c[0].dhn[i] * c[1].dhn[j]) * c[2].dhn[k];
+        const size_t flo = fid(i, j, k);
+        const double kl = K ? (*K)[flo] : 1.0;
+        w[flo] = c[d].cc2nD[t - 1] * kl * c[d].n2ccD[t] * vol;
+        if (t == s[d] - 1) {
+          const size_t fhi = fid(i + (d == 0), j + (d == 1), k + (d == 2));
+          const double kr = K ? (*K)[fhi] : 1.0;
+          w[fhi] = c[d].cc2nU[t] * kr * c[d].n2ccU[t] * vol;
+        }
+      }
+  return w;
+}
+
 // area-weighted mean of the fine faces covering each coarse face of axis d
 std::vector<double> coarsen_faces(const std::vector<double>& kf, int d, const std::array<int, 3>& sf,
                                   const std::array<int, 3>& sc, const host::HostCoord* cf, const bool* cz) {
@@ -392,6 +420,13 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
     Ld.s0 = Lf.s0 = h->s[l][0];
     Ld.s1 = Lf.s1 = h->s[l][1];
     Ld.s2 = Lf.s2 = h->s[l][2];
+    const host::HostCoord cl[3] = {C[0][l], C[1][l], C[2][l]};
+    for (int d = 0; d < 3; d++) {
+      const std::vector<double> W = face_weights(cl, h->s[l], d, kf ? &K[l][d] : nullptr);
+      if (!h->mixed) Ld.w[d] = dev_copy(h.get(), W, st);
+      else Lf.w[d] = dev_copy(h.get(), conv<float>(W), st);
+      if (!(h->mixed ? (const void*)Lf.w[d] : (const void*)Ld.w[d])) return MOONS_ERR_NOMEM;
+    }
     if (!h->mixed) {
       for (int d = 0; d < 3; d++) Ld.ax[d] = axis_tables<double>(h.get(), C[d][l], st);
       Ld.e = l == 0 ? s->z[0].f : dev_zeros<double>(h.get(), n, st);

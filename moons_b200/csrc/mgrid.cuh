@@ -47,6 +47,7 @@ struct MGLev {
   T *e, *r, *t;      // correction, right-hand side, residual (CC, with ghosts)
   int s0, s1, s2;
   MGAxis<T> ax[3];
+  const T* w[3];     // face weights of the operator per axis (face arrays): (A e)(c) = sum_f W_f (e_nb - e_c)
   const T* kx;       // face coefficients (LAP_PROPS) or null
   const T* ky;
   const T* kz;
@@ -104,18 +105,6 @@ __device__ __forceinline__ T ev(const MGLev<T>& L, const T* e, int i, int j, int
   return fac * e[lidx(L, I[0], I[1], I[2])];
 }
 
-// factor by which the ghost neighbour on side `hi` of axis d (index t of the
-// point) repeats the point itself (Neumann +1, Dirichlet -1), 0 otherwise:
-// that share belongs to the operator's true diagonal
-template <typename T>
-__device__ __forceinline__ T self_ghost(const MGLev<T>& L, int d, bool hi, int t) {
-  const int s = d == 0 ? L.s0 : (d == 1 ? L.s1 : L.s2);
-  if (hi ? t != s - 1 : t != 2) return T(0);
-  const int ty = L.bt[2 * d + (hi ? 2 : 1)];
-  if (ty == MOONS_BC_PERIODIC) return T(0);
-  return ty == MOONS_BC_DIRICHLET ? T(-1) : T(1);
-}
-
 // index of face (i,j,k) of a face-`d` array on the level's grid (the face
 // array has one more entry along d)
 template <typename T>
@@ -124,80 +113,85 @@ __device__ __forceinline__ size_t fidx(const MGLev<T>& L, int d, int i, int j, i
   return (size_t)((unsigned)(i - 1) + f0 * ((unsigned)(j - 1) + f1 * (unsigned)(k - 1)));
 }
 
-// diagonal share of the ghost neighbours that repeat the point (per unit volume)
-template <typename T>
-__device__ __forceinline__ T diag_self(const MGLev<T>& L, const MGAxis<T>& A, const T* kf, int d, int i, int j, int k,
-                                       int t) {
-  const T flo = self_ghost(L, d, false, t), fhi = self_ghost(L, d, true, t);
-  if (flo == T(0) && fhi == T(0)) return T(0);
-  const int di = d == 0, dj = d == 1, dk = d == 2;
-  T kl = T(1), kr = T(1);
-  if (kf) {
-    kl = kf[fidx(L, d, i, j, k)];
-    kr = kf[fidx(L, d, i + di, j + dj, k + dk)];
-  }
-  return flo * (A.cD[t - 1] * kl) * A.nD[t] + fhi * (A.cU[t] * kr) * A.nU[t];
-}
-
 // (A e)(i,j,k) = vol * div(k grad e) at an interior point (k = 1 without
-// face coefficients), and its true diagonal D (the smoother's divisor)
+// face coefficients) as a sum over the cell's six faces, sum_f W_f (e_nb -
+// e0), with the level's precomputed face weights W (the volume-weighted
+// operator is symmetric, so one weight per face), and its true diagonal D
+// (the smoother's divisor).  A ghost neighbour is implied by the level's
+// homogeneous BCs: periodic reads the opposite cell, Neumann repeats the
+// point (the face drops out), Dirichlet negates it (-2 W e0 and -2 W in D).
 template <typename T>
 __device__ __forceinline__ T apply_A(const MGLev<T>& L, const T* e, int i, int j, int k, T& D) {
   const size_t id = lidx(L, i, j, k);
+  const size_t sy = (size_t)L.s0, sz = (size_t)L.s0 * L.s1;
+  const size_t fx = id + (size_t)(j - 1) + (size_t)L.s1 * (size_t)(k - 1);  // x face (i,j,k)
+  const size_t fy = id + (size_t)L.s0 * (size_t)(k - 1);                       // y face (i,j,k)
+  const T w[6] = {L.w[0][fx], L.w[0][fx + 1], L.w[1][fy], L.w[1][fy + sy], L.w[2][id], L.w[2][id + sz]};
   const T e0 = e[id];
-  const int ii[3] = {i, j, k};
   // points two or more away from every boundary read no ghost value
-  const bool inner = i > 2 && i < L.s0 - 1 && j > 2 && j < L.s1 - 1 && k > 2 && k < L.s2 - 1;
-  const size_t st[3] = {1, (size_t)L.s0, (size_t)L.s0 * L.s1};
-  T v = T(0);
-  T dg = T(0);
+  if (i > 2 && i < L.s0 - 1 && j > 2 && j < L.s1 - 1 && k > 2 && k < L.s2 - 1) {
+    const T s = ((w[0] + w[1]) + (w[2] + w[3])) + (w[4] + w[5]);
+    const T nb = ((w[0] * e[id - 1] + w[1] * e[id + 1]) + (w[2] * e[id - sy] + w[3] * e[id + sy])) +
+                 (w[4] * e[id - sz] + w[5] * e[id + sz]);
+    D = -s;
+    return nb - s * e0;
+  }
+  const int ii[3] = {i, j, k};
+  const int s[3] = {L.s0, L.s1, L.s2};
+  const size_t st[3] = {1, sy, sz};
+  T acc = T(0), dg = T(0);
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    const MGAxis<T>& A = L.ax[d];
-    const int t = ii[d];
-    const int di = d == 0, dj = d == 1, dk = d == 2;
-    const T em = inner ? e[id - st[d]] : ev(L, e, i - di, j - dj, k - dk);
-    const T ep = inner ? e[id + st[d]] : ev(L, e, i + di, j + dj, k + dk);
-    T gl = em * A.cD[t - 1] + e0 * A.cU[t - 1];
-    T gr = e0 * A.cD[t] + ep * A.cU[t];
-    T dgl = A.cU[t - 1], dgr = A.cD[t];
-    const T* kf = d == 0 ? L.kx : (d == 1 ? L.ky : L.kz);
-    if (kf) {
-      const T kl = kf[fidx(L, d, i, j, k)], kr = kf[fidx(L, d, i + di, j + dj, k + dk)];
-      gl = gl * kl;
-      gr = gr * kr;
-      dgl = dgl * kl;
-      dgr = dgr * kr;
+#pragma unroll
+    for (int hi = 0; hi < 2; hi++) {
+      const T wf = w[2 * d + hi];
+      const int nbi = ii[d] + (hi ? 1 : -1);
+      if (nbi >= 2 && nbi <= s[d] - 1) {
+        acc = acc + wf * (hi ? e[id + st[d]] : e[id - st[d]]) - wf * e0;
+        dg = dg - wf;
+      } else {
+        const int ty = L.bt[2 * d + 1 + hi];
+        if (ty == MOONS_BC_PERIODIC) {
+          const long long off = (long long)(hi ? 2 - ii[d] : s[d] - 1 - ii[d]) * (long long)st[d];
+          acc = acc + wf * e[(size_t)((long long)id + off)] - wf * e0;
+          dg = dg - wf;
+        } else if (ty == MOONS_BC_DIRICHLET) {
+          acc = acc - T(2) * wf * e0;
+          dg = dg - T(2) * wf;
+        }  // Neumann: the ghost repeats the point, the face drops out
+      }
     }
-    v = v + (gl * A.nD[t] + gr * A.nU[t]);
-    dg = dg + (dgl * A.nD[t] + dgr * A.nU[t]);
-    if (!inner) dg = dg + diag_self<T>(L, A, kf, d, i, j, k, t);
   }
-  const T vol = (L.ax[0].hv[i] * L.ax[1].hv[j]) * L.ax[2].hv[k];
-  D = dg * vol;
-  return v * vol;
+  D = dg;
+  return acc;
 }
 
 // the diagonal D alone
 template <typename T>
 __device__ __forceinline__ T diag_A(const MGLev<T>& L, int i, int j, int k) {
+  const size_t id = lidx(L, i, j, k);
+  const size_t sy = (size_t)L.s0, sz = (size_t)L.s0 * L.s1;
+  const size_t fx = id + (size_t)(j - 1) + (size_t)L.s1 * (size_t)(k - 1);
+  const size_t fy = id + (size_t)L.s0 * (size_t)(k - 1);
+  const T w[6] = {L.w[0][fx], L.w[0][fx + 1], L.w[1][fy], L.w[1][fy + sy], L.w[2][id], L.w[2][id + sz]};
   const int ii[3] = {i, j, k};
+  const int s[3] = {L.s0, L.s1, L.s2};
   T dg = T(0);
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    const MGAxis<T>& A = L.ax[d];
-    const int t = ii[d];
-    const int di = d == 0, dj = d == 1, dk = d == 2;
-    T dgl = A.cU[t - 1], dgr = A.cD[t];
-    const T* kf = d == 0 ? L.kx : (d == 1 ? L.ky : L.kz);
-    if (kf) {
-      dgl = dgl * kf[fidx(L, d, i, j, k)];
-      dgr = dgr * kf[fidx(L, d, i + di, j + dj, k + dk)];
+#pragma unroll
+    for (int hi = 0; hi < 2; hi++) {
+      const int nbi = ii[d] + (hi ? 1 : -1);
+      if (nbi >= 2 && nbi <= s[d] - 1) {
+        dg = dg - w[2 * d + hi];
+      } else {
+        const int ty = L.bt[2 * d + 1 + hi];
+        if (ty == MOONS_BC_PERIODIC) dg = dg - w[2 * d + hi];
+        else if (ty == MOONS_BC_DIRICHLET) dg = dg - T(2) * w[2 * d + hi];
+      }
     }
-    dg = dg + (dgl * A.nD[t] + dgr * A.nU[t]);
-    dg = dg + diag_self<T>(L, A, kf, d, i, j, k, t);
   }
-  return dg * ((L.ax[0].hv[i] * L.ax[1].hv[j]) * L.ax[2].hv[k]);
+  return dg;
 }
 
 // one red-black half sweep of colour `color` (points with (i+j+k)&1 == color).
