@@ -277,7 +277,9 @@ typedef struct {
                                tests, far fewer iterations), or MOONS_PREC_FD
                                (direct solve of the separable pressure and
                                cleaning potential; the sigma-weighted potential
-                               of the low-Rem form takes MG_MIXED)            */
+                               of the low-Rem form takes MG_MIXED), or
+                               MOONS_PREC_UNET_MG (learned + mixed, networks
+                               from moons_mhd_set_unet)                       */
   /* energy equation (energy_extend.f90:236-262, add_all_energy_sources.f90:
    * 21-67), solved on the induction mesh before the momentum step as
    * solve_MOONS does (MOONS_solver.f90:81-85); fields MOONS_MHD_T, _KT,
@@ -381,6 +383,13 @@ int moons_mg_debug(moons_pcg* s, int op, int level, const double* a, const doubl
  * dec0b 16->16), then the 1x1 head w[16], b. */
 typedef struct moons_unet moons_unet;
 int moons_unet_create(moons_mesh* m, unsigned long long seed, moons_unet** out);
+/* networks of the learned + mixed Poisson solves (prec_poisson =
+ * MOONS_PREC_UNET_MG; no reference counterpart): which = 0 the pressure
+ * (net on the fluid mesh), 1 the B-form cleaning potential (net on the
+ * induction mesh); before or after moons_mhd_init.  The low-Rem potential
+ * (sigma-weighted) takes MOONS_PREC_MG_MIXED under this setting.  A step
+ * whose learned solver has no network returns MOONS_ERR_STATE. */
+int moons_mhd_set_unet(moons_mhd* s, int which, moons_unet* u);
 int moons_unet_destroy(moons_unet* u);
 int moons_unet_nparams(const moons_unet* u, long long* n);
 int moons_unet_get_params(moons_unet* u, float* host, long long n);

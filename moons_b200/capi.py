@@ -216,6 +216,7 @@ def lib() -> C.CDLL:
             "moons_mhd_destroy": (C.c_int, [_P]),
             "moons_mhd_field": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P)]),
             "moons_mhd_init": (C.c_int, [_P]),
+            "moons_mhd_set_unet": (C.c_int, [_P, C.c_int, _P]),
             "moons_mhd_step": (C.c_int, [_P, C.c_int, C.POINTER(StepInfo)]),
             "moons_mhd_divergence": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             "moons_kernel_launches": (C.c_longlong, []),
@@ -437,6 +438,14 @@ class MHD:
 
     def init(self):
         _check(lib().moons_mhd_init(self.h))
+
+    def set_unet(self, which: int, net: "UNet"):
+        """Network of the learned + mixed pressure (0) or B-form cleaning
+        potential (1) solve (prec_poisson = PREC_UNET_MG); kept alive here."""
+        _check(lib().moons_mhd_set_unet(self.h, int(which), net.h))
+        if not hasattr(self, "nets"):
+            self.nets = {}
+        self.nets[which] = net
 
     def step(self, n: int = 1) -> dict:
         info = StepInfo()

@@ -281,16 +281,26 @@ def full_bc(N: int = 80, N_w: int = 9, vacuum: bool = True, Re: float = 2000.0, 
     return m.mom, m.ind, prm, init
 
 
-def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, **kw):
+def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, unets=None, meshes=None, **kw):
     """Create meshes + the MHD object on ``backend`` (moons_b200.capi or the
     oracle module) from a builder, upload the seeded initial state and init.
     ``prec_poisson`` selects the pressure/potential preconditioner (0: the
-    reference's Jacobi prec_Lap; capi.PREC_MG / PREC_MG_MIXED: multigrid)."""
+    reference's Jacobi prec_Lap; capi.PREC_MG / PREC_MG_MIXED: multigrid;
+    PREC_FD: the direct solve; PREC_UNET_MG: learned + mixed, with
+    ``unets`` = (pressure net, potential net) built on ``meshes`` = (fluid
+    mesh, induction mesh), which the simulation then uses)."""
     mom, ind, prm, init = builder(*args, **kw)
     prm.prec_poisson = prec_poisson
-    mm = backend.Mesh(*mom)
-    mi = mm if ind is mom else backend.Mesh(*ind)
+    if meshes is not None:
+        mm, mi = meshes
+    else:
+        mm = backend.Mesh(*mom)
+        mi = mm if ind is mom else backend.Mesh(*ind)
     sim = backend.MHD(mm, mi, prm)
+    if unets is not None:
+        for which, net in enumerate(unets):
+            if net is not None:
+                sim.set_unet(which, net)
     init(sim, np.random.default_rng(seed))
     sim.init()
     return sim

@@ -194,16 +194,17 @@ __device__ __forceinline__ T diag_A(const MGLev<T>& L, int i, int j, int k) {
   return dg;
 }
 
+// ---- V-cycle steps as grid-stride point loops (thread t0 of nt) ----------
+
 // one red-black half sweep of colour `color` (points with (i+j+k)&1 == color).
 // first != 0: e starts at zero (both colours are written).
 template <typename T>
-__global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int first, T omega, const PcgScalars* S) {
-  pdl_enter();
-  if (S && S->done) return;
+__device__ __forceinline__ void mg_smooth_pts(const MGLev<T>& L, int color, int first, T omega, unsigned t0,
+                                              unsigned nt) {
   const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
   const int nxh = (nx + 1) / 2;
   const unsigned n = (unsigned)nxh * (unsigned)ny * (unsigned)nz;
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (unsigned t = t0; t < n; t += nt) {
     const unsigned q = t / (unsigned)nxh;
     const int ih = (int)(t - q * (unsigned)nxh);
     const unsigned kk = q / (unsigned)ny;
@@ -229,12 +230,10 @@ __global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int fi
 
 // t = r - A e at interior points
 template <typename T>
-__global__ void __launch_bounds__(256) k_mg_resid(MGLev<T> L, const PcgScalars* S) {
-  pdl_enter();
-  if (S && S->done) return;
+__device__ __forceinline__ void mg_resid_pts(const MGLev<T>& L, unsigned t0, unsigned nt) {
   const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
   const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (unsigned t = t0; t < n; t += nt) {
     const unsigned q = t / (unsigned)nx;
     const int i = (int)(t - q * (unsigned)nx) + 2;
     const unsigned kk = q / (unsigned)ny;
@@ -248,13 +247,11 @@ __global__ void __launch_bounds__(256) k_mg_resid(MGLev<T> L, const PcgScalars* 
 
 // coarse r = R (fine t), R the transpose of the prolongation
 template <typename T>
-__global__ void __launch_bounds__(256) k_mg_restrict(MGLev<T> F, MGLev<T> C, MGRest<T> Rx, MGRest<T> Ry,
-                                                     MGRest<T> Rz, const PcgScalars* S) {
-  pdl_enter();
-  if (S && S->done) return;
+__device__ __forceinline__ void mg_restrict_pts(const MGLev<T>& F, const MGLev<T>& C, const MGRest<T>& Rx,
+                                                const MGRest<T>& Ry, const MGRest<T>& Rz, unsigned t0, unsigned nt) {
   const int nx = C.s0 - 2, ny = C.s1 - 2, nz = C.s2 - 2;
   const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (unsigned t = t0; t < n; t += nt) {
     const unsigned q = t / (unsigned)nx;
     const int I = (int)(t - q * (unsigned)nx) + 2;
     const unsigned kk = q / (unsigned)ny;
@@ -277,13 +274,11 @@ __global__ void __launch_bounds__(256) k_mg_restrict(MGLev<T> F, MGLev<T> C, MGR
 
 // fine e += P (coarse e)
 template <typename T>
-__global__ void __launch_bounds__(256) k_mg_prolong(MGLev<T> F, MGLev<T> C, MGProl<T> Px, MGProl<T> Py,
-                                                    MGProl<T> Pz, const PcgScalars* S) {
-  pdl_enter();
-  if (S && S->done) return;
+__device__ __forceinline__ void mg_prolong_pts(const MGLev<T>& F, const MGLev<T>& C, const MGProl<T>& Px,
+                                               const MGProl<T>& Py, const MGProl<T>& Pz, unsigned t0, unsigned nt) {
   const int nx = F.s0 - 2, ny = F.s1 - 2, nz = F.s2 - 2;
   const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (unsigned t = t0; t < n; t += nt) {
     const unsigned q = t / (unsigned)nx;
     const int i = (int)(t - q * (unsigned)nx) + 2;
     const unsigned kk = q / (unsigned)ny;
@@ -301,6 +296,68 @@ __global__ void __launch_bounds__(256) k_mg_prolong(MGLev<T> F, MGLev<T> C, MGPr
     const size_t id = lidx(F, i, j, k);
     F.e[id] = F.e[id] + acc;
   }
+}
+
+// coarsest level solved directly: e = Minv r over the n interior cells
+// (Minv: the inverse of the level's operator, regularised on the constant
+// mode when no face is Dirichlet; built on the host, row-major).  Each block
+// gathers r into shared memory (rs, n entries) in the inverse's order; warp
+// w0, w0 + nw, ... forms one row's dot product each.  Minv and the sum are
+// FP64 on every level type: a stretched, high-contrast coarsest operator can
+// have a condition number at which an FP32 inverse is no solve at all.
+constexpr int kDirectMax = 1024;        // largest coarsest level solved by the dense inverse
+constexpr int kDirectRowsPerBlock = 8;  // one warp per row of the inverse
+template <typename T>
+__device__ __forceinline__ void mg_direct_rows(const MGLev<T>& L, const double* Minv, int n, double* rs, int w0,
+                                               int nw) {
+  const int nx = L.s0 - 2, ny = L.s1 - 2;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    const int i = c % nx + 2, q = c / nx, j = q % ny + 2, k = q / ny + 2;
+    rs[c] = (double)L.r[lidx(L, i, j, k)];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int row = w0; row < n; row += nw) {
+    const double* mr = Minv + (size_t)row * n;
+    double acc = 0.0;
+    for (int c = lane; c < n; c += 32) acc += mr[c] * rs[c];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      const int i = row % nx + 2, q = row / nx, j = q % ny + 2, k = q / ny + 2;
+      L.e[lidx(L, i, j, k)] = (T)acc;
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_smooth(MGLev<T> L, int color, int first, T omega, const PcgScalars* S) {
+  pdl_enter();
+  if (S && S->done) return;
+  mg_smooth_pts(L, color, first, omega, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_resid(MGLev<T> L, const PcgScalars* S) {
+  pdl_enter();
+  if (S && S->done) return;
+  mg_resid_pts(L, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_restrict(MGLev<T> F, MGLev<T> C, MGRest<T> Rx, MGRest<T> Ry,
+                                                     MGRest<T> Rz, const PcgScalars* S) {
+  pdl_enter();
+  if (S && S->done) return;
+  mg_restrict_pts(F, C, Rx, Ry, Rz, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_prolong(MGLev<T> F, MGLev<T> C, MGProl<T> Px, MGProl<T> Py,
+                                                    MGProl<T> Pz, const PcgScalars* S) {
+  pdl_enter();
+  if (S && S->done) return;
+  mg_prolong_pts(F, C, Px, Py, Pz, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // coarsest level: e = 0, then `sweeps` forward red-black sweeps and as many
@@ -331,39 +388,12 @@ __global__ void __launch_bounds__(256) k_mg_coarse(MGLev<T> L, int sweeps, const
   }
 }
 
-// coarsest level solved directly: e = Minv r over the n interior cells
-// (Minv: the inverse of the level's operator, regularised on the constant
-// mode when no face is Dirichlet; built on the host, row-major).  One warp
-// forms one row's dot product from the block's gathered copy of r.  Minv and
-// the sum are
-// FP64 on every level type: a stretched, high-contrast coarsest operator can
-// have a condition number at which an FP32 inverse is no solve at all.
-constexpr int kDirectMax = 1024;        // largest coarsest level solved by the dense inverse
-constexpr int kDirectRowsPerBlock = 8;  // one warp per row of the inverse
 template <typename T>
 __global__ void __launch_bounds__(256) k_mg_direct(MGLev<T> L, const double* Minv, int n, const PcgScalars* S) {
   pdl_enter();
   if (S && S->done) return;
   __shared__ double rs[kDirectMax];
-  const int nx = L.s0 - 2, ny = L.s1 - 2;
-  // the level's right-hand side, gathered once per block in the inverse's order
-  for (int c = threadIdx.x; c < n; c += blockDim.x) {
-    const int i = c % nx + 2, q = c / nx, j = q % ny + 2, k = q / ny + 2;
-    rs[c] = (double)L.r[lidx(L, i, j, k)];
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int row = blockIdx.x * kDirectRowsPerBlock + (threadIdx.x >> 5);
-  if (row >= n) return;
-  const double* mr = Minv + (size_t)row * n;  // row-major
-  double acc = 0.0;
-  for (int c = lane; c < n; c += 32) acc += mr[c] * rs[c];
-#pragma unroll
-  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) {
-    const int i = row % nx + 2, q = row / nx, j = q % ny + 2, k = q / ny + 2;
-    L.e[lidx(L, i, j, k)] = (T)acc;
-  }
+  mg_direct_rows(L, Minv, n, rs, blockIdx.x * kDirectRowsPerBlock + (threadIdx.x >> 5), n);
 }
 
 // ---- the learned + mixed (two-stage) preconditioner's scaling -------------

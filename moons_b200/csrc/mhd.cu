@@ -113,6 +113,7 @@ struct moons_mhd {
   moons_sf *U[3], *Ustar[3], *Unm1[3], *F[3], *Fnm1[3], *L[3], *tF1[3], *tF2[3], *tF3[3], *tCC, *p, *UCC[3], *divU;
   moons_sf* UE[3][3];
   moons_pcg *pcgU = nullptr, *pcgP = nullptr;
+  moons_unet* unet[2] = {nullptr, nullptr};  // networks of the learned + mixed pressure / potential solves
   // induction
   moons_sf *B[3], *Bstar[3], *Bnm1[3], *B0[3], *Btot[3], *Fi[3], *Fnm1i[3], *Li[3], *J[3], *jxb[3], *sig[3], *phi,
       *tCCi, *tFi1[3], *tFi2[3], *tE[3], *curlUxB[3], *divB, *Ui[3], *E[3];
@@ -774,15 +775,21 @@ int moons_mhd_init(moons_mhd* s) {
     if ((r = moons_pcg_create(m, MOONS_OP_MOM_DIFFUSION, MOONS_PREC_MOM, 3, s->Ustar, xbu, nullptr, &s->pcgU))) return r;
     moons_sf* xp[1] = {s->p};
     const int pq = s->P.prec_poisson;
-    const int pp = pq == MOONS_PREC_MG || pq == MOONS_PREC_MG_MIXED || pq == MOONS_PREC_FD ? pq : MOONS_PREC_LAP;
-    // the sigma-weighted potential solve is not separable: multigrid under FD
-    const int pv = pp == MOONS_PREC_FD ? MOONS_PREC_MG_MIXED : pp;
+    const int pp = pq == MOONS_PREC_MG || pq == MOONS_PREC_MG_MIXED || pq == MOONS_PREC_FD ||
+                           pq == MOONS_PREC_UNET_MG
+                       ? pq
+                       : MOONS_PREC_LAP;
+    // the sigma-weighted potential solve is not separable (multigrid under
+    // FD), and the networks are trained for the constant-coefficient solves
+    const int pv = pp == MOONS_PREC_FD || pp == MOONS_PREC_UNET_MG ? MOONS_PREC_MG_MIXED : pp;
     if ((r = moons_pcg_create(m, MOONS_OP_LAP_UNIFORM, pp, 1, xp, xp, nullptr, &s->pcgP))) return r;
+    if (pp == MOONS_PREC_UNET_MG && s->unet[0] && (r = moons_pcg_set_unet(s->pcgP, s->unet[0]))) return r;
     if (s->P.induction == MOONS_IND_B) {
       if ((r = moons_pcg_create(s->mi, MOONS_OP_IND_DIFFUSION, MOONS_PREC_IND, 3, s->Bstar, s->B, s->sig, &s->pcgB)))
         return r;
       moons_sf* xf[1] = {s->phi};
       if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_UNIFORM, pp, 1, xf, xf, nullptr, &s->pcgPhi))) return r;
+      if (pp == MOONS_PREC_UNET_MG && s->unet[1] && (r = moons_pcg_set_unet(s->pcgPhi, s->unet[1]))) return r;
     } else if (s->P.induction == MOONS_IND_POTENTIAL) {
       moons_sf* xf[1] = {s->phi};
       if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_PROPS, pv, 1, xf, xf, s->sig, &s->pcgPhi))) return r;
@@ -880,6 +887,25 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
     info->res_phi = s->res_phi;
     info->ms = ms;
   }
+  return MOONS_OK;
+}
+
+int moons_mhd_set_unet(moons_mhd* s, int which, moons_unet* u) {
+  if (!s || !u || which < 0 || which > 1) {
+    set_error("moons_mhd_set_unet: bad argument");
+    return MOONS_ERR_ARG;
+  }
+  if (s->P.prec_poisson != MOONS_PREC_UNET_MG) {
+    set_error("moons_mhd_set_unet: prec_poisson is not MOONS_PREC_UNET_MG");
+    return MOONS_ERR_STATE;
+  }
+  if (unet_mesh(u) != (which == 0 ? s->mm : s->mi)) {
+    set_error("moons_mhd_set_unet: the network lives on another mesh");
+    return MOONS_ERR_SHAPE;
+  }
+  s->unet[which] = u;
+  moons_pcg* p = which == 0 ? s->pcgP : s->pcgPhi;
+  if (p && !(which == 1 && s->P.induction != MOONS_IND_B)) return moons_pcg_set_unet(p, u);
   return MOONS_OK;
 }
 

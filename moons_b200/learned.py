@@ -97,6 +97,44 @@ class ShellCase:
 
 
 @dataclass
+class UniformCase:
+    """One draw of a constant-coefficient Poisson problem (the pressure or
+    B-form cleaning-potential operator, LAP_UNIFORM) on a given mesh with
+    given BCs: the right-hand side is the divergence of i.i.d. N(0,1) face
+    values (seeded).  Same surface as ShellCase (k is empty: the network's
+    coefficient feature stays 0, the value of a unit coefficient)."""
+    mesh: G.Mesh
+    bcs: object
+    seed: int
+    k: List[G.Field] = field(default_factory=list)
+    rhs: G.Field = None
+    phi: G.Field = None
+    op: G.PCG = None
+
+    @classmethod
+    def build(cls, mesh: G.Mesh, bcs, seed: int) -> "UniformCase":
+        rng = np.random.default_rng(seed)
+        c = cls(mesh, bcs, seed)
+        es = []
+        for dl in (G.FX, G.FY, G.FZ):
+            f = mesh.field(dl)
+            f.upload(rng.standard_normal(f.shape))
+            es.append(f)
+        c.rhs = mesh.field(G.CC)
+        G.div(c.rhs, *es)
+        c.phi = mesh.field(G.CC)
+        c.phi.set_bcs(bcs)
+        c.op = c.solver(G.PREC_MG_MIXED)
+        return c
+
+    def solver(self, prec: int) -> G.PCG:
+        return G.PCG(self.mesh, G.OP_LAP_UNIFORM, prec, [self.phi], [self.phi])
+
+    release = ShellCase.release
+    operator = ShellCase.operator
+
+
+@dataclass
 class Pair:
     r: G.Field
     e: G.Field
@@ -267,7 +305,8 @@ def train(net: G.UNet, cases: Sequence[ShellCase], pairs: Sequence[Pair], epochs
             if p.case != cur_case:
                 if blocked and cur_case >= 0:
                     cases[cur_case].release(rhs=False)
-                net.set_coeff(cases[p.case].k)
+                if cases[p.case].k:
+                    net.set_coeff(cases[p.case].k)
                 if loss == 2:
                     net.set_operator(cases[p.case].operator())
                 cur_case = p.case
@@ -327,6 +366,35 @@ def train_two_stage(n: int = 128, shell: int = 4, draws: int = 250, epochs: int 
             "loss_first_last": [hist[0], hist[-1]], "data_seconds": t1 - t0, "train_seconds": t2 - t1,
             "out_scale": net.out_scale}
     return net, mesh, meta
+
+
+def train_two_stage_uniform(mesh: G.Mesh, bcs, draws: int = 25, epochs: int = 8, lr: float = 1e-3,
+                            lr_min: float = 5e-5, seed: int = 0, seed0: int = 0, log=None):
+    """The learned + mixed network of constant-coefficient solves (pressure
+    and cleaning potential) on `mesh`: `draws` seeded right-hand sides (seeds
+    seed0 ..), draw i with the BCs bcs[i % len(bcs)] (one BC set or a list),
+    8 two-stage pairs each, Adam with the energy-norm cosine loss in blocked
+    order.  Returns (net, summary)."""
+    import time
+    bl = list(bcs) if isinstance(bcs, (list, tuple)) else [bcs]
+    t0 = time.perf_counter()
+    cases, pairs = [], []
+    for i in range(draws):
+        c = UniformCase.build(mesh, bl[i % len(bl)], seed0 + i)
+        ps = make_pairs_two_stage([c], release=True)
+        for p in ps:
+            p.case = i
+        cases.append(c)
+        pairs += ps
+    t1 = time.perf_counter()
+    net = G.UNet(mesh, seed=seed)
+    net.out_scale = output_scale(pairs)
+    hist = train(net, cases, pairs, epochs=epochs, lr=lr, lr_min=lr_min, seed=seed, blocked=True, log=log)
+    t2 = time.perf_counter()
+    meta = {"draws": draws, "pairs": len(pairs), "epochs": epochs, "adam_steps": epochs * len(pairs),
+            "loss": "energy-norm cosine (kind 2)", "loss_first_last": [hist[0], hist[-1]],
+            "data_seconds": t1 - t0, "train_seconds": t2 - t1, "out_scale": net.out_scale}
+    return net, meta
 
 
 if __name__ == "__main__":

@@ -116,6 +116,32 @@ def test_apply_prec_is_one_vcycle():
     assert np.abs(x1 - a * v).max() <= 1e-12 * np.abs(x1).max()
 
 
+def test_mhd_step_learned_mixed_with_zero_networks_is_the_mixed_step():
+    """prec_poisson = MOONS_PREC_UNET_MG with N = 0 under the pressure and
+    cleaning-potential solves of the finite-Rem duct (no wall layer: one
+    mesh) steps exactly like MOONS_PREC_MG_MIXED; without a network the
+    step refuses to run."""
+    from moons_b200 import configs
+    kw = dict(nx=8, ny=8, nz=16)
+    mom, _, _, _ = configs.at_scale(**kw)
+    mm = G.Mesh(*mom)
+    zero = G.UNet(mm, seed=1)
+    zero.set_params(np.zeros(zero.nparams, dtype=np.float32))
+    a = configs.make(G, configs.at_scale, seed=0, prec_poisson=G.PREC_UNET_MG, meshes=(mm, mm), unets=(zero, zero),
+                     **kw)
+    b = configs.make(G, configs.at_scale, seed=0, prec_poisson=G.PREC_MG_MIXED, **kw)
+    ia, ib = a.step(3), b.step(3)
+    for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+        assert ia[k] == ib[k], (k, ia, ib)
+    for which in (G.MHD_U, G.MHD_B, G.MHD_P):
+        for c in range(1 if which == G.MHD_P else 3):
+            assert np.array_equal(a.download(which, c), b.download(which, c)), (which, c)
+    mm2 = G.Mesh(*mom)
+    c = configs.make(G, configs.at_scale, seed=0, prec_poisson=G.PREC_UNET_MG, meshes=(mm2, mm2), **kw)
+    with pytest.raises(G.MoonsError):
+        c.step(1)
+
+
 def test_unet_solver_needs_a_network():
     mesh = L.shell_mesh(16)
     case = L.ShellCase.build(mesh, 16, SHELL, 0)
