@@ -405,8 +405,19 @@ if __name__ == "__main__":
     ap.add_argument("--shell", type=int, default=4)
     ap.add_argument("--draws", type=int, default=250)
     ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--case", choices=["shell", "at_scale"], default="shell",
+                    help="shell: the sigma-shell case (--n, --shell); at_scale: the pressure and cleaning-potential "
+                         "solves of the 128 x 128 x 256 finite-Rem duct (its pressure and potential BCs alternate)")
     ap.add_argument("--out", required=True)
     a = ap.parse_args()
-    net_, _, meta_ = train_two_stage(a.n, a.shell, a.draws, a.epochs, log=lambda s: print(s, flush=True))
+    log_ = lambda s: print(s, flush=True)
+    if a.case == "shell":
+        net_, _, meta_ = train_two_stage(a.n, a.shell, a.draws, a.epochs, log=log_)
+    else:
+        mom_, _, prm_, _ = configs.at_scale()
+        mesh_ = G.Mesh(*mom_)
+        net_, meta_ = train_two_stage_uniform(mesh_, [prm_.bc_p, prm_.bc_phi], draws=a.draws, epochs=a.epochs,
+                                              log=log_)
+        meta_["case"] = "at_scale 128x128x256, pressure and cleaning-potential BCs"
     save(net_, a.out, meta_)
     print(meta_, flush=True)
