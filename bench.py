@@ -729,8 +729,9 @@ def main():
             "at_scale": scale5,
             "full_bc_vacuum": fullbc,
             "config1_ldc32": ldc,
-            "roofline": {"bound": "hbm", "kernel": "pressure Jacobi-PCG iteration (k_l_lap + k_l_update + k_l_pupd "
-                                                  "+ k_l_bcfill) on configuration 5's mesh, 128x128x256 cells",
+            "roofline": {"bound": "hbm", "kernel": "pressure Jacobi-PCG iteration (the fused cell-centred pair "
+                                                  "k_cc_lap + k_l_update) on configuration 5's mesh, 128x128x256 "
+                                                  "cells",
                          "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                          "alg_bytes_per_launch": 88.0 * ncc_r, "cells": ncc_r,
