@@ -48,6 +48,10 @@ def parse():
                          "forward applies / training steps on the 128^3 sigma-shell grid; prints what ran, no "
                          "bench line")
     ap.add_argument("--profile-iters", type=int, default=40)
+    ap.add_argument("--leg", choices=["at_scale"], default=None,
+                    help="run one leg alone and print its JSON (no bench line): at_scale = configuration 5 with "
+                         "--leg-steps steps per variant")
+    ap.add_argument("--leg-steps", type=int, default=200)
     ap.add_argument("--profile-mesh", choices=["duct", "at_scale", "shell"], default="duct",
                     help="mesh of the --profile Poisson solve: the duct fluid mesh (64x64x256), the "
                          "configuration-5 mesh (128x128x256, working set above the L2) or the 128^3 "
@@ -456,7 +460,8 @@ def at_scale_steps(G, small=False, steps=3, weights=WEIGHTS_AT_SCALE):
     out["workload"] = (f"finite-Rem MHD with constrained transport, {n[0]}x{n[1]}x{n[2]} cells as (x, y, z): x and y "
                        f"the Roberts-stretched cross-section, z the uniform streamwise axis (the case's 256 x 128 x 128 "
                        f"lists the streamwise axis first), Re=1000, Ha=500, Rem=10, dt=2e-4; {steps} steps after 1 "
-                       f"warm-up step (the case's 200 steps shortened to keep the bench within minutes)")
+                       f"warm-up step" + ("" if steps >= 200 else " (the case's 200 steps shortened to keep the bench "
+                                                                  "within minutes; bench.py --leg at_scale runs 200)"))
     return out
 
 
@@ -585,6 +590,11 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.leg == "at_scale":
+        from moons_b200 import capi as G
+        print(json.dumps({"leg": "at_scale", "result": at_scale_steps(G, small=args.small, steps=args.leg_steps)}),
+              flush=True)
         return
     rank, world, local, dist = dist_setup(args.gpus)
     import torch

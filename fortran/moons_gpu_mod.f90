@@ -215,6 +215,13 @@ module moons_gpu_mod
       integer(c_int) :: st
     end function
 
+    function moons_mhd_set_unet(s, which, u) bind(C, name="moons_mhd_set_unet") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s, u
+      integer(c_int), value :: which
+      integer(c_int) :: st
+    end function
+
     function moons_pcg_apply_prec(s, z, r) bind(C, name="moons_pcg_apply_prec") result(st)
       import :: c_ptr, c_int
       type(c_ptr), value :: s

@@ -204,27 +204,48 @@ __device__ __forceinline__ void mg_smooth_pts(const MGLev<T>& L, int color, int 
   const int nx = L.s0 - 2, ny = L.s1 - 2, nz = L.s2 - 2;
   const int nxh = (nx + 1) / 2;
   const unsigned n = (unsigned)nxh * (unsigned)ny * (unsigned)nz;
-  for (unsigned t = t0; t < n; t += nt) {
+  // point t of this colour: (i, j, k), false past the row's end
+  auto point = [&](unsigned t, int& i, int& j, int& k) -> bool {
     const unsigned q = t / (unsigned)nxh;
     const int ih = (int)(t - q * (unsigned)nxh);
     const unsigned kk = q / (unsigned)ny;
-    const int j = (int)(q - kk * (unsigned)ny) + 2, k = (int)kk + 2;
-    const int i0 = 2 + ((color + j + k) & 1);
-    const int i = i0 + 2 * ih;
-    if (first) {  // the other colour of this pair starts at zero
-      const int io = 2 + ((color + 1 + j + k) & 1) + 2 * ih;
+    j = (int)(q - kk * (unsigned)ny) + 2;
+    k = (int)kk + 2;
+    i = 2 + ((color + j + k) & 1) + 2 * ih;
+    return i <= L.s0 - 1;
+  };
+  if (first) {
+    for (unsigned t = t0; t < n; t += nt) {
+      int i, j, k;
+      const bool in = point(t, i, j, k);
+      // the other colour of this pair starts at zero
+      const int io = 2 + ((color + 1 + j + k) & 1) + (i - 2 - ((color + j + k) & 1));
       if (io <= L.s0 - 1) L.e[lidx(L, io, j, k)] = T(0);
-    }
-    if (i > L.s0 - 1) continue;
-    const size_t id = lidx(L, i, j, k);
-    if (first) {
       // e = 0 everywhere before this sweep, so A e = 0 and e = r / D
-      L.e[id] = omega * L.r[id] / diag_A<T>(L, i, j, k);
-    } else {
-      T D;
-      const T Ae = apply_A<T>(L, L.e, i, j, k, D);
-      L.e[id] = L.e[id] + omega * (L.r[id] - Ae) / D;
+      if (in) L.e[lidx(L, i, j, k)] = omega * L.r[lidx(L, i, j, k)] / diag_A<T>(L, i, j, k);
     }
+    return;
+  }
+  // two points of the colour per trip (t and t + nt): the points of one
+  // colour are independent, and both points' loads are in flight together
+  for (unsigned t = t0; t < n; t += 2 * nt) {
+    int ia, ja, ka, ib = 2, jb = 2, kb = 2;
+    const bool a = point(t, ia, ja, ka);
+    const bool b = t + nt < n && point(t + nt, ib, jb, kb);
+    T Da = T(1), Db = T(1), Aea = T(0), Aeb = T(0), ra = T(0), rb = T(0), ea = T(0), eb = T(0);
+    const size_t ida = lidx(L, ia, ja, ka), idb = lidx(L, ib, jb, kb);
+    if (a) {
+      Aea = apply_A<T>(L, L.e, ia, ja, ka, Da);
+      ra = L.r[ida];
+      ea = L.e[ida];
+    }
+    if (b) {
+      Aeb = apply_A<T>(L, L.e, ib, jb, kb, Db);
+      rb = L.r[idb];
+      eb = L.e[idb];
+    }
+    if (a) L.e[ida] = ea + omega * (ra - Aea) / Da;
+    if (b) L.e[idb] = eb + omega * (rb - Aeb) / Db;
   }
 }
 

@@ -403,6 +403,46 @@ unsigned resident_grid(const moons_pcg* s, const void* kern, size_t items) {
 // kernels, twice: p -> p2 -> p (K3 reads one buffer and writes the other)
 int enqueue_mg_iteration(moons_pcg* s, DF* x);
 
+// the cell-centred operator step k_cc_lap on the direction of this half
+// (p for half 0, p2 for half 1): Ap, p.Ap and alpha; with the fused
+// iteration (L.fz) also p' = beta p + z into pn and x += alpha_prev p
+int enqueue_cc_lap(moons_pcg* s, int half, DF* pc, DF* pn, DF* x, const FBC& b0, unsigned* tA) {
+  moons_mesh* m = s->m;
+  const LeanGrids& L = s->lg;
+  DF z0{};
+  const bool ev = (s->Ax[0].s0 & 1) == 0;
+  const CUtensorMap& tm = L.tmap[half];
+  const CUtensorMap& tz = L.tmap[2];
+  const size_t sm = cc_smem(L.klen, L.fz);
+#define MG_CC_LAP(MD, EV, T, F, KX, KY, KZ, CF)                                                            \
+  MG_LAUNCH_PDL_SMEM((k_cc_lap<MD, EV, T, F>), L.gF, kCThreads, sm, m->stream, tm, tz, s->Ax[0], pc[0], s->z[0], \
+                     pn[0], x[0], m->dg, b0, KX, KY, KZ, CF, L.klen, s->S, s->partial, tA)
+#define MG_CC_LAP_F(MD, KX, KY, KZ, CF)                                            \
+  if (L.fz) {                                                                      \
+    if (L.tm) MG_CC_LAP(MD, true, true, true, KX, KY, KZ, CF);                     \
+    else if (ev) MG_CC_LAP(MD, true, false, true, KX, KY, KZ, CF);                 \
+    else MG_CC_LAP(MD, false, false, true, KX, KY, KZ, CF);                        \
+  } else {                                                                         \
+    if (L.tm) MG_CC_LAP(MD, true, true, false, KX, KY, KZ, CF);                    \
+    else if (ev) MG_CC_LAP(MD, true, false, false, KX, KY, KZ, CF);                \
+    else MG_CC_LAP(MD, false, false, false, KX, KY, KZ, CF);                       \
+  }
+  switch (s->op) {
+    case MOONS_OP_LAP_UNIFORM:
+      MG_CC_LAP_F(0, z0, z0, z0, 0.0);
+      break;
+    case MOONS_OP_LAP_PROPS:
+      MG_CC_LAP_F(1, s->k[0], s->k[1], s->k[2], 0.0);
+      break;
+    default:
+      MG_CC_LAP_F(3, s->k[0], s->k[1], s->k[2], s->coeff);
+      break;
+  }
+#undef MG_CC_LAP_F
+#undef MG_CC_LAP
+  return MOONS_OK;
+}
+
 int enqueue_iteration(moons_pcg* s, DF* x) {
   if (s->mgh) return enqueue_mg_iteration(s, x);
   moons_mesh* m = s->m;
@@ -420,36 +460,8 @@ int enqueue_iteration(moons_pcg* s, DF* x) {
     DF* pc = half == 0 ? s->p : s->p2;
     DF* pn = half == 0 ? s->p2 : s->p;
     if (L.cc) {
-      const bool ev = (s->Ax[0].s0 & 1) == 0;
-      const CUtensorMap& tm = L.tmap[half];
-      const CUtensorMap& tz = L.tmap[2];
-      const size_t sm = cc_smem(L.klen, L.fz);
-#define MG_CC_LAP(MD, EV, T, F, KX, KY, KZ, CF)                                                            \
-  MG_LAUNCH_PDL_SMEM((k_cc_lap<MD, EV, T, F>), L.gF, kCThreads, sm, m->stream, tm, tz, s->Ax[0], pc[0], s->z[0], \
-                     pn[0], x[0], m->dg, b[0], KX, KY, KZ, CF, L.klen, s->S, s->partial, tA)
-#define MG_CC_LAP_F(MD, KX, KY, KZ, CF)                                            \
-  if (L.fz) {                                                                      \
-    if (L.tm) MG_CC_LAP(MD, true, true, true, KX, KY, KZ, CF);                     \
-    else if (ev) MG_CC_LAP(MD, true, false, true, KX, KY, KZ, CF);                 \
-    else MG_CC_LAP(MD, false, false, true, KX, KY, KZ, CF);                        \
-  } else {                                                                         \
-    if (L.tm) MG_CC_LAP(MD, true, true, false, KX, KY, KZ, CF);                    \
-    else if (ev) MG_CC_LAP(MD, true, false, false, KX, KY, KZ, CF);                \
-    else MG_CC_LAP(MD, false, false, false, KX, KY, KZ, CF);                       \
-  }
-      switch (s->op) {
-        case MOONS_OP_LAP_UNIFORM:
-          MG_CC_LAP_F(0, z0, z0, z0, 0.0);
-          break;
-        case MOONS_OP_LAP_PROPS:
-          MG_CC_LAP_F(1, s->k[0], s->k[1], s->k[2], 0.0);
-          break;
-        default:
-          MG_CC_LAP_F(3, s->k[0], s->k[1], s->k[2], s->coeff);
-          break;
-      }
-#undef MG_CC_LAP_F
-#undef MG_CC_LAP
+      int r = enqueue_cc_lap(s, half, pc, pn, x, b[0], tA);
+      if (r) return r;
     } else switch (s->op) {
       case MOONS_OP_LAP_UNIFORM:
         MG_LAUNCH_PDL(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, nc), fc(pc, nc), m->dg, b[0], b[1], b[2], z0, z0, z0,
@@ -543,18 +555,24 @@ int enqueue_mg_iteration(moons_pcg* s, DF* x) {
   for (int half = 0; half < 2; half++) {
     DF* pc = half == 0 ? s->p : s->p2;
     DF* pn = half == 0 ? s->p2 : s->p;
-    if (s->op == MOONS_OP_LAP_PROPS)
+    if (L.cc) {
+      // shared-memory staged operator with the ghost values formed from the
+      // interior: p needs no BC fill
+      int r = enqueue_cc_lap(s, half, pc, pn, x, b[0], tA);
+      if (r) return r;
+    } else if (s->op == MOONS_OP_LAP_PROPS) {
       MG_LAUNCH_PDL(k_l_lap<1>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], s->k[0], s->k[1],
                 s->k[2], 0.0, s->S, s->partial, tA);
-    else
+    } else {
       MG_LAUNCH_PDL(k_l_lap<0>, L.gA, kLB, m->stream, fc(s->Ax, 1), fc(pc, 1), m->dg, b[0], b[1], b[2], z0, z0, z0, 0.0,
                 s->S, s->partial, tA);
+    }
     MG_LAUNCH_PDL(k_m_update, gF, kLB, m->stream, x[0], pc[0], s->r[0], s->Ax[0], rprev, s->S, s->partial, tB);
     int r = apply_prec_dev(s, &s->S->done, s->S);
     if (r) return r;
     MG_LAUNCH_PDL(k_m_beta, gF, kLB, m->stream, s->z[0], s->r[0], rprev, s->S, s->partial, tA);
     MG_LAUNCH_PDL(k_m_pupd, gF, kLB, m->stream, pn[0], pc[0], s->z[0], s->S);
-    if (L.bc) MG_LAUNCH_PDL(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, 1), b[0], b[1], b[2], L.npbP, s->S);
+    if (L.bc && !L.cc) MG_LAUNCH_PDL(k_l_bcfill, L.gD, kLB, m->stream, fc(pn, 1), b[0], b[1], b[2], L.npbP, s->S);
   }
   MG_CUDA(cudaGetLastError());
   return MOONS_OK;
@@ -1030,7 +1048,7 @@ int mg_pcg_enqueue(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const m
             &s->S->rhok, m->d_partial, m->d_ticket);
   MG_LAUNCH(k_pcg_start, 1, 1, m->stream, s->S);
   // k_cc_lap writes Ap on interior points only: its ghost points stay 0
-  if (s->lg.cc && !s->mgh) MG_CUDA(cudaMemsetAsync(s->Ax[0].f, 0, s->Ax[0].n() * sizeof(double), m->stream));
+  if (s->lg.cc) MG_CUDA(cudaMemsetAsync(s->Ax[0].f, 0, s->Ax[0].n() * sizeof(double), m->stream));
   MG_CUDA(cudaGetLastError());
   // ---- the loop.  MOONS_PCG_HOSTLOOP=1 launches the iteration as separate
   // kernels from the host in chunks of 32 iterations (kernels skip
