@@ -604,7 +604,7 @@ void plan_lean(moons_pcg* s) {
                    : s->op == MOONS_OP_MOM_DIFFUSION ? (const void*)k_l_lap<2>
                    : s->op == MOONS_OP_NRG_DIFFUSION ? (const void*)k_l_lap<3>
                                                     : (const void*)k_l_curl_ap;
-  L.gA = lean_grid(s, ka, s->Ax, nc, kKC);
+  L.gA = lean_grid(s, ka, s->Ax, nc, s->op == MOONS_OP_IND_DIFFUSION ? kKCc : kKC);
   L.mm = (s->prec == MOONS_PREC_LAP) ? 1 : (s->prec == MOONS_PREC_MOM ? 2 : 0);
   // grids sized with the variant that runs (its occupancy sets the wave)
   const void* kB = L.mm == 1 ? (const void*)k_l_update<kKCU, 1>
@@ -644,7 +644,7 @@ void plan_lean(moons_pcg* s) {
     }
   }
   L.gE = dim3(1, 1, 1);
-  if (s->op == MOONS_OP_IND_DIFFUSION) L.gE = lean_grid(s, (const void*)k_l_curl_sig, s->tempk, 3, kKC);
+  if (s->op == MOONS_OP_IND_DIFFUSION) L.gE = lean_grid(s, (const void*)k_l_curl_sig, s->tempk, 3, kKCc);
   // BC fill: perimeter blocks over every plane, then inner blocks (ghost planes)
   unsigned npbP = 0, npbI = 0, smax = 0;
   L.bc = false;
