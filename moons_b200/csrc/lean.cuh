@@ -444,13 +444,15 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
   const size_t sz = (size_t)x.s0 * x.s1;
   const int nkc = (x.s2 + KC - 1) / KC;
   const MinvCol mc = minv_col<MM>(g, x.dl, i, j);
-  for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+  // a chunk's loads; with SZ (two arrays a point) the next chunk's loads are
+  // issued before this chunk's stores (2 % per over-L2 iteration; the
+  // three-array form would spill)
+  auto load = [&](int kc, double* xv, double* pv, double* rv, double* av, double* mv) {
     const int k0 = kc * KC + 1, k1 = min(k0 + KC - 1, x.s2);
-    const size_t idx0 = x.at(i, j, k0);
-    double xv[KC], pv[KC], rv[KC], av[KC], mv[KC];
+    const size_t idx0 = x.at(i, j, min(k0, x.s2));
 #pragma unroll
     for (int q = 0; q < KC; q++) {
-      const bool in = k0 + q <= k1;
+      const bool in = kc < nkc && k0 + q <= k1;
       const size_t idx = idx0 + (size_t)q * sz;
       xv[q] = (!SZ && in) ? x.f[idx] : 0.0;
       pv[q] = (!SZ && in) ? ld(p.f + idx) : 0.0;
@@ -458,6 +460,15 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
       av[q] = in ? ld(Ap.f + idx) : 0.0;
       mv[q] = (MM == 0 && in) ? ld(M.f + idx) : 0.0;
     }
+  };
+  double xv[KC], pv[KC], rv[KC], av[KC], mv[KC];
+  if constexpr (SZ) load(blockIdx.y, xv, pv, rv, av, mv);
+  for (int kc = blockIdx.y; kc < nkc; kc += gridDim.y) {
+    double nx[KC], np[KC], nr[KC], na[KC], nm[KC];
+    if constexpr (SZ) load(kc + gridDim.y, nx, np, nr, na, nm);
+    else load(kc, xv, pv, rv, av, mv);
+    const int k0 = kc * KC + 1, k1 = min(k0 + KC - 1, x.s2);
+    const size_t idx0 = x.at(i, j, k0);
 #pragma unroll
     for (int q = 0; q < KC; q++) {
       const int k = k0 + q;
@@ -481,6 +492,14 @@ __device__ __forceinline__ void update_col(const DF& x, const DF& p, const DF& r
         const double zv = m * rn;
         arr += rn * rn;
         azr += zv * rn;
+      }
+    }
+    if constexpr (SZ) {
+#pragma unroll
+      for (int q = 0; q < KC; q++) {
+        rv[q] = nr[q];
+        av[q] = na[q];
+        mv[q] = nm[q];
       }
     }
   }
