@@ -229,6 +229,38 @@ def poisson_ms(G, kw, prec=None, builder=None):
     return best, b.n
 
 
+def vcycle_roofline(G, n=128, shell=4, reps=20, peak=None):
+    """One V(2,2) cycle on the 128^3 sigma-shell case (seed 0), FP64 and
+    FP32, applied through moons_pcg_apply_prec (separate launches, the call
+    synchronises its stream): mean time over `reps` calls after 3 warm-up
+    calls, and the algorithmic bytes of a V(nu1, nu2) cycle, (32 (nu1 + nu2)
+    + 58) * 8/7 B per finest cell in FP64 and half that in FP32, over it."""
+    from moons_b200 import learned as L
+    mesh = L.shell_mesh(n)
+    case = L.ShellCase.build(mesh, n, shell, 0)
+    cells = n ** 3
+    out = {}
+    for name, prec, bpc in (("fp64", G.PREC_MG, (32 * 4 + 58) * 8.0 / 7.0),
+                            ("fp32", G.PREC_MG_MIXED, (32 * 4 + 58) * 4.0 / 7.0)):
+        s = case.solver(prec)
+        r, z = mesh.field(G.CC), mesh.field(G.CC)
+        case.phi.fill(0.0)
+        s.residual([case.phi], [case.rhs], [r])
+        for _ in range(3):
+            s.apply_prec([z], [r])
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            s.apply_prec([z], [r])
+        sec = (time.perf_counter() - t0) / reps
+        gbs = bpc * cells / sec / 1e9
+        out[name] = {"us_per_vcycle": sec * 1e6, "alg_bytes_per_cell": bpc, "achieved_gbs": gbs,
+                     "frac": gbs / peak if peak else None}
+        s.close()
+    out["note"] = ("host-timed single V-cycles (launch latency included; inside the CUDA-graph solve the same "
+                   "kernels run under dependent launch); the coarse levels are latency-bound in both precisions")
+    return out
+
+
 def sigma_shell_poisson(G, n=128, shell=4, seeds_plain=4, seeds_mg=64):
     """Mixed-precision Poisson case: div(sigma grad phi) = div(u x B) on a
     128^3 grid with a 10^U(-3,3) wall shell, to 1e-10 relative residual.
@@ -290,6 +322,14 @@ def unet_flops(n):
     layers = [(2, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 128, 3),
               (128, 128, 3), (192, 64, 2), (64, 64, 2), (96, 32, 1), (32, 32, 1), (48, 16, 0), (16, 16, 0)]
     return sum(2 * 27 * ci * co * (n >> lv) ** 3 for ci, co, lv in layers)
+
+
+def bf16_peak() -> float:
+    """Dense bf16 TFLOP/s measured on this pool (burst), else the fallback."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+    except Exception:
+        return 1590.0
 
 
 WEIGHTS_TWO_STAGE = os.path.join(ROOT, "moons_b200", "weights", "unet_two_stage_shell128.npz")
@@ -394,7 +434,8 @@ def learned_mixed_poisson(G, n=128, shell=4, held=tuple(range(1000, 1064)), trai
         "gate_3x_vs_fp64_mg": {"met": base / summ["fcg_v_plus_n"]["ms_mean"] >= 3.0,
                                "measured": base / summ["fcg_v_plus_n"]["ms_mean"]},
         "per_seed": rows[:4],
-        "unet_forward": {"ms_host_synced": fwd_ms, "gflop": fl / 1e9, "tflops": fl / (fwd_ms / 1e3) / 1e12},
+        "unet_forward": {"ms_host_synced": fwd_ms, "gflop": fl / 1e9, "tflops": fl / (fwd_ms / 1e3) / 1e12,
+                         "frac_of_measured_bf16": fl / (fwd_ms / 1e3) / 1e12 / bf16_peak()},
         "note": "fcg_v_plus_n: z = V(r) + gamma N(r - A V(r)) in FP64 flexible CG; exit_reason 11 means the "
                 "learned phase stagnated and the FP32 V-cycle finished the solve (ms include both phases)",
     }
@@ -672,6 +713,11 @@ def main():
     shell = sigma_shell_poisson(G, n=32 if args.small else 128, seeds_plain=1 if args.small else 4,
                                 seeds_mg=2 if args.small else 16)
     mxinfo, _ = poisson_ms(G, kw, G.PREC_MG_MIXED)
+    try:
+        peak_v = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        peak_v = 6650.0
+    vcyc = vcycle_roofline(G, n=32 if args.small else 128, shell=2 if args.small else 4, peak=peak_v)
     fdinfo, _ = poisson_ms(G, kw, G.PREC_FD)
     scale5 = at_scale_steps(G, small=args.small)
     fullbc = full_bc_steps(G, small=args.small)
@@ -735,6 +781,7 @@ def main():
                         "speedup_mixed_vs_plain": pinfo["ms"] / mxinfo["ms"],
                         "speedup_fd_vs_plain": pinfo["ms"] / fdinfo["ms"]},
             "poisson_sigma_shell": shell,
+            "vcycle_roofline_sigma_shell": vcyc,
             "poisson_learned_mixed": learned,
             "at_scale": scale5,
             "full_bc_vacuum": fullbc,
