@@ -388,7 +388,9 @@ int moons_unet_create(moons_mesh* m, unsigned long long seed, moons_unet** out);
  * (net on the fluid mesh), 1 the B-form cleaning potential (net on the
  * induction mesh); before or after moons_mhd_init.  The low-Rem potential
  * (sigma-weighted) takes MOONS_PREC_MG_MIXED under this setting.  A step
- * whose learned solver has no network returns MOONS_ERR_STATE. */
+ * whose learned solver has no network returns MOONS_ERR_STATE.  The
+ * simulation does not own the network: keep it alive while the simulation
+ * steps (one network may serve both solves when the meshes coincide). */
 int moons_mhd_set_unet(moons_mhd* s, int which, moons_unet* u);
 int moons_unet_destroy(moons_unet* u);
 int moons_unet_nparams(const moons_unet* u, long long* n);
