@@ -142,6 +142,25 @@ def test_mhd_step_learned_mixed_with_zero_networks_is_the_mixed_step():
         c.step(1)
 
 
+def test_mhd_set_unet_rejects_a_wrong_setting():
+    """moons_mhd_set_unet: refused when the step does not use the learned +
+    mixed solves (MOONS_ERR_STATE) and for a network on another mesh
+    (MOONS_ERR_SHAPE)."""
+    from moons_b200 import configs
+    kw = dict(nx=8, ny=8, nz=16)
+    mom, _, _, _ = configs.at_scale(**kw)
+    mm = G.Mesh(*mom)
+    other = G.Mesh(*configs.at_scale(nx=16, ny=8, nz=16)[0])
+    plain = configs.make(G, configs.at_scale, seed=0, meshes=(mm, mm), **kw)
+    with pytest.raises(G.MoonsError) as e:
+        plain.set_unet(0, G.UNet(mm, seed=0))
+    assert e.value.code == 5  # MOONS_ERR_STATE
+    learned = configs.make(G, configs.at_scale, seed=0, prec_poisson=G.PREC_UNET_MG, meshes=(mm, mm), **kw)
+    with pytest.raises(G.MoonsError) as e:
+        learned.set_unet(0, G.UNet(other, seed=0))
+    assert e.value.code == 2  # MOONS_ERR_SHAPE
+
+
 def test_unet_solver_needs_a_network():
     mesh = L.shell_mesh(16)
     case = L.ShellCase.build(mesh, 16, SHELL, 0)
