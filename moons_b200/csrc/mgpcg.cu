@@ -42,6 +42,7 @@ struct MGHier {
   std::vector<std::array<MGRest<double>, 3>> Rd;
   std::vector<std::array<MGRest<float>, 3>> Rf;
   double* rprev = nullptr;  // flexible CG: previous residual
+  std::vector<void*> rt1, rt2;  // separable restriction temporaries per coarse level (compact, level type)
   double* ts_part = nullptr;   // two-stage scaling: block partials of N.t, N.A N
   double* ts_gamma = nullptr;  // and the resulting multiple of N
   // coarsest level: dense inverse (direct solve) when small enough
@@ -484,6 +485,20 @@ int mg_build(moons_pcg* s, moons_mesh* m, int mixed, const DBC& bc, const DF* kf
     h->ts_gamma = dev_zeros<double>(h.get(), 1, st);
     if (!h->rprev || !h->ts_part || !h->ts_gamma) return MOONS_ERR_NOMEM;
   }
+  // separable restriction temporaries (x pass: cx*fy*fz, y pass: cx*cy*fz)
+  h->rt1.assign(h->nl, nullptr);
+  h->rt2.assign(h->nl, nullptr);
+  for (int l = 1; l < h->nl; l++) {
+    const size_t cx = h->s[l][0] - 2, cy = h->s[l][1] - 2, fy = h->s[l - 1][1] - 2, fz = h->s[l - 1][2] - 2;
+    const size_t es = h->mixed ? sizeof(float) : sizeof(double);
+    for (int q = 0; q < 2; q++) {
+      void* ptr = nullptr;
+      if (cudaMalloc(&ptr, es * std::max<size_t>(1, q == 0 ? cx * fy * fz : cx * cy * fz)) != cudaSuccess)
+        return MOONS_ERR_NOMEM;
+      h->allocs.push_back(ptr);
+      (q == 0 ? h->rt1 : h->rt2)[l] = ptr;
+    }
+  }
   {  // coarsest level: dense inverse, regularised on the constants when singular
     const int l = h->nl - 1;
     const auto& sc = h->s[l];
@@ -628,6 +643,37 @@ unsigned vgrid(size_t n, int occ = 8, int nsm = 148) {
 }
 
 
+// coarse r = R (fine t) from level l to l + 1: three separable passes
+// (large levels) or one gather per coarse cell; pdl: dependent launches
+template <typename T>
+int restrict_level(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::array<MGRest<T>, 3>>& R,
+                   int l, bool sep, bool pdl, cudaStream_t st, const PcgScalars* S) {
+  const MGLev<T>& F = L[l];
+  const MGLev<T>& C = L[l + 1];
+  const int cx = C.s0 - 2, cy = C.s1 - 2, fy = F.s1 - 2, fz = F.s2 - 2;
+  const size_t nc = (size_t)cx * (C.s1 - 2) * (C.s2 - 2);
+  if (!sep) {
+    if (pdl) MG_LAUNCH_PDL(k_mg_restrict<T>, vgrid(nc, h->occ[2], h->nsm), 256, st, F, C, R[l + 1][0], R[l + 1][1],
+                           R[l + 1][2], S);
+    else MG_LAUNCH(k_mg_restrict<T>, vgrid(nc, h->occ[2], h->nsm), 256, st, F, C, R[l + 1][0], R[l + 1][1],
+                   R[l + 1][2], S);
+    return MOONS_OK;
+  }
+  T* t1 = (T*)h->rt1[l + 1];
+  T* t2 = (T*)h->rt2[l + 1];
+  const size_t n1 = (size_t)cx * fy * fz, n2 = (size_t)cx * cy * fz;
+  if (pdl) {
+    MG_LAUNCH_PDL(k_mg_rx<T>, vgrid(n1, 8, h->nsm), 256, st, F, R[l + 1][0], t1, cx, S);
+    MG_LAUNCH_PDL(k_mg_ry<T>, vgrid(n2, 8, h->nsm), 256, st, (const T*)t1, cx, fy, cy, fz, R[l + 1][1], t2, S);
+    MG_LAUNCH_PDL(k_mg_rz<T>, vgrid(nc, 8, h->nsm), 256, st, (const T*)t2, C, R[l + 1][2], S);
+  } else {
+    MG_LAUNCH(k_mg_rx<T>, vgrid(n1, 8, h->nsm), 256, st, F, R[l + 1][0], t1, cx, S);
+    MG_LAUNCH(k_mg_ry<T>, vgrid(n2, 8, h->nsm), 256, st, (const T*)t1, cx, fy, cy, fz, R[l + 1][1], t2, S);
+    MG_LAUNCH(k_mg_rz<T>, vgrid(nc, 8, h->nsm), 256, st, (const T*)t2, C, R[l + 1][2], S);
+  }
+  return MOONS_OK;
+}
+
 template <typename T>
 int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::array<MGProl<T>, 3>>& P,
              const std::vector<std::array<MGRest<T>, 3>>& R, cudaStream_t st, const PcgScalars* S) {
@@ -641,8 +687,8 @@ int vcycle_t(MGHier* h, const std::vector<MGLev<T>>& L, const std::vector<std::a
       MG_LAUNCH_PDL(k_mg_smooth<T>, g, 256, st, L[l], 1, 0, om, S);
     }
     MG_LAUNCH_PDL(k_mg_resid<T>, vgrid(npts(l), h->occ[1], h->nsm), 256, st, L[l], S);
-    MG_LAUNCH_PDL(k_mg_restrict<T>, vgrid(npts(l + 1), h->occ[2], h->nsm), 256, st, L[l], L[l + 1], R[l + 1][0],
-              R[l + 1][1], R[l + 1][2], S);
+    const int rc = restrict_level<T>(h, L, R, l, npts(l) >= kRsepMin, true, st, S);
+    if (rc) return rc;
   }
   if (h->ncoarse > 0) {
     MG_LAUNCH_PDL(k_mg_direct<T>, (unsigned)((h->ncoarse + kDirectRowsPerBlock - 1) / kDirectRowsPerBlock), 256, st,
@@ -1043,8 +1089,9 @@ int moons_mg_debug(moons_pcg* s, int op, int level, const double* a, const doubl
     const MGLev<double>& C = h->Ld[level + 1];
     MG_CUDA(cudaMemcpyAsync(L.t, a, bytes(level), cudaMemcpyHostToDevice, st));
     MG_CUDA(cudaMemsetAsync(C.r, 0, bytes(level + 1), st));
-    MG_LAUNCH(k_mg_restrict<double>, vgrid(npts(level + 1), h->occ[2], h->nsm), 256, st, L, C, h->Rd[level + 1][0],
-              h->Rd[level + 1][1], h->Rd[level + 1][2], (const PcgScalars*)nullptr);
+    // the separable passes, the V-cycle's restriction of its large levels
+    const int rc = restrict_level<double>(h, h->Ld, h->Rd, level, true, false, st, nullptr);
+    if (rc) return rc;
     MG_CUDA(cudaMemcpyAsync(out, C.r, bytes(level + 1), cudaMemcpyDeviceToHost, st));
   } else {
     MG_CUDA(cudaMemcpyAsync(L.e, a, bytes(level), cudaMemcpyHostToDevice, st));
