@@ -222,6 +222,13 @@ module moons_gpu_mod
       integer(c_int) :: st
     end function
 
+    function moons_pcg_apply_op(s, ax, x) bind(C, name="moons_pcg_apply_op") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s
+      type(c_ptr), intent(in) :: ax(*), x(*)
+      integer(c_int) :: st
+    end function
+
     function moons_pcg_apply_prec(s, z, r) bind(C, name="moons_pcg_apply_prec") result(st)
       import :: c_ptr, c_int
       type(c_ptr), value :: s

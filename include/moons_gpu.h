@@ -428,6 +428,13 @@ int moons_pcg_residual(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, moo
  * MOONS_PREC_UNET_MG (same mesh; the solver does not own it and reads its
  * current weights at every solve) */
 int moons_pcg_set_unet(moons_pcg* s, moons_unet* u);
+/* out = A x with the solver's operator in its explicit form, the abstract
+ * op_SF / op_VF of matrix_free_operators_interfaces.f90:14-60 as
+ * operator_explicit binds it (matrix_free_operators.f90: Lap_uniform,
+ * Lap_nonuniform_props, mom_diffusion, ind_diffusion, nrg_diffusion
+ * _explicit): the values in x's ghost cells are used as they are, no
+ * volume weighting; out and x are fields of the solver's unknown's layout */
+int moons_pcg_apply_op(moons_pcg* s, moons_sf* const* out, moons_sf* const* x);
 /* z = M(r) with the solver's preconditioner (no reference counterpart): the
  * Jacobi Minv r, or one multigrid V-cycle (MOONS_PREC_MG / _MG_MIXED /
  * _UNET / _UNET_MG: the V-cycle alone), or the direct solve (MOONS_PREC_FD);

@@ -238,6 +238,7 @@ def lib() -> C.CDLL:
             "moons_pcg_set_unet": (C.c_int, [_P, _P]),
             "moons_pcg_residual": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
             "moons_pcg_apply_prec": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
+            "moons_pcg_apply_op": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
             "moons_unet_loss_grad": (C.c_int, [_P, _P, _P, _F, _F, C.c_longlong]),
             "moons_unet_train_step": (C.c_int, [_P, _P, _P, C.c_float, _F]),
             "moons_unet_layer_check": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -508,6 +509,10 @@ class PCG:
     def residual(self, x: Sequence[Field], b: Sequence[Field], out: Sequence[Field]):
         """The solver's internal residual vol*(b - A x) for the iterate x."""
         _check(lib().moons_pcg_residual(self.h, _ptrs(x), _ptrs(b), _ptrs(out)))
+
+    def apply_op(self, out: Sequence[Field], x: Sequence[Field]):
+        """out = A x with the solver's operator (operator_explicit form)."""
+        _check(lib().moons_pcg_apply_op(self.h, _ptrs(out), _ptrs(x)))
 
     def apply_prec(self, z: Sequence[Field], r: Sequence[Field]):
         """z = M(r) with the solver's preconditioner (a multigrid-family

@@ -1198,6 +1198,29 @@ int moons_pcg_residual(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, moo
   return r;
 }
 
+int moons_pcg_apply_op(moons_pcg* s, moons_sf* const* out, moons_sf* const* x) {
+  if (!s || !out || !x) {
+    set_error("moons_pcg_apply_op: null argument");
+    return MOONS_ERR_ARG;
+  }
+  moons_mesh* m = s->m;
+  cudaSetDevice(m->device);
+  DF O[3], X[3];
+  for (int c = 0; c < s->nc; c++) {
+    if (!out[c] || !x[c] || out[c]->f.n() != s->Ax[c].n() || x[c]->f.n() != s->Ax[c].n() ||
+        out[c]->f.dl != s->x_dl[c] || x[c]->f.dl != s->x_dl[c]) {
+      set_error("moons_pcg_apply_op: field does not match the solver's unknown");
+      return MOONS_ERR_SHAPE;
+    }
+    O[c] = out[c]->f;
+    X[c] = x[c]->f;
+  }
+  const int rc = apply_op_explicit(s, O, X);
+  if (rc) return rc;
+  MG_CUDA(cudaStreamSynchronize(m->stream));
+  return MOONS_OK;
+}
+
 int moons_pcg_apply_prec(moons_pcg* s, moons_sf* const* z, moons_sf* const* r) {
   if (!s || !z || !r) {
     set_error("moons_pcg_apply_prec: null argument");

@@ -63,6 +63,7 @@ def lib():
             "or_pcg_destroy": (None, [_P]),
             "or_pcg_update_mfp": (C.c_int, [_P, C.c_double, C.c_int]),
             "or_pcg_solve": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(ISP), C.POINTER(SolveInfo)]),
+            "or_pcg_apply_op": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
             "or_mhd_create": (_P, [_P, _P, C.POINTER(MHDParams)]),
             "or_mhd_destroy": (None, [_P]),
             "or_mhd_upload": (C.c_int, [_P, C.c_int, C.c_int, _D, C.c_longlong]),
@@ -224,6 +225,10 @@ class PCG:
 
     def update_mfp(self, coeff, update_prec=True):
         _check(lib().or_pcg_update_mfp(self.h, float(coeff), 1 if update_prec else 0))
+
+    def apply_op(self, out, x):
+        """out = A x with the solver's operator_explicit (matrix_free_operators.f90)."""
+        _check(lib().or_pcg_apply_op(self.h, _ptrs(out), _ptrs(x)))
 
     def solve(self, x, b, params):
         info = SolveInfo()

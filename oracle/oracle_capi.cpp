@@ -131,6 +131,23 @@ void* or_pcg_create(int op, int prec, int nc, void** x, void** xbc, void** k, do
 }
 void or_pcg_destroy(void* p) { delete (OPCG*)p; }
 int or_pcg_update_mfp(void* p, double c, int upd) { OR_TRY(((OPCG*)p)->s.update_MFP(c, upd != 0)) }
+// operator_explicit of the solver (matrix_free_operators.f90), out = A x
+int or_pcg_apply_op(void* p, void** out, void** x) {
+  auto* s = (OPCG*)p;
+  try {
+    std::vector<mo::SF> A, xs;
+    for (int c = 0; c < s->s.nc; c++) {
+      A.push_back(F(out[c]));
+      xs.push_back(F(x[c]));
+    }
+    s->s.apply_operator(A, xs, true);
+    for (int c = 0; c < s->s.nc; c++) F(out[c]).f = A[c].f;
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
 int or_pcg_solve(void* p, void** x, void** b, const moons_isp* isp, moons_solve_info* info) {
   auto* s = (OPCG*)p;
   try {
