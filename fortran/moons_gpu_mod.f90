@@ -222,6 +222,17 @@ module moons_gpu_mod
       integer(c_int) :: st
     end function
 
+    function moons_clean_div(s, x, xstar, phi, scale, temp_f, temp_cc, isp, info) &
+        bind(C, name="moons_clean_div") result(st)
+      import :: c_ptr, c_int, c_double, moons_isp, moons_solve_info
+      type(c_ptr), value :: s, phi, temp_cc
+      type(c_ptr), intent(in) :: x(*), xstar(*), temp_f(*)
+      real(c_double), value :: scale
+      type(moons_isp), intent(in) :: isp
+      type(moons_solve_info), intent(out) :: info
+      integer(c_int) :: st
+    end function
+
     function moons_pcg_apply_op(s, ax, x) bind(C, name="moons_pcg_apply_op") result(st)
       import :: c_ptr, c_int
       type(c_ptr), value :: s

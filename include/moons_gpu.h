@@ -233,6 +233,14 @@ int moons_pcg_update_mfp(moons_pcg* s, double coeff_implicit_time_split,
 int moons_pcg_solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b,
                     const moons_isp* isp, moons_solve_info* info);
 
+/* clean_div (clean_divergence.f90:37-59) with PCG_phi: temp_CC = scale *
+ * div(Xstar); solve(PCG, phi, temp_CC); temp_F = grad(phi) / scale;
+ * X = Xstar - temp_F; apply_BCs(X).  X, Xstar, temp_F: x, y, z face fields;
+ * phi, temp_CC: cell-centred, all on the solver's mesh; the caller's
+ * temporaries are overwritten (as the reference's temp_F, temp_CC are). */
+int moons_clean_div(moons_pcg* pcg, moons_sf* const* X, moons_sf* const* Xstar, moons_sf* phi, double scale,
+                    moons_sf* const* temp_F, moons_sf* temp_CC, const moons_isp* isp, moons_solve_info* info);
+
 /* ---- the MHD time step (HW/MOONS/MOONS_solver.f90:47-144, one RK stage) --
  * Momentum: add_all_momentum_sources (add_all_momentum_sources.f90:22-86)
  * + Euler_time_AB2_sources (time_marching_methods.f90:117-150) with PCG_U

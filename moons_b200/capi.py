@@ -239,6 +239,8 @@ def lib() -> C.CDLL:
             "moons_pcg_residual": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
             "moons_pcg_apply_prec": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
             "moons_pcg_apply_op": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
+            "moons_clean_div": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), _P, C.c_double, C.POINTER(_P), _P,
+                                          C.POINTER(ISP), C.POINTER(SolveInfo)]),
             "moons_unet_loss_grad": (C.c_int, [_P, _P, _P, _F, _F, C.c_longlong]),
             "moons_unet_train_step": (C.c_int, [_P, _P, _P, C.c_float, _F]),
             "moons_unet_layer_check": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -411,6 +413,15 @@ class _FieldView:
 
     def download_ptr(self, ptr: int):
         _check(lib().moons_sf_download(self.h, C.cast(ptr, _D), self.n))
+
+
+def clean_div(pcg: "PCG", X, Xstar, phi, scale: float, temp_F, temp_CC, params) -> dict:
+    """clean_div (clean_divergence.f90:37-59): project Xstar onto X with the
+    potential phi solved by `pcg` (LAP_UNIFORM on phi's layout)."""
+    info = SolveInfo()
+    _check(lib().moons_clean_div(pcg.h, _ptrs(X), _ptrs(Xstar), phi.h, float(scale), _ptrs(temp_F), temp_CC.h,
+                                 C.byref(params), C.byref(info)))
+    return info.as_dict()
 
 
 class MHD:

@@ -890,6 +890,43 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
   return MOONS_OK;
 }
 
+int moons_clean_div(moons_pcg* p, moons_sf* const* X, moons_sf* const* Xstar, moons_sf* phi, double scale,
+                    moons_sf* const* temp_F, moons_sf* temp_CC, const moons_isp* isp, moons_solve_info* info) {
+  if (!p || !X || !Xstar || !phi || !temp_F || !temp_CC || !isp || !(scale != 0.0)) {
+    set_error("moons_clean_div: null argument or zero scale");
+    return MOONS_ERR_ARG;
+  }
+  moons_mesh* m = mg::pcg_mesh(p);
+  for (int k = 0; k < 3; k++) {
+    const int dl = k == 0 ? MOONS_FX : (k == 1 ? MOONS_FY : MOONS_FZ);
+    if (!X[k] || !Xstar[k] || !temp_F[k] || D(X[k]).dl != dl || D(Xstar[k]).dl != dl || D(temp_F[k]).dl != dl) {
+      set_error("moons_clean_div: X, Xstar and temp_F must be x, y, z face fields");
+      return MOONS_ERR_SHAPE;
+    }
+  }
+  if (D(phi).dl != MOONS_CC || D(temp_CC).dl != MOONS_CC) {
+    set_error("moons_clean_div: phi and temp_CC must be cell-centred");
+    return MOONS_ERR_SHAPE;
+  }
+  cudaSetDevice(m->device);
+  // div(temp_CC, Xstar) ; temp_CC *= scale ; solve(PCG, phi, temp_CC)
+  int r = div3(m, temp_CC, Xstar);
+  if (!r) r = launch_pw(m, PW_SCALE, D(temp_CC), nullptr, scale);
+  if (r) return r;
+  moons_sf* xp[1] = {phi};
+  moons_sf* bp[1] = {temp_CC};
+  if ((r = moons_pcg_solve(p, xp, bp, isp, info))) return r;
+  // grad(temp_F, phi) ; temp_F *= 1/scale ; X = Xstar - temp_F ; apply_BCs(X)
+  if ((r = grad3(m, temp_F, phi))) return r;
+  for (int k = 0; k < 3; k++) {
+    MG_LAUNCH(k_project, nblocks(D(X[k]).n()), kBlock, m->stream, D(X[k]), D(Xstar[k]), D(temp_F[k]), 1.0 / scale);
+    if ((r = launch_bcs(m, D(X[k]), X[k]->bc, false))) return r;
+  }
+  MG_CUDA(cudaGetLastError());
+  MG_CUDA(cudaStreamSynchronize(m->stream));
+  return MOONS_OK;
+}
+
 int moons_mhd_set_unet(moons_mhd* s, int which, moons_unet* u) {
   if (!s || !u || which < 0 || which > 1) {
     set_error("moons_mhd_set_unet: bad argument");

@@ -64,6 +64,8 @@ def lib():
             "or_pcg_update_mfp": (C.c_int, [_P, C.c_double, C.c_int]),
             "or_pcg_solve": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(ISP), C.POINTER(SolveInfo)]),
             "or_pcg_apply_op": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
+            "or_clean_div": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), _P, C.c_double, C.POINTER(_P), _P,
+                                       C.POINTER(ISP), C.POINTER(SolveInfo)]),
             "or_mhd_create": (_P, [_P, _P, C.POINTER(MHDParams)]),
             "or_mhd_destroy": (None, [_P]),
             "or_mhd_upload": (C.c_int, [_P, C.c_int, C.c_int, _D, C.c_longlong]),
@@ -242,6 +244,14 @@ class PCG:
                 self.h = None
         except Exception:
             pass
+
+
+def clean_div(pcg, X, Xstar, phi, scale, temp_F, temp_CC, params) -> dict:
+    """clean_div (clean_divergence.f90:37-59) with the solver pcg."""
+    info = SolveInfo()
+    _check(lib().or_clean_div(pcg.h, _ptrs(X), _ptrs(Xstar), phi.h, float(scale), _ptrs(temp_F), temp_CC.h,
+                              C.byref(params), C.byref(info)))
+    return info.as_dict()
 
 
 class MHD:

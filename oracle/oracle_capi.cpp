@@ -148,6 +148,9 @@ int or_pcg_apply_op(void* p, void** out, void** x) {
     return 1;
   }
 }
+// clean_div (clean_divergence.f90:37-59) with the solver p
+int or_clean_div(void* p, void** X, void** Xs, void* phi, double scale, void** tF, void* tCC, const moons_isp* isp,
+                 moons_solve_info* info);
 int or_pcg_solve(void* p, void** x, void** b, const moons_isp* isp, moons_solve_info* info) {
   auto* s = (OPCG*)p;
   try {
@@ -171,6 +174,32 @@ int or_pcg_solve(void* p, void** x, void** b, const moons_isp* isp, moons_solve_
       info->ms = 0;
     }
     return r.nan ? MOONS_ERR_NAN : MOONS_OK;
+  } catch (const std::exception& e) {
+    return fail(e.what());
+  }
+}
+int or_clean_div(void* p, void** X, void** Xs, void* phi, double scale, void** tF, void* tCC, const moons_isp* isp,
+                 moons_solve_info* info) {
+  try {
+    mo::SF& tc = F(tCC);
+    // div(temp_CC, Xstar); multiply(temp_CC, scale)
+    mo::div(tc, F(Xs[0]), F(Xs[1]), F(Xs[2]), G(tCC));
+    mo::multiply(tc, scale);
+    void* xp[1] = {phi};
+    void* bp[1] = {tCC};
+    const int r = or_pcg_solve(p, xp, bp, isp, info);
+    if (r) return r;
+    // grad(temp_F, phi); multiply(temp_F, 1/scale); subtract(X, Xstar, temp_F); apply_BCs(X)
+    mo::grad(F(tF[0]), F(tF[1]), F(tF[2]), F(phi), G(phi));
+    for (int k = 0; k < 3; k++) {
+      mo::multiply(F(tF[k]), 1.0 / scale);
+      mo::SF& x = F(X[k]);
+      const mo::SF& xs = F(Xs[k]);
+      const mo::SF& t = F(tF[k]);
+      for (size_t i = 0; i < x.f.size(); i++) x.f[i] = xs.f[i] - t.f[i];
+      mo::apply_BCs(x);
+    }
+    return 0;
   } catch (const std::exception& e) {
     return fail(e.what());
   }
