@@ -311,6 +311,18 @@ typedef struct {
   double scale_viscous_dissipation_T; /* SP%ET%viscous_dissipation%scale: F += s sum_cd (d_d U_CC,c)^2 */
   double scale_joule_heating_T;       /* SP%ET%joule_heating%scale: F += s (sum_c J_CC,c^2) sigmaInv_CC,
                                          J_CC = edge2CellCenter(J) (faces in the potential form) */
+  /* time schemes of the momentum and (B form) induction steps, the
+   * solve_method switch of solve_momentum (momentum_extend.f90:335-367) and
+   * solve_induction (induction_extend.f90:484-514), time_marching_methods.f90:
+   *   0 or 6: Euler_time_AB2_sources (:117-150), (I + dt c A) X* =
+   *           X + dt (AB2(F, Fnm1) + L), clean_div scale 1/dt;
+   *   5:      Euler_time_Euler_sources (:47-79), (I + dt c A) X* = X + dt F,
+   *           clean_div scale 1;
+   *   7:      O2_BDF_time_AB2_sources (:81-115), (I + 2/3 dt c A) X* =
+   *           4/3 X - 1/3 Xnm1 + 2/3 dt AB2(F, Fnm1), clean_div scale 1.
+   * Source terms on wall-normal Dirichlet faces are zeroed in all three. */
+  int solve_method_U;
+  int solve_method_B;
 } moons_mhd_params;
 
 typedef struct {

@@ -117,6 +117,8 @@ class MHDParams(C.Structure):
         ("scale_KE_diffusion_T", C.c_double),
         ("scale_viscous_dissipation_T", C.c_double),
         ("scale_joule_heating_T", C.c_double),
+        ("solve_method_U", C.c_int),
+        ("solve_method_B", C.c_int),
     ]
 
 

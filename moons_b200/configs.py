@@ -281,16 +281,22 @@ def full_bc(N: int = 80, N_w: int = 9, vacuum: bool = True, Re: float = 2000.0, 
     return m.mom, m.ind, prm, init
 
 
-def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, unets=None, meshes=None, **kw):
+def make(backend, builder, *args, seed: int = 0, prec_poisson: int = 0, unets=None, meshes=None,
+         solve_method_U: int = 0, solve_method_B: int = 0, **kw):
     """Create meshes + the MHD object on ``backend`` (moons_b200.capi or the
     oracle module) from a builder, upload the seeded initial state and init.
     ``prec_poisson`` selects the pressure/potential preconditioner (0: the
     reference's Jacobi prec_Lap; capi.PREC_MG / PREC_MG_MIXED: multigrid;
     PREC_FD: the direct solve; PREC_UNET_MG: learned + mixed, with
     ``unets`` = (pressure net, potential net) built on ``meshes`` = (fluid
-    mesh, induction mesh), which the simulation then uses)."""
+    mesh, induction mesh), which the simulation then uses).
+    ``solve_method_U`` / ``solve_method_B`` pick the momentum / induction
+    time scheme (0 or 6: Euler_time_AB2_sources, 5: Euler_time_Euler_sources,
+    7: O2_BDF_time_AB2_sources; time_marching_methods.f90:47-150)."""
     mom, ind, prm, init = builder(*args, **kw)
     prm.prec_poisson = prec_poisson
+    prm.solve_method_U = solve_method_U
+    prm.solve_method_B = solve_method_B
     if meshes is not None:
         mm, mi = meshes
     else:

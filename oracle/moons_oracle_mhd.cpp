@@ -113,6 +113,7 @@ struct MHD {
   bool pcgT_made = false;
   int iters[5] = {0, 0, 0, 0, 0};
   double res_p = 0, res_phi = 0;
+  int n_step = 0;  // TMP%n_step: steps taken (time_marching_params_extend.f90:43,59)
 
   void create(const Grid& gmom, const Grid& gind, const moons_mhd_params& prm) {
     gm = gmom;
@@ -436,27 +437,52 @@ struct MHD {
     }
   }
 
-  // Euler_time_AB2_sources (time_marching_methods.f90:117-150)
+  // The implicit schemes of solve_momentum / solve_induction
+  // (momentum_extend.f90:335-367, induction_extend.f90:484-514), selected by
+  // solve_method: 6 = Euler_time_AB2_sources (time_marching_methods.f90:
+  // 117-150), 5 = Euler_time_Euler_sources (:47-79), 7 =
+  // O2_BDF_time_AB2_sources (:81-115); each ends in clean_div_PCG.
   void euler_ab2(PCG& pv, PCG& ps, ISP& iv, ISP& is, SF* X, SF* Xstar, SF* Xnm1, SF& ph, SF* Fn, SF* Fm, SF* Lx,
-                 SF* t1, SF& tcc, const Grid& g, double coeff_implicit, int slot_v, int slot_s, double* res_s) {
+                 SF* t1, SF& tcc, const Grid& g, double coeff_implicit, int slot_v, int slot_s, double* res_s,
+                 int method) {
+    const double two_thirds = 2.0 / 3.0, four_thirds = 4.0 / 3.0, neg_one_third = -1.0 / 3.0;
     double dt = P.dt;
     for (int c = 0; c < 3; c++) {
-      // AB2_VF (AB2.f90:53-64): AB2 = Fn*1.5 ; AB2 += Fnm1*(-0.5)
-      for (size_t i = 0; i < t1[c].n(); i++) t1[c].f[i] = Fn[c].f[i] * 1.5;
-      add_product(t1[c], Fm[c], -0.5);
-      add(t1[c], Lx[c]);
-      multiply(t1[c], dt);
-      assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
-      add(t1[c], X[c]);
+      if (method == 5) {
+        assign(t1[c], Fn[c]);
+        multiply(t1[c], dt);
+        assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
+        add(t1[c], X[c]);
+      } else {
+        // AB2_VF (AB2.f90:53-64): AB2 = Fn*1.5 ; AB2 += Fnm1*(-0.5)
+        for (size_t i = 0; i < t1[c].n(); i++) t1[c].f[i] = Fn[c].f[i] * 1.5;
+        add_product(t1[c], Fm[c], -0.5);
+        if (method == 6) {
+          add(t1[c], Lx[c]);
+          multiply(t1[c], dt);
+          assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
+          add(t1[c], X[c]);
+        } else {
+          multiply(t1[c], two_thirds * dt);
+          assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
+          add_product(t1[c], X[c], four_thirds);
+          add_product(t1[c], Xnm1[c], neg_one_third);
+        }
+      }
       assign(Xnm1[c], X[c]);
     }
-    pv.update_MFP(dt * 1.0 * coeff_implicit, true);
+    // update_MFP: method 6 rebuilds the preconditioner every step, methods 5
+    // and 7 while TMP%n_step <= 2
+    if (method == 6) pv.update_MFP(dt * 1.0 * coeff_implicit, true);
+    else if (method == 5) pv.update_MFP(dt * 1.0 * coeff_implicit, n_step <= 2);
+    else pv.update_MFP(dt * two_thirds * coeff_implicit, n_step <= 2);
     SF* xs[3] = {&Xstar[0], &Xstar[1], &Xstar[2]};
     SF* bs[3] = {&t1[0], &t1[1], &t1[2]};
     SolveInfo si = pv.solve(xs, bs, iv);
     iters[slot_v] += si.iterations;
-    // clean_div_PCG (clean_divergence.f90:37-59), scale = 1/dt
-    double scale = 1.0 / dt;
+    // clean_div_PCG (clean_divergence.f90:37-59), scale = 1/dt for method 6,
+    // 1 for methods 5 and 7
+    double scale = method == 6 ? 1.0 / dt : 1.0;
     div(tcc, Xstar[0], Xstar[1], Xstar[2], g);
     multiply(tcc, scale);
     SF* xp[1] = {&ph};
@@ -504,8 +530,9 @@ struct MHD {
       }
     }
     if (P.energy && P.scale_buoyancy != 0.0) add_buoyancy();
-    // ---- solve_momentum (method 6)
-    euler_ab2(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p);
+    // ---- solve_momentum (solve_method 5, 6 or 7; 0 = 6)
+    euler_ab2(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p,
+              P.solve_method_U ? P.solve_method_U : 6);
     for (int c = 0; c < 3; c++) interp(UCC[c], U[c], gm, c + 1);
     SF* Up[3] = {&U[0], &U[1], &U[2]};
     face2edge_nd(UE, Up, gm);
@@ -532,7 +559,7 @@ struct MHD {
         for (int c = 0; c < 3; c++) add_product(Fi[c], tFi2[c], P.scale_diffusion_B);
       }
       euler_ab2(pcgB, pcgPhi, ispB, ispPhi, B, Bstar, Bnm1, phi, Fi, Fnm1i, Li, tFi1, tCCi, gi, P.coeff_implicit_B,
-                2, 3, &res_phi);
+                2, 3, &res_phi, P.solve_method_B ? P.solve_method_B : 6);
       compute_J();
       compute_Btot();
       compute_JxB();
@@ -541,6 +568,7 @@ struct MHD {
       potential_solve();
       compute_JxB();
     }
+    n_step++;
   }
 
   // advect_U_convection1 (ops_advect.f90:71-127) into tF3
@@ -618,6 +646,8 @@ struct OSFView {
 
 extern "C" {
 void* or_mhd_create(void* mesh_mom, void* mesh_ind, const moons_mhd_params* prm) {
+  for (int m : {prm->solve_method_U, prm->solve_method_B})
+    if (m != 0 && m != 5 && m != 6 && m != 7) return nullptr;  // solve_method 5, 6, 7 (0 = 6)
   auto* s = new mo::MHD();
   const mo::Grid& gm = ((OMeshView*)mesh_mom)->g;
   const mo::Grid& gi = ((OMeshView*)mesh_ind)->g;

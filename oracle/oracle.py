@@ -261,6 +261,8 @@ class MHD:
         self.meshes = (mesh_mom, mesh_ind)
         self.params = params
         self.h = lib().or_mhd_create(mesh_mom.h, mesh_ind.h, C.byref(params))
+        if not self.h:
+            raise ValueError("or_mhd_create: solve_method_U and solve_method_B must be 0, 5, 6 or 7")
 
     def shape(self, which, comp=0):
         s = (C.c_int * 3)()

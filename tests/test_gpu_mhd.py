@@ -102,3 +102,41 @@ def test_mhd_steps_multigrid_poisson(name, builder, kw, prec):
     duo, _ = o.divergence()
     assert dug <= max(100 * duo, 1e-22)
     assert ig["iters_p"] < 40 * nsteps
+
+
+SCHEME_CASES = [CASES[1], CASES[2]]  # LDC in the B form, the duct with walls
+
+
+@pytest.mark.parametrize("method", [5, 7])
+@pytest.mark.parametrize("name,builder,kw", SCHEME_CASES, ids=[c[0] for c in SCHEME_CASES])
+def test_mhd_time_schemes_match_oracle(name, builder, kw, method):
+    """solve_method 5 (Euler_time_Euler_sources) and 7 (O2_BDF_time_AB2_sources,
+    time_marching_methods.f90:47-115) for both the momentum and the induction
+    step: 4 steps against the oracle's restatement of the same schemes, every
+    field within the step test's 1e-10."""
+    g = configs.make(G, builder, seed=3, solve_method_U=method, solve_method_B=method, **kw)
+    o = configs.make(O, builder, seed=3, solve_method_U=method, solve_method_B=method, **kw)
+    nsteps = 4
+    ig = g.step(nsteps)
+    io = o.step(nsteps)
+    fields = ([(G.MHD_U, c) for c in range(3)] + [(G.MHD_P, 0)] + [(G.MHD_B, c) for c in range(3)] +
+              [(G.MHD_J, c) for c in range(3)] + [(G.MHD_JXB, c) for c in range(3)])
+    for which, c in fields:
+        e = rel_l2(g.download(which, c), o.download(which, c))
+        assert e < 1e-10, f"{name} method {method}: field {which}/{c} rel L2 {e}"
+    dug, dbg = g.divergence()
+    duo, dbo = o.divergence()
+    assert dug <= max(10 * duo, 1e-24)
+    assert dbg <= max(10 * dbo, 1e-24)
+    for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
+        assert abs(ig[k] - io[k]) <= max(nsteps, 0.005 * io[k]), (k, ig, io)
+
+
+@pytest.mark.parametrize("field", ["solve_method_U", "solve_method_B"])
+def test_mhd_rejects_unknown_time_scheme(field):
+    mom, ind, prm, _ = configs.ldc(n=6, induction=G.IND_B)
+    setattr(prm, field, 4)
+    mm = G.Mesh(*mom)
+    with pytest.raises(G.MoonsError) as e:
+        G.MHD(mm, mm, prm)
+    assert e.value.code == 1  # MOONS_ERR_ARG
