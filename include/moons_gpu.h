@@ -319,8 +319,13 @@ typedef struct {
    *   5:      Euler_time_Euler_sources (:47-79), (I + dt c A) X* = X + dt F,
    *           clean_div scale 1;
    *   7:      O2_BDF_time_AB2_sources (:81-115), (I + 2/3 dt c A) X* =
-   *           4/3 X - 1/3 Xnm1 + 2/3 dt AB2(F, Fnm1), clean_div scale 1.
-   * Source terms on wall-normal Dirichlet faces are zeroed in all three. */
+   *           4/3 X - 1/3 Xnm1 + 2/3 dt AB2(F, Fnm1), clean_div scale 1;
+   *   3, 4:   Euler_time_no_diff_Euler_sources (:298-327) and
+   *           Euler_time_no_diff_AB2_sources (:266-296), no diffusion solve:
+   *           X* = X + dt F or X + dt AB2(F, Fnm1), clean_div scale 1;
+   *   1, 2:   the same without the projection (:329-366): X += dt F or
+   *           dt AB2(F, Fnm1), then X's BCs.
+   * Source terms on wall-normal Dirichlet faces are zeroed in all of them. */
   int solve_method_U;
   int solve_method_B;
 } moons_mhd_params;

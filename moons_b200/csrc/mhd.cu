@@ -16,31 +16,37 @@
 namespace mg {
 
 // ---- fused pointwise kernels ----------------------------------------------
-// Predictor RHS of the three implicit schemes (time_marching_methods.f90),
-// each a chain of whole-array passes in the reference, one pass here with the
-// same operations in the same order per point:
-//  method 6, Euler_time_AB2_sources (:137-142):
+// Predictor RHS of the time schemes (time_marching_methods.f90), each a
+// chain of whole-array passes in the reference, one pass here with the same
+// operations in the same order per point.  form:
+//  6, Euler_time_AB2_sources (:137-142):
 //   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t + L ; t = t*dt ;
-//   assign_wall_Dirichlet(t,0,X) ; t = t + X ; Xnm1 = X
-//  method 5, Euler_time_Euler_sources (:70-74):
-//   t = F ; t = t*dt ; assign_wall_Dirichlet(t,0,X) ; t = t + X ; Xnm1 = X
-//  method 7, O2_BDF_time_AB2_sources (:104-110):
+//   assign_wall_Dirichlet(t,0,X) ; t = t + X
+//  4, the AB2 schemes without diffusion (:289-292, :342-345):
+//   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t*dt ; assign_wall_Dirichlet(t,0,X) ;
+//   t = t + X
+//  5, Euler_time_Euler_sources and the Euler schemes without diffusion
+//   (:70-73, :321-323, :362-364):
+//   t = F*dt ; assign_wall_Dirichlet(t,0,X) ; t = t + X
+//  7, O2_BDF_time_AB2_sources (:104-108):
 //   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t*(2/3 dt) ;
-//   assign_wall_Dirichlet(t,0,X) ; t = t + X*(4/3) ; t = t + Xnm1*(-1/3) ;
-//   Xnm1 = X
-// (dts is dt for methods 5 and 6 and the product 2/3*dt for method 7)
-__global__ void k_ab2_rhs(DF t, DF F, DF Fm, DF L, DF X, DF Xnm1, double dts, int wallbits, int method) {
+//   assign_wall_Dirichlet(t,0,X) ; t = t + X*(4/3) ; t = t + Xnm1*(-1/3)
+// then Xnm1 = X when set_nm1 (every scheme but the two "no_correction" ones,
+// whose t is X itself: X = X + increment).  dts is dt, or the product 2/3*dt
+// for form 7.  t may alias X: each point reads X and Xnm1 before writing t.
+__global__ void k_ab2_rhs(DF t, DF F, DF Fm, DF L, DF X, DF Xnm1, double dts, int wallbits, int form,
+                          int set_nm1) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= t.n()) return;
   int i, j, k;
   ijk_of(idx, t, i, j, k);
   double v;
-  if (method == 5) {
+  if (form == 5) {
     v = F.f[idx];
   } else {
     v = F.f[idx] * 1.5;
     v = v + Fm.f[idx] * (-0.5);
-    if (method == 6) v = v + L.f[idx];
+    if (form == 6) v = v + L.f[idx];
   }
   v = v * dts;
   if (wallbits) {
@@ -49,14 +55,14 @@ __global__ void k_ab2_rhs(DF t, DF F, DF Fm, DF L, DF X, DF Xnm1, double dts, in
       v = 0.0;
   }
   double x = X.f[idx];
-  if (method == 7) {
+  if (form == 7) {
     v = v + x * (4.0 / 3.0);
     v = v + Xnm1.f[idx] * (-1.0 / 3.0);
   } else {
     v = v + x;
   }
   t.f[idx] = v;
-  Xnm1.f[idx] = x;
+  if (set_nm1) Xnm1.f[idx] = x;
 }
 // clean_div tail: temp_F = grad(phi) ; temp_F *= 1/scale ; X = Xstar - temp_F
 __global__ void k_project(DF X, DF Xstar, DF g, double inv_scale) {
@@ -122,8 +128,8 @@ using namespace mg;
 
 namespace {
 inline int orth(int a, int b) { return 6 - a - b; }  // 1-based directions
-// solve_method of the momentum / induction step: 0 selects the default, 6
-inline bool time_method_ok(int m) { return m == 0 || m == 5 || m == 6 || m == 7; }
+// solve_method of the momentum / induction step: 1 to 7, 0 selects the default, 6
+inline bool time_method_ok(int m) { return m >= 0 && m <= 7; }
 inline int time_method(int m) { return m == 0 ? 6 : m; }
 }
 
@@ -246,21 +252,33 @@ int solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp&
   return mg_pcg_enqueue(s, x, b, &isp);
 }
 
-// The implicit predictor + clean_div_PCG of solve_momentum / solve_induction
-// for solve_method 5, 6 and 7 (time_marching_methods.f90:47-150,
-// clean_divergence.f90:37-59): the scheme's RHS, update_MFP with the scheme's
-// implicit factor, the PCG solve for X*, and the projection with clean_div's
-// scale (1/dt for method 6, 1 for methods 5 and 7).
+// One solve_momentum / solve_induction time step for solve_method 1 to 7
+// (time_marching_methods.f90:47-150, :266-366, clean_divergence.f90:37-59):
+//  5, 6, 7: the scheme's RHS, update_MFP with its implicit factor, the PCG
+//           solve for X*, then clean_div;
+//  3, 4:    X* = X + dt F (Euler) or X + dt AB2(F, Fnm1), then clean_div;
+//  1, 2:    X = X + dt F or X + dt AB2(F, Fnm1), then apply_BCs(X).
+// clean_div's scale is 1/dt for method 6 and 1 for the others.
 int euler_ab2(moons_mhd* s, moons_mesh* m, moons_pcg* pv, moons_pcg* ps, const moons_isp& iv, const moons_isp& is,
               moons_sf** X, moons_sf** Xstar, moons_sf** Xnm1, moons_sf* ph, moons_sf** Fn, moons_sf** Fm,
               moons_sf** Lx, moons_sf** t1, moons_sf* tcc, double coeff_implicit, double* coef_cache, int slot_v,
               int slot_s, double* res_s, int method) {
   double dt = s->P.dt;
   double dts = method == 7 ? (2.0 / 3.0) * dt : dt;
+  const int form = (method == 1 || method == 3 || method == 5) ? 5 : (method == 2 || method == 4) ? 4 : method;
+  const bool no_correction = method <= 2, implicit = method >= 5;
+  moons_sf** out = no_correction ? X : implicit ? t1 : Xstar;
   for (int c = 0; c < 3; c++) {
     int wb = dirichlet_wall_bits(X[c]->bc.defined ? &X[c]->bc : nullptr, D(X[c]).dl);
-    MG_LAUNCH(k_ab2_rhs, nblocks(D(t1[c]).n()), kBlock, m->stream, D(t1[c]), D(Fn[c]), D(Fm[c]), D(Lx[c]), D(X[c]),
-                                                                 D(Xnm1[c]), dts, wb, method);
+    MG_LAUNCH(k_ab2_rhs, nblocks(D(out[c]).n()), kBlock, m->stream, D(out[c]), D(Fn[c]), D(Fm[c]), D(Lx[c]),
+              D(X[c]), D(Xnm1[c]), dts, wb, form, no_correction ? 0 : 1);
+  }
+  int r;
+  if (no_correction) {
+    for (int k = 0; k < 3; k++)
+      if ((r = launch_bcs(m, D(X[k]), X[k]->bc, false))) return r;
+    MG_CUDA(cudaGetLastError());
+    return MOONS_OK;
   }
   MG_CUDA(cudaGetLastError());
   // update_MFP(PCG, m, dt*f*coeff_implicit, ...) with f = 1 or 2/3; the
@@ -268,12 +286,11 @@ int euler_ab2(moons_mhd* s, moons_mesh* m, moons_pcg* pv, moons_pcg* ps, const m
   // (methods 5 and 7 rebuild it on the first steps only, TMP%n_step <= 2,
   // which is the same thing for a fixed dt)
   double c = method == 7 ? dt * (2.0 / 3.0) * coeff_implicit : dt * 1.0 * coeff_implicit;
-  int r;
-  if (!(c == *coef_cache)) {
+  if (implicit && !(c == *coef_cache)) {
     if ((r = moons_pcg_update_mfp(pv, c, 1))) return r;
     *coef_cache = c;
   }
-  if ((r = solve(pv, Xstar, t1, iv, &s->iters[slot_v], nullptr))) return r;
+  if (implicit && (r = solve(pv, Xstar, t1, iv, &s->iters[slot_v], nullptr))) return r;
   double scale = method == 6 ? 1.0 / dt : 1.0;
   if ((r = div3(m, tcc, Xstar))) return r;
   if ((r = launch_pw(m, PW_SCALE, D(tcc), nullptr, scale))) return r;
@@ -478,7 +495,7 @@ int energy_step(moons_mhd* s) {
   // X* = X + dt AB2(F, Fnm1) (wall-Dirichlet points of the increment zeroed)
   const int wb = dirichlet_wall_bits(s->T->bc.defined ? &s->T->bc : nullptr, D(s->T).dl);
   MG_LAUNCH(k_ab2_rhs, nblocks(D(s->tmpT).n()), kBlock, mi->stream, D(s->tmpT), D(s->FT), D(s->FnmT), D(s->LT),
-            D(s->T), D(s->Tnm1), P.dt, wb, 6);
+            D(s->T), D(s->Tnm1), P.dt, wb, 6, 1);
   MG_CUDA(cudaGetLastError());
   if (P.solve_method_T == 2) return copy(mi, s->T, s->tmpT);  // X = X + dt AB2 (no diffusion solve)
   const double c = P.dt * 1.0 * P.coeff_implicit_T;
@@ -546,7 +563,7 @@ int step_once(moons_mhd* s) {
   }
   if (!r && P.energy && P.scale_buoyancy != 0.0) r = add_buoyancy(s);
   if (r) return r;
-  // ---- solve_momentum (solve_method 5, 6 or 7)
+  // ---- solve_momentum (solve_method 1 to 7)
   r = euler_ab2(s, m, s->pcgU, s->pcgP, P.isp_U, P.isp_p, s->U, s->Ustar, s->Unm1, s->p, s->F, s->Fnm1, s->L, s->tF1,
                 s->tCC, P.coeff_implicit_U, &s->coefU, 0, 1, &s->res_p, time_method(P.solve_method_U));
   if (r) return r;
@@ -618,7 +635,7 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
     return MOONS_ERR_ARG;
   }
   if (!time_method_ok(prm->solve_method_U) || !time_method_ok(prm->solve_method_B)) {
-    set_error("moons_mhd_create: solve_method_U and solve_method_B must be 0, 5, 6 or 7");
+    set_error("moons_mhd_create: solve_method_U and solve_method_B must be 0 to 7");
     return MOONS_ERR_ARG;
   }
   auto* s = new moons_mhd();

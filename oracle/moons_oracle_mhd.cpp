@@ -437,51 +437,80 @@ struct MHD {
     }
   }
 
-  // The implicit schemes of solve_momentum / solve_induction
+  // The time schemes of solve_momentum / solve_induction
   // (momentum_extend.f90:335-367, induction_extend.f90:484-514), selected by
-  // solve_method: 6 = Euler_time_AB2_sources (time_marching_methods.f90:
-  // 117-150), 5 = Euler_time_Euler_sources (:47-79), 7 =
-  // O2_BDF_time_AB2_sources (:81-115); each ends in clean_div_PCG.
+  // solve_method (time_marching_methods.f90):
+  //   1 Euler_time_no_diff_Euler_sources_no_correction (:349-366)
+  //   2 Euler_time_no_diff_AB2_sources_no_correction (:329-347)
+  //   3 Euler_time_no_diff_Euler_sources (:298-327)
+  //   4 Euler_time_no_diff_AB2_sources (:266-296)
+  //   5 Euler_time_Euler_sources (:47-79)
+  //   6 Euler_time_AB2_sources (:117-150)
+  //   7 O2_BDF_time_AB2_sources (:81-115)
+  // 3 to 7 end in clean_div_PCG (clean_divergence.f90:37-59).
   void euler_ab2(PCG& pv, PCG& ps, ISP& iv, ISP& is, SF* X, SF* Xstar, SF* Xnm1, SF& ph, SF* Fn, SF* Fm, SF* Lx,
                  SF* t1, SF& tcc, const Grid& g, double coeff_implicit, int slot_v, int slot_s, double* res_s,
                  int method) {
     const double two_thirds = 2.0 / 3.0, four_thirds = 4.0 / 3.0, neg_one_third = -1.0 / 3.0;
     double dt = P.dt;
-    for (int c = 0; c < 3; c++) {
-      if (method == 5) {
-        assign(t1[c], Fn[c]);
-        multiply(t1[c], dt);
-        assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
-        add(t1[c], X[c]);
-      } else {
-        // AB2_VF (AB2.f90:53-64): AB2 = Fn*1.5 ; AB2 += Fnm1*(-0.5)
-        for (size_t i = 0; i < t1[c].n(); i++) t1[c].f[i] = Fn[c].f[i] * 1.5;
-        add_product(t1[c], Fm[c], -0.5);
-        if (method == 6) {
+    // AB2_VF (AB2.f90:53-64): AB2 = Fn*1.5 ; AB2 += Fnm1*(-0.5)
+    auto ab2 = [&](SF& o, int c) {
+      for (size_t i = 0; i < o.n(); i++) o.f[i] = Fn[c].f[i] * 1.5;
+      add_product(o, Fm[c], -0.5);
+    };
+    if (method <= 4) {
+      for (int c = 0; c < 3; c++) {
+        if (method == 1 || method == 3) {
+          assign(Xstar[c], Fn[c]);  // multiply(Xstar,F,dt)
+          multiply(Xstar[c], dt);
+        } else {
+          ab2(Xstar[c], c);
+          multiply(Xstar[c], dt);
+        }
+        assign_wall_Dirichlet(Xstar[c], 0.0, &X[c]);
+        if (method <= 2) {
+          add(X[c], Xstar[c]);
+          apply_BCs(X[c]);
+        } else {
+          add(Xstar[c], X[c]);
+          assign(Xnm1[c], X[c]);
+        }
+      }
+      if (method <= 2) return;
+    } else {
+      for (int c = 0; c < 3; c++) {
+        if (method == 5) {
+          assign(t1[c], Fn[c]);
+          multiply(t1[c], dt);
+          assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
+          add(t1[c], X[c]);
+        } else if (method == 6) {
+          ab2(t1[c], c);
           add(t1[c], Lx[c]);
           multiply(t1[c], dt);
           assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
           add(t1[c], X[c]);
         } else {
+          ab2(t1[c], c);
           multiply(t1[c], two_thirds * dt);
           assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
           add_product(t1[c], X[c], four_thirds);
           add_product(t1[c], Xnm1[c], neg_one_third);
         }
+        assign(Xnm1[c], X[c]);
       }
-      assign(Xnm1[c], X[c]);
+      // update_MFP: method 6 rebuilds the preconditioner every step, methods 5
+      // and 7 while TMP%n_step <= 2
+      if (method == 6) pv.update_MFP(dt * 1.0 * coeff_implicit, true);
+      else if (method == 5) pv.update_MFP(dt * 1.0 * coeff_implicit, n_step <= 2);
+      else pv.update_MFP(dt * two_thirds * coeff_implicit, n_step <= 2);
+      SF* xs[3] = {&Xstar[0], &Xstar[1], &Xstar[2]};
+      SF* bs[3] = {&t1[0], &t1[1], &t1[2]};
+      SolveInfo si = pv.solve(xs, bs, iv);
+      iters[slot_v] += si.iterations;
     }
-    // update_MFP: method 6 rebuilds the preconditioner every step, methods 5
-    // and 7 while TMP%n_step <= 2
-    if (method == 6) pv.update_MFP(dt * 1.0 * coeff_implicit, true);
-    else if (method == 5) pv.update_MFP(dt * 1.0 * coeff_implicit, n_step <= 2);
-    else pv.update_MFP(dt * two_thirds * coeff_implicit, n_step <= 2);
-    SF* xs[3] = {&Xstar[0], &Xstar[1], &Xstar[2]};
-    SF* bs[3] = {&t1[0], &t1[1], &t1[2]};
-    SolveInfo si = pv.solve(xs, bs, iv);
-    iters[slot_v] += si.iterations;
     // clean_div_PCG (clean_divergence.f90:37-59), scale = 1/dt for method 6,
-    // 1 for methods 5 and 7
+    // 1 for the others
     double scale = method == 6 ? 1.0 / dt : 1.0;
     div(tcc, Xstar[0], Xstar[1], Xstar[2], g);
     multiply(tcc, scale);
@@ -530,7 +559,7 @@ struct MHD {
       }
     }
     if (P.energy && P.scale_buoyancy != 0.0) add_buoyancy();
-    // ---- solve_momentum (solve_method 5, 6 or 7; 0 = 6)
+    // ---- solve_momentum (solve_method 1 to 7; 0 = 6)
     euler_ab2(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p,
               P.solve_method_U ? P.solve_method_U : 6);
     for (int c = 0; c < 3; c++) interp(UCC[c], U[c], gm, c + 1);
@@ -647,7 +676,7 @@ struct OSFView {
 extern "C" {
 void* or_mhd_create(void* mesh_mom, void* mesh_ind, const moons_mhd_params* prm) {
   for (int m : {prm->solve_method_U, prm->solve_method_B})
-    if (m != 0 && m != 5 && m != 6 && m != 7) return nullptr;  // solve_method 5, 6, 7 (0 = 6)
+    if (m < 0 || m > 7) return nullptr;  // solve_method 1 to 7 (0 = 6)
   auto* s = new mo::MHD();
   const mo::Grid& gm = ((OMeshView*)mesh_mom)->g;
   const mo::Grid& gi = ((OMeshView*)mesh_ind)->g;

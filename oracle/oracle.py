@@ -262,7 +262,7 @@ class MHD:
         self.params = params
         self.h = lib().or_mhd_create(mesh_mom.h, mesh_ind.h, C.byref(params))
         if not self.h:
-            raise ValueError("or_mhd_create: solve_method_U and solve_method_B must be 0, 5, 6 or 7")
+            raise ValueError("or_mhd_create: solve_method_U and solve_method_B must be 0 to 7")
 
     def shape(self, which, comp=0):
         s = (C.c_int * 3)()

@@ -107,13 +107,27 @@ def test_mhd_steps_multigrid_poisson(name, builder, kw, prec):
 SCHEME_CASES = [CASES[1], CASES[2]]  # LDC in the B form, the duct with walls
 
 
-@pytest.mark.parametrize("method", [5, 7])
+def explicit_diffusion(builder):
+    """builder with the diffusion terms in the sources (beta = 1,
+    var_set_extend.f90:55-86), as the schemes without a diffusion solve use."""
+    def b(*a, **kw):
+        mom, ind, prm, init = builder(*a, **kw)
+        prm.scale_diffusion_U = -prm.coeff_implicit_U
+        prm.scale_diffusion_B = -1.0
+        return mom, ind, prm, init
+    return b
+
+
+@pytest.mark.parametrize("method", [1, 2, 3, 4, 5, 7])
 @pytest.mark.parametrize("name,builder,kw", SCHEME_CASES, ids=[c[0] for c in SCHEME_CASES])
 def test_mhd_time_schemes_match_oracle(name, builder, kw, method):
-    """solve_method 5 (Euler_time_Euler_sources) and 7 (O2_BDF_time_AB2_sources,
-    time_marching_methods.f90:47-115) for both the momentum and the induction
-    step: 4 steps against the oracle's restatement of the same schemes, every
-    field within the step test's 1e-10."""
+    """solve_method 1 to 5 and 7 (time_marching_methods.f90:47-115, :266-366)
+    for both the momentum and the induction step: 4 steps against the oracle's
+    restatement of the same schemes, every field within the step test's 1e-10.
+    The schemes without a diffusion solve (1 to 4) take the diffusion in the
+    sources."""
+    if method <= 4:
+        builder = explicit_diffusion(builder)
     g = configs.make(G, builder, seed=3, solve_method_U=method, solve_method_B=method, **kw)
     o = configs.make(O, builder, seed=3, solve_method_U=method, solve_method_B=method, **kw)
     nsteps = 4
@@ -135,7 +149,7 @@ def test_mhd_time_schemes_match_oracle(name, builder, kw, method):
 @pytest.mark.parametrize("field", ["solve_method_U", "solve_method_B"])
 def test_mhd_rejects_unknown_time_scheme(field):
     mom, ind, prm, _ = configs.ldc(n=6, induction=G.IND_B)
-    setattr(prm, field, 4)
+    setattr(prm, field, 8)
     mm = G.Mesh(*mom)
     with pytest.raises(G.MoonsError) as e:
         G.MHD(mm, mm, prm)

@@ -1,12 +1,18 @@
-"""The oracle's three implicit time schemes of the momentum and induction
-steps (solve_method 5, 6, 7: Euler_time_Euler_sources, Euler_time_AB2_sources,
-O2_BDF_time_AB2_sources, time_marching_methods.f90:47-150), on the CPU.
+"""The oracle's time schemes of the momentum and induction steps, solve_method
+1 to 7 (time_marching_methods.f90:47-150, :266-366), on the CPU.
 
-Properties that hold whatever the scheme: each step ends divergence-free
-(clean_div with its scale), and the three schemes integrate the same
-equations, so over a fixed interval their increments agree to O(dt) and the
-disagreement shrinks as dt does.  A scheme number outside 0, 5, 6, 7 is
-refused at create, as the reference's select case stops."""
+Properties that pin each scheme's arithmetic without a second implementation:
+* the implicit schemes (5, 6, 7) integrate the same equations, so over a fixed
+  interval their increments agree to O(dt): the disagreement halves with dt;
+* with a zero implicit coefficient the implicit operator is the identity, so
+  Euler_time_Euler_sources (5) reduces to Euler_time_no_diff_Euler_sources (3)
+  and Euler_time_AB2_sources (6) to Euler_time_no_diff_AB2_sources (4);
+* every scheme but the two "no_correction" ones ends divergence-free;
+* the "no_correction" schemes (1, 2) are one explicit update: over one step
+  the velocity increment is linear in dt, and AB2's first step (Fnm1 = 0) is
+  exactly 1.5 times Euler's;
+* a scheme number outside 0..7 is refused at create, as the reference's
+  select case stops."""
 import numpy as np
 import pytest
 
@@ -14,10 +20,27 @@ import oracle.oracle as O
 from moons_b200 import configs
 from moons_b200.capi import IND_B, MHD_U, MHD_B
 
+LDC = dict(n=6, induction=IND_B)
 
-def run(method, dt, nsteps):
-    sim = configs.make(O, configs.ldc, seed=3, n=6, induction=IND_B, dt=dt, tol=1e-12,
-                       solve_method_U=method, solve_method_B=method)
+
+def with_params(builder, **fields):
+    """builder whose parameters get ``fields`` (callables take the params)."""
+    def b(*a, **kw):
+        mom, ind, prm, init = builder(*a, **kw)
+        for k, v in fields.items():
+            setattr(prm, k, v(prm) if callable(v) else v)
+        return mom, ind, prm, init
+    return b
+
+
+# explicit diffusion (beta = 1, var_set_extend.f90:55-86): F_U += (1/Re) lap U,
+# F_B += -curl(sigma^-1 J)
+explicit_diffusion = dict(scale_diffusion_U=lambda p: -p.coeff_implicit_U, scale_diffusion_B=-1.0)
+
+
+def run(method, dt, nsteps, builder=configs.ldc, **kw):
+    sim = configs.make(O, builder, seed=3, dt=dt, tol=1e-12, solve_method_U=method, solve_method_B=method,
+                       **(kw or LDC))
     u0 = [sim.download(MHD_U, c).copy() for c in range(3)]
     b0 = [sim.download(MHD_B, c).copy() for c in range(3)]
     sim.step(nsteps)
@@ -27,15 +50,16 @@ def run(method, dt, nsteps):
 
 
 @pytest.mark.parametrize("field", ["solve_method_U", "solve_method_B"])
-def test_unknown_scheme_refused(field):
+@pytest.mark.parametrize("bad", [-1, 8, 9])
+def test_unknown_scheme_refused(field, bad):
     mom, ind, prm, _ = configs.ldc(n=6, induction=IND_B)
-    setattr(prm, field, 8)
+    setattr(prm, field, bad)
     mm = O.Mesh(*mom)
     with pytest.raises(ValueError):
         O.MHD(mm, mm, prm)
 
 
-def test_schemes_agree_to_first_order_in_dt():
+def test_implicit_schemes_agree_to_first_order_in_dt():
     T = 8e-3
     gaps = []
     for dt in (2e-3, 1e-3):
@@ -51,3 +75,27 @@ def test_schemes_agree_to_first_order_in_dt():
         assert gap < 0.2, (dt, gap)
     # halving dt halves (about) the disagreement between the schemes
     assert gaps[1] < 0.75 * gaps[0], gaps
+
+
+@pytest.mark.parametrize("explicit,implicit", [(3, 5), (4, 6)])
+def test_implicit_scheme_reduces_to_explicit_at_zero_coefficient(explicit, implicit):
+    b = with_params(configs.ldc, coeff_implicit_U=0.0, coeff_implicit_B=0.0)
+    se, due, dbe = run(explicit, 1e-3, 4, b, **LDC)
+    si, dui, dbi = run(implicit, 1e-3, 4, b, **LDC)
+    assert np.linalg.norm(due - dui) <= 1e-8 * np.linalg.norm(dui)
+    assert np.linalg.norm(dbe - dbi) <= 1e-8 * np.linalg.norm(dbi)
+    duv, dbv = se.divergence()
+    assert duv < 1e-18 and dbv < 1e-18
+
+
+def test_no_correction_schemes_are_one_explicit_update():
+    b = with_params(configs.ldc, **explicit_diffusion)
+    _, du1, _ = run(1, 1e-3, 1, b, **LDC)
+    _, du1b, _ = run(1, 2e-3, 1, b, **LDC)
+    _, du2, _ = run(2, 1e-3, 1, b, **LDC)
+    _, du2b, _ = run(2, 2e-3, 1, b, **LDC)
+    assert np.linalg.norm(du1) > 0
+    assert np.linalg.norm(du1b - 2 * du1) <= 1e-11 * np.linalg.norm(du1b)
+    assert np.linalg.norm(du2b - 2 * du2) <= 1e-11 * np.linalg.norm(du2b)
+    # AB2(F, Fnm1) = 1.5 F - 0.5 Fnm1 with Fnm1 = 0 on the first step
+    assert np.linalg.norm(du2 - 1.5 * du1) <= 1e-11 * np.linalg.norm(du2)
