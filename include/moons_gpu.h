@@ -324,10 +324,27 @@ typedef struct {
    *           Euler_time_no_diff_AB2_sources (:266-296), no diffusion solve:
    *           X* = X + dt F or X + dt AB2(F, Fnm1), clean_div scale 1;
    *   1, 2:   the same without the projection (:329-366): X += dt F or
-   *           dt AB2(F, Fnm1), then X's BCs.
+   *           dt AB2(F, Fnm1), then X's BCs;
+   *   8:      Euler_time_RK_sources (:186-208), with rk_stages below.
    * Source terms on wall-normal Dirichlet faces are zeroed in all of them. */
   int solve_method_U;
   int solve_method_B;
+  /* Runge-Kutta stages of the step (RKP%n_stages, the stage loop of
+   * solve_MOONS, MOONS_solver.f90:73-97): 0 or 1 = one stage with the
+   * inactive coefficients (all 1), 3 = the three-stage low-storage scheme of
+   * init_RKP (RK_params_extend.f90:22-55).  Every stage runs the sources and
+   * the solves of the whole step; solve_method 8 (Euler_time_RK_sources,
+   * time_marching_methods.f90:186-208) uses the stage's coefficients:
+   * (I + 2 beta dt c A) X* = X + dt (gamma F + zeta Fnm1 + 2 alpha L),
+   * clean_div scale 1.  The energy equation takes no RK stages here. */
+  int rk_stages;
+  /* SP%MT%diffusion_linear / SP%IT%diffusion_linear: the diffusion term into
+   * L instead of F (add_all_momentum_sources.f90:49-51,
+   * add_all_induction_sources.f90:39-41), with the diffusion scale:
+   * L_U += s lap(U), L_B += s curl(sigma^-1 J).  Only Euler_time_AB2_sources
+   * (6) and Euler_time_RK_sources (8) read L. */
+  double scale_diffusion_linear_U;
+  double scale_diffusion_linear_B;
 } moons_mhd_params;
 
 typedef struct {

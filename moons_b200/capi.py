@@ -119,6 +119,9 @@ class MHDParams(C.Structure):
         ("scale_joule_heating_T", C.c_double),
         ("solve_method_U", C.c_int),
         ("solve_method_B", C.c_int),
+        ("rk_stages", C.c_int),
+        ("scale_diffusion_linear_U", C.c_double),
+        ("scale_diffusion_linear_B", C.c_double),
     ]
 
 

@@ -31,24 +31,34 @@ namespace mg {
 //  7, O2_BDF_time_AB2_sources (:104-108):
 //   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t*(2/3 dt) ;
 //   assign_wall_Dirichlet(t,0,X) ; t = t + X*(4/3) ; t = t + Xnm1*(-1/3)
+//  8, Euler_time_RK_sources (:217-222), with the stage's a = (dt gamma,
+//   dt zeta, (dt 2) alpha):
+//   t = F*a0 ; t = t + Fnm1*a1 ; t = t + L*a2 ; assign_wall_Dirichlet(t,0,X) ;
+//   t = t + X
 // then Xnm1 = X when set_nm1 (every scheme but the two "no_correction" ones,
 // whose t is X itself: X = X + increment).  dts is dt, or the product 2/3*dt
 // for form 7.  t may alias X: each point reads X and Xnm1 before writing t.
 __global__ void k_ab2_rhs(DF t, DF F, DF Fm, DF L, DF X, DF Xnm1, double dts, int wallbits, int form,
-                          int set_nm1) {
+                          int set_nm1, double a0, double a1, double a2) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= t.n()) return;
   int i, j, k;
   ijk_of(idx, t, i, j, k);
   double v;
-  if (form == 5) {
-    v = F.f[idx];
+  if (form == 8) {
+    v = F.f[idx] * a0;
+    v = v + Fm.f[idx] * a1;
+    v = v + L.f[idx] * a2;
   } else {
-    v = F.f[idx] * 1.5;
-    v = v + Fm.f[idx] * (-0.5);
-    if (form == 6) v = v + L.f[idx];
+    if (form == 5) {
+      v = F.f[idx];
+    } else {
+      v = F.f[idx] * 1.5;
+      v = v + Fm.f[idx] * (-0.5);
+      if (form == 6) v = v + L.f[idx];
+    }
+    v = v * dts;
   }
-  v = v * dts;
   if (wallbits) {
     if (((wallbits & 1) && i == 2) || ((wallbits & 2) && i == t.s0 - 1) || ((wallbits & 4) && j == 2) ||
         ((wallbits & 8) && j == t.s1 - 1) || ((wallbits & 16) && k == 2) || ((wallbits & 32) && k == t.s2 - 1))
@@ -128,8 +138,21 @@ using namespace mg;
 
 namespace {
 inline int orth(int a, int b) { return 6 - a - b; }  // 1-based directions
-// solve_method of the momentum / induction step: 1 to 7, 0 selects the default, 6
-inline bool time_method_ok(int m) { return m >= 0 && m <= 7; }
+// solve_method of the momentum / induction step: 1 to 8, 0 selects the default, 6
+inline bool time_method_ok(int m) { return m >= 0 && m <= 8; }
+// RK_Params of one stage (init_RKP, RK_params_extend.f90:22-55): the
+// three-stage coefficients of Lundbladh et al. (1999), or all 1 when the
+// step has one stage (RK inactive); beta = alpha
+struct RKStage {
+  double gamma, zeta, alpha, beta;
+};
+inline RKStage rk_stage(int stages, int n) {
+  if (stages != 3) return {1.0, 1.0, 1.0, 1.0};
+  static const double g[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+  static const double z[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+  static const double a[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+  return {g[n - 1], z[n - 1], a[n - 1], a[n - 1]};
+}
 inline int time_method(int m) { return m == 0 ? 6 : m; }
 }
 
@@ -252,9 +275,9 @@ int solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp&
   return mg_pcg_enqueue(s, x, b, &isp);
 }
 
-// One solve_momentum / solve_induction time step for solve_method 1 to 7
-// (time_marching_methods.f90:47-150, :266-366, clean_divergence.f90:37-59):
-//  5, 6, 7: the scheme's RHS, update_MFP with its implicit factor, the PCG
+// One solve_momentum / solve_induction time step for solve_method 1 to 8
+// (time_marching_methods.f90:47-208, :266-366, clean_divergence.f90:37-59):
+//  5 to 8:  the scheme's RHS, update_MFP with its implicit factor, the PCG
 //           solve for X*, then clean_div;
 //  3, 4:    X* = X + dt F (Euler) or X + dt AB2(F, Fnm1), then clean_div;
 //  1, 2:    X = X + dt F or X + dt AB2(F, Fnm1), then apply_BCs(X).
@@ -262,16 +285,19 @@ int solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp&
 int euler_ab2(moons_mhd* s, moons_mesh* m, moons_pcg* pv, moons_pcg* ps, const moons_isp& iv, const moons_isp& is,
               moons_sf** X, moons_sf** Xstar, moons_sf** Xnm1, moons_sf* ph, moons_sf** Fn, moons_sf** Fm,
               moons_sf** Lx, moons_sf** t1, moons_sf* tcc, double coeff_implicit, double* coef_cache, int slot_v,
-              int slot_s, double* res_s, int method) {
+              int slot_s, double* res_s, int method, const RKStage& rk) {
   double dt = s->P.dt;
   double dts = method == 7 ? (2.0 / 3.0) * dt : dt;
+  // multiply(temp_F1,F,dt*gamma) ; add_product(temp_F1,Fnm1,dt*zeta) ;
+  // add_product(temp_F1,L,dt*2*alpha)
+  const double a0 = dt * rk.gamma, a1 = dt * rk.zeta, a2 = dt * 2.0 * rk.alpha;
   const int form = (method == 1 || method == 3 || method == 5) ? 5 : (method == 2 || method == 4) ? 4 : method;
-  const bool no_correction = method <= 2, implicit = method >= 5;
+  const bool no_correction = method <= 2, implicit = method >= 5;  // 5 to 8
   moons_sf** out = no_correction ? X : implicit ? t1 : Xstar;
   for (int c = 0; c < 3; c++) {
     int wb = dirichlet_wall_bits(X[c]->bc.defined ? &X[c]->bc : nullptr, D(X[c]).dl);
     MG_LAUNCH(k_ab2_rhs, nblocks(D(out[c]).n()), kBlock, m->stream, D(out[c]), D(Fn[c]), D(Fm[c]), D(Lx[c]),
-              D(X[c]), D(Xnm1[c]), dts, wb, form, no_correction ? 0 : 1);
+              D(X[c]), D(Xnm1[c]), dts, wb, form, no_correction ? 0 : 1, a0, a1, a2);
   }
   int r;
   if (no_correction) {
@@ -281,11 +307,13 @@ int euler_ab2(moons_mhd* s, moons_mesh* m, moons_pcg* pv, moons_pcg* ps, const m
     return MOONS_OK;
   }
   MG_CUDA(cudaGetLastError());
-  // update_MFP(PCG, m, dt*f*coeff_implicit, ...) with f = 1 or 2/3; the
-  // preconditioner only changes with c, so it is rebuilt when c changes
-  // (methods 5 and 7 rebuild it on the first steps only, TMP%n_step <= 2,
-  // which is the same thing for a fixed dt)
-  double c = method == 7 ? dt * (2.0 / 3.0) * coeff_implicit : dt * 1.0 * coeff_implicit;
+  // update_MFP(PCG, m, dt*f*coeff_implicit, ...) with f = 1, 2/3 or, for
+  // method 8, 2*beta; the preconditioner only changes with c, so it is rebuilt
+  // when c changes (methods 5 and 7 rebuild it on the first steps only,
+  // TMP%n_step <= 2, which is the same thing for a fixed dt)
+  double c = method == 7   ? dt * (2.0 / 3.0) * coeff_implicit
+             : method == 8 ? dt * 2.0 * rk.beta * coeff_implicit
+                           : dt * 1.0 * coeff_implicit;
   if (implicit && !(c == *coef_cache)) {
     if ((r = moons_pcg_update_mfp(pv, c, 1))) return r;
     *coef_cache = c;
@@ -495,7 +523,7 @@ int energy_step(moons_mhd* s) {
   // X* = X + dt AB2(F, Fnm1) (wall-Dirichlet points of the increment zeroed)
   const int wb = dirichlet_wall_bits(s->T->bc.defined ? &s->T->bc : nullptr, D(s->T).dl);
   MG_LAUNCH(k_ab2_rhs, nblocks(D(s->tmpT).n()), kBlock, mi->stream, D(s->tmpT), D(s->FT), D(s->FnmT), D(s->LT),
-            D(s->T), D(s->Tnm1), P.dt, wb, 6, 1);
+            D(s->T), D(s->Tnm1), P.dt, wb, 6, 1, 0.0, 0.0, 0.0);
   MG_CUDA(cudaGetLastError());
   if (P.solve_method_T == 2) return copy(mi, s->T, s->tmpT);  // X = X + dt AB2 (no diffusion solve)
   const double c = P.dt * 1.0 * P.coeff_implicit_T;
@@ -525,7 +553,8 @@ int add_buoyancy(moons_mhd* s) {
   return r;
 }
 
-int step_once(moons_mhd* s) {
+// One stage of the step (the body of the RK stage loop, MOONS_solver.f90:73-97)
+int step_once(moons_mhd* s, const RKStage& rk) {
   moons_mesh* m = s->mm;
   const moons_mhd_params& P = s->P;
   double dt = P.dt;
@@ -553,6 +582,14 @@ int step_once(moons_mhd* s) {
       if (!r) r = launch_pw(m, PW_ADD_PRODUCT, D(s->F[c]), &D(s->tF1[c]), P.scale_diffusion_U);
     }
   }
+  if (!r && P.scale_diffusion_linear_U != 0.0) {  // diffusion_linear: compute_add_diffusion(L, ...)
+    for (int c = 0; c < 3 && !r; c++) {
+      r = launch_del(m, D(s->tF1[c]), D(s->U[c]), 2, 1, 0, 1);
+      if (!r) r = launch_del(m, D(s->tF1[c]), D(s->U[c]), 2, 2, 0, 2);
+      if (!r) r = launch_del(m, D(s->tF1[c]), D(s->U[c]), 2, 3, 0, 2);
+      if (!r) r = launch_pw(m, PW_ADD_PRODUCT, D(s->L[c]), &D(s->tF1[c]), P.scale_diffusion_linear_U);
+    }
+  }
   if (!r && P.induction != MOONS_IND_OFF) {
     for (int c = 0; c < 3 && !r; c++) {
       if (s->same) r = copy(m, s->tF1[c], s->jxb[c]);
@@ -565,7 +602,7 @@ int step_once(moons_mhd* s) {
   if (r) return r;
   // ---- solve_momentum (solve_method 1 to 7)
   r = euler_ab2(s, m, s->pcgU, s->pcgP, P.isp_U, P.isp_p, s->U, s->Ustar, s->Unm1, s->p, s->F, s->Fnm1, s->L, s->tF1,
-                s->tCC, P.coeff_implicit_U, &s->coefU, 0, 1, &s->res_p, time_method(P.solve_method_U));
+                s->tCC, P.coeff_implicit_U, &s->coefU, 0, 1, &s->res_p, time_method(P.solve_method_U), rk);
   if (r) return r;
   for (int c = 0; c < 3 && !r; c++) r = launch_interp(m, D(s->UCC[c]), D(s->U[c]), c + 1);
   if (!r) r = face2edge_nd(m, s->UE, s->U);
@@ -589,6 +626,15 @@ int step_once(moons_mhd* s) {
     if (!r) r = curl3(mi, s->curlUxB, s->tE);
     for (int c = 0; c < 3 && !r; c++)
       r = launch_pw(mi, PW_ADD_PRODUCT, D(s->Fi[c]), &D(s->curlUxB[c]), P.scale_advection_B);
+    if (!r && P.scale_diffusion_linear_B != 0.0) {  // diffusion_linear: add_curl_J(L, ...)
+      for (int c = 0; c < 3 && !r; c++) {
+        r = copy(mi, s->tE[c], s->J[c]);
+        if (!r) r = launch_pw(mi, PW_MUL, D(s->tE[c]), &D(s->sig[c]), 0.0);
+      }
+      if (!r) r = curl3(mi, s->tFi2, s->tE);
+      for (int c = 0; c < 3 && !r; c++)
+        r = launch_pw(mi, PW_ADD_PRODUCT, D(s->Li[c]), &D(s->tFi2[c]), P.scale_diffusion_linear_B);
+    }
     if (!r && P.scale_diffusion_B != 0.0) {
       for (int c = 0; c < 3 && !r; c++) {
         r = copy(mi, s->tE[c], s->J[c]);
@@ -601,7 +647,7 @@ int step_once(moons_mhd* s) {
     if (r) return r;
     r = euler_ab2(s, mi, s->pcgB, s->pcgPhi, P.isp_B, P.isp_phi, s->B, s->Bstar, s->Bnm1, s->phi, s->Fi, s->Fnm1i,
                   s->Li, s->tFi1, s->tCCi, P.coeff_implicit_B, &s->coefB, 2, 3, &s->res_phi,
-                  time_method(P.solve_method_B));
+                  time_method(P.solve_method_B), rk);
     if (!r) r = compute_J(s);
     if (!r) r = compute_Btot(s);
     if (!r) r = compute_JxB(s);
@@ -635,7 +681,15 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
     return MOONS_ERR_ARG;
   }
   if (!time_method_ok(prm->solve_method_U) || !time_method_ok(prm->solve_method_B)) {
-    set_error("moons_mhd_create: solve_method_U and solve_method_B must be 0 to 7");
+    set_error("moons_mhd_create: solve_method_U and solve_method_B must be 0 to 8");
+    return MOONS_ERR_ARG;
+  }
+  if (prm->rk_stages != 0 && prm->rk_stages != 1 && prm->rk_stages != 3) {
+    set_error("moons_mhd_create: rk_stages must be 0, 1 or 3");
+    return MOONS_ERR_ARG;
+  }
+  if (prm->rk_stages == 3 && prm->energy) {
+    set_error("moons_mhd_create: the energy equation takes no RK stages");
     return MOONS_ERR_ARG;
   }
   auto* s = new moons_mhd();
@@ -904,9 +958,9 @@ int moons_mhd_step(moons_mhd* s, int nsteps, moons_step_info* info) {
   cudaEventCreate(&e1);
   cudaEventRecord(e0, m->stream);
   int r = MOONS_OK;
-  for (int n = 0; n < nsteps && !r; n++) {
-    r = step_once(s);
-  }
+  const int stages = s->P.rk_stages == 3 ? 3 : 1;
+  for (int n = 0; n < nsteps && !r; n++)
+    for (int st = 1; st <= stages && !r; st++) r = step_once(s, rk_stage(stages, st));
   cudaEventRecord(e1, m->stream);
   cudaError_t e = cudaStreamSynchronize(m->stream);
   float ms = 0;

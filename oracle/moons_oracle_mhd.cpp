@@ -88,6 +88,20 @@ static void embed_extract(SF& dst, const SF& src, const int o[3], bool embed) {
       }
 }
 
+// RK_Params of one stage (init_RKP, RK_params_extend.f90:22-55): the
+// three-stage coefficients of Lundbladh et al. (1999), or all 1 when the
+// step has one stage (RK inactive); beta = alpha
+struct RKStage {
+  double gamma, zeta, alpha, beta;
+};
+inline RKStage rk_stage(int stages, int n) {
+  if (stages != 3) return {1.0, 1.0, 1.0, 1.0};
+  const double g[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+  const double z[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+  const double a[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+  return {g[n - 1], z[n - 1], a[n - 1], a[n - 1]};
+}
+
 struct MHD {
   Grid gm, gi;
   bool same = true;
@@ -447,10 +461,11 @@ struct MHD {
   //   5 Euler_time_Euler_sources (:47-79)
   //   6 Euler_time_AB2_sources (:117-150)
   //   7 O2_BDF_time_AB2_sources (:81-115)
-  // 3 to 7 end in clean_div_PCG (clean_divergence.f90:37-59).
+  //   8 Euler_time_RK_sources (:186-208), with the stage's RK_Params
+  // 3 to 8 end in clean_div_PCG (clean_divergence.f90:37-59).
   void euler_ab2(PCG& pv, PCG& ps, ISP& iv, ISP& is, SF* X, SF* Xstar, SF* Xnm1, SF& ph, SF* Fn, SF* Fm, SF* Lx,
                  SF* t1, SF& tcc, const Grid& g, double coeff_implicit, int slot_v, int slot_s, double* res_s,
-                 int method) {
+                 int method, const RKStage& rk) {
     const double two_thirds = 2.0 / 3.0, four_thirds = 4.0 / 3.0, neg_one_third = -1.0 / 3.0;
     double dt = P.dt;
     // AB2_VF (AB2.f90:53-64): AB2 = Fn*1.5 ; AB2 += Fnm1*(-0.5)
@@ -490,6 +505,14 @@ struct MHD {
           multiply(t1[c], dt);
           assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
           add(t1[c], X[c]);
+        } else if (method == 8) {
+          // multiply(temp_F1,F,dt*gamma) ; add_product(temp_F1,Fnm1,dt*zeta) ;
+          // add_product(temp_F1,L,dt*2*alpha)
+          for (size_t i = 0; i < t1[c].n(); i++) t1[c].f[i] = Fn[c].f[i] * (dt * rk.gamma);
+          add_product(t1[c], Fm[c], dt * rk.zeta);
+          add_product(t1[c], Lx[c], dt * 2.0 * rk.alpha);
+          assign_wall_Dirichlet(t1[c], 0.0, &X[c]);
+          add(t1[c], X[c]);
         } else {
           ab2(t1[c], c);
           multiply(t1[c], two_thirds * dt);
@@ -499,9 +522,10 @@ struct MHD {
         }
         assign(Xnm1[c], X[c]);
       }
-      // update_MFP: method 6 rebuilds the preconditioner every step, methods 5
-      // and 7 while TMP%n_step <= 2
+      // update_MFP: methods 6 and 8 rebuild the preconditioner every call,
+      // methods 5 and 7 while TMP%n_step <= 2
       if (method == 6) pv.update_MFP(dt * 1.0 * coeff_implicit, true);
+      else if (method == 8) pv.update_MFP(dt * 2.0 * rk.beta * coeff_implicit, true);
       else if (method == 5) pv.update_MFP(dt * 1.0 * coeff_implicit, n_step <= 2);
       else pv.update_MFP(dt * two_thirds * coeff_implicit, n_step <= 2);
       SF* xs[3] = {&Xstar[0], &Xstar[1], &Xstar[2]};
@@ -528,7 +552,15 @@ struct MHD {
     }
   }
 
+  // solve_MOONS's stage loop (MOONS_solver.f90:73-97): every stage runs the
+  // sources and solves of the whole step; TMP%n_step advances once per step
   void step() {
+    const int stages = P.rk_stages == 3 ? 3 : 1;
+    for (int n = 1; n <= stages; n++) step_stage(rk_stage(stages, n));
+    n_step++;
+  }
+
+  void step_stage(const RKStage& rk) {
     double dt = P.dt;
     if (P.energy) energy_step();
     // ---- add_all_momentum_sources
@@ -550,6 +582,12 @@ struct MHD {
         add_product(F[c], tF1[c], P.scale_diffusion_U);
       }
     }
+    if (P.scale_diffusion_linear_U != 0.0) {  // diffusion_linear: compute_add_diffusion into L
+      for (int c = 0; c < 3; c++) {
+        lap_uniform_coeff(tF1[c], U[c], gm);
+        add_product(L[c], tF1[c], P.scale_diffusion_linear_U);
+      }
+    }
     if (P.induction != MOONS_IND_OFF) {  // extract_add_JCrossB (momentum_sources.f90:111-121)
       for (int c = 0; c < 3; c++) {
         if (same) assign(tF1[c], jxb[c]);
@@ -559,9 +597,9 @@ struct MHD {
       }
     }
     if (P.energy && P.scale_buoyancy != 0.0) add_buoyancy();
-    // ---- solve_momentum (solve_method 1 to 7; 0 = 6)
+    // ---- solve_momentum (solve_method 1 to 8; 0 = 6)
     euler_ab2(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p,
-              P.solve_method_U ? P.solve_method_U : 6);
+              P.solve_method_U ? P.solve_method_U : 6, rk);
     for (int c = 0; c < 3; c++) interp(UCC[c], U[c], gm, c + 1);
     SF* Up[3] = {&U[0], &U[1], &U[2]};
     face2edge_nd(UE, Up, gm);
@@ -579,6 +617,14 @@ struct MHD {
       cross_TF(tE, UEi, BE);
       curl(curlUxB[0], curlUxB[1], curlUxB[2], tE[0], tE[1], tE[2], gi);
       for (int c = 0; c < 3; c++) add_product(Fi[c], curlUxB[c], P.scale_advection_B);
+      if (P.scale_diffusion_linear_B != 0.0) {  // diffusion_linear: add_curl_J into L
+        for (int c = 0; c < 3; c++) {
+          assign(tE[c], J[c]);
+          multiply(tE[c], sig[c]);
+        }
+        curl(tFi2[0], tFi2[1], tFi2[2], tE[0], tE[1], tE[2], gi);
+        for (int c = 0; c < 3; c++) add_product(Li[c], tFi2[c], P.scale_diffusion_linear_B);
+      }
       if (P.scale_diffusion_B != 0.0) {  // add_curl_J (induction_sources.f90:40-49)
         for (int c = 0; c < 3; c++) {
           assign(tE[c], J[c]);
@@ -588,7 +634,7 @@ struct MHD {
         for (int c = 0; c < 3; c++) add_product(Fi[c], tFi2[c], P.scale_diffusion_B);
       }
       euler_ab2(pcgB, pcgPhi, ispB, ispPhi, B, Bstar, Bnm1, phi, Fi, Fnm1i, Li, tFi1, tCCi, gi, P.coeff_implicit_B,
-                2, 3, &res_phi, P.solve_method_B ? P.solve_method_B : 6);
+                2, 3, &res_phi, P.solve_method_B ? P.solve_method_B : 6, rk);
       compute_J();
       compute_Btot();
       compute_JxB();
@@ -597,7 +643,6 @@ struct MHD {
       potential_solve();
       compute_JxB();
     }
-    n_step++;
   }
 
   // advect_U_convection1 (ops_advect.f90:71-127) into tF3
@@ -676,7 +721,9 @@ struct OSFView {
 extern "C" {
 void* or_mhd_create(void* mesh_mom, void* mesh_ind, const moons_mhd_params* prm) {
   for (int m : {prm->solve_method_U, prm->solve_method_B})
-    if (m < 0 || m > 7) return nullptr;  // solve_method 1 to 7 (0 = 6)
+    if (m < 0 || m > 8) return nullptr;  // solve_method 1 to 8 (0 = 6)
+  if (prm->rk_stages != 0 && prm->rk_stages != 1 && prm->rk_stages != 3) return nullptr;
+  if (prm->rk_stages == 3 && prm->energy) return nullptr;  // no RK energy scheme
   auto* s = new mo::MHD();
   const mo::Grid& gm = ((OMeshView*)mesh_mom)->g;
   const mo::Grid& gi = ((OMeshView*)mesh_ind)->g;

@@ -118,16 +118,32 @@ def explicit_diffusion(builder):
     return b
 
 
-@pytest.mark.parametrize("method", [1, 2, 3, 4, 5, 7])
+def rk3_linear_diffusion(builder):
+    """builder with three RK stages (MOONS_solver.f90:73-97) and the
+    diffusion_linear terms, whose L Euler_time_RK_sources weighs by 2 alpha:
+    half the diffusion explicit through L, the implicit solve keeps its own."""
+    def b(*a, **kw):
+        mom, ind, prm, init = builder(*a, **kw)
+        prm.rk_stages = 3
+        prm.scale_diffusion_linear_U = -0.5 * prm.coeff_implicit_U
+        prm.scale_diffusion_linear_B = -0.5
+        return mom, ind, prm, init
+    return b
+
+
+@pytest.mark.parametrize("method", [1, 2, 3, 4, 5, 7, 8])
 @pytest.mark.parametrize("name,builder,kw", SCHEME_CASES, ids=[c[0] for c in SCHEME_CASES])
 def test_mhd_time_schemes_match_oracle(name, builder, kw, method):
-    """solve_method 1 to 5 and 7 (time_marching_methods.f90:47-115, :266-366)
-    for both the momentum and the induction step: 4 steps against the oracle's
-    restatement of the same schemes, every field within the step test's 1e-10.
-    The schemes without a diffusion solve (1 to 4) take the diffusion in the
-    sources."""
+    """solve_method 1 to 5, 7 and 8 (time_marching_methods.f90:47-208,
+    :266-366) for both the momentum and the induction step: 4 steps against
+    the oracle's restatement of the same schemes, every field within the step
+    test's 1e-10.  The schemes without a diffusion solve (1 to 4) take the
+    diffusion in the sources; Euler_time_RK_sources (8) runs three RK stages
+    per step with the diffusion_linear terms in L."""
     if method <= 4:
         builder = explicit_diffusion(builder)
+    if method == 8:
+        builder = rk3_linear_diffusion(builder)
     g = configs.make(G, builder, seed=3, solve_method_U=method, solve_method_B=method, **kw)
     o = configs.make(O, builder, seed=3, solve_method_U=method, solve_method_B=method, **kw)
     nsteps = 4
@@ -142,14 +158,25 @@ def test_mhd_time_schemes_match_oracle(name, builder, kw, method):
     duo, dbo = o.divergence()
     assert dug <= max(10 * duo, 1e-24)
     assert dbg <= max(10 * dbo, 1e-24)
+    nsolves = nsteps * (3 if method == 8 else 1)  # one solve per RK stage
     for k in ("iters_U", "iters_p", "iters_B", "iters_phi"):
-        assert abs(ig[k] - io[k]) <= max(nsteps, 0.005 * io[k]), (k, ig, io)
+        assert abs(ig[k] - io[k]) <= max(nsolves, 0.005 * io[k]), (k, ig, io)
 
 
 @pytest.mark.parametrize("field", ["solve_method_U", "solve_method_B"])
 def test_mhd_rejects_unknown_time_scheme(field):
     mom, ind, prm, _ = configs.ldc(n=6, induction=G.IND_B)
-    setattr(prm, field, 8)
+    setattr(prm, field, 9)
+    mm = G.Mesh(*mom)
+    with pytest.raises(G.MoonsError) as e:
+        G.MHD(mm, mm, prm)
+    assert e.value.code == 1  # MOONS_ERR_ARG
+
+
+@pytest.mark.parametrize("stages,energy", [(2, False), (3, True)])
+def test_mhd_rejects_bad_rk_stages(stages, energy):
+    mom, ind, prm, _ = configs.ldc_energy(n=6) if energy else configs.ldc(n=6, induction=G.IND_B)
+    prm.rk_stages = stages
     mm = G.Mesh(*mom)
     with pytest.raises(G.MoonsError) as e:
         G.MHD(mm, mm, prm)

@@ -1,5 +1,6 @@
 """The oracle's time schemes of the momentum and induction steps, solve_method
-1 to 7 (time_marching_methods.f90:47-150, :266-366), on the CPU.
+1 to 8 (time_marching_methods.f90:47-208, :266-366), and the RK stage loop of
+solve_MOONS (MOONS_solver.f90:73-97), on the CPU.
 
 Properties that pin each scheme's arithmetic without a second implementation:
 * the implicit schemes (5, 6, 7) integrate the same equations, so over a fixed
@@ -11,8 +12,15 @@ Properties that pin each scheme's arithmetic without a second implementation:
 * the "no_correction" schemes (1, 2) are one explicit update: over one step
   the velocity increment is linear in dt, and AB2's first step (Fnm1 = 0) is
   exactly 1.5 times Euler's;
-* a scheme number outside 0..7 is refused at create, as the reference's
-  select case stops."""
+* one inactive RK stage of Euler_time_RK_sources (8, all coefficients 1) is,
+  on the first step (Fnm1 = L = 0), Euler_time_Euler_sources with twice the
+  implicit coefficient, bit for bit; three stages are consistent with the
+  default scheme and end divergence-free;
+* the diffusion_linear terms enter through L: on the first step of
+  Euler_time_AB2_sources the diffusion through F (AB2: 1.5 F) moves the state
+  1.5 times as far as the same diffusion through L;
+* a scheme number outside 0..8, or a stage count other than 1 or 3, is
+  refused at create, as the reference's select case stops."""
 import numpy as np
 import pytest
 
@@ -50,7 +58,7 @@ def run(method, dt, nsteps, builder=configs.ldc, **kw):
 
 
 @pytest.mark.parametrize("field", ["solve_method_U", "solve_method_B"])
-@pytest.mark.parametrize("bad", [-1, 8, 9])
+@pytest.mark.parametrize("bad", [-1, 9])
 def test_unknown_scheme_refused(field, bad):
     mom, ind, prm, _ = configs.ldc(n=6, induction=IND_B)
     setattr(prm, field, bad)
@@ -99,3 +107,54 @@ def test_no_correction_schemes_are_one_explicit_update():
     assert np.linalg.norm(du2b - 2 * du2) <= 1e-11 * np.linalg.norm(du2b)
     # AB2(F, Fnm1) = 1.5 F - 0.5 Fnm1 with Fnm1 = 0 on the first step
     assert np.linalg.norm(du2 - 1.5 * du1) <= 1e-11 * np.linalg.norm(du2)
+
+
+@pytest.mark.parametrize("stages", [2, 4])
+def test_unknown_stage_count_refused(stages):
+    mom, ind, prm, _ = configs.ldc(n=6, induction=IND_B)
+    prm.rk_stages = stages
+    mm = O.Mesh(*mom)
+    with pytest.raises(ValueError):
+        O.MHD(mm, mm, prm)
+
+
+def test_rk_stages_with_energy_refused():
+    mom, ind, prm, _ = configs.ldc_energy(n=6)
+    prm.rk_stages = 3
+    mm = O.Mesh(*mom)
+    with pytest.raises(ValueError):
+        O.MHD(mm, mm, prm)
+
+
+def test_inactive_rk_stage_is_euler_with_twice_the_coefficient():
+    b8 = with_params(configs.ldc, rk_stages=1)
+    b5 = with_params(configs.ldc, coeff_implicit_U=lambda p: 2 * p.coeff_implicit_U,
+                     coeff_implicit_B=lambda p: 2 * p.coeff_implicit_B)
+    _, du8, db8 = run(8, 1e-3, 1, b8, **LDC)
+    _, du5, db5 = run(5, 1e-3, 1, b5, **LDC)
+    assert np.linalg.norm(du5) > 0 and np.linalg.norm(db5) > 0
+    assert np.array_equal(du8, du5) and np.array_equal(db8, db5)
+
+
+def test_rk3_is_consistent_with_the_default_scheme():
+    T = 8e-3
+    gaps = []
+    for dt in (2e-3, 1e-3):
+        n = int(round(T / dt))
+        _, d6, _ = run(6, dt, n)
+        sim, d8, _ = run(8, dt, n, with_params(configs.ldc, rk_stages=3), **LDC)
+        duv, dbv = sim.divergence()
+        assert duv < 1e-18 and dbv < 1e-18
+        gaps.append(np.linalg.norm(d8 - d6) / np.linalg.norm(d6))
+    assert gaps[0] < 0.05 and gaps[1] < 0.75 * gaps[0], gaps
+
+
+def test_linear_diffusion_enters_through_L():
+    s_u = lambda p: -p.coeff_implicit_U  # noqa: E731
+    _, d0, b0 = run(6, 1e-3, 1)
+    _, dF, bF = run(6, 1e-3, 1, with_params(configs.ldc, scale_diffusion_U=s_u, scale_diffusion_B=-1.0), **LDC)
+    _, dL, bL = run(6, 1e-3, 1, with_params(configs.ldc, scale_diffusion_linear_U=s_u,
+                                            scale_diffusion_linear_B=-1.0), **LDC)
+    assert np.linalg.norm(dF - d0) > 0 and np.linalg.norm(bF - b0) > 0
+    assert np.linalg.norm((dF - d0) - 1.5 * (dL - d0)) <= 1e-10 * np.linalg.norm(dF - d0)
+    assert np.linalg.norm((bF - b0) - 1.5 * (bL - b0)) <= 1e-9 * np.linalg.norm(bF - b0)
