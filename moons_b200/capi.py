@@ -65,7 +65,6 @@ class SolveInfo(C.Structure):
         ("rel", C.c_double),
         ("exit_reason", C.c_int),
         ("ms", C.c_double),
-        ("iters_T", C.c_int),
     ]
 
     def as_dict(self):

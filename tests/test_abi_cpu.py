@@ -37,3 +37,45 @@ def test_last_error_without_gpu():
     lib = ctypes.CDLL(build.LIB)
     lib.moons_last_error.restype = ctypes.c_char_p
     assert isinstance(lib.moons_last_error(), bytes)
+
+
+def _c_layout(structs):
+    """sizeof and field offsets of the header's structs, as the C compiler
+    lays them out (gcc on a small program that includes the header)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("gcc not available")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "moons_gpu.h"', "int main(void) {"]
+    for cname, fields in structs:
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    d = os.path.join(ROOT, "tests", "_build")
+    os.makedirs(d, exist_ok=True)
+    src, exe = os.path.join(d, "abi_layout.c"), os.path.join(d, "abi_layout")
+    with open(src, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln:
+            parts = ln.split()
+            got[(parts[0], parts[1])] = int(parts[2])
+    return got
+
+
+def test_ctypes_structs_match_the_header_layout():
+    """The ctypes mirrors of the parameter and report structs (moons_b200.capi,
+    also used by the oracle's bindings) have the C sizes and field offsets."""
+    from moons_b200 import capi as G
+    mirrors = [("moons_bc_spec", G.BCSpec), ("moons_isp", G.ISP), ("moons_solve_info", G.SolveInfo),
+               ("moons_mhd_params", G.MHDParams), ("moons_step_info", G.StepInfo)]
+    got = _c_layout([(c, [f for f, _ in py._fields_]) for c, py in mirrors])
+    for cname, py in mirrors:
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
