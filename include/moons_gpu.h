@@ -325,7 +325,12 @@ typedef struct {
    *           X* = X + dt F or X + dt AB2(F, Fnm1), clean_div scale 1;
    *   1, 2:   the same without the projection (:329-366): X += dt F or
    *           dt AB2(F, Fnm1), then X's BCs;
-   *   8:      Euler_time_RK_sources (:186-208), with rk_stages below.
+   *   8:      Euler_time_RK_sources (:186-208), with rk_stages below;
+   *   9:      Euler_time_AB2_sources_FFT (:152-185): 6 with the cleaning
+   *           Poisson equation solved directly (clean_div_FFT), which here
+   *           is the fast-diagonalization solve, MOONS_PREC_FD, in place of
+   *           prec_poisson for that equation (pressure for solve_method_U,
+   *           the B-cleaning potential for solve_method_B).
    * Source terms on wall-normal Dirichlet faces are zeroed in all of them. */
   int solve_method_U;
   int solve_method_B;

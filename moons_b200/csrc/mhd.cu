@@ -138,8 +138,12 @@ using namespace mg;
 
 namespace {
 inline int orth(int a, int b) { return 6 - a - b; }  // 1-based directions
-// solve_method of the momentum / induction step: 1 to 8, 0 selects the default, 6
-inline bool time_method_ok(int m) { return m >= 0 && m <= 8; }
+// solve_method of the momentum / induction step: 1 to 9, 0 selects the
+// default, 6.  Euler_time_AB2_sources_FFT (9, time_marching_methods.f90:
+// 152-185) is 6 with its cleaning Poisson equation solved directly
+// (clean_div_FFT, clean_divergence.f90:61-83): the step runs 6 and the
+// solver of that equation is created with the direct solve (MOONS_PREC_FD).
+inline bool time_method_ok(int m) { return m >= 0 && m <= 9; }
 // RK_Params of one stage (init_RKP, RK_params_extend.f90:22-55): the
 // three-stage coefficients of Lundbladh et al. (1999), or all 1 when the
 // step has one stage (RK inactive); beta = alpha
@@ -153,7 +157,7 @@ inline RKStage rk_stage(int stages, int n) {
   static const double a[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
   return {g[n - 1], z[n - 1], a[n - 1], a[n - 1]};
 }
-inline int time_method(int m) { return m == 0 ? 6 : m; }
+inline int time_method(int m) { return m == 0 || m == 9 ? 6 : m; }
 }
 
 struct moons_mhd {
@@ -600,7 +604,7 @@ int step_once(moons_mhd* s, const RKStage& rk) {
   }
   if (!r && P.energy && P.scale_buoyancy != 0.0) r = add_buoyancy(s);
   if (r) return r;
-  // ---- solve_momentum (solve_method 1 to 7)
+  // ---- solve_momentum (solve_method 1 to 9)
   r = euler_ab2(s, m, s->pcgU, s->pcgP, P.isp_U, P.isp_p, s->U, s->Ustar, s->Unm1, s->p, s->F, s->Fnm1, s->L, s->tF1,
                 s->tCC, P.coeff_implicit_U, &s->coefU, 0, 1, &s->res_p, time_method(P.solve_method_U), rk);
   if (r) return r;
@@ -681,7 +685,7 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
     return MOONS_ERR_ARG;
   }
   if (!time_method_ok(prm->solve_method_U) || !time_method_ok(prm->solve_method_B)) {
-    set_error("moons_mhd_create: solve_method_U and solve_method_B must be 0 to 8");
+    set_error("moons_mhd_create: solve_method_U and solve_method_B must be 0 to 9");
     return MOONS_ERR_ARG;
   }
   if (prm->rk_stages != 0 && prm->rk_stages != 1 && prm->rk_stages != 3) {
@@ -890,14 +894,16 @@ int moons_mhd_init(moons_mhd* s) {
     // the sigma-weighted potential solve is not separable (multigrid under
     // FD), and the networks are trained for the constant-coefficient solves
     const int pv = pp == MOONS_PREC_FD || pp == MOONS_PREC_UNET_MG ? MOONS_PREC_MG_MIXED : pp;
-    if ((r = moons_pcg_create(m, MOONS_OP_LAP_UNIFORM, pp, 1, xp, xp, nullptr, &s->pcgP))) return r;
-    if (pp == MOONS_PREC_UNET_MG && s->unet[0] && (r = moons_pcg_set_unet(s->pcgP, s->unet[0]))) return r;
+    const int ppU = s->P.solve_method_U == 9 ? MOONS_PREC_FD : pp;  // FFT_P of solve_method 9
+    if ((r = moons_pcg_create(m, MOONS_OP_LAP_UNIFORM, ppU, 1, xp, xp, nullptr, &s->pcgP))) return r;
+    if (ppU == MOONS_PREC_UNET_MG && s->unet[0] && (r = moons_pcg_set_unet(s->pcgP, s->unet[0]))) return r;
     if (s->P.induction == MOONS_IND_B) {
       if ((r = moons_pcg_create(s->mi, MOONS_OP_IND_DIFFUSION, MOONS_PREC_IND, 3, s->Bstar, s->B, s->sig, &s->pcgB)))
         return r;
       moons_sf* xf[1] = {s->phi};
-      if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_UNIFORM, pp, 1, xf, xf, nullptr, &s->pcgPhi))) return r;
-      if (pp == MOONS_PREC_UNET_MG && s->unet[1] && (r = moons_pcg_set_unet(s->pcgPhi, s->unet[1]))) return r;
+      const int ppB = s->P.solve_method_B == 9 ? MOONS_PREC_FD : pp;  // FFT_cleanB of solve_method 9
+      if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_UNIFORM, ppB, 1, xf, xf, nullptr, &s->pcgPhi))) return r;
+      if (ppB == MOONS_PREC_UNET_MG && s->unet[1] && (r = moons_pcg_set_unet(s->pcgPhi, s->unet[1]))) return r;
     } else if (s->P.induction == MOONS_IND_POTENTIAL) {
       moons_sf* xf[1] = {s->phi};
       if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_PROPS, pv, 1, xf, xf, s->sig, &s->pcgPhi))) return r;

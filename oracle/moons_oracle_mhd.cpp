@@ -94,6 +94,9 @@ static void embed_extract(SF& dst, const SF& src, const int o[3], bool embed) {
 struct RKStage {
   double gamma, zeta, alpha, beta;
 };
+// solve_method 0 is the default, 6; 9 runs 6 (the direct cleaning solve is
+// a solver choice, not a different arithmetic of the step)
+inline int time_method(int m) { return m == 0 || m == 9 ? 6 : m; }
 inline RKStage rk_stage(int stages, int n) {
   if (stages != 3) return {1.0, 1.0, 1.0, 1.0};
   const double g[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
@@ -462,6 +465,9 @@ struct MHD {
   //   6 Euler_time_AB2_sources (:117-150)
   //   7 O2_BDF_time_AB2_sources (:81-115)
   //   8 Euler_time_RK_sources (:186-208), with the stage's RK_Params
+  //   9 Euler_time_AB2_sources_FFT (:152-185): 6 with clean_div_FFT's direct
+  //     solve of the cleaning equation; here that equation is solved by the
+  //     PCG of 6 to its tolerance (the caller maps 9 to 6)
   // 3 to 8 end in clean_div_PCG (clean_divergence.f90:37-59).
   void euler_ab2(PCG& pv, PCG& ps, ISP& iv, ISP& is, SF* X, SF* Xstar, SF* Xnm1, SF& ph, SF* Fn, SF* Fm, SF* Lx,
                  SF* t1, SF& tcc, const Grid& g, double coeff_implicit, int slot_v, int slot_s, double* res_s,
@@ -597,9 +603,9 @@ struct MHD {
       }
     }
     if (P.energy && P.scale_buoyancy != 0.0) add_buoyancy();
-    // ---- solve_momentum (solve_method 1 to 8; 0 = 6)
+    // ---- solve_momentum (solve_method 1 to 9; 0 = 6)
     euler_ab2(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p,
-              P.solve_method_U ? P.solve_method_U : 6, rk);
+              time_method(P.solve_method_U), rk);
     for (int c = 0; c < 3; c++) interp(UCC[c], U[c], gm, c + 1);
     SF* Up[3] = {&U[0], &U[1], &U[2]};
     face2edge_nd(UE, Up, gm);
@@ -634,7 +640,7 @@ struct MHD {
         for (int c = 0; c < 3; c++) add_product(Fi[c], tFi2[c], P.scale_diffusion_B);
       }
       euler_ab2(pcgB, pcgPhi, ispB, ispPhi, B, Bstar, Bnm1, phi, Fi, Fnm1i, Li, tFi1, tCCi, gi, P.coeff_implicit_B,
-                2, 3, &res_phi, P.solve_method_B ? P.solve_method_B : 6, rk);
+                2, 3, &res_phi, time_method(P.solve_method_B), rk);
       compute_J();
       compute_Btot();
       compute_JxB();
@@ -721,7 +727,7 @@ struct OSFView {
 extern "C" {
 void* or_mhd_create(void* mesh_mom, void* mesh_ind, const moons_mhd_params* prm) {
   for (int m : {prm->solve_method_U, prm->solve_method_B})
-    if (m < 0 || m > 8) return nullptr;  // solve_method 1 to 8 (0 = 6)
+    if (m < 0 || m > 9) return nullptr;  // solve_method 1 to 9 (0 = 6)
   if (prm->rk_stages != 0 && prm->rk_stages != 1 && prm->rk_stages != 3) return nullptr;
   if (prm->rk_stages == 3 && prm->energy) return nullptr;  // no RK energy scheme
   auto* s = new mo::MHD();

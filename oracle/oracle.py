@@ -262,7 +262,7 @@ class MHD:
         self.params = params
         self.h = lib().or_mhd_create(mesh_mom.h, mesh_ind.h, C.byref(params))
         if not self.h:
-            raise ValueError("or_mhd_create: solve_method_U and solve_method_B must be 0 to 8, rk_stages 0, 1 "
+            raise ValueError("or_mhd_create: solve_method_U and solve_method_B must be 0 to 9, rk_stages 0, 1 "
                              "or 3 (3 without the energy equation)")
 
     def shape(self, which, comp=0):

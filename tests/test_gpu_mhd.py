@@ -166,7 +166,7 @@ def test_mhd_time_schemes_match_oracle(name, builder, kw, method):
 @pytest.mark.parametrize("field", ["solve_method_U", "solve_method_B"])
 def test_mhd_rejects_unknown_time_scheme(field):
     mom, ind, prm, _ = configs.ldc(n=6, induction=G.IND_B)
-    setattr(prm, field, 9)
+    setattr(prm, field, 10)
     mm = G.Mesh(*mom)
     with pytest.raises(G.MoonsError) as e:
         G.MHD(mm, mm, prm)
@@ -181,3 +181,30 @@ def test_mhd_rejects_bad_rk_stages(stages, energy):
     with pytest.raises(G.MoonsError) as e:
         G.MHD(mm, mm, prm)
     assert e.value.code == 1  # MOONS_ERR_ARG
+
+
+@pytest.mark.parametrize("name,builder,kw", SCHEME_CASES, ids=[c[0] for c in SCHEME_CASES])
+def test_mhd_fft_scheme_direct_cleaning(name, builder, kw):
+    """solve_method 9 (Euler_time_AB2_sources_FFT, time_marching_methods.f90:
+    152-185): the default scheme with the cleaning equations solved directly
+    (clean_div_FFT), here by the fast-diagonalization solve.  Against the
+    oracle's Jacobi-PCG cleaning, both to 1e-12: fields agree to solver
+    accuracy (the bound of the direct-solve step test) and each cleaning
+    solve takes a few CG iterations at most."""
+    g = configs.make(G, builder, seed=3, solve_method_U=9, solve_method_B=9, **kw)
+    o = configs.make(O, builder, seed=3, **kw)
+    nsteps = 4
+    ig = g.step(nsteps)
+    o.step(nsteps)
+    fields = ([(G.MHD_U, c) for c in range(3)] + [(G.MHD_B, c) for c in range(3)] +
+              [(G.MHD_J, c) for c in range(3)] + [(G.MHD_JXB, c) for c in range(3)])
+    for which, c in fields:
+        e = rel_l2(g.download(which, c), o.download(which, c))
+        assert e < 1e-7, f"{name}: field {which}/{c} rel L2 {e}"
+    dug, dbg = g.divergence()
+    duo, dbo = o.divergence()
+    assert dug <= max(100 * duo, 1e-22)
+    assert dbg <= max(100 * dbo, 1e-22)
+    # at most three CG iterations per direct-preconditioned solve, the bound of
+    # the direct solve's own test (hundreds with the Jacobi preconditioner)
+    assert ig["iters_p"] <= 3 * nsteps and ig["iters_phi"] <= 3 * nsteps, ig

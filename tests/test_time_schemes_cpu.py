@@ -19,7 +19,9 @@ Properties that pin each scheme's arithmetic without a second implementation:
 * the diffusion_linear terms enter through L: on the first step of
   Euler_time_AB2_sources the diffusion through F (AB2: 1.5 F) moves the state
   1.5 times as far as the same diffusion through L;
-* a scheme number outside 0..8, or a stage count other than 1 or 3, is
+* Euler_time_AB2_sources_FFT (9) is 6 with a direct cleaning solve, so the
+  oracle runs it as 6;
+* a scheme number outside 0..9, or a stage count other than 1 or 3, is
   refused at create, as the reference's select case stops."""
 import numpy as np
 import pytest
@@ -58,7 +60,7 @@ def run(method, dt, nsteps, builder=configs.ldc, **kw):
 
 
 @pytest.mark.parametrize("field", ["solve_method_U", "solve_method_B"])
-@pytest.mark.parametrize("bad", [-1, 9])
+@pytest.mark.parametrize("bad", [-1, 10])
 def test_unknown_scheme_refused(field, bad):
     mom, ind, prm, _ = configs.ldc(n=6, induction=IND_B)
     setattr(prm, field, bad)
@@ -158,3 +160,9 @@ def test_linear_diffusion_enters_through_L():
     assert np.linalg.norm(dF - d0) > 0 and np.linalg.norm(bF - b0) > 0
     assert np.linalg.norm((dF - d0) - 1.5 * (dL - d0)) <= 1e-10 * np.linalg.norm(dF - d0)
     assert np.linalg.norm((bF - b0) - 1.5 * (bL - b0)) <= 1e-9 * np.linalg.norm(bF - b0)
+
+
+def test_fft_scheme_runs_the_default_arithmetic():
+    _, du6, db6 = run(6, 1e-3, 2)
+    _, du9, db9 = run(9, 1e-3, 2)
+    assert np.array_equal(du6, du9) and np.array_equal(db6, db9)
