@@ -286,7 +286,7 @@ int solve(moons_pcg* s, moons_sf* const* x, moons_sf* const* b, const moons_isp&
 //  3, 4:    X* = X + dt F (Euler) or X + dt AB2(F, Fnm1), then clean_div;
 //  1, 2:    X = X + dt F or X + dt AB2(F, Fnm1), then apply_BCs(X).
 // clean_div's scale is 1/dt for method 6 and 1 for the others.
-int euler_ab2(moons_mhd* s, moons_mesh* m, moons_pcg* pv, moons_pcg* ps, const moons_isp& iv, const moons_isp& is,
+int time_scheme_step(moons_mhd* s, moons_mesh* m, moons_pcg* pv, moons_pcg* ps, const moons_isp& iv, const moons_isp& is,
               moons_sf** X, moons_sf** Xstar, moons_sf** Xnm1, moons_sf* ph, moons_sf** Fn, moons_sf** Fm,
               moons_sf** Lx, moons_sf** t1, moons_sf* tcc, double coeff_implicit, double* coef_cache, int slot_v,
               int slot_s, double* res_s, int method, const RKStage& rk) {
@@ -605,7 +605,7 @@ int step_once(moons_mhd* s, const RKStage& rk) {
   if (!r && P.energy && P.scale_buoyancy != 0.0) r = add_buoyancy(s);
   if (r) return r;
   // ---- solve_momentum (solve_method 1 to 9)
-  r = euler_ab2(s, m, s->pcgU, s->pcgP, P.isp_U, P.isp_p, s->U, s->Ustar, s->Unm1, s->p, s->F, s->Fnm1, s->L, s->tF1,
+  r = time_scheme_step(s, m, s->pcgU, s->pcgP, P.isp_U, P.isp_p, s->U, s->Ustar, s->Unm1, s->p, s->F, s->Fnm1, s->L, s->tF1,
                 s->tCC, P.coeff_implicit_U, &s->coefU, 0, 1, &s->res_p, time_method(P.solve_method_U), rk);
   if (r) return r;
   for (int c = 0; c < 3 && !r; c++) r = launch_interp(m, D(s->UCC[c]), D(s->U[c]), c + 1);
@@ -649,7 +649,7 @@ int step_once(moons_mhd* s, const RKStage& rk) {
         r = launch_pw(mi, PW_ADD_PRODUCT, D(s->Fi[c]), &D(s->tFi2[c]), P.scale_diffusion_B);
     }
     if (r) return r;
-    r = euler_ab2(s, mi, s->pcgB, s->pcgPhi, P.isp_B, P.isp_phi, s->B, s->Bstar, s->Bnm1, s->phi, s->Fi, s->Fnm1i,
+    r = time_scheme_step(s, mi, s->pcgB, s->pcgPhi, P.isp_B, P.isp_phi, s->B, s->Bstar, s->Bnm1, s->phi, s->Fi, s->Fnm1i,
                   s->Li, s->tFi1, s->tCCi, P.coeff_implicit_B, &s->coefB, 2, 3, &s->res_phi,
                   time_method(P.solve_method_B), rk);
     if (!r) r = compute_J(s);

@@ -469,7 +469,7 @@ struct MHD {
   //     solve of the cleaning equation; here that equation is solved by the
   //     PCG of 6 to its tolerance (the caller maps 9 to 6)
   // 3 to 8 end in clean_div_PCG (clean_divergence.f90:37-59).
-  void euler_ab2(PCG& pv, PCG& ps, ISP& iv, ISP& is, SF* X, SF* Xstar, SF* Xnm1, SF& ph, SF* Fn, SF* Fm, SF* Lx,
+  void time_scheme_step(PCG& pv, PCG& ps, ISP& iv, ISP& is, SF* X, SF* Xstar, SF* Xnm1, SF& ph, SF* Fn, SF* Fm, SF* Lx,
                  SF* t1, SF& tcc, const Grid& g, double coeff_implicit, int slot_v, int slot_s, double* res_s,
                  int method, const RKStage& rk) {
     const double two_thirds = 2.0 / 3.0, four_thirds = 4.0 / 3.0, neg_one_third = -1.0 / 3.0;
@@ -604,7 +604,7 @@ struct MHD {
     }
     if (P.energy && P.scale_buoyancy != 0.0) add_buoyancy();
     // ---- solve_momentum (solve_method 1 to 9; 0 = 6)
-    euler_ab2(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p,
+    time_scheme_step(pcgU, pcgP, ispU, ispP, U, Ustar, Unm1, p, F, Fnm1, L, tF1, tCC, gm, P.coeff_implicit_U, 0, 1, &res_p,
               time_method(P.solve_method_U), rk);
     for (int c = 0; c < 3; c++) interp(UCC[c], U[c], gm, c + 1);
     SF* Up[3] = {&U[0], &U[1], &U[2]};
@@ -639,7 +639,7 @@ struct MHD {
         curl(tFi2[0], tFi2[1], tFi2[2], tE[0], tE[1], tE[2], gi);
         for (int c = 0; c < 3; c++) add_product(Fi[c], tFi2[c], P.scale_diffusion_B);
       }
-      euler_ab2(pcgB, pcgPhi, ispB, ispPhi, B, Bstar, Bnm1, phi, Fi, Fnm1i, Li, tFi1, tCCi, gi, P.coeff_implicit_B,
+      time_scheme_step(pcgB, pcgPhi, ispB, ispPhi, B, Bstar, Bnm1, phi, Fi, Fnm1i, Li, tFi1, tCCi, gi, P.coeff_implicit_B,
                 2, 3, &res_phi, time_method(P.solve_method_B), rk);
       compute_J();
       compute_Btot();
