@@ -293,9 +293,16 @@ typedef struct {
    * solve_MOONS does (MOONS_solver.f90:81-85); fields MOONS_MHD_T, _KT,
    * _GRAVITY */
   int energy;               /* 1: solve for T                               */
-  int solve_method_T;       /* 2: Euler_time_no_diff_AB2_sources_SF (explicit),
-                               3: Euler_time_AB2_sources_SF (PCG_T, nrg_diffusion,
-                               prec_lap_SF) (time_marching_methods_SF.f90:71-160) */
+  int solve_method_T;       /* solve_energy's select case (energy_extend.f90:
+                               244-257), time_marching_methods_SF.f90:
+                               1: Euler_time_no_diff_Euler_sources_SF (:154-170),
+                               2: Euler_time_no_diff_AB2_sources_SF (:135-152),
+                                  X += dt F or dt AB2(F, Fnm1), no solve;
+                               3: Euler_time_AB2_sources_SF (:71-98),
+                               4: O2_BDF_time_AB2_sources_SF (:42-69),
+                               5: Euler_time_RK_sources_SF (:100-133), with
+                                  the rk_stages coefficients: PCG_T solves
+                                  (nrg_diffusion, prec_lap_SF)              */
   double coeff_implicit_T;  /* SP%VS%T%MFP%coeff_implicit                    */
   double scale_advection_T; /* SP%ET%advection%scale: F += s (-div(u T))     */
   double scale_diffusion_T; /* SP%ET%diffusion%scale: F += s lap(T) (explicit) */
@@ -341,7 +348,9 @@ typedef struct {
    * the solves of the whole step; solve_method 8 (Euler_time_RK_sources,
    * time_marching_methods.f90:186-208) uses the stage's coefficients:
    * (I + 2 beta dt c A) X* = X + dt (gamma F + zeta Fnm1 + 2 alpha L),
-   * clean_div scale 1.  The energy equation takes no RK stages here. */
+   * clean_div scale 1.  With three stages the energy's explicit diffusion
+   * goes into its L (add_all_energy_sources.f90:35-48), which only
+   * solve_method_T 5 reads. */
   int rk_stages;
   /* SP%MT%diffusion_linear / SP%IT%diffusion_linear: the diffusion term into
    * L instead of F (add_all_momentum_sources.f90:49-51,

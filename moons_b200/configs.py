@@ -173,8 +173,11 @@ def ldc_energy(n: int = 16, Pe: float = 100.0, Gr_Re2: float = 10.0, heating: fl
     """The lid-driven cavity with the energy equation: T = 1 on the x-min
     wall, 0 on x-max, insulated elsewhere; conductivity on the faces varying
     by +-20% (seeded); gravity -y; advection scale 1 (S += -div(u T)),
-    diffusion by the implicit nrg_diffusion PCG (solve_method 3, coefficient
-    -1/Pe) or explicitly (solve_method 2, scale 1/Pe); volumetric heating
+    diffusion by the implicit nrg_diffusion PCG (solve_method 3 and 4,
+    coefficient -1/Pe), explicitly (solve_method 1 and 2, scale 1/Pe), or
+    half and half (solve_method 5 with three RK stages: the explicit part
+    goes into L and is weighed by alpha, the implicit by beta, each summing
+    to 1/2 over the stages); volumetric heating
     (add_volumetric_heating_Nuclear) and buoyancy Gr/Re^2 in momentum;
     optionally the KE-diffusion, viscous-dissipation and Joule-heating
     sources with the given scales (sigma^-1 at cell centres then 1 + 0.5 x,
@@ -185,7 +188,7 @@ def ldc_energy(n: int = 16, Pe: float = 100.0, Gr_Re2: float = 10.0, heating: fl
     prm.solve_method_T = solve_method_T
     prm.coeff_implicit_T = -1.0 / Pe
     prm.scale_advection_T = 1.0
-    prm.scale_diffusion_T = 0.0 if solve_method_T == 3 else 1.0 / Pe
+    prm.scale_diffusion_T = 0.0 if solve_method_T in (3, 4) else 1.0 / Pe
     prm.scale_heating_T = heating
     prm.scale_buoyancy = Gr_Re2
     prm.isp_T = _isp(5000, tol)

@@ -491,10 +491,14 @@ int energy_sources_KE_visc_joule(moons_mhd* s) {
 // add_all_energy_sources (add_all_energy_sources.f90:21-67) with the
 // advection, diffusion and volumetric-heating terms (energy_sources.f90),
 // then solve_energy (energy_extend.f90:236-262), methods 2 and 3
-int energy_step(moons_mhd* s) {
+// add_all_energy_sources + solve_energy (add_all_energy_sources.f90:21-67,
+// energy_extend.f90:236-262) for one stage of the step
+int energy_step(moons_mhd* s, const RKStage& rk) {
   moons_mesh* mi = s->mi;
   const moons_mhd_params& P = s->P;
+  const bool rk_active = P.rk_stages == 3;
   int r = copy(mi, s->FnmT, s->FT);
+  if (!r && rk_active) r = launch_pw(mi, PW_FILL, D(s->LT), nullptr, 0.0);
   if (!r) r = launch_pw(mi, PW_FILL, D(s->FT), nullptr, 0.0);
   if (!r && P.scale_advection_T != 0.0) {
     // add_advection: S += scale * (-div(face(T) * U_F)), U_F = embedFace(U)
@@ -511,11 +515,12 @@ int energy_step(moons_mhd* s) {
     if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_advection_T);
   }
   if (!r && P.scale_diffusion_T != 0.0) {
-    // add_diffusion: S += scale * lap(T) (lapUniformCoeff_SF)
+    // add_diffusion: S += scale * lap(T) (lapUniformCoeff_SF), into L when
+    // the RK stages are active
     r = launch_del(mi, D(s->tCCT), D(s->T), 2, 1, 0, 1);
     if (!r) r = launch_del(mi, D(s->tCCT), D(s->T), 2, 2, 0, 2);
     if (!r) r = launch_del(mi, D(s->tCCT), D(s->T), 2, 3, 0, 2);
-    if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_diffusion_T);
+    if (!r) r = launch_pw(mi, PW_ADD_PRODUCT, rk_active ? D(s->LT) : D(s->FT), &D(s->tCCT), P.scale_diffusion_T);
   }
   if (!r) r = energy_sources_KE_visc_joule(s);
   if (!r && P.scale_heating_T != 0.0) {
@@ -524,13 +529,30 @@ int energy_step(moons_mhd* s) {
     r = launch_pw(mi, PW_ADD_PRODUCT, D(s->FT), &D(s->tCCT), P.scale_heating_T);
   }
   if (r) return r;
-  // X* = X + dt AB2(F, Fnm1) (wall-Dirichlet points of the increment zeroed)
+  // the energy time schemes (solve_energy's select case, energy_extend.f90:
+  // 244-257; time_marching_methods_SF.f90), RHS forms of k_ab2_rhs:
+  //  1 Euler_time_no_diff_Euler_sources_SF (:154-170): X += dt F
+  //  2 Euler_time_no_diff_AB2_sources_SF (:135-152): X += dt AB2(F, Fnm1)
+  //  3 Euler_time_AB2_sources_SF (:71-98): solve (I + dt c A) X = X + dt AB2
+  //  4 O2_BDF_time_AB2_sources_SF (:42-69): solve (I + 2/3 dt c A) X =
+  //    4/3 X - 1/3 Xnm1 + 2/3 dt AB2
+  //  5 Euler_time_RK_sources_SF (:100-133): solve (I + beta dt c A) X =
+  //    X + dt (gamma F + zeta Fnm1 + alpha L)
+  // (increments on wall-Dirichlet points zeroed; CC data has none)
+  const int mT = P.solve_method_T;
   const int wb = dirichlet_wall_bits(s->T->bc.defined ? &s->T->bc : nullptr, D(s->T).dl);
-  MG_LAUNCH(k_ab2_rhs, nblocks(D(s->tmpT).n()), kBlock, mi->stream, D(s->tmpT), D(s->FT), D(s->FnmT), D(s->LT),
-            D(s->T), D(s->Tnm1), P.dt, wb, 6, 1, 0.0, 0.0, 0.0);
+  const int form = mT == 1 ? 5 : mT == 4 ? 7 : mT == 5 ? 8 : 4;
+  const double dts = mT == 4 ? (2.0 / 3.0) * P.dt : P.dt;
+  moons_sf* out = mT <= 2 ? s->T : s->tmpT;  // 1, 2: X = X + increment
+  MG_LAUNCH(k_ab2_rhs, nblocks(D(out).n()), kBlock, mi->stream, D(out), D(s->FT), D(s->FnmT), D(s->LT), D(s->T),
+            D(s->Tnm1), dts, wb, form, mT <= 2 ? 0 : 1, P.dt * rk.gamma, P.dt * rk.zeta, P.dt * rk.alpha);
   MG_CUDA(cudaGetLastError());
-  if (P.solve_method_T == 2) return copy(mi, s->T, s->tmpT);  // X = X + dt AB2 (no diffusion solve)
-  const double c = P.dt * 1.0 * P.coeff_implicit_T;
+  if (mT <= 2) return MOONS_OK;
+  // update_MFP: 3 and 4 rebuild the preconditioner while TMP%n_step <= 2,
+  // 5 every stage; it only changes with c, so it is rebuilt when c changes
+  const double c = mT == 4   ? P.dt * (2.0 / 3.0) * P.coeff_implicit_T
+                   : mT == 5 ? P.dt * rk.beta * P.coeff_implicit_T
+                             : P.dt * 1.0 * P.coeff_implicit_T;
   if (!(c == s->coefT)) {
     if ((r = moons_pcg_update_mfp(s->pcgT, c, 1))) return r;
     s->coefT = c;
@@ -564,7 +586,7 @@ int step_once(moons_mhd* s, const RKStage& rk) {
   double dt = P.dt;
   int r = MOONS_OK;
   // ---- energy (solve_MOONS: energy sources and solve before momentum)
-  if (P.energy && (r = energy_step(s))) return r;
+  if (P.energy && (r = energy_step(s, rk))) return r;
   // ---- add_all_momentum_sources
   if (P.mpg_dir >= 1 && P.mpg_dir <= 3) {
     DF u = D(s->U[P.mpg_dir - 1]);
@@ -680,8 +702,8 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
     set_error("moons_mhd_create: bad induction mode or dt");
     return MOONS_ERR_ARG;
   }
-  if (prm->energy && prm->solve_method_T != 2 && prm->solve_method_T != 3) {
-    set_error("moons_mhd_create: solve_method_T must be 2 or 3");
+  if (prm->energy && (prm->solve_method_T < 1 || prm->solve_method_T > 5)) {
+    set_error("moons_mhd_create: solve_method_T must be 1 to 5");
     return MOONS_ERR_ARG;
   }
   if (!time_method_ok(prm->solve_method_U) || !time_method_ok(prm->solve_method_B)) {
@@ -690,10 +712,6 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
   }
   if (prm->rk_stages != 0 && prm->rk_stages != 1 && prm->rk_stages != 3) {
     set_error("moons_mhd_create: rk_stages must be 0, 1 or 3");
-    return MOONS_ERR_ARG;
-  }
-  if (prm->rk_stages == 3 && prm->energy) {
-    set_error("moons_mhd_create: the energy equation takes no RK stages");
     return MOONS_ERR_ARG;
   }
   auto* s = new moons_mhd();
@@ -908,7 +926,7 @@ int moons_mhd_init(moons_mhd* s) {
       moons_sf* xf[1] = {s->phi};
       if ((r = moons_pcg_create(s->mi, MOONS_OP_LAP_PROPS, pv, 1, xf, xf, s->sig, &s->pcgPhi))) return r;
     }
-    if (s->P.energy && s->P.solve_method_T == 3) {
+    if (s->P.energy && s->P.solve_method_T >= 3) {
       // init(nrg%PCG_T, nrg_diffusion, nrg_diffusion_explicit, prec_lap_SF, ...) (energy_extend.f90:129)
       moons_sf* xt[1] = {s->T};
       if ((r = moons_pcg_create(s->mi, MOONS_OP_NRG_DIFFUSION, MOONS_PREC_LAP, 1, xt, xt, s->kT, &s->pcgT))) return r;

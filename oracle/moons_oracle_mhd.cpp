@@ -236,7 +236,7 @@ struct MHD {
       SF* ks[3] = {&sig[0], &sig[1], &sig[2]};
       pcgPhi.init(gi, OP_LAP_PROPS, PREC_LAP, 1, xf, xf, ks, 0.0);
     }
-    if (P.energy && P.solve_method_T == 3) {
+    if (P.energy && P.solve_method_T >= 3) {
       // init(nrg%PCG_T, nrg_diffusion, nrg_diffusion_explicit, prec_lap_SF, ...) (energy_extend.f90:129)
       SF* xt[1] = {&T};
       SF* ks[3] = {&kT[0], &kT[1], &kT[2]};
@@ -249,8 +249,12 @@ struct MHD {
   // advection / diffusion / volumetric heating (energy_sources.f90), then
   // solve_energy methods 2 and 3 (energy_extend.f90:236-262,
   // time_marching_methods_SF.f90:71-160)
-  void energy_step() {
+  // add_all_energy_sources + solve_energy (add_all_energy_sources.f90:21-67,
+  // energy_extend.f90:236-262) for one stage of the step
+  void energy_step(const RKStage& rk) {
+    const bool rk_active = P.rk_stages == 3;
     assign(FnmT, FT);
+    if (rk_active) assign(LT, 0.0);
     assign(FT, 0.0);
     if (P.scale_advection_T != 0.0) {  // add_advection (energy_sources.f90:22-35)
       for (int c = 0; c < 3; c++) {
@@ -265,9 +269,9 @@ struct MHD {
       multiply(tCCT, -1.0);
       add_product(FT, tCCT, P.scale_advection_T);
     }
-    if (P.scale_diffusion_T != 0.0) {  // add_diffusion: lap = lapUniformCoeff_SF
+    if (P.scale_diffusion_T != 0.0) {  // add_diffusion: lap = lapUniformCoeff_SF, into L when RK is active
       lap_uniform_coeff(tCCT, T, gi);
-      add_product(FT, tCCT, P.scale_diffusion_T);
+      add_product(rk_active ? LT : FT, tCCT, P.scale_diffusion_T);
     }
     if (P.scale_KE_diffusion_T != 0.0 || P.scale_viscous_dissipation_T != 0.0) {
       // embedCC(nrg%U_CC, mom%U_CC, nrg%MD) (add_all_energy_sources.f90:30-32)
@@ -327,19 +331,53 @@ struct MHD {
           for (int i = 1; i <= tCCT.s[1]; i++) tCCT(i, j, k) = Fh * std::exp(-m_ * (cy.hc(j) + 1.0));
       add_product(FT, tCCT, P.scale_heating_T);
     }
-    // AB2_SF: temp = Fn*1.5 ; temp += Fnm1*(-0.5) ; temp *= dt ; wall Dirichlet 0
-    for (size_t i = 0; i < tmpT.n(); i++) tmpT.f[i] = FT.f[i] * 1.5;
-    add_product(tmpT, FnmT, -0.5);
-    add(tmpT, LT);
-    multiply(tmpT, P.dt);
-    assign_wall_Dirichlet(tmpT, 0.0, &T);
-    if (P.solve_method_T == 2) {  // Euler_time_no_diff_AB2_sources_SF: X += X*
+    // the energy time schemes (solve_energy, energy_extend.f90:244-257;
+    // time_marching_methods_SF.f90)
+    const double two_thirds = 2.0 / 3.0, four_thirds = 4.0 / 3.0, neg_one_third = -1.0 / 3.0;
+    const int mT = P.solve_method_T;
+    // AB2_SF: temp = Fn*1.5 ; temp += Fnm1*(-0.5)
+    auto ab2 = [&]() {
+      for (size_t i = 0; i < tmpT.n(); i++) tmpT.f[i] = FT.f[i] * 1.5;
+      add_product(tmpT, FnmT, -0.5);
+    };
+    if (mT == 1) {  // Euler_time_no_diff_Euler_sources_SF (:154-170)
+      assign(tmpT, FT);  // multiply(Xstar,F,dt)
+      multiply(tmpT, P.dt);
+      assign_wall_Dirichlet(tmpT, 0.0, &T);
       add(T, tmpT);
       return;
     }
-    add(tmpT, T);  // Euler_time_AB2_sources_SF
-    assign(Tnm1, T);
-    pcgT.update_MFP(P.dt * 1.0 * P.coeff_implicit_T, true);
+    if (mT == 2) {  // Euler_time_no_diff_AB2_sources_SF (:135-152)
+      ab2();
+      multiply(tmpT, P.dt);
+      assign_wall_Dirichlet(tmpT, 0.0, &T);
+      add(T, tmpT);
+      return;
+    }
+    if (mT == 3) {  // Euler_time_AB2_sources_SF (:71-98)
+      ab2();
+      multiply(tmpT, P.dt);
+      assign_wall_Dirichlet(tmpT, 0.0, &T);
+      add(tmpT, T);
+      assign(Tnm1, T);
+      pcgT.update_MFP(P.dt * 1.0 * P.coeff_implicit_T, n_step <= 2);
+    } else if (mT == 4) {  // O2_BDF_time_AB2_sources_SF (:42-69)
+      ab2();
+      multiply(tmpT, two_thirds * P.dt);
+      assign_wall_Dirichlet(tmpT, 0.0, &T);
+      add_product(tmpT, T, four_thirds);
+      add_product(tmpT, Tnm1, neg_one_third);
+      assign(Tnm1, T);
+      pcgT.update_MFP(P.dt * two_thirds * P.coeff_implicit_T, n_step <= 2);
+    } else {  // Euler_time_RK_sources_SF (:100-133)
+      for (size_t i = 0; i < tmpT.n(); i++) tmpT.f[i] = FT.f[i] * (P.dt * rk.gamma);
+      add_product(tmpT, FnmT, P.dt * rk.zeta);
+      add_product(tmpT, LT, P.dt * rk.alpha);
+      assign_wall_Dirichlet(tmpT, 0.0, &T);
+      add(tmpT, T);
+      assign(Tnm1, T);
+      pcgT.update_MFP(P.dt * rk.beta * P.coeff_implicit_T, true);
+    }
     SF* xt[1] = {&T};
     SF* bt[1] = {&tmpT};
     SolveInfo si = pcgT.solve(xt, bt, ispT);
@@ -568,7 +606,7 @@ struct MHD {
 
   void step_stage(const RKStage& rk) {
     double dt = P.dt;
-    if (P.energy) energy_step();
+    if (P.energy) energy_step(rk);
     // ---- add_all_momentum_sources
     if (P.mpg_dir >= 1 && P.mpg_dir <= 3) {  // compute_add_MPG (momentum_sources.f90:97-109)
       SF& u = U[P.mpg_dir - 1];
@@ -729,7 +767,7 @@ void* or_mhd_create(void* mesh_mom, void* mesh_ind, const moons_mhd_params* prm)
   for (int m : {prm->solve_method_U, prm->solve_method_B})
     if (m < 0 || m > 9) return nullptr;  // solve_method 1 to 9 (0 = 6)
   if (prm->rk_stages != 0 && prm->rk_stages != 1 && prm->rk_stages != 3) return nullptr;
-  if (prm->rk_stages == 3 && prm->energy) return nullptr;  // no RK energy scheme
+  if (prm->energy && (prm->solve_method_T < 1 || prm->solve_method_T > 5)) return nullptr;
   auto* s = new mo::MHD();
   const mo::Grid& gm = ((OMeshView*)mesh_mom)->g;
   const mo::Grid& gi = ((OMeshView*)mesh_ind)->g;

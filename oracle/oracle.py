@@ -263,7 +263,7 @@ class MHD:
         self.h = lib().or_mhd_create(mesh_mom.h, mesh_ind.h, C.byref(params))
         if not self.h:
             raise ValueError("or_mhd_create: solve_method_U and solve_method_B must be 0 to 9, rk_stages 0, 1 "
-                             "or 3 (3 without the energy equation)")
+                             "or 3, solve_method_T 1 to 5")
 
     def shape(self, which, comp=0):
         s = (C.c_int * 3)()

@@ -21,14 +21,19 @@ Properties that pin each scheme's arithmetic without a second implementation:
   1.5 times as far as the same diffusion through L;
 * Euler_time_AB2_sources_FFT (9) is 6 with a direct cleaning solve, so the
   oracle runs it as 6;
-* a scheme number outside 0..9, or a stage count other than 1 or 3, is
-  refused at create, as the reference's select case stops."""
+* the energy schemes (solve_energy, energy_extend.f90:244-257): the
+  explicit ones (1, 2) are linear in dt with AB2's first step 1.5 times
+  Euler's; BDF2 (4) and RK3 (5, all diffusion implicit) agree with the
+  implicit AB2 scheme (3) to O(dt);
+* a scheme number outside 0..9 (1..5 for the energy), or a stage count
+  other than 1 or 3, is refused at create, as the reference's select case
+  stops."""
 import numpy as np
 import pytest
 
 import oracle.oracle as O
 from moons_b200 import configs
-from moons_b200.capi import IND_B, MHD_U, MHD_B
+from moons_b200.capi import IND_B, MHD_U, MHD_B, MHD_T
 
 LDC = dict(n=6, induction=IND_B)
 
@@ -120,9 +125,9 @@ def test_unknown_stage_count_refused(stages):
         O.MHD(mm, mm, prm)
 
 
-def test_rk_stages_with_energy_refused():
-    mom, ind, prm, _ = configs.ldc_energy(n=6)
-    prm.rk_stages = 3
+@pytest.mark.parametrize("bad", [0, 6])
+def test_unknown_energy_scheme_refused(bad):
+    mom, ind, prm, _ = configs.ldc_energy(n=6, solve_method_T=bad)
     mm = O.Mesh(*mom)
     with pytest.raises(ValueError):
         O.MHD(mm, mm, prm)
@@ -166,3 +171,37 @@ def test_fft_scheme_runs_the_default_arithmetic():
     _, du6, db6 = run(6, 1e-3, 2)
     _, du9, db9 = run(9, 1e-3, 2)
     assert np.array_equal(du6, du9) and np.array_equal(db6, db9)
+
+
+def run_T(mT, dt, nsteps, rk=0, implicit_only=False):
+    """heated cavity (6^3): the temperature increment after nsteps."""
+    def b(*a, **kw):
+        mom, ind, prm, init = configs.ldc_energy(*a, **kw)
+        prm.rk_stages = rk
+        if implicit_only:  # all diffusion in the solve: beta sums to 1/2 over the stages
+            prm.scale_diffusion_T = 0.0
+            prm.coeff_implicit_T = 2 * prm.coeff_implicit_T
+        return mom, ind, prm, init
+    sim = configs.make(O, b, seed=3, n=6, dt=dt, tol=1e-12, solve_method_T=mT, solve_method_U=8 if rk == 3 else 0)
+    t0 = sim.download(MHD_T, 0).copy()
+    sim.step(nsteps)
+    return (sim.download(MHD_T, 0) - t0).ravel()
+
+
+def test_explicit_energy_schemes_are_one_explicit_update():
+    d1, d1b, d2 = run_T(1, 1e-3, 1), run_T(1, 2e-3, 1), run_T(2, 1e-3, 1)
+    assert np.linalg.norm(d1) > 0
+    assert np.linalg.norm(d1b - 2 * d1) <= 1e-11 * np.linalg.norm(d1b)
+    assert np.linalg.norm(d2 - 1.5 * d1) <= 1e-11 * np.linalg.norm(d2)
+
+
+def test_implicit_energy_schemes_agree_to_first_order_in_dt():
+    T = 8e-3
+    gaps = {4: [], 5: []}
+    for dt in (2e-3, 1e-3):
+        n = int(round(T / dt))
+        d3 = run_T(3, dt, n)
+        gaps[4].append(np.linalg.norm(run_T(4, dt, n) - d3) / np.linalg.norm(d3))
+        gaps[5].append(np.linalg.norm(run_T(5, dt, n, rk=3, implicit_only=True) - d3) / np.linalg.norm(d3))
+    for m, g in gaps.items():
+        assert g[0] < 0.2 and g[1] < 0.75 * g[0], (m, g)
