@@ -12,30 +12,20 @@
 
 #include "kernels.cuh"
 #include "runtime.cuh"
+#include "schemes.cuh"
 
 namespace mg {
 
 // ---- fused pointwise kernels ----------------------------------------------
-// Predictor RHS of the time schemes (time_marching_methods.f90), each a
-// chain of whole-array passes in the reference, one pass here with the same
-// operations in the same order per point.  form:
-//  6, Euler_time_AB2_sources (:137-142):
-//   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t + L ; t = t*dt ;
-//   assign_wall_Dirichlet(t,0,X) ; t = t + X
-//  4, the AB2 schemes without diffusion (:289-292, :342-345):
-//   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t*dt ; assign_wall_Dirichlet(t,0,X) ;
-//   t = t + X
-//  5, Euler_time_Euler_sources and the Euler schemes without diffusion
-//   (:70-73, :321-323, :362-364):
-//   t = F*dt ; assign_wall_Dirichlet(t,0,X) ; t = t + X
-//  7, O2_BDF_time_AB2_sources (:104-108):
-//   t = F*1.5 ; t = t + Fnm1*(-0.5) ; t = t*(2/3 dt) ;
-//   assign_wall_Dirichlet(t,0,X) ; t = t + X*(4/3) ; t = t + Xnm1*(-1/3)
-//  8, Euler_time_RK_sources (:217-222), with the stage's a = (dt gamma,
-//   dt zeta, (dt 2) alpha):
-//   t = F*a0 ; t = t + Fnm1*a1 ; t = t + L*a2 ; assign_wall_Dirichlet(t,0,X) ;
-//   t = t + X
-// then Xnm1 = X when set_nm1 (every scheme but the two "no_correction" ones,
+// Predictor RHS of the time schemes (time_marching_methods.f90,
+// time_marching_methods_SF.f90) in one pass: the point arithmetic of each
+// form is in schemes.cuh (scheme_increment, the wall mask, scheme_rhs):
+//  6 Euler_time_AB2_sources (:137-142); 4 the AB2 schemes without diffusion
+//  (:289-292, :342-345) and the SF AB2 schemes; 5 Euler_time_Euler_sources
+//  and the Euler schemes without diffusion (:70-73, :321-323, :362-364);
+//  7 O2_BDF_time_AB2_sources (:104-108); 8 Euler_time_RK_sources (:217-222)
+//  with a = (dt gamma, dt zeta, dt 2 alpha) (dt alpha for the SF scheme).
+// Then Xnm1 = X when set_nm1 (every scheme but the "no_correction" ones,
 // whose t is X itself: X = X + increment).  dts is dt, or the product 2/3*dt
 // for form 7.  t may alias X: each point reads X and Xnm1 before writing t.
 __global__ void k_ab2_rhs(DF t, DF F, DF Fm, DF L, DF X, DF Xnm1, double dts, int wallbits, int form,
@@ -44,34 +34,17 @@ __global__ void k_ab2_rhs(DF t, DF F, DF Fm, DF L, DF X, DF Xnm1, double dts, in
   if (idx >= t.n()) return;
   int i, j, k;
   ijk_of(idx, t, i, j, k);
-  double v;
-  if (form == 8) {
-    v = F.f[idx] * a0;
-    v = v + Fm.f[idx] * a1;
-    v = v + L.f[idx] * a2;
-  } else {
-    if (form == 5) {
-      v = F.f[idx];
-    } else {
-      v = F.f[idx] * 1.5;
-      v = v + Fm.f[idx] * (-0.5);
-      if (form == 6) v = v + L.f[idx];
-    }
-    v = v * dts;
-  }
+  const double fm = form == kFormEuler ? 0.0 : Fm.f[idx];
+  const double l = (form == kFormAB2L || form == kFormRK) ? L.f[idx] : 0.0;
+  double v = scheme_increment(form, F.f[idx], fm, l, dts, a0, a1, a2);
   if (wallbits) {
     if (((wallbits & 1) && i == 2) || ((wallbits & 2) && i == t.s0 - 1) || ((wallbits & 4) && j == 2) ||
         ((wallbits & 8) && j == t.s1 - 1) || ((wallbits & 16) && k == 2) || ((wallbits & 32) && k == t.s2 - 1))
       v = 0.0;
   }
-  double x = X.f[idx];
-  if (form == 7) {
-    v = v + x * (4.0 / 3.0);
-    v = v + Xnm1.f[idx] * (-1.0 / 3.0);
-  } else {
-    v = v + x;
-  }
-  t.f[idx] = v;
+  const double x = X.f[idx];
+  const double xnm1 = form == kFormBDF2 ? Xnm1.f[idx] : 0.0;
+  t.f[idx] = scheme_rhs(form, v, x, xnm1);
   if (set_nm1) Xnm1.f[idx] = x;
 }
 // clean_div tail: temp_F = grad(phi) ; temp_F *= 1/scale ; X = Xstar - temp_F

@@ -25,3 +25,20 @@ def test_fused_point_math_matches_oracle():
     r = subprocess.run([out], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout[-3000:]
     assert "ALL OK" in r.stdout
+
+
+@pytest.mark.skipif(shutil.which("nvcc") is None and not os.path.exists("/usr/local/cuda/bin/nvcc"),
+                    reason="nvcc not available")
+def test_time_scheme_point_math_matches_oracle():
+    """scheme_increment / scheme_rhs (moons_b200/csrc/schemes.cuh), the point
+    arithmetic k_ab2_rhs runs for every time scheme, bit for bit against the
+    reference's whole-array sequences on the oracle's primitives."""
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    out = os.path.join(ROOT, "tests", "_build", "emu_schemes")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    subprocess.run([nvcc, "-std=c++17", "-O1", "-gencode", "arch=compute_100a,code=sm_100a", "-o", out,
+                    os.path.join(ROOT, "tests", "emu", "emu_schemes.cu"), os.path.join(ROOT, "oracle", "moons_oracle.cpp")],
+                   check=True, capture_output=True)
+    r = subprocess.run([out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout[-3000:]
+    assert "ALL OK" in r.stdout
