@@ -79,3 +79,57 @@ def test_ctypes_structs_match_the_header_layout():
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+FORTRAN = os.path.join(ROOT, "fortran", "moons_gpu_mod.f90")
+
+
+def _header_functions():
+    """{name: number of parameters} of the header's function declarations."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(moons_[a-z0-9_]+)\s*\(([^()]*)\)\s*;", text):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else len(params.split(","))
+    return out
+
+
+def _fortran_text():
+    text = open(FORTRAN).read()
+    text = re.sub(r"!.*", "", text)                 # comments
+    return re.sub(r"&\s*\n\s*&?", " ", text)          # continuation lines
+
+
+def test_fortran_bindings_match_the_header():
+    """Every bind(C) interface of the Fortran module names a function the
+    header declares, with the same number of arguments."""
+    decl = _header_functions()
+    bound = re.findall(r"function\s+\w+\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)", _fortran_text(), flags=re.I)
+    assert len(bound) >= 20
+    for args, name in bound:
+        assert name in decl, name
+        n = 0 if not args.strip() else len(args.split(","))
+        assert n == decl[name], (name, n, decl[name])
+
+
+def test_fortran_types_match_the_header_structs():
+    """The module's bind(C) derived types list the C structs' fields in the
+    same order (same names), so their layouts agree."""
+    ftext = _fortran_text()
+    ctext = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    for tname in ("moons_bc_spec", "moons_isp", "moons_solve_info"):
+        m = re.search(r"type,\s*bind\(C\)\s*::\s*" + tname + r"(.*?)end type", ftext, flags=re.S | re.I)
+        assert m, tname
+        ffields = []
+        for line in m.group(1).strip().splitlines():
+            names = line.split("::")[1]
+            ffields += [re.sub(r"\(.*\)", "", x).strip() for x in names.split(",")]
+        c = re.search(r"typedef struct \{([^{}]*)\}\s*" + tname + r"\s*;", ctext)
+        assert c, tname
+        cfields = []
+        for decl in c.group(1).split(";"):
+            decl = decl.strip()
+            if decl:
+                rest = decl.split(None, 1)[1]
+                cfields += [re.sub(r"\[.*\]", "", x).strip(" *") for x in rest.split(",")]
+        assert ffields == cfields, (tname, ffields, cfields)
