@@ -11,18 +11,28 @@ module moons_gpu_mod
   use, intrinsic :: iso_c_binding
   implicit none
 
-  integer(c_int), parameter :: MOONS_OK = 0
+  integer(c_int), parameter :: MOONS_OK = 0, MOONS_ERR_ARG = 1, MOONS_ERR_SHAPE = 2, MOONS_ERR_CUDA = 3
+  integer(c_int), parameter :: MOONS_ERR_NAN = 4, MOONS_ERR_STATE = 5, MOONS_ERR_NOMEM = 6
+  integer(c_int), parameter :: MOONS_ERR_LIMIT = 7
   integer(c_int), parameter :: MOONS_CC = 0, MOONS_FX = 1, MOONS_FY = 2, MOONS_FZ = 3
   integer(c_int), parameter :: MOONS_EX = 4, MOONS_EY = 5, MOONS_EZ = 6, MOONS_NODE = 7
   integer(c_int), parameter :: MOONS_BC_NONE = 0, MOONS_BC_DIRICHLET = 1, MOONS_BC_NEUMANN = 2
   integer(c_int), parameter :: MOONS_BC_PERIODIC = 3, MOONS_BC_ROBIN = 4
   integer(c_int), parameter :: MOONS_OP_LAP_UNIFORM = 1, MOONS_OP_LAP_PROPS = 2
   integer(c_int), parameter :: MOONS_OP_IND_DIFFUSION = 3, MOONS_OP_MOM_DIFFUSION = 4
+  integer(c_int), parameter :: MOONS_OP_NRG_DIFFUSION = 5
   integer(c_int), parameter :: MOONS_PREC_IDENTITY = 0, MOONS_PREC_LAP = 1
   integer(c_int), parameter :: MOONS_PREC_MOM = 2, MOONS_PREC_IND = 3
   integer(c_int), parameter :: MOONS_PREC_MG = 4, MOONS_PREC_MG_MIXED = 5, MOONS_PREC_UNET = 6
   integer(c_int), parameter :: MOONS_PREC_FD = 7
   integer(c_int), parameter :: MOONS_PREC_UNET_MG = 8
+  ! the MHD step: induction forms and field handles of moons_mhd_field
+  integer(c_int), parameter :: MOONS_IND_OFF = 0, MOONS_IND_B = 1, MOONS_IND_POTENTIAL = 2
+  integer(c_int), parameter :: MOONS_MHD_U = 0, MOONS_MHD_P = 1, MOONS_MHD_B = 2, MOONS_MHD_B0 = 3
+  integer(c_int), parameter :: MOONS_MHD_PHI = 4, MOONS_MHD_J = 5, MOONS_MHD_SIGMA_INV = 6
+  integer(c_int), parameter :: MOONS_MHD_JXB = 7, MOONS_MHD_DIVU = 8, MOONS_MHD_DIVB = 9
+  integer(c_int), parameter :: MOONS_MHD_T = 10, MOONS_MHD_KT = 11, MOONS_MHD_GRAVITY = 12
+  integer(c_int), parameter :: MOONS_MHD_SIGMA_INV_CC = 13, MOONS_MHD_U_CC = 14
   ! largest face temporary (points) that moons_lap_var_noalloc accepts
   integer(c_long_long), parameter :: MOONS_LAP_VAR_NOALLOC_MAX_POINTS = 131072_c_long_long
 
@@ -47,6 +57,55 @@ module moons_gpu_mod
     real(c_double) :: res0, res, rel
     integer(c_int) :: exit_reason
     real(c_double) :: ms
+  end type
+
+  ! parameters of the MHD step (solve_MOONS); the meaning of each field is
+  ! given in the C header
+  type, bind(C) :: moons_mhd_params
+    real(c_double) :: dt
+    integer(c_int) :: induction
+    integer(c_int) :: finite_Rem
+    integer(c_int) :: mpg_dir
+    real(c_double) :: mpg_scale
+    real(c_double) :: scale_advection_U
+    real(c_double) :: scale_diffusion_U
+    real(c_double) :: scale_JxB
+    real(c_double) :: scale_advection_B
+    real(c_double) :: scale_diffusion_B
+    real(c_double) :: scale_current
+    real(c_double) :: coeff_implicit_U
+    real(c_double) :: coeff_implicit_B
+    type(moons_isp) :: isp_U, isp_p, isp_B, isp_phi
+    type(moons_bc_spec) :: bc_U(3), bc_p, bc_B(3), bc_phi
+    integer(c_int) :: ind_offset(3)
+    integer(c_int) :: prescribed_Ustar
+    integer(c_int) :: prescribed_Bstar
+    integer(c_int) :: prec_poisson
+    integer(c_int) :: energy
+    integer(c_int) :: solve_method_T
+    real(c_double) :: coeff_implicit_T
+    real(c_double) :: scale_advection_T
+    real(c_double) :: scale_diffusion_T
+    real(c_double) :: scale_heating_T
+    real(c_double) :: scale_buoyancy
+    type(moons_isp) :: isp_T
+    type(moons_bc_spec) :: bc_T
+    real(c_double) :: scale_KE_diffusion_T
+    real(c_double) :: scale_viscous_dissipation_T
+    real(c_double) :: scale_joule_heating_T
+    integer(c_int) :: solve_method_U
+    integer(c_int) :: solve_method_B
+    integer(c_int) :: rk_stages
+    real(c_double) :: scale_diffusion_linear_U
+    real(c_double) :: scale_diffusion_linear_B
+  end type
+
+  type, bind(C) :: moons_step_info
+    integer(c_int) :: steps
+    integer(c_int) :: iters_U, iters_p, iters_B, iters_phi
+    real(c_double) :: res_p, res_phi
+    real(c_double) :: ms
+    integer(c_int) :: iters_T
   end type
 
   interface
@@ -250,6 +309,52 @@ module moons_gpu_mod
     function moons_unet_destroy(u) bind(C, name="moons_unet_destroy") result(st)
       import :: c_ptr, c_int
       type(c_ptr), value :: u
+      integer(c_int) :: st
+    end function
+
+    ! the whole step on the device (solve_MOONS, MOONS_solver.f90:47-144):
+    ! create from the two meshes and the parameters, upload the initial U, B,
+    ! B0 and sigma through the field handles, init, then step
+    function moons_mhd_create(mesh_mom, mesh_ind, prm, s) bind(C, name="moons_mhd_create") result(st)
+      import :: c_ptr, c_int, moons_mhd_params
+      type(c_ptr), value :: mesh_mom, mesh_ind
+      type(moons_mhd_params), intent(in) :: prm
+      type(c_ptr) :: s
+      integer(c_int) :: st
+    end function
+
+    function moons_mhd_destroy(s) bind(C, name="moons_mhd_destroy") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s
+      integer(c_int) :: st
+    end function
+
+    function moons_mhd_field(s, which, comp, f) bind(C, name="moons_mhd_field") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s
+      integer(c_int), value :: which, comp
+      type(c_ptr) :: f
+      integer(c_int) :: st
+    end function
+
+    function moons_mhd_init(s) bind(C, name="moons_mhd_init") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s
+      integer(c_int) :: st
+    end function
+
+    function moons_mhd_step(s, nsteps, info) bind(C, name="moons_mhd_step") result(st)
+      import :: c_ptr, c_int, moons_step_info
+      type(c_ptr), value :: s
+      integer(c_int), value :: nsteps
+      type(moons_step_info), intent(out) :: info
+      integer(c_int) :: st
+    end function
+
+    function moons_mhd_divergence(s, l2_divu, l2_divb) bind(C, name="moons_mhd_divergence") result(st)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: s
+      real(c_double), intent(out) :: l2_divu, l2_divb
       integer(c_int) :: st
     end function
   end interface

@@ -114,16 +114,17 @@ def test_fortran_bindings_match_the_header():
 
 def test_fortran_types_match_the_header_structs():
     """The module's bind(C) derived types list the C structs' fields in the
-    same order (same names), so their layouts agree."""
+    same order, with the same names and array extents, so their layouts
+    agree."""
     ftext = _fortran_text()
     ctext = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
-    for tname in ("moons_bc_spec", "moons_isp", "moons_solve_info"):
+    for tname in ("moons_bc_spec", "moons_isp", "moons_solve_info", "moons_mhd_params", "moons_step_info"):
         m = re.search(r"type,\s*bind\(C\)\s*::\s*" + tname + r"(.*?)end type", ftext, flags=re.S | re.I)
         assert m, tname
         ffields = []
         for line in m.group(1).strip().splitlines():
             names = line.split("::")[1]
-            ffields += [re.sub(r"\(.*\)", "", x).strip() for x in names.split(",")]
+            ffields += [x.strip().replace("(", "[").replace(")", "]") for x in names.split(",")]
         c = re.search(r"typedef struct \{([^{}]*)\}\s*" + tname + r"\s*;", ctext)
         assert c, tname
         cfields = []
@@ -131,5 +132,5 @@ def test_fortran_types_match_the_header_structs():
             decl = decl.strip()
             if decl:
                 rest = decl.split(None, 1)[1]
-                cfields += [re.sub(r"\[.*\]", "", x).strip(" *") for x in rest.split(",")]
+                cfields += [x.strip(" *") for x in rest.split(",")]
         assert ffields == cfields, (tname, ffields, cfields)
