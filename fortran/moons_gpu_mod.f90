@@ -312,6 +312,63 @@ module moons_gpu_mod
       integer(c_int) :: st
     end function
 
+    ! fields, BCs and the remaining discrete operators
+    function moons_sf_shape(f, shp) bind(C, name="moons_sf_shape") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: f
+      integer(c_int), intent(out) :: shp(3)
+      integer(c_int) :: st
+    end function
+
+    function moons_sf_fill(f, val) bind(C, name="moons_sf_fill") result(st)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: f
+      real(c_double), value :: val
+      integer(c_int) :: st
+    end function
+
+    function moons_mesh_sync(m) bind(C, name="moons_mesh_sync") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: m
+      integer(c_int) :: st
+    end function
+
+    function moons_apply_bcs_implicit(f) bind(C, name="moons_apply_bcs_implicit") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: f
+      integer(c_int) :: st
+    end function
+
+    ! del%assign/add/subtract (ops_del.f90:236-261): gen 1 assign, 2 add,
+    ! 3 subtract; n the derivative order, dir 1..3, pad 0/1
+    function moons_del(out, in, n, dir, pad, gen) bind(C, name="moons_del") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: out, in
+      integer(c_int), value :: n, dir, pad, gen
+      integer(c_int) :: st
+    end function
+
+    function moons_interp(out, in, dir) bind(C, name="moons_interp") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: out, in
+      integer(c_int), value :: dir
+      integer(c_int) :: st
+    end function
+
+    function moons_lap_centered(out, u) bind(C, name="moons_lap_centered") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: out, u
+      integer(c_int) :: st
+    end function
+
+    ! the solver's residual r = vol*(b - A x_BC - A x) for the iterate x
+    function moons_pcg_residual(s, x, b, r) bind(C, name="moons_pcg_residual") result(st)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: s
+      type(c_ptr), intent(in) :: x(*), b(*), r(*)
+      integer(c_int) :: st
+    end function
+
     ! the whole step on the device (solve_MOONS, MOONS_solver.f90:47-144):
     ! create from the two meshes and the parameters, upload the initial U, B,
     ! B0 and sigma through the field handles, init, then step
