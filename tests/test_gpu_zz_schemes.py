@@ -5,14 +5,26 @@ directly).  Collected after the other GPU test files so that the rest of the
 suite runs first; the arithmetic of every RHS form is also checked on the CPU
 (tests/test_emu_cpu.py) and the oracle's schemes by property tests
 (tests/test_time_schemes_cpu.py)."""
+import numpy as np
 import pytest
 
 import oracle.oracle as O
 from moons_b200 import capi as G
 from moons_b200 import configs
-from tests.test_gpu_mhd import SCHEME_CASES, rel_l2
 
 pytestmark = pytest.mark.gpu
+
+# the step test's LDC in the B form and duct with walls (tests/test_gpu_mhd.py)
+SCHEME_CASES = [
+    ("ldc_bform", configs.ldc, dict(n=10, induction=G.IND_B, tol=1e-12)),
+    ("duct_walls", configs.duct, dict(nx=10, ny=8, nz=12, n_wall=2, t_wall=0.5, tol=1e-12, noise=1e-2)),
+]
+
+
+def rel_l2(a, b):
+    d = np.linalg.norm((a - b).ravel())
+    n = np.linalg.norm(b.ravel())
+    return d / n if n > 0 else d
 
 
 @pytest.mark.parametrize("mT", [1, 4, 5])
