@@ -287,7 +287,9 @@ typedef struct {
                                cleaning potential; the sigma-weighted potential
                                of the low-Rem form takes MG_MIXED), or
                                MOONS_PREC_UNET_MG (learned + mixed, networks
-                               from moons_mhd_set_unet)                       */
+                               from moons_mhd_set_unet); MOONS_PREC_LAP is
+                               the same as 0; other values are refused
+                               (MOONS_ERR_ARG)                                */
   /* energy equation (energy_extend.f90:236-262, add_all_energy_sources.f90:
    * 21-67), solved on the induction mesh before the momentum step as
    * solve_MOONS does (MOONS_solver.f90:81-85); fields MOONS_MHD_T, _KT,

@@ -683,6 +683,14 @@ int moons_mhd_create(moons_mesh* mm, moons_mesh* mi, const moons_mhd_params* prm
     set_error("moons_mhd_create: solve_method_U and solve_method_B must be 0 to 9");
     return MOONS_ERR_ARG;
   }
+  {
+    const int pq = prm->prec_poisson;  // the Poisson solvers the step can use
+    if (!(pq == 0 || pq == MOONS_PREC_LAP || pq == MOONS_PREC_MG || pq == MOONS_PREC_MG_MIXED ||
+          pq == MOONS_PREC_FD || pq == MOONS_PREC_UNET_MG)) {
+      set_error("moons_mhd_create: prec_poisson must be 0, LAP, MG, MG_MIXED, FD or UNET_MG");
+      return MOONS_ERR_ARG;
+    }
+  }
   if (prm->rk_stages != 0 && prm->rk_stages != 1 && prm->rk_stages != 3) {
     set_error("moons_mhd_create: rk_stages must be 0, 1 or 3");
     return MOONS_ERR_ARG;

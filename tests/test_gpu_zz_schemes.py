@@ -79,3 +79,14 @@ def test_mhd_fft_scheme_direct_cleaning(name, builder, kw):
     # at most three CG iterations per direct-preconditioned solve, the bound of
     # the direct solve's own test (hundreds with the Jacobi preconditioner)
     assert ig["iters_p"] <= 3 * nsteps and ig["iters_phi"] <= 3 * nsteps, ig
+
+
+@pytest.mark.parametrize("bad", [G.PREC_MOM, G.PREC_UNET, 9])
+def test_mhd_rejects_unknown_poisson_solver(bad):
+    """prec_poisson values the step cannot use are refused, not replaced."""
+    mom, ind, prm, _ = configs.ldc(n=6)
+    prm.prec_poisson = bad
+    mm = G.Mesh(*mom)
+    with pytest.raises(G.MoonsError) as e:
+        G.MHD(mm, mm, prm)
+    assert e.value.code == 1  # MOONS_ERR_ARG
