@@ -7,10 +7,15 @@ CPU tests of the oracle and the GPU tests of the library.
   series over alpha_k = (k + 1/2) pi / L, k = 0..1000.  The result variable
   starts at zero here (the reference accumulates into an uninitialised
   function result; its SH_profile variant zeroes it).
+* ``hunt`` -- the same duct with perfectly conducting Hartmann walls
+  (y = +-a, normal to B0) and insulating side walls (profile_funcs.f90:
+  147-193, hunt_profile, and hunt_coeff :131-145).
 * ``duct_steady`` -- runs a backend's MHD step (the B form with the
   constrained-transport induction source, finite Rem) on the square duct to
-  its steady state, where it must reproduce the Shercliff profile at second
-  order in the mesh spacing.
+  its steady state, where it must reproduce the Shercliff profile (walls
+  insulating: pseudo-vacuum BCs) or the Hunt profile (``walls="hunt"``: the
+  induced field's BCs of a perfectly conducting Hartmann wall, B_y = 0 and
+  d(B_x, B_z)/dn = 0 on y = +-a) at second order in the mesh spacing.
 * ``taylor_green`` -- the decaying Taylor-Green vortex of
   GF_distributions.f90:720-769 (u = cos x sin y F, v = -sin x cos y F,
   F = exp(-2 t / Re)) with the BCs of init_U_BCs.f90:107-124 (Neumann /
@@ -49,12 +54,43 @@ def shercliff(x, y, Ha: float, Re: float, a: float = 1.0, b: float = 1.0, terms:
     return w * Re * a ** 2
 
 
+def hunt(x, y, Ha: float, Re: float, a: float = 1.0, b: float = 1.0, terms: int = 1000):
+    L = b / a
+    X, Y = np.meshgrid(np.asarray(x, float), np.asarray(y, float), indexing="ij")
+    eta = Y / a
+    w = np.zeros_like(X)
+
+    def coeff(r1k, r2k, N):  # hunt_coeff
+        return (r2k / N) * (np.exp(-r1k * (1.0 - eta)) + np.exp(-r1k * (1.0 + eta))) / (1.0 + np.exp(-2.0 * r1k))
+
+    for k in range(terms + 1):
+        al = (k + 0.5) * math.pi / L
+        N = math.sqrt(Ha ** 2 + 4.0 * al ** 2)
+        r1, r2 = 0.5 * (Ha + N), 0.5 * (-Ha + N)
+        w += 2.0 * (-1.0) ** k * np.cos(al * X / a) / (L * al ** 3) * (1.0 - coeff(r1, r2, N) - coeff(r2, r1, N))
+    return w * Re * a ** 2
+
+
+def _hunt_duct(*args, **kw):
+    """configs.duct with conducting Hartmann walls (y) and insulating side
+    walls (x) for the induced field."""
+    mom, ind, prm, init = configs.duct(*args, **kw)
+    P, D, N = G.PERIODIC, G.DIRICHLET, G.NEUMANN
+    types = ([N, N, N, N, P, P], [D, D, D, D, P, P], [D, D, N, N, P, P])
+    for c in range(3):
+        prm.bc_B[c] = G.bc_spec(types[c], order=configs.ORDER_PZ)
+    return mom, ind, prm, init
+
+
 def duct_steady(backend, n: int, beta: float = 1.05, Ha: float = 5.0, Re: float = 1.0, Rem: float = 1.0,
-                dt: float = 0.01, max_steps: int = 1000, chunk: int = 50, settle: float = 1e-11):
+                dt: float = 0.01, max_steps: int = 1000, chunk: int = 50, settle: float = 1e-11,
+                walls: str = "insulating"):
     """Relative max-norm error of the steady streamwise velocity against the
-    Shercliff series, and the number of steps taken."""
+    Shercliff series (insulating walls) or the Hunt series (walls="hunt"),
+    and the number of steps taken."""
     kw = dict(nx=n, ny=n, nz=4, Re=Re, Ha=Ha, Rem=Rem, dt=dt, n_wall=0, noise=0.0, beta=beta)
-    sim = configs.make(backend, configs.duct, seed=0, tol=1e-12, **kw)
+    builder = _hunt_duct if walls == "hunt" else configs.duct
+    sim = configs.make(backend, builder, seed=0, tol=1e-12, **kw)
     prev, steps = None, 0
     while steps < max_steps:
         sim.step(chunk)
@@ -65,7 +101,7 @@ def duct_steady(backend, n: int, beta: float = 1.05, Ha: float = 5.0, Re: float 
         prev = w.copy()
     mom = configs.duct(**kw)[0]
     hc = [0.5 * (h[1:] + h[:-1]) for h in mom]
-    wa = shercliff(hc[0][1:-1], hc[1][1:-1], Ha, Re)
+    wa = (hunt if walls == "hunt" else shercliff)(hc[0][1:-1], hc[1][1:-1], Ha, Re)
     wn = w[1:-1, 1:-1, 2]
     return float(np.abs(wn - wa).max() / np.abs(wa).max()), steps
 

@@ -1,16 +1,19 @@
-"""GPU parity of the time schemes added after the other MHD step tests:
-the energy schemes 1, 4 and 5 of solve_energy and Euler_time_AB2_sources_FFT
-(solve_method 9, the default scheme with the cleaning equations solved
-directly).  Collected after the other GPU test files so that the rest of the
-suite runs first; the arithmetic of every RHS form is also checked on the CPU
-(tests/test_emu_cpu.py) and the oracle's schemes by property tests
-(tests/test_time_schemes_cpu.py)."""
+"""GPU tests added after the other GPU test files had last run on a B200:
+the energy schemes 1, 4 and 5 of solve_energy, Euler_time_AB2_sources_FFT
+(solve_method 9: the default scheme with the cleaning equations solved
+directly), the refusal of Poisson solver choices the step cannot use, and
+Hunt's duct profile.  Collected after the other GPU test files so that a
+failure here cannot stop the rest of the suite under -x; the arithmetic of
+every RHS form is also checked on the CPU (tests/test_emu_cpu.py), the
+oracle's schemes by property tests (tests/test_time_schemes_cpu.py) and its
+Hunt profile by tests/test_known_answer_cpu.py."""
 import numpy as np
 import pytest
 
 import oracle.oracle as O
 from moons_b200 import capi as G
 from moons_b200 import configs
+from tests import known_answers as KA
 
 pytestmark = pytest.mark.gpu
 
@@ -90,3 +93,13 @@ def test_mhd_rejects_unknown_poisson_solver(bad):
     with pytest.raises(G.MoonsError) as e:
         G.MHD(mm, mm, prm)
     assert e.value.code == 1  # MOONS_ERR_ARG
+
+
+def test_hunt_profile_second_order_gpu():
+    """The steady duct with conducting Hartmann walls reproduces Hunt's
+    profile (profile_funcs.f90:147-193) at second order (oracle: 0.0465,
+    0.0110, 0.0027 at 8, 16, 32 cells)."""
+    errs = [KA.duct_steady(G, n, walls="hunt")[0] for n in (16, 32, 64)]
+    assert errs[-1] < 1.5e-3, errs
+    for a, b in zip(errs, errs[1:]):
+        assert a / b > 3.5, errs

@@ -39,6 +39,14 @@ def test_shercliff_profile_second_order():
     assert e8 / e16 > 3.5, (e8, e16)
 
 
+def test_hunt_profile_second_order():
+    """Conducting Hartmann walls, insulating side walls: Hunt's profile."""
+    e8, _ = KA.duct_steady(O, 8, walls="hunt")
+    e16, _ = KA.duct_steady(O, 16, walls="hunt")
+    assert e16 < 0.02, (e8, e16)
+    assert e8 / e16 > 3.5, (e8, e16)
+
+
 def test_taylor_green_decay_first_order_in_time():
     e1 = KA.taylor_green(O, 16, 2e-3)
     e2 = KA.taylor_green(O, 16, 1e-3)
