@@ -70,3 +70,36 @@ def test_ldc32_fixture_is_the_oracle():
     shapes = {name: sim.shape(which, c) for name, which, c in mk.FIELDS_LONG}
     for name, shp in shapes.items():
         assert z[name].shape == shp
+
+
+def test_sigma_laplacian_series_resistance():
+    """div(k grad phi) = 0 (Lap_nonuniform_props, matrix_free_operators.f90:
+    92-118) with phi = 1 on x = 0, phi = 0 on x = 1, insulated elsewhere and k
+    varying along x on the x-faces: the discrete solution is resistances in
+    series, R_f = dx / k_f, the Dirichlet walls entering through half their
+    face's resistance (ghost 2 b - phi_1).  Solved by the oracle's Jacobi-PCG."""
+    from moons_b200 import mesh_gen as mg
+    from moons_b200.capi import CC, DIRICHLET, FX, FY, FZ, NEUMANN, OP_LAP_PROPS, PREC_LAP, bc_spec, isp
+    n = 8
+    h = mg.add_ghost_nodes(mg.uniform(0.0, 1.0, n))
+    m = O.Mesh(h, h.copy(), h.copy())
+    phi = m.field(CC)
+    phi.upload(np.zeros(phi.shape))
+    phi.set_bcs(bc_spec([DIRICHLET, DIRICHLET, NEUMANN, NEUMANN, NEUMANN, NEUMANN], values=[1.0, 0, 0, 0, 0, 0]))
+    kx = 1.0 + 0.5 * np.sin(3.0 * h)
+    ks = []
+    for dl in (FX, FY, FZ):
+        f = m.field(dl)
+        k = np.ones(f.shape)
+        if dl == FX:
+            k[:] = kx[:, None, None]
+        f.upload(k)
+        ks.append(f)
+    b = m.field(CC)
+    b.upload(np.zeros(b.shape))
+    info = O.PCG(m, OP_LAP_PROPS, PREC_LAP, [phi], [phi], ks).solve([phi], [b], isp(2000, 1e-14, 1e-300))
+    assert info["exit_reason"] == 1
+    R = (h[2] - h[1]) / kx[1:n + 2]
+    q = 1.0 / (R[0] / 2 + R[1:-1].sum() + R[-1] / 2)
+    expect = 1.0 - q * (R[0] / 2 + np.concatenate([[0.0], np.cumsum(R[1:n])]))
+    assert np.abs(phi.download()[1:-1, 1:-1, 1:-1] - expect[:, None, None]).max() <= 1e-12
