@@ -134,3 +134,24 @@ def test_fortran_types_match_the_header_structs():
                 rest = decl.split(None, 1)[1]
                 cfields += [x.strip(" *") for x in rest.split(",")]
         assert ffields == cfields, (tname, ffields, cfields)
+
+
+def test_ctypes_bindings_match_the_header():
+    """moons_b200/capi.py declares every header function, with the header's
+    number of arguments (its signature table, read without loading it)."""
+    import ast
+    tree = ast.parse(open(os.path.join(ROOT, "moons_b200", "capi.py")).read())
+    table = None
+    for node in ast.walk(tree):
+        if isinstance(node, ast.Assign) and isinstance(node.value, ast.Dict) and \
+                any(isinstance(t, ast.Name) and t.id == "sig" for t in node.targets):
+            table = node.value
+    assert table is not None
+    decl = _header_functions()
+    names = []
+    for k, v in zip(table.keys, table.values):
+        name, nargs = k.value, len(v.elts[1].elts)
+        names.append(name)
+        assert name in decl, name
+        assert nargs == decl[name], (name, nargs, decl[name])
+    assert sorted(names) == sorted(decl)
